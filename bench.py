@@ -1,0 +1,376 @@
+"""Benchmark: N=26 time steps/s of the emu-sv Krylov step on one B200 (complex64 vectors,
+FP64 Krylov scalars), with the H*psi roofline, an end-to-end number through the public
+backend API, and the CPU baseline.  One JSON line on stdout (rank 0).
+
+Workload (ladder_n26): 2x13 ladder at 5.5 um, C6 = 5420158.53, Omega = 4 rad/us,
+delta -10 -> 10 rad/us over 2 us, dt = 5 ns (400 steps), tolerance 1e-10, from |g...g>.
+A bench step is one time step exp(-i dt H(t_k)) psi.  Timed steps continue the pulse
+after the warm-up steps.  The state (512 MiB) and every Krylov vector are larger than
+the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (torchrun, one rank per GPU) every rank evolves its own replica of the
+workload ("replicas only": a single state is not sharded), `value` is the sum of steps
+over ranks divided by the max over ranks of the timed region.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "N=26 steps/s & batched adjoint grads/s vs plain GPU at err<=1e-6; H·ψ HBM GB/s"
+UNIT = "steps/s"
+
+
+def peaks() -> tuple[float, str]:
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
+    import torch
+
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian, _lib, krylov
+    from emulators_b200 import workloads as wl
+    from emulators_b200.krylov import fused_step
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    w = wl.ladder_n26()
+    n, D = w.nqubits, 1 << w.nqubits
+    vdtype = torch.complex64
+    es = 8
+    L = _lib.load()
+    krylov.use_iteration_hint = True
+    U = torch.as_tensor(w.U)
+
+    def ham(k):
+        k = k % w.nsteps
+        return RydbergHamiltonian(torch.as_tensor(w.omega[k]), torch.as_tensor(w.delta[k]),
+                                  torch.as_tensor(w.phi[k]), U, dev)
+
+    a = torch.zeros(D, dtype=vdtype, device=dev)
+    a[0] = 1.0
+    b = torch.empty_like(a)
+    iters = []
+
+    def step(k, src, dst):
+        _, info, st = fused_step(HamiltonianExpOperator(ham(k), w.dt), src, w.tolerance,
+                                 w.tolerance, w.max_krylov_dim, out=dst)
+        _lib.check(st, "krylov step")
+        iters.append(info.iterations)
+
+    W, K = args.warmup, args.steps
+    for k in range(W):
+        step(k, a, b)
+        a, b = b, a
+    torch.cuda.synchronize()
+    iters.clear()
+
+    # ---- timed region: K steps, inputs resident in HBM
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    L.emusv_profile_begin(0)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        for k in range(W, W + K):
+            step(k, a, b)
+            a, b = b, a
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_by = (np.zeros(8)).astype(np.float64)
+    launches = np.zeros(8, dtype=np.int64)
+    L.emusv_profile_end(ms_by.ctypes.data, launches.ctypes.data, 8)
+    elapsed = e0.elapsed_time(e1) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = t.item()
+        dist.barrier()
+    value = world * K / elapsed
+    timed_iters = list(iters)
+
+    # ---- profiled pass (not part of `value`): per-kernel device time by kind
+    iters.clear()
+    KP = min(K, 6)
+    L.emusv_profile_begin(1)
+    for k in range(W + K, W + K + KP):
+        step(k, a, b)
+        a, b = b, a
+    torch.cuda.synchronize()
+    pms = np.zeros(8)
+    pl = np.zeros(8, dtype=np.int64)
+    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
+    hpsi_avg_s = pms[0] / max(pl[0], 1) / 1e3
+    hbm, which = peaks()
+    alg_hpsi = 2 * D * es  # read v, write H v (diagonal rebuilt on chip)
+    achieved = alg_hpsi / hpsi_avg_s / 1e9
+    total_ms = pms.sum()
+    kinds = ["hpsi", "orth", "small", "combine", "obs", "adjoint", "batch", "other"]
+    shares = {kinds[i]: round(pms[i] / total_ms, 4) for i in range(8) if pl[i]}
+
+    # ---- H*psi alone (standalone launches, for the kernel roofline at both precisions)
+    hstand = {}
+    for name, dt_ in (("c64", torch.complex64), ("c128", torch.complex128)):
+        v = torch.randn(D, dtype=dt_, device=dev)
+        o = torch.empty_like(v)
+        H = ham(0)
+        for _ in range(2):
+            H * v
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        s0.record()
+        for _ in range(reps):
+            L.emusv_hpsi(n, _lib.dtype_code(dt_), *H._params(), v.data_ptr(), o.data_ptr(),
+                         torch.cuda.current_stream().cuda_stream)
+        s1.record()
+        torch.cuda.synchronize()
+        t1 = s0.elapsed_time(s1) / 1e3 / reps
+        byts = 2 * D * (8 if name == "c64" else 16)
+        hstand[name] = {"ms": round(t1 * 1e3, 4), "GB/s": round(byts / t1 / 1e9, 1),
+                        "frac": round(byts / t1 / 1e9 / hbm, 4)}
+        del v, o
+
+    # ---- end-to-end through the public backend API, host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(w, W, K, dev, dist, world)
+
+    result = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": round(elapsed / K * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 vectors + f64 scalars", "data": "synthetic",
+        "config": {"workload": "ladder_n26: N=26 2x13 ladder 5.5um, Omega=4, delta -10->10 "
+                               "over 2us, dt=5ns, tol=1e-10, complex64/FP64",
+                   "nqubits": n, "dt_ns": 5.0, "tolerance": w.tolerance,
+                   "krylov_iterations_mean": round(float(np.mean(timed_iters)), 2),
+                   "l2": "state and Krylov vectors (512 MiB each) exceed L2; no flush",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "k_hpsi (fused H*psi + Lanczos reductions)",
+                     "achieved": round(achieved, 1), "peak": hbm, "peak_source": which,
+                     "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                     "algorithmic_bytes_per_launch": alg_hpsi,
+                     "avg_launch_ms": round(hpsi_avg_s * 1e3, 4),
+                     "kernel_time_shares": shares},
+        "gpu_launches": int(launches.sum()),
+        "clocks": clk.summary(),
+        "secondary": {"hpsi_standalone": hstand},
+        "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
+    if dist:
+        dist.destroy_process_group()
+    return result if rank == 0 else None
+
+
+def run_e2e(w, W, K, dev, dist, world) -> dict:
+    """Same metric through SVBackendImpl: initial state from pinned host memory, per-step
+    host drive samples, the per-step norm read the reference loop does, occupation and
+    energy at the workload's observation times, final state back to pinned host memory."""
+    import torch
+
+    from emulators_b200 import StateVector
+    from emulators_b200.sv_backend import Energy, Occupation, SequenceData, SVBackendImpl, SVConfig
+
+    n, D = w.nqubits, 1 << w.nqubits
+    sl = slice(W, W + K)
+    sub = type(w)(**{**w.__dict__, "omega": w.omega[sl], "delta": w.delta[sl], "phi": w.phi[sl]})
+    data = SequenceData.from_workload(sub)
+    host0 = torch.zeros(D, dtype=torch.complex64).pin_memory()
+    host0[0] = 1.0
+    host_out = torch.empty(D, dtype=torch.complex64).pin_memory()
+    obs_at = [k / K for k in range(1, K + 1) if k % max(1, w.obs_every // 10) == 0 or k == K]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    init = StateVector(host0.to(dev, non_blocking=True))
+    cfg = SVConfig(dt=w.dt * 1000, krylov_tolerance=w.tolerance, precision="c64",
+                   observables=[Occupation(obs_at), Energy(obs_at)], initial_state=init)
+    impl = SVBackendImpl(cfg, data)
+    res = impl._run()
+    host_out.copy_(impl.state.data, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    wall = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([el], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = t.item()
+    n_obs = len(res.get("occupation"))
+    h2d = (D * 8 + K * (3 * n + n * n) * 8) / K
+    d2h = (D * 8 + K * 8 + n_obs * (n + 1) * 8) / K
+    return {"value": round(world * K / el, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "wall_s": round(wall, 3),
+            "api": "SVBackendImpl(SVConfig(precision='c64'), SequenceData)._run()",
+            "observations": n_obs}
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_baseline(w, budget_s: float) -> dict:
+    """The oracle (C/OpenMP restatement of the reference path, FP64/complex128) timed on
+    this host's cores on the first steps of the same workload; stops after budget_s."""
+    from oracle import oracle
+
+    oracle.build()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    n = w.nqubits
+    s = np.zeros(1 << n, dtype=np.complex128)
+    s[0] = 1.0
+    t0 = time.perf_counter()
+    done = 0
+    iters = []
+    while done < w.nsteps:
+        s, _, info = oracle.evolve_step(w.dt, w.omega[done], w.delta[done], w.phi[done], w.U, s,
+                                        w.tolerance, w.max_krylov_dim)
+        iters.append(info.iteration_count)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": round(done / el, 6), "unit": UNIT, "cores": oracle.num_threads(),
+            "kind": "port",
+            "sample": f"first {done} time step(s) of ladder_n26 in complex128 on the host "
+                      f"({el:.1f} s, Krylov iterations {iters})"}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, rank: int) -> dict | None:
+    if rank != 0:
+        return None
+    from emulators_b200 import workloads as wl
+
+    w = wl.ladder_n26()
+    cb = cpu_baseline(w, args.cpu_seconds)
+    return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "ladder_n26 (same as the ours arm), reference algorithm "
+                                   "restated on the host CPU (oracle port)",
+                       "steps_note": "each step is a bounded sample: time steps run until "
+                                     f"{args.cpu_seconds:.0f} s of CPU work"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=30.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+    else:
+        out = run_ours(args, rank, world, local_rank)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

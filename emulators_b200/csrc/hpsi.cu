@@ -1,0 +1,385 @@
+// C ABI: Hamiltonian diagonal, fused H*psi, energy moments, occupations, correlations.
+#include <stdio.h>
+#include <string.h>
+
+#include "hpsi_kernel.cuh"
+#include "profile.cuh"
+
+namespace emusv {
+
+bool make_params(int n, const double *omegas, const double *deltas, const double *phis,
+                 const double *interaction, HamParams *P) {
+    if (n < 1 || n > EMUSV_MAX_QUBITS || !omegas || !deltas || !phis || !interaction || !P)
+        return false;
+    memset(P, 0, sizeof(*P));
+    P->n = n;
+    int real = 1;
+    for (int i = 0; i < n; ++i) {
+        const int p = n - 1 - i;  // qubit i is bit n-1-i
+        const double h = 0.5 * omegas[i];  // hamiltonian.py:52
+        const double c = cos(phis[i]), s = sin(phis[i]);
+        if (phis[i] != 0.0) real = 0;      // hamiltonian.py:61
+        P->up_re[p] = h * c;               // Omega/2 e^{i phi} (hamiltonian.py:62-64)
+        P->up_im[p] = h * s;
+        P->dn_re[p] = h * c;               // its conjugate
+        P->dn_im[p] = -h * s;
+        P->field[p] = -deltas[i];
+        if (!isfinite(omegas[i]) || !isfinite(deltas[i]) || !isfinite(phis[i])) return false;
+    }
+    if (real) {
+        for (int p = 0; p < n; ++p) P->up_im[p] = P->dn_im[p] = 0.0;
+    }
+    P->real_coef = real;
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+            const double u = interaction[i * n + j];  // upper triangle only
+            if (!isfinite(u)) return false;
+            const int p = n - 1 - i, q = n - 1 - j;
+            P->U[p * MAXQ + q] = u;
+            P->U[q * MAXQ + p] = u;
+        }
+    return true;
+}
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
+
+int stream_status(cudaError_t e) { return e == cudaSuccess ? EMUSV_OK : EMUSV_CUDA_ERROR; }
+
+int hpsi_tile_bits(int n) {
+    int b = n - 8;
+    if (b > 11) b = 11;
+    if (b < 6) b = 6;
+    if (b > n) b = n;
+    return b;
+}
+
+template <typename R, bool REALC, int MODE>
+static int launch_one(const HamParams &P, HpsiArgs A, int max_grid, cudaStream_t s, int *grid_out) {
+    typedef typename cvec<R>::T C;
+    const int b = A.tile_bits;
+    const size_t smem = hpsi_smem<C>(b).total;
+    auto kern = k_hpsi<R, REALC, MODE>;
+    EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, smem));
+    if (per_sm < 1) per_sm = 1;
+    const i64 ntiles = i64(1) << (P.n - b);
+    i64 grid = (i64)sm_count() * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    if (max_grid > 0 && grid > max_grid) grid = max_grid;
+    {
+        ProfScope ps_(PROF_HPSI, s);
+        kern<<<(int)grid, BLOCK, smem, s>>>(P, A);
+    }
+    EMUSV_CHECK_LAUNCH();
+    if (grid_out) *grid_out = (int)grid;
+    return EMUSV_OK;
+}
+
+// Dispatch on dtype / real coefficients / mode.
+int launch_hpsi(int dtype, int mode, const HamParams &P, HpsiArgs A, int max_grid,
+                cudaStream_t s, int *grid_out) {
+#define EMUSV_DISPATCH(R, M)                                                           \
+    return P.real_coef ? launch_one<R, true, M>(P, A, max_grid, s, grid_out)           \
+                       : launch_one<R, false, M>(P, A, max_grid, s, grid_out)
+    if (dtype == EMUSV_C128) {
+        switch (mode) {
+        case HP_STORE: EMUSV_DISPATCH(double, HP_STORE);
+        case HP_ENERGY: EMUSV_DISPATCH(double, HP_ENERGY);
+        case HP_LANCZOS: EMUSV_DISPATCH(double, HP_LANCZOS);
+        case HP_DIAG: return launch_one<double, true, HP_DIAG>(P, A, max_grid, s, grid_out);
+        }
+    } else if (dtype == EMUSV_C64) {
+        switch (mode) {
+        case HP_STORE: EMUSV_DISPATCH(float, HP_STORE);
+        case HP_ENERGY: EMUSV_DISPATCH(float, HP_ENERGY);
+        case HP_LANCZOS: EMUSV_DISPATCH(float, HP_LANCZOS);
+        case HP_DIAG: return launch_one<float, true, HP_DIAG>(P, A, max_grid, s, grid_out);
+        }
+    }
+#undef EMUSV_DISPATCH
+    return EMUSV_BAD_ARGUMENT;
+}
+
+// Largest grid any streaming kernel of this library launches (bounds partial buffers).
+int max_grid_blocks() { return sm_count() * 8; }
+
+// ---------------------------------------------------------------- reduction kernels
+// Sum partials[nblocks][NRED] into out[NRED] (one block, fixed order).
+__global__ void k_sum_partials(const double *partials, int nblocks, double *out) {
+    __shared__ double scratch[(BLOCK / 32) * NRED];
+    double v[NRED];
+    sum_partials<NRED>(partials, nblocks, NRED, v, scratch);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NRED; ++k) out[k] = v[k];
+}
+
+// Occupation / correlation in one pass.  For a grid-stride loop with a power-of-two
+// stride S, the low log2(S) bits of a thread's indices are fixed: those bits get the
+// thread's total weight once; the bits above vary with the loop and are accumulated
+// per amplitude.  CORR additionally accumulates the n*n pair sums (n <= 32).
+template <typename R, bool CORR>
+__global__ void __launch_bounds__(BLOCK) k_occupation(const void *psi_, int n, double *partials) {
+    typedef typename cvec<R>::T C;
+    const C *psi = reinterpret_cast<const C *>(psi_);
+    __shared__ double red[(BLOCK / 32) * MAXQ];
+    const i64 D = i64(1) << n;
+    const i64 S = (i64)gridDim.x * blockDim.x;  // power of two by construction
+    int sbits = 0;
+    while ((i64(1) << sbits) < S) ++sbits;
+    const i64 start = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    double total = 0.0;
+    double hi[MAXQ];
+#pragma unroll
+    for (int p = 0; p < MAXQ; ++p) hi[p] = 0.0;
+    for (i64 x = start; x < D; x += S) {
+        const C a = psi[x];
+        const double w = double(a.x) * double(a.x) + double(a.y) * double(a.y);
+        total += w;
+#pragma unroll
+        for (int p = 0; p < MAXQ; ++p)
+            if (p >= sbits && p < n && ((x >> p) & 1)) hi[p] += w;
+    }
+    // occupation by qubit i (bit p = n-1-i)
+    double occ[MAXQ];
+#pragma unroll
+    for (int p = 0; p < MAXQ; ++p) occ[p] = (p < sbits) ? (((start >> p) & 1) ? total : 0.0) : hi[p];
+    // block reduction of MAXQ values
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int p = 0; p < MAXQ; ++p) occ[p] = warp_sum(occ[p]);
+    if (lane == 0)
+        for (int p = 0; p < MAXQ; ++p) red[warp * MAXQ + p] = occ[p];
+    __syncthreads();
+    if (threadIdx.x < MAXQ) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w * MAXQ + threadIdx.x];
+        partials[(i64)blockIdx.x * MAXQ + threadIdx.x] = s;
+    }
+}
+
+// Pair sums sum_x |psi_x|^2 x_p x_q for p <= q: one block per (tile of amplitudes),
+// each thread accumulates the n(n+1)/2 pairs of its amplitudes in shared memory rows.
+template <typename R>
+__global__ void __launch_bounds__(BLOCK) k_correlation(const void *psi_, int n, double *partials) {
+    typedef typename cvec<R>::T C;
+    const C *psi = reinterpret_cast<const C *>(psi_);
+    __shared__ double acc[MAXQ * MAXQ];
+    for (int k = threadIdx.x; k < MAXQ * MAXQ; k += blockDim.x) acc[k] = 0.0;
+    __syncthreads();
+    const i64 D = i64(1) << n;
+    const i64 S = (i64)gridDim.x * blockDim.x;
+    // each thread handles the pair rows p = lane-strided, after a warp shares weights
+    const int lane = threadIdx.x & 31;
+    double rowacc[MAXQ];
+#pragma unroll
+    for (int q = 0; q < MAXQ; ++q) rowacc[q] = 0.0;
+    for (i64 x0 = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); x0 < D; x0 += S) {
+        // the warp loads 32 consecutive amplitudes; lane p then accumulates row p
+        const i64 xl = x0 + lane;
+        double w = 0.0;
+        if (xl < D) {
+            const C a = psi[xl];
+            w = double(a.x) * double(a.x) + double(a.y) * double(a.y);
+        }
+        for (int j = 0; j < 32; ++j) {
+            const double wj = __shfl_sync(0xffffffffu, w, j);
+            const i64 xj = x0 + j;
+            if (lane < n && ((xj >> lane) & 1)) {
+#pragma unroll
+                for (int q = 0; q < MAXQ; ++q)
+                    if (q < n && ((xj >> q) & 1)) rowacc[q] += wj;
+            }
+        }
+    }
+    if (lane < n) {
+        for (int q = 0; q < n; ++q) atomicAdd(&acc[lane * MAXQ + q], rowacc[q]);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        const int p = k / n, q = k % n;
+        partials[(i64)blockIdx.x * n * n + k] = acc[p * MAXQ + q];
+    }
+}
+
+// Sum occupation partials into qubit order: out[i] = sum_b partials[b][n-1-i].
+__global__ void k_finish_occ(const double *partials, int nblocks, int n, int stride, double *out) {
+    const int i = threadIdx.x;
+    if (i >= n) return;
+    const int p = n - 1 - i;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partials[(i64)b * stride + p];
+    out[i] = s;
+}
+
+__global__ void k_finish_corr(const double *partials, int nblocks, int n, double *out) {
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        const int i = k / n, j = k % n;
+        const int p = n - 1 - i, q = n - 1 - j;
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += partials[(i64)b * n * n + p * n + q];
+        out[k] = s;
+    }
+}
+
+static int occ_grid(int n) {
+    // power-of-two grid with at most one block per 256 amplitudes
+    i64 D = i64(1) << n;
+    i64 g = 1;
+    while (g * 2 * BLOCK <= D && g * 2 <= (i64)sm_count() * 4) g *= 2;
+    return (int)g;
+}
+
+}  // namespace emusv
+
+using namespace emusv;
+
+extern "C" {
+
+int emusv_build_arch(void) { return 100; }
+
+const char *emusv_status_string(int status) {
+    switch (status) {
+    case EMUSV_OK: return "ok";
+    case EMUSV_NOT_CONVERGED: return "Krylov iteration did not converge within max_krylov_dim";
+    case EMUSV_NONFINITE: return "non-finite value in a reduction";
+    case EMUSV_BAD_ARGUMENT: return "bad argument";
+    case EMUSV_WORKSPACE_TOO_SMALL: return "workspace too small";
+    case EMUSV_CUDA_ERROR: return "CUDA runtime error";
+    case EMUSV_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+    }
+}
+
+size_t emusv_scratch_bytes(int nqubits, int dtype) {
+    (void)dtype;
+    if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS) return 0;
+    const size_t per = (size_t)MAXQ * MAXQ > NRED ? (size_t)MAXQ * MAXQ : NRED;
+    return sizeof(double) * ((size_t)max_grid_blocks() * per + 64);
+}
+
+int emusv_hamiltonian_diag(int nqubits, const double *deltas, const double *interaction,
+                           double *diag_out, void *stream) {
+    HamParams P;
+    static const double zeros[EMUSV_MAX_QUBITS] = {0};
+    if (!diag_out || !make_params(nqubits, zeros, deltas, zeros, interaction, &P))
+        return EMUSV_BAD_ARGUMENT;
+    HpsiArgs A = {};
+    A.out = diag_out;
+    A.tile_bits = hpsi_tile_bits(nqubits);
+    A.su = 1.0;
+    return launch_hpsi(EMUSV_C128, HP_DIAG, P, A, 0, as_stream(stream), nullptr);
+}
+
+int emusv_hpsi(int nqubits, int dtype, const double *omegas, const double *deltas,
+               const double *phis, const double *interaction, const void *psi, void *out,
+               void *stream) {
+    HamParams P;
+    if (!psi || !out || psi == out || !make_params(nqubits, omegas, deltas, phis, interaction, &P))
+        return EMUSV_BAD_ARGUMENT;
+    HpsiArgs A = {};
+    A.u = psi;
+    A.su = 1.0;
+    A.out = out;
+    A.tile_bits = hpsi_tile_bits(nqubits);
+    return launch_hpsi(dtype, HP_STORE, P, A, 0, as_stream(stream), nullptr);
+}
+
+// result_dev[0..1] = <psi|H|psi> (re, im), result_dev[2] = ||H psi||^2.
+int emusv_expect(int nqubits, int dtype, const double *omegas, const double *deltas,
+                 const double *phis, const double *interaction, const void *psi,
+                 double *result_dev, void *scratch, size_t scratch_bytes, void *stream) {
+    HamParams P;
+    if (!psi || !result_dev || !scratch || scratch_bytes < emusv_scratch_bytes(nqubits, dtype) ||
+        !make_params(nqubits, omegas, deltas, phis, interaction, &P))
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    double *partials = reinterpret_cast<double *>(scratch);
+    double *sums = partials + (size_t)max_grid_blocks() * NRED;
+    HpsiArgs A = {};
+    A.u = psi;
+    A.su = 1.0;
+    A.partials = partials;
+    A.tile_bits = hpsi_tile_bits(nqubits);
+    int grid = 0;
+    int st = launch_hpsi(dtype, HP_ENERGY, P, A, max_grid_blocks(), s, &grid);
+    if (st) return st;
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_sum_partials<<<1, BLOCK, 0, s>>>(partials, grid, sums);
+    }
+    EMUSV_CHECK_LAUNCH();
+    // result layout: [<v,Hv> re, im, ||Hv||^2]
+    EMUSV_CHECK(cudaMemcpyAsync(result_dev, sums + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    EMUSV_CHECK(cudaMemcpyAsync(result_dev + 2, sums, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return EMUSV_OK;
+}
+
+int emusv_occupation(int nqubits, int dtype, const void *psi, double *occ_dev, void *scratch,
+                     size_t scratch_bytes, void *stream) {
+    if (!psi || !occ_dev || !scratch || nqubits < 1 || nqubits > EMUSV_MAX_QUBITS ||
+        scratch_bytes < emusv_scratch_bytes(nqubits, dtype) || (dtype != EMUSV_C128 && dtype != EMUSV_C64))
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    double *partials = reinterpret_cast<double *>(scratch);
+    const int grid = occ_grid(nqubits);
+    const int block = (i64(1) << nqubits) < BLOCK ? 32 : BLOCK;
+    if (dtype == EMUSV_C128)
+        {
+            ProfScope ps_(PROF_OBS, s);
+            k_occupation<double, false><<<grid, block, 0, s>>>(psi, nqubits, partials);
+        }
+    else
+        {
+            ProfScope ps_(PROF_OBS, s);
+            k_occupation<float, false><<<grid, block, 0, s>>>(psi, nqubits, partials);
+        }
+    EMUSV_CHECK_LAUNCH();
+    {
+        ProfScope ps_(PROF_OBS, s);
+        k_finish_occ<<<1, 32, 0, s>>>(partials, grid, nqubits, MAXQ, occ_dev);
+    }
+    EMUSV_CHECK_LAUNCH();
+    return EMUSV_OK;
+}
+
+int emusv_correlation(int nqubits, int dtype, const void *psi, double *corr_dev, void *scratch,
+                      size_t scratch_bytes, void *stream) {
+    if (!psi || !corr_dev || !scratch || nqubits < 1 || nqubits > EMUSV_MAX_QUBITS ||
+        scratch_bytes < emusv_scratch_bytes(nqubits, dtype) || (dtype != EMUSV_C128 && dtype != EMUSV_C64))
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    double *partials = reinterpret_cast<double *>(scratch);
+    int grid = occ_grid(nqubits);
+    if (grid > max_grid_blocks()) grid = max_grid_blocks();
+    if (dtype == EMUSV_C128)
+        {
+            ProfScope ps_(PROF_OBS, s);
+            k_correlation<double><<<grid, BLOCK, 0, s>>>(psi, nqubits, partials);
+        }
+    else
+        {
+            ProfScope ps_(PROF_OBS, s);
+            k_correlation<float><<<grid, BLOCK, 0, s>>>(psi, nqubits, partials);
+        }
+    EMUSV_CHECK_LAUNCH();
+    {
+        ProfScope ps_(PROF_OBS, s);
+        k_finish_corr<<<1, BLOCK, 0, s>>>(partials, grid, nqubits, corr_dev);
+    }
+    EMUSV_CHECK_LAUNCH();
+    return EMUSV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,722 @@
+// Lanczos time step exp(-i dt H) psi on the GPU (C ABI emusv_krylov_step) and the
+// building blocks of the generic krylov_exp.
+//
+// Per Lanczos iteration j (reference emu_base/math/krylov_exp.py:49-96):
+//   1. k_hpsi<HP_LANCZOS>: w = H v_j stored into basis slot j+1, fused FP64 reductions
+//      ||Hv||^2, <v_j,Hv>, <v_{j-1},Hv>, <v_j,v_{j-1}>.
+//   2. k_orth: modified Gram-Schmidt against v_{j-1} then v_j (krylov_exp.py:55-58),
+//      coefficients derived from the fused reductions; ||w||^2 partials.
+//   3. k_small (one warp): ||w||, happy-breakdown test (krylov_exp.py:63-71), the
+//      exponential of the extended Krylov matrix and the Expokit error estimate
+//      (krylov_exp.py:77-86), all FP64 on the device.
+// Basis vectors are stored unnormalised with a device scale factor (v_k = scale_k u_k),
+// so no separate normalisation pass exists; the input vector is basis vector 0 in place.
+// Every kernel after the first reads a device status word and exits at once when the
+// iteration has already finished, so the host only synchronises where it tests
+// convergence.
+#include <string.h>
+
+#include "hpsi_kernel.cuh"
+#include "profile.cuh"
+
+namespace emusv {
+
+int hpsi_tile_bits(int n);
+int launch_hpsi(int dtype, int mode, const HamParams &P, HpsiArgs A, int max_grid,
+                cudaStream_t s, int *grid_out);
+int max_grid_blocks();
+
+constexpr int KMAX = 128;  // largest max_krylov_dim supported
+
+enum KStatus { KS_RUNNING = 0, KS_CONVERGED = 1, KS_HAPPY = 2, KS_MAXDIM = 3, KS_NONFINITE = 4 };
+
+struct KState {
+    int status;
+    int iters;
+    int nvec;
+    int pad;
+    double s0, err, outnorm2, pad2;
+    double a_re[KMAX], a_im[KMAX];   // T_H[k][k]   = <v_k, H v_k> - b_k <v_k, v_{k-1}>
+    double b_re[KMAX], b_im[KMAX];   // T_H[k-1][k] = <v_{k-1}, H v_k>
+    double r[KMAX];                  // T_H[k+1][k] = ||w_k||
+    double hn[KMAX];                 // ||H v_k||
+    double scale[KMAX + 2];          // v_k = scale[k] * stored_k
+    double c_re[KMAX + 2], c_im[KMAX + 2];  // result coefficients
+};
+
+struct Workspace {
+    KState *ks;
+    double *part_h, *part_o, *part_c;
+    unsigned char *basis;
+    size_t basis_bytes;
+};
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+static size_t header_bytes() {
+    return align_up(sizeof(KState), 256) + 3 * align_up(sizeof(double) * max_grid_blocks() * NRED, 256);
+}
+
+static Workspace carve(void *ws, size_t bytes) {
+    Workspace W;
+    unsigned char *p = reinterpret_cast<unsigned char *>(ws);
+    size_t off = 0;
+    W.ks = reinterpret_cast<KState *>(p);
+    off += align_up(sizeof(KState), 256);
+    const size_t pb = align_up(sizeof(double) * max_grid_blocks() * NRED, 256);
+    W.part_h = reinterpret_cast<double *>(p + off);
+    off += pb;
+    W.part_o = reinterpret_cast<double *>(p + off);
+    off += pb;
+    W.part_c = reinterpret_cast<double *>(p + off);
+    off += pb;
+    W.basis = p + off;
+    W.basis_bytes = bytes > off ? bytes - off : 0;
+    return W;
+}
+
+static int stream_grid(i64 D) {
+    i64 g = (D + BLOCK - 1) / BLOCK;
+    const i64 cap = (i64)sm_count() * 4;
+    return (int)(g < cap ? g : cap);
+}
+
+// ---------------------------------------------------------------- small kernels
+template <typename R>
+__global__ void __launch_bounds__(BLOCK) k_norm2(const void *v_, i64 D, double *partials) {
+    typedef typename cvec<R>::T C;
+    const C *v = reinterpret_cast<const C *>(v_);
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double acc[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) acc[k] = 0.0;
+    for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < D; x += (i64)gridDim.x * blockDim.x) {
+        const C a = v[x];
+        acc[0] += double(a.x) * double(a.x) + double(a.y) * double(a.y);
+    }
+    block_sum<NRED>(acc, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NRED; ++k) partials[(i64)blockIdx.x * NRED + k] = acc[k];
+}
+
+__global__ void k_init(KState *ks, const double *partials, int nblocks) {
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double v[NRED];
+    sum_partials<NRED>(partials, nblocks, NRED, v, red);
+    if (threadIdx.x == 0) {
+        const double s0 = sqrt(v[0]);  // krylov_exp.py:43
+        ks->s0 = s0;
+        ks->scale[0] = 1.0 / s0;       // krylov_exp.py:44 (applied on load)
+        ks->status = (isfinite(s0) && s0 > 0.0) ? KS_RUNNING : KS_NONFINITE;
+        ks->iters = 0;
+        ks->nvec = 0;
+        ks->err = 0.0;
+        ks->outnorm2 = 0.0;
+    }
+}
+
+// w <- w - b v_{j-1} - a v_j  (MGS order, krylov_exp.py:55-58), ||w||^2 partials.
+template <typename R>
+__global__ void __launch_bounds__(BLOCK)
+k_orth(KState *ks, int j, const double *part_h, int nb_h, const void *vj_, const void *vp_,
+       void *w_, i64 D, double *part_o) {
+    typedef typename cvec<R>::T C;
+    if (ks->status != KS_RUNNING) return;
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double s[NRED];
+    sum_partials<NRED>(part_h, nb_h, NRED, s, red);
+    // s: 0 ||Hv||^2, 1-2 <v,Hv>, 3-4 <vp,Hv>, 5-6 <v,vp>
+    double br = 0.0, bi = 0.0;
+    if (j > 0) {
+        br = s[3];
+        bi = s[4];
+    }
+    // a = <v,Hv> - b <v,vp>
+    const double ar = s[1] - (j > 0 ? (br * s[5] - bi * s[6]) : 0.0);
+    const double ai = s[2] - (j > 0 ? (br * s[6] + bi * s[5]) : 0.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ks->a_re[j] = ar;
+        ks->a_im[j] = ai;
+        ks->b_re[j] = br;
+        ks->b_im[j] = bi;
+        ks->hn[j] = sqrt(s[0]);
+    }
+    const double sj = ks->scale[j];
+    const double sp = j > 0 ? ks->scale[j - 1] : 0.0;
+    // coefficients on the stored (unscaled) vectors
+    const double car = ar * sj, cai = ai * sj, cbr = br * sp, cbi = bi * sp;
+    const C *vj = reinterpret_cast<const C *>(vj_);
+    const C *vp = reinterpret_cast<const C *>(vp_);
+    C *w = reinterpret_cast<C *>(w_);
+    double acc[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) acc[k] = 0.0;
+    for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < D; x += (i64)gridDim.x * blockDim.x) {
+        const C h = w[x];
+        const C a = vj[x];
+        double wr = double(h.x) - (car * double(a.x) - cai * double(a.y));
+        double wi = double(h.y) - (car * double(a.y) + cai * double(a.x));
+        if (j > 0) {
+            const C p = vp[x];
+            wr -= cbr * double(p.x) - cbi * double(p.y);
+            wi -= cbr * double(p.y) + cbi * double(p.x);
+        }
+        const C o = cmake<C>(wr, wi);
+        w[x] = o;
+        acc[0] += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+    }
+    block_sum<NRED>(acc, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NRED; ++k) part_o[(i64)blockIdx.x * NRED + k] = acc[k];
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// One warp: y = exp(A) e_0 for a complex tridiagonal m x m matrix A
+//   (d[k] = A[k][k], up[k] = A[k-1][k], lo[k] = A[k+1][k]),
+// plus Z1 = int_0^1 y_{m-1}(s) ds and Z2 = int_0^1 (1-s) y_{m-1}(s) ds, which give the
+// two Expokit extension rows exactly: for the extended matrix
+// [[A,0,0],[l e_{m-1}^T,0,0],[0,1,0]],  exp(.) e_0 = (y, l Z1, l Z2).
+// Method: Taylor series of exp(hA) applied to the vector, h = 1/s with ||hA||_1 <= 2,
+// repeated s times; the integrals come from the same series term by term
+// (int_0^h (tau/h)^q dtau = h/(q+1), int_0^h (h-tau)(tau/h)^q dtau = h^2/((q+1)(q+2))).
+// smem arrays hold m+2 entries with a zero pad on each side (index k+1 for entry k).
+__device__ void warp_expm_col(int m, const double2 *d, const double2 *up, const double2 *lo,
+                              double2 *y, double2 *t, double2 *tn, double2 *acc,
+                              double2 *Z1, double2 *Z2) {
+    const int lane = threadIdx.x & 31;
+    double nrm = 0.0;
+    for (int k = lane; k < m; k += 32) {
+        double c = hypot(d[k].x, d[k].y);
+        if (k > 0) c += hypot(up[k].x, up[k].y);
+        if (k < m - 1) c += hypot(lo[k].x, lo[k].y);
+        nrm = fmax(nrm, c);
+    }
+    nrm = warp_max(nrm);
+    const double THETA = 2.0;
+    // ||hA||_1 <= THETA; the sub-step count is capped (callers check finiteness first)
+    int s = 1;
+    if (nrm > THETA) s = nrm < THETA * (1 << 20) ? (int)ceil(nrm / THETA) : (1 << 20);
+    const double h = 1.0 / s;
+    // padded vectors: index k+1 holds entry k; pads stay zero
+    for (int k = lane; k < m + 2; k += 32) {
+        y[k] = make_double2(k == 1 ? 1.0 : 0.0, 0.0);
+        t[k] = make_double2(0.0, 0.0);
+        tn[k] = make_double2(0.0, 0.0);
+        acc[k] = make_double2(0.0, 0.0);
+    }
+    __syncwarp();
+    double2 z1 = make_double2(0.0, 0.0), z2 = make_double2(0.0, 0.0);
+    for (int step = 0; step < s; ++step) {
+        for (int k = lane; k < m; k += 32) {
+            t[k + 1] = y[k + 1];
+            acc[k + 1] = y[k + 1];
+        }
+        __syncwarp();
+        double2 tl = t[m];  // last entry of t_0
+        double2 S1 = tl, S2 = make_double2(0.5 * tl.x, 0.5 * tl.y);
+        double2 *cur = t, *nxt = tn;
+        for (int q = 1; q < 80; ++q) {
+            const double f = h / q;
+            double tmax = 0.0, amax = 0.0;
+            for (int k = lane; k < m; k += 32) {
+                const double2 a0 = cur[k + 1], am = cur[k], ap = cur[k + 2];
+                double re = d[k].x * a0.x - d[k].y * a0.y;
+                double im = d[k].x * a0.y + d[k].y * a0.x;
+                if (k > 0) {  // A[k][k-1] = lo[k-1]
+                    re += lo[k - 1].x * am.x - lo[k - 1].y * am.y;
+                    im += lo[k - 1].x * am.y + lo[k - 1].y * am.x;
+                }
+                if (k < m - 1) {  // A[k][k+1] = up[k+1]
+                    re += up[k + 1].x * ap.x - up[k + 1].y * ap.y;
+                    im += up[k + 1].x * ap.y + up[k + 1].y * ap.x;
+                }
+                const double2 o = make_double2(f * re, f * im);
+                nxt[k + 1] = o;
+                double2 ac = acc[k + 1];
+                ac.x += o.x;
+                ac.y += o.y;
+                acc[k + 1] = ac;
+                tmax = fmax(tmax, fmax(fabs(o.x), fabs(o.y)));
+                amax = fmax(amax, fmax(fabs(ac.x), fabs(ac.y)));
+            }
+            __syncwarp();
+            tmax = warp_max(tmax);
+            amax = warp_max(amax);
+            const double2 last = nxt[m];
+            const double w1 = 1.0 / (q + 1), w2 = 1.0 / ((double)(q + 1) * (q + 2));
+            S1.x += w1 * last.x;
+            S1.y += w1 * last.y;
+            S2.x += w2 * last.x;
+            S2.y += w2 * last.y;
+            double2 *tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+            if (tmax <= 1e-18 * fmax(amax, 1e-300)) break;
+        }
+        z2.x += h * z1.x + h * h * S2.x;
+        z2.y += h * z1.y + h * h * S2.y;
+        z1.x += h * S1.x;
+        z1.y += h * S1.y;
+        for (int k = lane; k < m; k += 32) y[k + 1] = acc[k + 1];
+        __syncwarp();
+    }
+    *Z1 = z1;
+    *Z2 = z2;
+}
+
+// Decide iteration j: ||w_j||, happy breakdown, extended exponential, error estimate.
+// do_exp = 0 skips the exponential (convergence is not tested at this j).
+__global__ void __launch_bounds__(32)
+k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp_tol,
+        double norm_tol, int do_exp, int maxdim) {
+    if (ks->status != KS_RUNNING) return;
+    __shared__ double2 d[KMAX + 2], up[KMAX + 2], lo[KMAX + 2];
+    __shared__ double2 y[KMAX + 4], t[KMAX + 4], tn[KMAX + 4], acc[KMAX + 4];
+    const int lane = threadIdx.x;
+    // deterministic sum of the ||w||^2 partials by one warp
+    double v = 0.0;
+    for (int b = lane; b < nb_o; b += 32) v += part_o[(i64)b * NRED];
+    v = warp_sum(v);
+    const double r = sqrt(v);
+    const double n2 = dt * r;  // ||w|| of the operator -i dt H (krylov_exp.py:60)
+    if (!isfinite(r) || !isfinite(ks->hn[j]) || !isfinite(ks->a_re[j]) || !isfinite(ks->a_im[j]) ||
+        !isfinite(ks->b_re[j]) || !isfinite(ks->b_im[j])) {
+        if (lane == 0) {
+            ks->status = KS_NONFINITE;
+            ks->iters = j + 1;
+        }
+        return;
+    }
+    if (lane == 0) ks->r[j] = r;
+    const bool happy = n2 < norm_tol;  // krylov_exp.py:63
+    if (!happy && !do_exp) {
+        if (lane == 0) ks->scale[j + 1] = 1.0 / r;
+        return;
+    }
+    // A = -i dt T_H (complex tridiagonal, size j+1)
+    const int m = j + 1;
+    for (int k = lane; k < m; k += 32) {
+        d[k] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
+        up[k] = k > 0 ? make_double2(dt * ks->b_im[k], -dt * ks->b_re[k]) : make_double2(0.0, 0.0);
+        lo[k] = make_double2(0.0, -dt * (k == j ? r : ks->r[k]));  // lo[j]: extension entry
+    }
+    __syncwarp();
+    double2 Z1, Z2;
+    warp_expm_col(m, d, up, lo, y, t, tn, acc, &Z1, &Z2);
+    if (happy) {  // krylov_exp.py:65-71: exp(T[:j+1,:j+1]) e_0 over j+1 vectors
+        for (int k = lane; k < m; k += 32) {
+            ks->c_re[k] = y[k + 1].x;
+            ks->c_im[k] = y[k + 1].y;
+        }
+        if (lane == 0) {
+            ks->nvec = m;
+            ks->iters = j + 1;
+            ks->status = KS_HAPPY;
+        }
+        return;
+    }
+    // extension: x_{j+1} = l Z1, x_{j+2} = l Z2 with l = A[j+1][j] = -i dt r_j
+    const double2 l = lo[j];
+    const double2 x1 = make_double2(l.x * Z1.x - l.y * Z1.y, l.x * Z1.y + l.y * Z1.x);
+    const double2 x2 = make_double2(l.x * Z2.x - l.y * Z2.y, l.x * Z2.y + l.y * Z2.x);
+    const double err1 = hypot(x1.x, x1.y);                       // krylov_exp.py:81
+    const double err2 = hypot(x2.x, x2.y) * (dt * ks->hn[j]);   // krylov_exp.py:82
+    const double err = err1 < err2 ? err1 : (err1 * err2 / (err1 - err2));  // :84
+    for (int k = lane; k < m; k += 32) {
+        ks->c_re[k] = y[k + 1].x;
+        ks->c_im[k] = y[k + 1].y;
+    }
+    if (lane == 0) {
+        ks->c_re[m] = x1.x;  // expd[j+1, 0] multiplies v_{j+1} (krylov_exp.py:88-90)
+        ks->c_im[m] = x1.y;
+        ks->scale[j + 1] = 1.0 / r;
+        ks->err = err;
+        ks->nvec = m + 1;
+        ks->iters = j + 1;
+        if (err < exp_tol)
+            ks->status = KS_CONVERGED;
+        else if (j + 1 >= maxdim)
+            ks->status = KS_MAXDIM;
+    }
+}
+
+// out = s0 * sum_k c_k scale_k stored_k ;  ||out||^2 partials.
+template <typename R>
+__global__ void __launch_bounds__(BLOCK)
+k_combine(const KState *ks, const void *v0_, const unsigned char *basis, i64 D, void *out_,
+          double *partials) {
+    typedef typename cvec<R>::T C;
+    __shared__ double cr[KMAX + 2], ci[KMAX + 2];
+    __shared__ double red[(BLOCK / 32) * NRED];
+    const int nv = ks->nvec;
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+        const double f = ks->s0 * ks->scale[k];
+        cr[k] = f * ks->c_re[k];
+        ci[k] = f * ks->c_im[k];
+    }
+    __syncthreads();
+    const C *v0 = reinterpret_cast<const C *>(v0_);
+    const C *bs = reinterpret_cast<const C *>(basis);
+    C *out = reinterpret_cast<C *>(out_);
+    double acc[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) acc[k] = 0.0;
+    for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < D; x += (i64)gridDim.x * blockDim.x) {
+        const C a = v0[x];
+        double re = cr[0] * double(a.x) - ci[0] * double(a.y);
+        double im = cr[0] * double(a.y) + ci[0] * double(a.x);
+        for (int k = 1; k < nv; ++k) {
+            const C b = bs[(i64)(k - 1) * D + x];
+            re += cr[k] * double(b.x) - ci[k] * double(b.y);
+            im += cr[k] * double(b.y) + ci[k] * double(b.x);
+        }
+        const C o = cmake<C>(re, im);
+        out[x] = o;
+        acc[0] += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+    }
+    block_sum<NRED>(acc, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NRED; ++k) partials[(i64)blockIdx.x * NRED + k] = acc[k];
+}
+
+__global__ void k_finish_combine(KState *ks, const double *partials, int nblocks) {
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double v[NRED];
+    sum_partials<NRED>(partials, nblocks, NRED, v, red);
+    if (threadIdx.x == 0) ks->outnorm2 = v[0];
+}
+
+// ---------------------------------------------------------------- generic helpers
+template <typename R>
+__global__ void __launch_bounds__(BLOCK)
+k_dot(const void *a_, const void *b_, i64 len, double *partials) {
+    typedef typename cvec<R>::T C;
+    const C *a = reinterpret_cast<const C *>(a_);
+    const C *b = reinterpret_cast<const C *>(b_);
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double acc[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) acc[k] = 0.0;
+    for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < len; x += (i64)gridDim.x * blockDim.x) {
+        const C p = a[x], q = b[x];
+        acc[0] += double(p.x) * double(q.x) + double(p.y) * double(q.y);
+        acc[1] += double(p.x) * double(q.y) - double(p.y) * double(q.x);
+    }
+    block_sum<NRED>(acc, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NRED; ++k) partials[(i64)blockIdx.x * NRED + k] = acc[k];
+}
+
+__global__ void k_sum2(const double *partials, int nblocks, double *out) {
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double v[NRED];
+    sum_partials<NRED>(partials, nblocks, NRED, v, red);
+    if (threadIdx.x == 0) {
+        out[0] = v[0];
+        out[1] = v[1];
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(BLOCK)
+k_axpy(double ar, double ai, const void *x_, void *y_, i64 len) {
+    typedef typename cvec<R>::T C;
+    const C *x = reinterpret_cast<const C *>(x_);
+    C *y = reinterpret_cast<C *>(y_);
+    for (i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x; k < len; k += (i64)gridDim.x * blockDim.x) {
+        const C a = x[k];
+        C b = y[k];
+        const double re = double(b.x) + ar * double(a.x) - ai * double(a.y);
+        const double im = double(b.y) + ar * double(a.y) + ai * double(a.x);
+        y[k] = cmake<C>(re, im);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(BLOCK)
+k_vcombine(int nk, const double2 *coef, const void *V_, i64 len, void *out_) {
+    typedef typename cvec<R>::T C;
+    const C *V = reinterpret_cast<const C *>(V_);
+    C *out = reinterpret_cast<C *>(out_);
+    for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < len; x += (i64)gridDim.x * blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k < nk; ++k) {
+            const C b = V[(i64)k * len + x];
+            const double2 c = coef[k];
+            re += c.x * double(b.x) - c.y * double(b.y);
+            im += c.x * double(b.y) + c.y * double(b.x);
+        }
+        out[x] = cmake<C>(re, im);
+    }
+}
+
+struct TriArgs {
+    double2 d[KMAX + 2], up[KMAX + 2], lo[KMAX + 2];
+};
+
+__global__ void __launch_bounds__(32) k_tridiag_expm(int m, const TriArgs *A, double2 *xout) {
+    __shared__ double2 y[KMAX + 4], t[KMAX + 4], tn[KMAX + 4], acc[KMAX + 4];
+    double2 Z1, Z2;
+    warp_expm_col(m, A->d, A->up, A->lo, y, t, tn, acc, &Z1, &Z2);
+    for (int k = threadIdx.x; k < m; k += 32) xout[k] = y[k + 1];
+}
+
+}  // namespace emusv
+
+using namespace emusv;
+
+namespace {
+thread_local int *pinned_status = nullptr;
+
+int read_status(KState *ks, cudaStream_t s, int *out) {
+    if (!pinned_status) {
+        if (cudaHostAlloc((void **)&pinned_status, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+            pinned_status = nullptr;
+            return EMUSV_CUDA_ERROR;
+        }
+    }
+    EMUSV_CHECK(cudaMemcpyAsync(pinned_status, &ks->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    EMUSV_CHECK(cudaStreamSynchronize(s));
+    *out = pinned_status[0];
+    return EMUSV_OK;
+}
+}  // namespace
+
+extern "C" {
+
+size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity) {
+    if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS || basis_capacity < 0) return 0;
+    const size_t es = dtype == EMUSV_C128 ? 16 : 8;
+    return header_bytes() + (size_t)basis_capacity * (size_t(1) << nqubits) * es;
+}
+
+int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
+                      const double *deltas, const double *phis, const double *interaction,
+                      const void *psi_in, void *psi_out, double exp_tolerance,
+                      double norm_tolerance, int max_krylov_dim, int krylov_dim_hint,
+                      void *workspace, size_t workspace_bytes, emusv_krylov_info *info,
+                      void *stream) {
+    HamParams P;
+    if (!psi_in || !psi_out || !workspace || (dtype != EMUSV_C128 && dtype != EMUSV_C64) ||
+        max_krylov_dim < 1 || max_krylov_dim > KMAX - 2 || !isfinite(dt) ||
+        !make_params(nqubits, omegas, deltas, phis, interaction, &P))
+        return EMUSV_BAD_ARGUMENT;
+    if (workspace_bytes < header_bytes()) return EMUSV_WORKSPACE_TOO_SMALL;
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) || (reinterpret_cast<uintptr_t>(psi_in) & 15) ||
+        (reinterpret_cast<uintptr_t>(psi_out) & 15))
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    const i64 D = i64(1) << nqubits;
+    const size_t es = dtype == EMUSV_C128 ? 16 : 8;
+    Workspace W = carve(workspace, workspace_bytes);
+    const int capacity = (int)(W.basis_bytes / (D * es));
+    if (capacity < 1) return EMUSV_WORKSPACE_TOO_SMALL;
+    auto stored = [&](int k) -> const void * {
+        return k == 0 ? psi_in : (const void *)(W.basis + (size_t)(k - 1) * D * es);
+    };
+    const int sg = stream_grid(D);
+
+    if (dtype == EMUSV_C128)
+        {
+            ProfScope ps_(PROF_ORTH, s);
+            k_norm2<double><<<sg, BLOCK, 0, s>>>(psi_in, D, W.part_h);
+        }
+    else
+        {
+            ProfScope ps_(PROF_ORTH, s);
+            k_norm2<float><<<sg, BLOCK, 0, s>>>(psi_in, D, W.part_h);
+        }
+    EMUSV_CHECK_LAUNCH();
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_init<<<1, BLOCK, 0, s>>>(W.ks, W.part_h, sg);
+    }
+    EMUSV_CHECK_LAUNCH();
+
+    int status = KS_RUNNING;
+    for (int j = 0; j < max_krylov_dim; ++j) {
+        if (j + 1 > capacity) {
+            int st = read_status(W.ks, s, &status);
+            if (st) return st;
+            if (status == KS_RUNNING) return EMUSV_WORKSPACE_TOO_SMALL;
+            break;
+        }
+        HpsiArgs A = {};
+        A.u = stored(j);
+        A.su_dev = &W.ks->scale[j];
+        A.up = j > 0 ? stored(j - 1) : nullptr;
+        A.sp_dev = j > 0 ? &W.ks->scale[j - 1] : nullptr;
+        A.out = const_cast<void *>(stored(j + 1));
+        A.partials = W.part_h;
+        A.tile_bits = hpsi_tile_bits(nqubits);
+        A.gate = &W.ks->status;
+        int gh = 0;
+        int st = launch_hpsi(dtype, HP_LANCZOS, P, A, max_grid_blocks(), s, &gh);
+        if (st) return st;
+        if (dtype == EMUSV_C128)
+            {
+                ProfScope ps_(PROF_ORTH, s);
+                k_orth<double><<<sg, BLOCK, 0, s>>>(W.ks, j, W.part_h, gh, stored(j),
+                                                    j > 0 ? stored(j - 1) : nullptr,
+                                                    const_cast<void *>(stored(j + 1)), D, W.part_o);
+            }
+        else
+            {
+                ProfScope ps_(PROF_ORTH, s);
+                k_orth<float><<<sg, BLOCK, 0, s>>>(W.ks, j, W.part_h, gh, stored(j),
+                                                   j > 0 ? stored(j - 1) : nullptr,
+                                                   const_cast<void *>(stored(j + 1)), D, W.part_o);
+            }
+        EMUSV_CHECK_LAUNCH();
+        const int do_exp = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
+        {
+            ProfScope ps_(PROF_SMALL, s);
+            k_small<<<1, 32, 0, s>>>(W.ks, j, W.part_o, sg, dt, exp_tolerance, norm_tolerance, do_exp,
+                                     max_krylov_dim);
+        }
+        EMUSV_CHECK_LAUNCH();
+        if (do_exp) {
+            st = read_status(W.ks, s, &status);
+            if (st) return st;
+            if (status != KS_RUNNING) break;
+        }
+    }
+    if (status == KS_RUNNING) {
+        int st = read_status(W.ks, s, &status);
+        if (st) return st;
+    }
+    if (status == KS_NONFINITE || status == KS_RUNNING) {
+        if (info) memset(info, 0, sizeof(*info));
+        return EMUSV_NONFINITE;
+    }
+    if (dtype == EMUSV_C128)
+        {
+            ProfScope ps_(PROF_COMBINE, s);
+            k_combine<double><<<sg, BLOCK, 0, s>>>(W.ks, psi_in, W.basis, D, psi_out, W.part_c);
+        }
+    else
+        {
+            ProfScope ps_(PROF_COMBINE, s);
+            k_combine<float><<<sg, BLOCK, 0, s>>>(W.ks, psi_in, W.basis, D, psi_out, W.part_c);
+        }
+    EMUSV_CHECK_LAUNCH();
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_finish_combine<<<1, BLOCK, 0, s>>>(W.ks, W.part_c, sg);
+    }
+    EMUSV_CHECK_LAUNCH();
+    if (info) {
+        KState h;
+        EMUSV_CHECK(cudaMemcpyAsync(&h, W.ks, offsetof(KState, a_re), cudaMemcpyDeviceToHost, s));
+        EMUSV_CHECK(cudaStreamSynchronize(s));
+        info->iterations = h.iters;
+        info->happy_breakdown = h.status == KS_HAPPY;
+        info->converged = h.status == KS_HAPPY || h.status == KS_CONVERGED;
+        info->basis_vectors = h.nvec;
+        info->error_estimate = h.err;
+        info->input_norm = h.s0;
+        info->output_norm = sqrt(h.outnorm2);
+    }
+    return status == KS_MAXDIM ? EMUSV_NOT_CONVERGED : EMUSV_OK;
+}
+
+int emusv_vec_dot(int64_t len, int dtype, const void *a, const void *b, double *res_dev,
+                  void *scratch, size_t scratch_bytes, void *stream) {
+    if (len < 1 || !a || !b || !res_dev || !scratch ||
+        scratch_bytes < sizeof(double) * (size_t)max_grid_blocks() * NRED)
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    double *partials = reinterpret_cast<double *>(scratch);
+    const int g = stream_grid(len);
+    if (dtype == EMUSV_C128)
+        {
+            ProfScope ps_(PROF_ORTH, s);
+            k_dot<double><<<g, BLOCK, 0, s>>>(a, b, len, partials);
+        }
+    else if (dtype == EMUSV_C64)
+        {
+            ProfScope ps_(PROF_ORTH, s);
+            k_dot<float><<<g, BLOCK, 0, s>>>(a, b, len, partials);
+        }
+    else
+        return EMUSV_BAD_ARGUMENT;
+    EMUSV_CHECK_LAUNCH();
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_sum2<<<1, BLOCK, 0, s>>>(partials, g, res_dev);
+    }
+    EMUSV_CHECK_LAUNCH();
+    return EMUSV_OK;
+}
+
+int emusv_vec_axpy(int64_t len, int dtype, const double *alpha, const void *x, void *y,
+                   void *stream) {
+    if (len < 1 || !alpha || !x || !y) return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    const int g = stream_grid(len);
+    if (dtype == EMUSV_C128)
+        {
+            ProfScope ps_(PROF_ORTH, s);
+            k_axpy<double><<<g, BLOCK, 0, s>>>(alpha[0], alpha[1], x, y, len);
+        }
+    else if (dtype == EMUSV_C64)
+        {
+            ProfScope ps_(PROF_ORTH, s);
+            k_axpy<float><<<g, BLOCK, 0, s>>>(alpha[0], alpha[1], x, y, len);
+        }
+    else
+        return EMUSV_BAD_ARGUMENT;
+    EMUSV_CHECK_LAUNCH();
+    return EMUSV_OK;
+}
+
+int emusv_vec_combine(int64_t len, int dtype, int k, const double *coef_dev, const void *V,
+                      void *out, void *stream) {
+    if (len < 1 || k < 1 || !coef_dev || !V || !out) return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    const int g = stream_grid(len);
+    const double2 *c = reinterpret_cast<const double2 *>(coef_dev);
+    if (dtype == EMUSV_C128)
+        {
+            ProfScope ps_(PROF_COMBINE, s);
+            k_vcombine<double><<<g, BLOCK, 0, s>>>(k, c, V, len, out);
+        }
+    else if (dtype == EMUSV_C64)
+        {
+            ProfScope ps_(PROF_COMBINE, s);
+            k_vcombine<float><<<g, BLOCK, 0, s>>>(k, c, V, len, out);
+        }
+    else
+        return EMUSV_BAD_ARGUMENT;
+    EMUSV_CHECK_LAUNCH();
+    return EMUSV_OK;
+}
+
+size_t emusv_tridiag_scratch_bytes(void) { return align_up(sizeof(TriArgs), 256); }
+
+int emusv_tridiag_expm_col(int m, const double *diag, const double *upper, const double *lower,
+                           double *x_dev, void *scratch, size_t scratch_bytes, void *stream) {
+    if (m < 1 || m > KMAX || !diag || !upper || !lower || !x_dev || !scratch ||
+        scratch_bytes < sizeof(TriArgs))
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    TriArgs *A = reinterpret_cast<TriArgs *>(scratch);
+    EMUSV_CHECK(cudaMemcpyAsync(A->d, diag, sizeof(double2) * m, cudaMemcpyHostToDevice, s));
+    EMUSV_CHECK(cudaMemcpyAsync(A->up, upper, sizeof(double2) * m, cudaMemcpyHostToDevice, s));
+    EMUSV_CHECK(cudaMemcpyAsync(A->lo, lower, sizeof(double2) * m, cudaMemcpyHostToDevice, s));
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_tridiag_expm<<<1, 32, 0, s>>>(m, A, reinterpret_cast<double2 *>(x_dev));
+    }
+    EMUSV_CHECK_LAUNCH();
+    // host arrays may be reused by the caller once this returns
+    EMUSV_CHECK(cudaStreamSynchronize(s));
+    return EMUSV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,277 @@
+"""Backend time loop and configuration, the drop-in for emu-sv's SVConfig / SVBackendImpl
+(reference emu_sv/sv_config.py:33-155, emu_sv/sv_backend_impl.py:74-262,
+emu_sv/sv_backend.py:7-42).
+
+pulser is not a dependency: the loop consumes a :class:`SequenceData` (the reference's
+adapter output, emu_base/pulser_adapter.py:259-280) -- per-step midpoint samples of
+Omega/delta/phi, the target-time grid in ns and the interaction matrix -- and the
+observables are small local classes with pulser's names and evaluation-time semantics.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import logging
+import time
+from typing import Callable, Sequence
+
+import numpy as np
+import torch
+
+from .hamiltonian import RydbergHamiltonian
+from .observables import (correlation_matrix_sv_impl, energy_second_moment_sv_impl,
+                          energy_sv_impl, energy_variance_sv_impl, qubit_occupation_sv_impl)
+from .state_vector import StateVector
+from .time_evolution import EvolveStateVector
+
+_TIME_CONVERSION_COEFF = 0.001  # Omega and delta in rad/us, dt in ns (sv_backend_impl.py:29)
+logger = logging.getLogger("emulators")
+
+
+# ---------------------------------------------------------------- observables
+class Observable:
+    tag = "observable"
+
+    def __init__(self, evaluation_times: Sequence[float] | None = None, tag_suffix: str = ""):
+        self.evaluation_times = None if evaluation_times is None else [float(t) for t in evaluation_times]
+        self.tag_suffix = tag_suffix
+
+    @property
+    def name(self) -> str:
+        return self.tag + (f"_{self.tag_suffix}" if self.tag_suffix else "")
+
+    def due(self, t: float, dt_frac: float) -> bool:
+        if self.evaluation_times is None:
+            return True
+        return any(abs(t - e) <= 0.5 * dt_frac + 1e-12 for e in self.evaluation_times)
+
+    def apply(self, *, config, state, hamiltonian):  # pragma: no cover - overridden
+        raise NotImplementedError
+
+
+class Occupation(Observable):
+    tag = "occupation"
+
+    def apply(self, *, config, state, hamiltonian):
+        return qubit_occupation_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+
+
+class CorrelationMatrix(Observable):
+    tag = "correlation_matrix"
+
+    def apply(self, *, config, state, hamiltonian):
+        return correlation_matrix_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+
+
+class Energy(Observable):
+    tag = "energy"
+
+    def apply(self, *, config, state, hamiltonian):
+        return energy_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+
+
+class EnergyVariance(Observable):
+    tag = "energy_variance"
+
+    def apply(self, *, config, state, hamiltonian):
+        return energy_variance_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+
+
+class EnergySecondMoment(Observable):
+    tag = "energy_second_moment"
+
+    def apply(self, *, config, state, hamiltonian):
+        return energy_second_moment_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+
+
+class StateResult(Observable):
+    tag = "state"
+
+    def apply(self, *, config, state, hamiltonian):
+        return StateVector(state.data.clone())
+
+
+class BitStrings(Observable):
+    tag = "bitstrings"
+
+    def __init__(self, evaluation_times=None, num_shots: int = 1000, tag_suffix: str = ""):
+        super().__init__(evaluation_times, tag_suffix)
+        self.num_shots = num_shots
+
+    def apply(self, *, config, state, hamiltonian):
+        return state.sample(self.num_shots)
+
+
+class Results:
+    """Per-observable time series: ``results.get(tag)`` -> list of values,
+    ``results.times(tag)`` -> their normalised times."""
+
+    def __init__(self, atom_order: Sequence[str], total_duration: int):
+        self.atom_order = tuple(atom_order)
+        self.total_duration = total_duration
+        self._data: dict[str, list] = {}
+        self._times: dict[str, list] = {}
+        self.statistics: list[dict] = []
+
+    def _store(self, tag: str, t: float, value) -> None:
+        self._data.setdefault(tag, []).append(value)
+        self._times.setdefault(tag, []).append(t)
+
+    def get(self, tag: str) -> list:
+        return self._data.get(tag, [])
+
+    def times(self, tag: str) -> list:
+        return self._times.get(tag, [])
+
+    def __getattr__(self, tag):
+        if tag.startswith("_"):
+            raise AttributeError(tag)
+        if tag in self._data:
+            return self._data[tag]
+        raise AttributeError(tag)
+
+
+# ---------------------------------------------------------------- config and data
+class SVConfig:
+    """sv_config.py:75-122 keyword set, plus the B200 knobs:
+
+    * ``precision``: "c128" (reference) or "c64" (complex64 vectors; FP64 Krylov scalars,
+      tridiagonal exponential and norms);
+    * ``krylov_dim_hint``: test convergence from the previous step's iteration count on.
+    """
+
+    def __init__(self, *, dt: float = 10.0, max_krylov_dim: int = 100,
+                 krylov_tolerance: float = 1e-10, gpu: bool | None = None,
+                 interaction_cutoff: float = 0.0, log_level: int = logging.INFO,
+                 log_file=None, solver: str = "default", observables: Sequence[Observable] = (),
+                 initial_state: StateVector | None = None, precision: str = "c128",
+                 krylov_dim_hint: bool = True, **kwargs):
+        if gpu is False:
+            raise ValueError("emulators_b200 runs on the GPU only (gpu=False is not supported)")
+        if precision not in ("c128", "c64"):
+            raise ValueError("precision must be 'c128' or 'c64'")
+        self.dt = dt
+        self.max_krylov_dim = max_krylov_dim
+        self.krylov_tolerance = krylov_tolerance
+        self.gpu = gpu
+        self.interaction_cutoff = interaction_cutoff
+        self.log_level = log_level
+        self.log_file = log_file
+        self.solver = solver
+        self.observables = tuple(observables)
+        self.initial_state = initial_state
+        self.precision = precision
+        self.krylov_dim_hint = krylov_dim_hint
+        self._backend_options = dict(kwargs)
+
+    @property
+    def vector_dtype(self) -> torch.dtype:
+        return torch.complex128 if self.precision == "c128" else torch.complex64
+
+
+@dataclasses.dataclass
+class SequenceData:
+    """emu_base/pulser_adapter.py:259-280: midpoint samples [nsteps, N] (rad/us), the
+    target-time grid in ns, and U(t) (a callable returning [1, N, N] like the adapter's
+    _InteractionMatrixCallable, or a fixed [N, N] tensor)."""
+
+    omega: torch.Tensor
+    delta: torch.Tensor
+    phi: torch.Tensor
+    target_times: list
+    interaction_matrix: Callable | torch.Tensor
+    qubit_ids: tuple = ()
+    lindblad_ops: list = dataclasses.field(default_factory=list)
+
+    def U(self, t: float) -> torch.Tensor:
+        if callable(self.interaction_matrix):
+            return self.interaction_matrix(t)[0]
+        return self.interaction_matrix
+
+    @classmethod
+    def from_workload(cls, w) -> "SequenceData":
+        times = list(np.round(np.arange(w.nsteps + 1) * w.dt * 1000.0, 9))
+        return cls(torch.as_tensor(w.omega), torch.as_tensor(w.delta), torch.as_tensor(w.phi),
+                   times, torch.as_tensor(w.U), tuple(f"q{i}" for i in range(w.nqubits)))
+
+
+# ---------------------------------------------------------------- time loop
+class SVBackendImpl:
+    """sv_backend_impl.py:74-262 for the noiseless state-vector stepper."""
+
+    def __init__(self, config: SVConfig, data: SequenceData):
+        if data.lindblad_ops:
+            raise NotImplementedError("emulators_b200: Lindblad noise is not implemented")
+        from . import krylov
+
+        krylov.use_iteration_hint = bool(config.krylov_dim_hint)
+        self._config = config
+        self._data = data
+        self.stepper = EvolveStateVector(config.max_krylov_dim)
+        self.target_times = data.target_times
+        self.omega, self.delta, self.phi = data.omega, data.delta, data.phi
+        self.nsteps = data.omega.shape[0]
+        self.nqubits = data.omega.shape[1]
+        if config.initial_state is not None:
+            if config.initial_state.n_qudits != self.nqubits:
+                raise ValueError(
+                    "Mismatch in number of atoms: initial state has "
+                    f"{config.initial_state.n_qudits} and the sequence has {self.nqubits}")
+            self.state = StateVector(config.initial_state.data.clone().to(config.vector_dtype))
+        else:
+            self.state = StateVector.make(self.nqubits, dtype=config.vector_dtype)
+        self.results = Results(data.qubit_ids, int(self.target_times[-1]))
+        self._current_H: RydbergHamiltonian | None = None
+        self.time = time.time()
+
+    def _dt_frac(self) -> float:
+        return (self.target_times[1] - self.target_times[0]) / self.target_times[-1]
+
+    def step(self, step_idx: int) -> None:
+        dt = self.target_times[step_idx + 1] - self.target_times[step_idx]
+        self._current_H = None
+        self.state.data, self._current_H = self.stepper.apply(
+            dt * _TIME_CONVERSION_COEFF, self.omega[step_idx], self.delta[step_idx],
+            self.phi[step_idx], self._data.U(self.target_times[step_idx]), self.state.data,
+            self._config.krylov_tolerance, self._data.lindblad_ops)
+        self._apply_observables(step_idx + 1)
+        self.results.statistics.append({"step": step_idx + 1, "duration": time.time() - self.time})
+        self.time = time.time()
+
+    def _apply_observables(self, step_idx: int) -> None:
+        """sv_backend_impl.py:211-242: renormalised state, H of the step just done."""
+        t = self.target_times[step_idx] / self.target_times[-1]
+        due = [o for o in self._config.observables if o.due(t, self._dt_frac())]
+        if not due:
+            return
+        norm = self.state.norm()
+        if not torch.allclose(norm, torch.tensor(1.0, dtype=torch.float64)):
+            state = StateVector((1.0 / norm.item()) * self.state.data)
+        else:
+            state = self.state
+        if self._current_H is None:  # t = 0 (sv_backend_impl.py:224-234)
+            self._current_H = self.stepper.get_hamiltonian(
+                self.omega[0], self.delta[0], self.phi[0], [], self._data.U(
+                    0.5 * (self.target_times[step_idx] + self.target_times[step_idx + 1])),
+                state.data.device)
+        for o in due:
+            self.results._store(o.name, t, o.apply(config=self._config, state=state,
+                                                   hamiltonian=self._current_H))
+
+    def _run(self) -> Results:
+        self._apply_observables(0)
+        for step in range(self.nsteps):
+            self.step(step)
+        return self.results
+
+
+class SVBackend:
+    """sv_backend.py:7-42 without pulser: ``SVBackend(sequence_data, config).run()``."""
+
+    def __init__(self, sequence: SequenceData | Sequence[SequenceData], config: SVConfig | None = None):
+        self._sequences = [sequence] if isinstance(sequence, SequenceData) else list(sequence)
+        self._config = config or SVConfig(observables=[BitStrings(evaluation_times=[1.0])])
+
+    def run(self) -> Results | list[Results]:
+        out = [SVBackendImpl(self._config, s)._run() for s in self._sequences]
+        return out[0] if len(out) == 1 else out

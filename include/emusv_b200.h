@@ -1,0 +1,152 @@
+/*
+ * emusv_b200 -- C ABI of the B200-native emu-sv time-evolution hot path.
+ *
+ * Every entry point takes plain pointers and sizes, runs on the CUDA stream passed as
+ * `stream` (a cudaStream_t; NULL = legacy default stream), and returns an emusv_status.
+ * Vectors are device pointers to interleaved complex amplitudes of length 2^nqubits:
+ * complex128 (double re, im) for EMUSV_C128 and complex64 (float re, im) for EMUSV_C64.
+ * Qubit 0 is the most significant bit of the amplitude index; bit value 1 is the Rydberg
+ * state |r> (reference emu_sv/state_vector.py, emu_sv/hamiltonian.py).
+ *
+ * Hamiltonian parameters are HOST pointers:
+ *   omegas[n]      Rabi frequencies Omega_i (rad/us; halved inside, hamiltonian.py:52)
+ *   deltas[n]      detunings delta_i (rad/us)
+ *   phis[n]        laser phases phi_i (rad)
+ *   interaction[n*n] row-major U_ij (rad/us); only the upper triangle i<j is read
+ *                  (hamiltonian.py:153-161).
+ *   H = sum_i Omega_i/2 (cos phi_i X_i + sin phi_i Y_i) - sum_i delta_i n_i
+ *       + sum_{i<j} U_ij n_i n_j
+ *
+ * Workspace-taking calls use only the memory they are given; none of them allocates.
+ */
+#ifndef EMUSV_B200_H
+#define EMUSV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMUSV_MAX_QUBITS 30
+
+typedef enum {
+    EMUSV_OK = 0,
+    EMUSV_NOT_CONVERGED = 1,      /* Krylov iteration reached max_krylov_dim (RecursionError) */
+    EMUSV_NONFINITE = 2,          /* NaN/Inf met in a reduction */
+    EMUSV_BAD_ARGUMENT = 3,       /* size, pointer or alignment check failed */
+    EMUSV_WORKSPACE_TOO_SMALL = 4, /* the Krylov basis needs more vectors than given */
+    EMUSV_CUDA_ERROR = 5,         /* a CUDA runtime call failed */
+    EMUSV_TIMEOUT = 6             /* a bounded device-side wait gave up */
+} emusv_status;
+
+typedef enum { EMUSV_C128 = 0, EMUSV_C64 = 1 } emusv_dtype;
+
+/* Per-call Krylov statistics (host struct, filled on return). */
+typedef struct {
+    int iterations;       /* Lanczos iterations j+1 at exit (krylov_exp.py:92-96) */
+    int happy_breakdown;  /* 1 if ||w|| < norm_tolerance ended the iteration */
+    int converged;        /* 1 if the error estimate fell below exp_tolerance */
+    int basis_vectors;    /* Krylov vectors combined into the result */
+    double error_estimate; /* last Expokit estimate (krylov_exp.py:81-84) */
+    double input_norm;    /* ||psi_in|| */
+    double output_norm;   /* ||psi_out|| (FP64 reduction fused into the combination) */
+} emusv_krylov_info;
+
+/* Library identification: returns the sm architecture compiled in (e.g. 100). */
+int emusv_build_arch(void);
+const char *emusv_status_string(int status);
+
+/* Diagonal of H, float64 [2^n] on the device.
+ * Replaces RydbergHamiltonian._create_diagonal (emu_sv/hamiltonian.py:139-162). */
+int emusv_hamiltonian_diag(int nqubits, const double *deltas, const double *interaction,
+                           double *diag_out, void *stream);
+
+/* out = H psi, fused in one pass (diagonal rebuilt on chip, all flip terms).
+ * Replaces RydbergHamiltonian.__mul__ (emu_sv/hamiltonian.py:69-137). out != psi. */
+int emusv_hpsi(int nqubits, int dtype, const double *omegas, const double *deltas,
+               const double *phis, const double *interaction, const void *psi, void *out,
+               void *stream);
+
+/* Bytes of device scratch the reduction entry points below need (FP64 partial sums). */
+size_t emusv_scratch_bytes(int nqubits, int dtype);
+
+/* result_dev[0..1] = <psi|H|psi> (re, im), result_dev[2] = <H psi|H psi>; device
+ * float64 [3], no vector store, no synchronisation.  Replaces RydbergHamiltonian.expect
+ * (hamiltonian.py:164-172) and the vdot(h, h) of energy_second_moment_sv_impl /
+ * energy_variance_sv_impl (emu_sv/custom_callback_implementations.py:131-185). */
+int emusv_expect(int nqubits, int dtype, const double *omegas, const double *deltas,
+                 const double *phis, const double *interaction, const void *psi,
+                 double *result_dev, void *scratch, size_t scratch_bytes, void *stream);
+
+/* occ_dev[i] = sum_x |psi_x|^2 x_i (device float64 [n]), one pass over psi.
+ * Replaces qubit_occupation_sv_impl (emu_sv/custom_callback_implementations.py:30-47). */
+int emusv_occupation(int nqubits, int dtype, const void *psi, double *occ_dev, void *scratch,
+                     size_t scratch_bytes, void *stream);
+
+/* corr_dev[i*n+j] = sum_x |psi_x|^2 x_i x_j (device float64 [n*n]), one pass over psi.
+ * Replaces correlation_matrix_sv_impl (custom_callback_implementations.py:77-102). */
+int emusv_correlation(int nqubits, int dtype, const void *psi, double *corr_dev, void *scratch,
+                      size_t scratch_bytes, void *stream);
+
+/* Bytes of device workspace emusv_krylov_step needs for a basis of `basis_capacity`
+ * stored Krylov vectors (the input vector is used in place and is not counted). */
+size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity);
+
+/* One time step psi_out = exp(-i dt H) psi_in by Lanczos with the Expokit error
+ * estimate, all arithmetic on the GPU (FP64 scalars and tridiagonal exponential).
+ * Replaces DifferentiableStateVectorEvolution.forward/evolve
+ * (emu_sv/time_evolution/torch.py:143-219) with krylov_exp
+ * (emu_base/math/krylov_exp.py:23-131) and RydbergHamiltonian.__mul__ as the operator.
+ * Convergence is tested from iteration `krylov_dim_hint` on (0: every iteration, as the
+ * reference does; a hint only ever adds iterations, never removes one).
+ * psi_out may equal psi_in.  Returns EMUSV_NOT_CONVERGED (result still written, as
+ * krylov_exp_impl does) or EMUSV_WORKSPACE_TOO_SMALL (nothing written; retry with a
+ * larger basis).  `info` (host) may be NULL.  Synchronises the stream at every
+ * convergence test. */
+int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
+                      const double *deltas, const double *phis, const double *interaction,
+                      const void *psi_in, void *psi_out, double exp_tolerance,
+                      double norm_tolerance, int max_krylov_dim, int krylov_dim_hint,
+                      void *workspace, size_t workspace_bytes, emusv_krylov_info *info,
+                      void *stream);
+
+/* ---- building blocks of the generic krylov_exp(op, v, ...) (krylov_exp.py:23-106) ----
+ * For an arbitrary operator applied by the caller, these give the FP64-accumulated
+ * Lanczos arithmetic and the on-device exponential of the extended Krylov matrix. */
+
+/* res_dev[0..1] (device float64) = <a, b> = sum conj(a) b.  scratch: emusv_scratch_bytes. */
+int emusv_vec_dot(int64_t len, int dtype, const void *a, const void *b, double *res_dev,
+                  void *scratch, size_t scratch_bytes, void *stream);
+/* y = y + alpha x  (alpha: host complex [2]) */
+int emusv_vec_axpy(int64_t len, int dtype, const double *alpha, const void *x, void *y,
+                   void *stream);
+/* out = sum_k coef[k] V[k]; V = k vectors of `len` amplitudes back to back; coef_dev is a
+ * device complex128 [k] array. */
+int emusv_vec_combine(int64_t len, int dtype, int k, const double *coef_dev, const void *V,
+                      void *out, void *stream);
+
+/* x_dev = exp(A) e_0 (device complex128 [m]) for a complex tridiagonal m x m matrix given
+ * by host complex arrays diag[m], upper[m] (upper[k] = A[k-1][k]) and lower[m]
+ * (lower[k] = A[k+1][k]); FP64 Taylor series with scaling, on the device.  Replaces the
+ * torch.linalg.matrix_exp of krylov_exp.py:66,78.  Synchronises the stream. */
+size_t emusv_tridiag_scratch_bytes(void);
+int emusv_tridiag_expm_col(int m, const double *diag, const double *upper, const double *lower,
+                           double *x_dev, void *scratch, size_t scratch_bytes, void *stream);
+
+/* ---- launch accounting (no reference counterpart: measurement support) ----
+ * emusv_profile_begin resets the per-kind launch counters; with event_timing != 0 every
+ * later launch is bracketed by CUDA events on its stream.  emusv_profile_end waits for
+ * those events and returns, per kind, the summed device milliseconds and the launch
+ * count.  Kinds: 0 H*psi, 1 orthogonalisation/axpy/norm passes, 2 small FP64 kernels,
+ * 3 basis combination, 4 observables, 5 adjoint contractions, 6 batched evolution. */
+#define EMUSV_PROFILE_KINDS 8
+void emusv_profile_begin(int event_timing);
+int emusv_profile_end(double *ms_by_kind, long long *launches_by_kind, int nkinds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMUSV_B200_H */

@@ -1,0 +1,509 @@
+"""Generate the golden fixtures under tests/golden/ by running the REFERENCE emu-sv code.
+
+This script is the only place that executes the reference implementation.  It runs in
+the build container where the reference checkout is readable (pass its path with
+``--reference``; default ``/root/reference``) and writes small ``.npz`` fixtures that the
+test suite reads on any machine.  Nothing else in the repository imports it.
+
+The reference's package ``__init__`` files pull in ``pulser``, which is not installed,
+so the four hot-path modules are loaded one by one behind package shells:
+
+* emu_base/math/krylov_exp.py       (krylov_exp_impl, krylov_exp)
+* emu_base/math/double_krylov.py    (double_krylov, lanczos)
+* emu_sv/hamiltonian.py             (RydbergHamiltonian)
+* emu_sv/time_evolution/torch.py    (DifferentiableStateVectorEvolution)
+* emu_sv/custom_callback_implementations.py (occupation / correlation / energy moments)
+
+``pulser.*`` and ``pyparsing`` imports are served by a meta-path finder that fabricates
+empty placeholder classes; none of them is called on the paths exercised here.
+``emu_sv.state_vector.StateVector`` is replaced by a minimal holder of ``.data`` (all the
+hot path reads from it).
+
+Fixtures (inputs and reference outputs, all complex128/float64):
+
+* hamiltonian.npz      H*psi and the diagonal: the reference's own test cases
+                       (test/emu_sv/test_hamiltonian.py:20-85) plus larger registers.
+* krylov_step.npz      one time step (test/emu_sv/test_time_evolution.py:58-76 cases)
+                       with the reference's Krylov iteration counts.
+* backward.npz         gradients of Re<r|psi_out> (test_time_evolution.py:79-103 cases).
+* double_krylov.npz    Frechet derivative blocks (test/emu_base/math/test_double_krylov.py).
+* observables.npz      occupation, correlation, energy, variance, second moment.
+* chain_n10.npz        the N=10 chain workload, 100 steps, observables every 10 steps.
+* lattice_n20.npz      the N=20 lattice workload: occupations/energy every 10 steps,
+                       final-state probes (inner products with seeded vectors).
+* ring_n16_grad.npz    reference autograd gradient of the Neel loss for 2 parameter sets
+                       of the N=16 ring over the first 2 segments (20 steps).
+
+Usage:  python tests/golden/make_golden.py [--reference PATH] [--only NAME ...]
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib.abc
+import importlib.machinery
+import importlib.util
+import os
+import sys
+import time
+import types
+import typing
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+import torch  # noqa: E402
+
+from emulators_b200 import workloads as wl  # noqa: E402
+
+torch.set_default_dtype(torch.float64)
+
+
+# --------------------------------------------------------------------------- ref loader
+class _Placeholder:
+    """Generic stand-in for any pulser class (subscriptable, constructible)."""
+
+    def __init__(self, *a, **k):
+        pass
+
+    def __class_getitem__(cls, item):
+        return cls
+
+
+class _FakeModule(types.ModuleType):
+    def __getattr__(self, name):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        if name == "TIME_TOLERANCE":
+            return 1e-6
+        cls = type(name, (_Placeholder,), {})
+        setattr(self, name, cls)
+        return cls
+
+
+class _FakeFinder(importlib.abc.MetaPathFinder, importlib.abc.Loader):
+    prefixes = ("pulser", "pyparsing")
+
+    def find_spec(self, fullname, path, target=None):
+        if fullname.split(".")[0] in self.prefixes:
+            return importlib.machinery.ModuleSpec(fullname, self, is_package=True)
+        return None
+
+    def create_module(self, spec):
+        m = _FakeModule(spec.name)
+        m.__path__ = []
+        if spec.name == "pyparsing":
+            m.Any = typing.Any
+        return m
+
+    def exec_module(self, module):
+        pass
+
+
+class StateVector:
+    """Minimal replacement for emu_sv.state_vector.StateVector (holds ``data``)."""
+
+    def __init__(self, data, gpu=False, eigenstates=("r", "g")):
+        self.data = data
+
+    @property
+    def n_qudits(self):
+        return int(round(np.log2(self.data.shape[0])))
+
+
+def load_reference(ref: str) -> dict:
+    sys.meta_path.insert(0, _FakeFinder())
+    for pkg, sub in [("emu_base", "emu_base"), ("emu_base.math", "emu_base/math"),
+                     ("emu_sv", "emu_sv"), ("emu_sv.time_evolution", "emu_sv/time_evolution")]:
+        m = types.ModuleType(pkg)
+        m.__path__ = [os.path.join(ref, sub)]
+        sys.modules[pkg] = m
+    sv = types.ModuleType("emu_sv.state_vector")
+    sv.StateVector = StateVector
+    sys.modules["emu_sv.state_vector"] = sv
+    for name in ["emu_sv.density_matrix_state", "emu_sv.dense_operator",
+                 "emu_sv.lindblad_operator"]:
+        m = _FakeModule(name)
+        sys.modules[name] = m
+
+    def load(name, rel):
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ref, rel))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+        return mod
+
+    mods = {
+        "krylov": load("emu_base.math.krylov_exp", "emu_base/math/krylov_exp.py"),
+        "double": load("emu_base.math.double_krylov", "emu_base/math/double_krylov.py"),
+        "ham": load("emu_sv.hamiltonian", "emu_sv/hamiltonian.py"),
+    }
+    mods["torch"] = load("emu_sv.time_evolution.torch", "emu_sv/time_evolution/torch.py")
+    mods["cb"] = load("emu_sv.custom_callback_implementations",
+                      "emu_sv/custom_callback_implementations.py")
+    return mods
+
+
+# --------------------------------------------------------------------------- helpers
+def nn_interaction_matrix(n):
+    u = torch.zeros(n, n)
+    for i in range(n - 1):
+        u[i, i + 1] = u[i + 1, i] = 1.0
+    return u
+
+
+def randn_interaction_matrix(n):
+    u = torch.zeros(n, n)
+    for i in range(n):
+        for j in range(i + 1, n):
+            t = torch.rand(1)
+            u[i, j] = u[j, i] = t
+    return u
+
+
+def dense_h(omegas, deltas, phis, U):
+    """Kronecker-product dense Hamiltonian (same operator as the reference's
+    test/utils_testing/utils_dense_hamiltonians.py:37-67), for the dense oracle."""
+    n = U.shape[0]
+    c = torch.complex128
+    sx = torch.tensor([[0, 1], [1, 0]], dtype=c)
+    sy = torch.tensor([[0, -1j], [1j, 0]], dtype=c)
+    pn = torch.tensor([[0, 0], [0, 1]], dtype=c)
+    eye = torch.eye(2, dtype=c)
+
+    def op(ops):
+        m = torch.ones(1, 1, dtype=c)
+        for o in ops:
+            m = torch.kron(m, o)
+        return m
+
+    h = torch.zeros(2**n, 2**n, dtype=c)
+    for i in range(n):
+        base = [eye] * n
+        b = list(base); b[i] = sx
+        h = h + omegas[i] * torch.cos(phis[i]) * op(b) / 2
+        b = list(base); b[i] = sy
+        h = h + omegas[i] * torch.sin(phis[i]) * op(b) / 2
+        b = list(base); b[i] = pn
+        h = h - deltas[i] * op(b)
+        for j in range(i + 1, n):
+            b = list(base); b[i] = pn; b[j] = pn
+            h = h + U[i, j] * op(b)
+    return h
+
+
+def np_(t):
+    t = t.detach()
+    return t.cpu().numpy()
+
+
+# --------------------------------------------------------------------------- generators
+def gen_hamiltonian(R):
+    Ham = R["ham"].RydbergHamiltonian
+    cases = []
+    for n in [3, 5, 7, 8]:  # test_hamiltonian.py:20-49
+        torch.manual_seed(1337)
+        om, de, ph = torch.randn(n), torch.randn(n), torch.zeros(n)
+        cases.append((n, om, de, ph, nn_interaction_matrix(n), "nophase"))
+    for n in [2, 4, 7, 9]:  # test_hamiltonian.py:52-85
+        torch.manual_seed(1337)
+        om, de, ph = torch.randn(n), torch.randn(n), torch.randn(n)
+        cases.append((n, om, de, ph, randn_interaction_matrix(n), "phase"))
+    g = torch.Generator().manual_seed(7)
+    for n, phase in [(10, False), (10, True), (12, False), (13, True)]:
+        om = torch.rand(n, generator=g) * 2 * np.pi
+        de = torch.randn(n, generator=g) * 10
+        ph = torch.randn(n, generator=g) if phase else torch.zeros(n)
+        U = torch.as_tensor(wl.interaction_matrix(wl.chain(n, 5.0 + 0.5 * torch.rand(1, generator=g).item())))
+        cases.append((n, om, de, ph, U, "phase" if phase else "nophase"))
+    # complex128 parameter tensors, as the pulser adapter passes them
+    n = 6
+    om = (torch.rand(n, generator=g) * 4).to(torch.complex128)
+    de = torch.randn(n, generator=g).to(torch.complex128)
+    ph = torch.zeros(n, dtype=torch.complex128)
+    cases.append((n, om, de, ph, torch.as_tensor(wl.interaction_matrix(wl.ring(n, 6.0))), "complexparams"))
+
+    out = {}
+    for k, (n, om, de, ph, U, tag) in enumerate(cases):
+        torch.manual_seed(1000 + k)
+        state = torch.randn(2**n, dtype=torch.complex128)
+        H = Ham(omegas=om, deltas=de, phis=ph, interaction_matrix=U, device="cpu", noise=None)
+        hpsi = H * state
+        if n <= 9:
+            hd = dense_h(om.real if om.is_complex() else om, de.real if de.is_complex() else de,
+                         ph.real if ph.is_complex() else ph, U)
+            assert torch.allclose(hd @ state, hpsi, atol=1e-10)
+        pre = f"c{k}_"
+        out[pre + "n"] = np.array(n)
+        out[pre + "tag"] = np.array(tag)
+        out[pre + "omegas"] = np_(om)
+        out[pre + "deltas"] = np_(de)
+        out[pre + "phis"] = np_(ph)
+        out[pre + "U"] = np_(U)
+        out[pre + "state"] = np_(state)
+        out[pre + "diag"] = np_(H.diag)
+        out[pre + "hpsi"] = np_(hpsi)
+        out[pre + "complex"] = np.array(bool(H.complex))
+    out["count"] = np.array(len(cases))
+    return out
+
+
+def get_randn_ham_params(n, with_phase):
+    om, de = torch.randn(n), torch.randn(n)
+    ph = torch.randn(n) if with_phase else torch.zeros(n)
+    return om, de, ph, randn_interaction_matrix(n)
+
+
+def gen_krylov_step(R):
+    DSE = R["torch"].DifferentiableStateVectorEvolution
+    Ham = R["ham"].RydbergHamiltonian
+    kimpl = R["krylov"].krylov_exp_impl
+    out, k = {}, 0
+    for n in [3, 5, 8]:  # test_time_evolution.py:58-76
+        for tol in [1e-8, 1e-10, 1e-12]:
+            for wp in [False, True]:
+                torch.manual_seed(1337)
+                p = get_randn_ham_params(n, wp)
+                s = torch.randn(2**n, dtype=torch.complex128)
+                s = s / s.norm()
+                dt = 1.0
+                expected = torch.linalg.matrix_exp(-1j * dt * dense_h(*p)) @ s
+                res, _ = DSE.apply(dt, *p, s.clone(), tol, 100)
+                H = Ham(*p, device="cpu", noise=None)
+                kr = kimpl(lambda x: -1j * dt * (H * x), s.clone(), True, tol, tol, 100)
+                pre = f"c{k}_"
+                for nm, v in zip(["omegas", "deltas", "phis", "U"], p):
+                    out[pre + nm] = np_(v)
+                out[pre + "n"] = np.array(n)
+                out[pre + "tol"] = np.array(tol)
+                out[pre + "dt"] = np.array(dt)
+                out[pre + "state"] = np_(s)
+                out[pre + "result"] = np_(res)
+                out[pre + "dense"] = np_(expected)
+                out[pre + "iters"] = np.array(kr.iteration_count)
+                out[pre + "happy"] = np.array(kr.happy_breakdown)
+                k += 1
+    # a few physical steps: the chain_n10 drive at its first midpoint, several dt
+    w = wl.chain_n10()
+    for dt in [0.005, 0.01, 0.02]:
+        p = [torch.as_tensor(w.omega[0]), torch.as_tensor(w.delta[0]),
+             torch.as_tensor(w.phi[0]), torch.as_tensor(w.U)]
+        torch.manual_seed(42)
+        s = torch.randn(2**w.nqubits, dtype=torch.complex128)
+        s = s / s.norm()
+        res, _ = DSE.apply(dt, *p, s.clone(), 1e-10, 100)
+        H = Ham(*p, device="cpu", noise=None)
+        kr = kimpl(lambda x: -1j * dt * (H * x), s.clone(), True, 1e-10, 1e-10, 100)
+        pre = f"c{k}_"
+        for nm, v in zip(["omegas", "deltas", "phis", "U"], p):
+            out[pre + nm] = np_(v)
+        out[pre + "n"] = np.array(w.nqubits)
+        out[pre + "tol"] = np.array(1e-10)
+        out[pre + "dt"] = np.array(dt)
+        out[pre + "state"] = np_(s)
+        out[pre + "result"] = np_(res)
+        out[pre + "dense"] = np_(res)
+        out[pre + "iters"] = np.array(kr.iteration_count)
+        out[pre + "happy"] = np.array(kr.happy_breakdown)
+        k += 1
+    out["count"] = np.array(k)
+    return out
+
+
+def gen_backward(R):
+    DSE = R["torch"].DifferentiableStateVectorEvolution
+    out, k = {}, 0
+    for n in [3, 5, 8]:  # test_time_evolution.py:79-103
+        for tol in [1e-8, 1e-10, 1e-12]:
+            torch.manual_seed(1337)
+            om, de, ph = torch.randn(n), torch.randn(n), torch.randn(n)
+            U = randn_interaction_matrix(n)
+            s = torch.randn(2**n, dtype=torch.complex128)
+            s = s / s.norm()
+            params = [x.clone().requires_grad_(True) for x in (om, de, ph, U)]
+            s_in = s.clone().requires_grad_(True)
+            dt = 1.0
+            r = torch.randn(2**n, dtype=torch.complex128)
+            r = r * (0.71 / r.norm())
+            so, _ = DSE.apply(dt, *params, s_in, tol, 100)
+            scalar = torch.vdot(r, so).real
+            grads = torch.autograd.grad(scalar, (*params, s_in))
+            pre = f"c{k}_"
+            for nm, v in zip(["omegas", "deltas", "phis", "U", "state"], (om, de, ph, U, s)):
+                out[pre + nm] = np_(v)
+            out[pre + "r"] = np_(r)
+            out[pre + "n"] = np.array(n)
+            out[pre + "tol"] = np.array(tol)
+            out[pre + "dt"] = np.array(dt)
+            for nm, g in zip(["g_omegas", "g_deltas", "g_phis", "g_U", "g_state"], grads):
+                out[pre + nm] = np_(g)
+            k += 1
+    out["count"] = np.array(k)
+    return out
+
+
+def gen_double_krylov(R):
+    Ham = R["ham"].RydbergHamiltonian
+    dk = R["double"].double_krylov
+    out, k = {}, 0
+    for n in [3, 4, 5, 7]:  # test_double_krylov.py:31-87
+        for tol in [1e-8, 1e-10, 1e-12]:
+            torch.manual_seed(1337)
+            om, de, ph = torch.randn(n), torch.randn(n), torch.randn(n)
+            U = randn_interaction_matrix(n)
+            s = torch.randn(2**n, dtype=torch.complex128)
+            s = s / s.norm()
+            g = torch.randn(2**n, dtype=torch.complex128)
+            H = Ham(om, de, ph, U, device="cpu", noise=None)
+            Vs, dS, Vg = dk(lambda x: -1j * 1.0 * (H * x), s, g, tol, 100)
+            dU = torch.stack(Vs).mT @ dS @ torch.stack(Vg).conj()
+            pre = f"c{k}_"
+            for nm, v in zip(["omegas", "deltas", "phis", "U", "state", "grad"], (om, de, ph, U, s, g)):
+                out[pre + nm] = np_(v)
+            out[pre + "n"] = np.array(n)
+            out[pre + "tol"] = np.array(tol)
+            out[pre + "dU"] = np_(dU)
+            out[pre + "len_s"] = np.array(len(Vs))
+            out[pre + "len_g"] = np.array(len(Vg))
+            k += 1
+    out["count"] = np.array(k)
+    return out
+
+
+def gen_observables(R):
+    cb = R["cb"]
+    Ham = R["ham"].RydbergHamiltonian
+    out, k = {}, 0
+    g = torch.Generator().manual_seed(99)
+    for n in [1, 2, 3, 5, 8, 11]:
+        s = torch.randn(2**n, dtype=torch.complex128, generator=g)
+        s = s / s.norm()
+        om = torch.rand(n, generator=g) * 5
+        de = torch.randn(n, generator=g) * 5
+        ph = torch.randn(n, generator=g) if n % 2 else torch.zeros(n)
+        U = randn_interaction_matrix(n) * 10
+        H = Ham(om, de, ph, U, device="cpu", noise=None)
+        st = StateVector(s)
+        pre = f"c{k}_"
+        out[pre + "n"] = np.array(n)
+        out[pre + "state"] = np_(s)
+        for nm, v in zip(["omegas", "deltas", "phis", "U"], (om, de, ph, U)):
+            out[pre + nm] = np_(v)
+        out[pre + "occupation"] = np_(cb.qubit_occupation_sv_impl(None, config=None, state=st, hamiltonian=None))
+        out[pre + "correlation"] = np_(cb.correlation_matrix_sv_impl(None, config=None, state=st, hamiltonian=None))
+        out[pre + "energy"] = np_(H.expect(st))
+        out[pre + "variance"] = np_(cb.energy_variance_sv_impl(None, config=None, state=st, hamiltonian=H))
+        out[pre + "second_moment"] = np_(cb.energy_second_moment_sv_impl(None, config=None, state=st, hamiltonian=H))
+        k += 1
+    out["count"] = np.array(k)
+    return out
+
+
+def run_reference(R, w: wl.Workload, probes: int = 0, store_final: bool = True):
+    """Step the reference chain exactly as SVBackendImpl does (sv_backend_impl.py:186-242):
+    one DifferentiableStateVectorEvolution.apply per step with that step's midpoint
+    samples; observables on the (renormalised) state with the H of the step just done."""
+    DSE = R["torch"].DifferentiableStateVectorEvolution
+    cb = R["cb"]
+    n = w.nqubits
+    U = torch.as_tensor(w.U)
+    s = torch.zeros(2**n, dtype=torch.complex128)
+    s[0] = 1.0
+    occ, en, steps_at, iters = [], [], [], []
+    t0 = time.time()
+    for k in range(w.nsteps):
+        om, de, ph = (torch.as_tensor(a[k]).to(torch.complex128) for a in (w.omega, w.delta, w.phi))
+        s, H = DSE.apply(w.dt, om, de, ph, U, s, w.tolerance, w.max_krylov_dim)
+        if (w.obs_every and (k + 1) % w.obs_every == 0) or k + 1 == w.nsteps:
+            nrm = torch.linalg.vector_norm(s)
+            st = StateVector(s / nrm if not torch.allclose(nrm, torch.tensor(1.0)) else s)
+            occ.append(np_(cb.qubit_occupation_sv_impl(None, config=None, state=st, hamiltonian=None)))
+            en.append(float(H.expect(st)))
+            steps_at.append(k + 1)
+    out = {"occupation": np.array(occ), "energy": np.array(en), "steps_at": np.array(steps_at),
+           "seconds": np.array(time.time() - t0)}
+    if store_final:
+        out["final"] = np_(s)
+    if probes:
+        g = torch.Generator().manual_seed(123)
+        P = torch.randn(probes, 2**n, dtype=torch.complex128, generator=g)
+        out["probe_overlaps"] = np_(P.conj() @ s)
+        out["final_norm"] = np.array(float(torch.linalg.vector_norm(s)))
+    return out
+
+
+def gen_chain_n10(R):
+    return run_reference(R, wl.chain_n10())
+
+
+def gen_lattice_n20(R):
+    return run_reference(R, wl.lattice_n20(), probes=4, store_final=False)
+
+
+def gen_ring_n16_grad(R):
+    """Reference autograd through the per-step autograd.Function for the first 2 segments
+    (20 steps) of 2 parameter sets of the N=16 ring workload."""
+    DSE = R["torch"].DifferentiableStateVectorEvolution
+    g = wl.ring_n16_grad()
+    n = g.nqubits
+    nseg, sets = 2, 2
+    U = torch.as_tensor(g.U)
+    out = {}
+    for p in range(sets):
+        om = torch.as_tensor(g.omega_seg[p, :nseg]).clone().requires_grad_(True)
+        de = torch.as_tensor(g.delta_seg[p, :nseg]).clone().requires_grad_(True)
+        s = torch.zeros(2**n, dtype=torch.complex128)
+        s[0] = 1.0
+        for seg in range(nseg):
+            for _ in range(g.steps_per_segment):
+                oms = om[seg].expand(n)
+                des = de[seg].expand(n)
+                s, _ = DSE.apply(g.dt, oms, des, torch.zeros(n), U, s, g.tolerance, 100)
+        occ = torch.stack([torch.linalg.vector_norm(s.view(2**i, 2, -1)[:, 1]) ** 2 for i in range(n)])
+        loss = torch.mean((occ - torch.as_tensor(g.target)) ** 2)
+        go, gd = torch.autograd.grad(loss, (om, de))
+        out[f"p{p}_omega"] = np_(om)
+        out[f"p{p}_delta"] = np_(de)
+        out[f"p{p}_loss"] = np.array(float(loss))
+        out[f"p{p}_g_omega"] = np_(go)
+        out[f"p{p}_g_delta"] = np_(gd)
+        out[f"p{p}_occupation"] = np_(occ)
+    out["nseg"] = np.array(nseg)
+    out["sets"] = np.array(sets)
+    return out
+
+
+GENERATORS = {
+    "hamiltonian": gen_hamiltonian,
+    "krylov_step": gen_krylov_step,
+    "backward": gen_backward,
+    "double_krylov": gen_double_krylov,
+    "observables": gen_observables,
+    "chain_n10": gen_chain_n10,
+    "lattice_n20": gen_lattice_n20,
+    "ring_n16_grad": gen_ring_n16_grad,
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", nargs="*", default=None)
+    ap.add_argument("--threads", type=int, default=os.cpu_count())
+    a = ap.parse_args()
+    torch.set_num_threads(a.threads)
+    R = load_reference(a.reference)
+    for name, fn in GENERATORS.items():
+        if a.only and name not in a.only:
+            continue
+        t = time.time()
+        data = fn(R)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+        print(f"{name}: {len(data)} arrays, {time.time() - t:.1f}s", flush=True)
+
+
+if __name__ == "__main__":
+    main()

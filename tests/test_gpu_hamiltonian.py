@@ -1,0 +1,108 @@
+"""GPU parity of the fused H*psi, diagonal and observables against the reference fixtures
+and the oracle (tolerances written per test)."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import cases, golden
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda"
+
+
+def _ham(c):
+    from emulators_b200 import RydbergHamiltonian
+
+    return RydbergHamiltonian(torch.as_tensor(c["omegas"]), torch.as_tensor(c["deltas"]),
+                              torch.as_tensor(c["phis"]), torch.as_tensor(c["U"]), DEV)
+
+
+def test_hpsi_c128_matches_reference_fixtures():
+    # reference test_hamiltonian.py uses atol=1e-12 on O(1) values; scale for large |H psi|
+    for c in cases(golden("hamiltonian")):
+        H = _ham(c)
+        assert H.complex == bool(c["complex"])
+        psi = torch.as_tensor(c["state"]).to(DEV)
+        out = (H * psi).cpu().numpy()
+        tol = 1e-12 * max(1.0, np.abs(c["hpsi"]).max())
+        np.testing.assert_allclose(out, c["hpsi"], atol=tol, rtol=0)
+        np.testing.assert_allclose(H.diag.cpu().numpy(), c["diag"], atol=1e-12 * max(1, np.abs(c["diag"]).max()), rtol=0)
+
+
+def test_hpsi_c64_matches_reference_fixtures():
+    # complex64 storage: relative error bound 1e-6 of the largest amplitude
+    for c in cases(golden("hamiltonian")):
+        H = _ham(c)
+        psi = torch.as_tensor(c["state"]).to(DEV, torch.complex64)
+        out = (H * psi).cpu().numpy()
+        np.testing.assert_allclose(out, c["hpsi"], atol=1e-6 * np.abs(c["hpsi"]).max(), rtol=0)
+
+
+@pytest.mark.parametrize("n,phase,dtype", [(14, False, torch.complex128), (16, True, torch.complex128),
+                                           (18, False, torch.complex64), (20, True, torch.complex128),
+                                           (21, False, torch.complex64)])
+def test_hpsi_large_registers_vs_oracle(oracle, n, phase, dtype):
+    """Registers whose high bits take the global-partner path (tile bits < n)."""
+    from emulators_b200 import RydbergHamiltonian
+    from emulators_b200 import workloads as wl
+
+    rng = np.random.default_rng(n)
+    om = rng.uniform(0, 2 * np.pi, n)
+    de = rng.uniform(-20, 20, n)
+    ph = rng.normal(size=n) if phase else np.zeros(n)
+    U = wl.interaction_matrix(wl.square_lattice(2, n // 2, 5.5) if n % 2 == 0 else wl.chain(n, 5.0))
+    psi = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)) / np.sqrt(2 << n)
+    ref = oracle.Hamiltonian(om, de, ph, U).apply(psi)
+    H = RydbergHamiltonian(torch.as_tensor(om), torch.as_tensor(de), torch.as_tensor(ph),
+                           torch.as_tensor(U), DEV)
+    out = (H * torch.as_tensor(psi).to(DEV, dtype)).cpu().numpy()
+    scale = np.abs(ref).max()
+    tol = 1e-13 if dtype == torch.complex128 else 1e-6
+    np.testing.assert_allclose(out, ref, atol=tol * scale, rtol=0)
+
+
+def test_observables_match_reference_fixtures():
+    from emulators_b200 import StateVector
+    from emulators_b200.observables import (correlation_matrix_sv_impl,
+                                            energy_second_moment_sv_impl, energy_variance_sv_impl,
+                                            qubit_occupation_sv_impl)
+
+    for c in cases(golden("observables")):
+        st = StateVector(torch.as_tensor(c["state"]))
+        H = _ham(c)
+        np.testing.assert_allclose(qubit_occupation_sv_impl(state=st).numpy(), c["occupation"], atol=1e-14)
+        np.testing.assert_allclose(correlation_matrix_sv_impl(state=st).numpy(), c["correlation"], atol=1e-14)
+        assert abs(H.expect(st).item() - float(c["energy"])) < 1e-12
+        assert abs(energy_variance_sv_impl(state=st, hamiltonian=H).item() - float(c["variance"])) < 1e-10
+        assert abs(energy_second_moment_sv_impl(state=st, hamiltonian=H).item()
+                   - float(c["second_moment"])) < 1e-10
+
+
+@pytest.mark.parametrize("n,dtype", [(12, torch.complex128), (19, torch.complex64), (22, torch.complex128)])
+def test_occupation_correlation_vs_oracle(oracle, n, dtype):
+    rng = np.random.default_rng(100 + n)
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi /= np.linalg.norm(psi)
+    from emulators_b200.observables import correlation, occupation
+
+    t = torch.as_tensor(psi).to(DEV, dtype)
+    ref_psi = t.cpu().to(torch.complex128).numpy()
+    tol = 1e-13 if dtype == torch.complex128 else 1e-12
+    np.testing.assert_allclose(occupation(t).cpu().numpy(), oracle.occupation(ref_psi), atol=tol)
+    np.testing.assert_allclose(correlation(t).cpu().numpy(), oracle.correlation(ref_psi), atol=tol)
+
+
+def test_empty_and_edge_registers():
+    """1- and 2-qubit registers (a single tile smaller than a warp) and zero drives."""
+    from emulators_b200 import RydbergHamiltonian
+
+    H = RydbergHamiltonian(torch.tensor([2.0]), torch.tensor([1.0]), torch.tensor([0.0]),
+                           torch.zeros(1, 1), DEV)
+    psi = torch.tensor([1.0, 2.0j], dtype=torch.complex128, device=DEV)
+    # H = X - n : [[0,1],[1,-1]]
+    np.testing.assert_allclose((H * psi).cpu().numpy(), [2.0j, 1.0 - 2.0j], atol=1e-15)
+    H0 = RydbergHamiltonian(torch.zeros(2), torch.zeros(2), torch.zeros(2), torch.zeros(2, 2), DEV)
+    psi = torch.randn(4, dtype=torch.complex128, device=DEV)
+    assert torch.count_nonzero(H0 * psi).item() == 0

@@ -1,0 +1,113 @@
+"""GPU parity of the Krylov time step against the reference fixtures and the oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import cases, golden
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+@pytest.fixture
+def no_hint():
+    """Test convergence at every iteration, exactly as the reference does."""
+    from emulators_b200 import krylov
+
+    old = krylov.use_iteration_hint
+    krylov.use_iteration_hint = False
+    yield
+    krylov.use_iteration_hint = old
+
+
+def _step(c, dtype=torch.complex128, tol=None):
+    from emulators_b200 import EvolveStateVector
+
+    tol = float(c["tol"]) if tol is None else tol
+    s = torch.as_tensor(c["state"]).to(DEV, dtype)
+    out, H = EvolveStateVector().apply(float(c["dt"]), torch.as_tensor(c["omegas"]),
+                                       torch.as_tensor(c["deltas"]), torch.as_tensor(c["phis"]),
+                                       torch.as_tensor(c["U"]), s, tol, None)
+    return out.cpu().to(torch.complex128).numpy()
+
+
+def test_step_matches_reference_fixtures(no_hint):
+    # reference test_time_evolution.py:58-76: atol = tolerance vs dense expm
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian, krylov_exp_impl
+
+    for c in cases(golden("krylov_step")):
+        out = _step(c)
+        np.testing.assert_allclose(out, c["dense"], atol=float(c["tol"]), rtol=0)
+        np.testing.assert_allclose(out, c["result"], atol=1e-12, rtol=0)
+        H = RydbergHamiltonian(*(torch.as_tensor(c[k]) for k in ("omegas", "deltas", "phis", "U")), DEV)
+        r = krylov_exp_impl(HamiltonianExpOperator(H, float(c["dt"])),
+                            torch.as_tensor(c["state"]).to(DEV), True, float(c["tol"]),
+                            float(c["tol"]), 100)
+        assert r.iteration_count == int(c["iters"])
+        assert r.happy_breakdown == bool(c["happy"])
+
+
+def test_step_c64_precision_form():
+    """complex64 vectors with FP64 scalars: error vs the complex128 reference ~1e-6."""
+    for c in cases(golden("krylov_step")):
+        out = _step(c, torch.complex64, tol=max(float(c["tol"]), 1e-10))
+        err = np.linalg.norm(out - c["result"])
+        assert err < 2e-6, err
+
+
+def test_chain_n10_run_matches_reference():
+    """Full 100-step N=10 run: final-state infidelity <= 1e-10 vs the reference."""
+    from emulators_b200 import workloads as wl
+    from emulators_b200.runner import run_workload
+
+    g = golden("chain_n10")
+    r = run_workload(wl.chain_n10())
+    ref = g["final"]
+    fid = abs(np.vdot(ref, r["final"])) ** 2 / (np.vdot(ref, ref).real * np.vdot(r["final"], r["final"]).real)
+    assert 1 - fid <= 1e-10
+    np.testing.assert_allclose(r["final"], ref, atol=1e-9, rtol=0)
+    np.testing.assert_allclose(r["occupation"], g["occupation"], atol=1e-9)
+    np.testing.assert_allclose(r["energy"], g["energy"], atol=1e-7)
+
+
+def test_lattice_n20_run_matches_reference():
+    """Full 300-step N=20 lattice run (Krylov dim <= 30) vs reference observables."""
+    from emulators_b200 import workloads as wl
+    from emulators_b200.runner import run_workload
+
+    g = golden("lattice_n20")
+    r = run_workload(wl.lattice_n20(), probes=len(g["probe_overlaps"]))
+    np.testing.assert_allclose(r["occupation"], g["occupation"], atol=1e-8)
+    np.testing.assert_allclose(r["energy"], g["energy"], atol=1e-6)
+    np.testing.assert_allclose(r["probe_overlaps"], g["probe_overlaps"], atol=1e-7)
+    assert abs(r["final_norm"] - float(g["final_norm"])) < 1e-9
+
+
+def test_not_converged_raises_recursion_error():
+    from emulators_b200 import EvolveStateVector
+
+    c = cases(golden("krylov_step"))[-1]
+    s = torch.as_tensor(c["state"]).to(DEV)
+    with pytest.raises(RecursionError):
+        EvolveStateVector(max_krylov_dim=3).apply(
+            float(c["dt"]), *(torch.as_tensor(c[k]) for k in ("omegas", "deltas", "phis", "U")),
+            s, 1e-12, None)
+
+
+def test_in_place_and_unitarity_large():
+    """N=22: the step is unitary to 1e-12 and forward(-dt) undoes forward(+dt)."""
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian
+    from emulators_b200 import workloads as wl
+    from emulators_b200.krylov import fused_step
+
+    n = 22
+    U = torch.as_tensor(wl.interaction_matrix(wl.ladder(11, 5.5)))
+    H = RydbergHamiltonian(torch.full((n,), 4.0), torch.full((n,), 3.0), torch.zeros(n), U, DEV)
+    g = torch.Generator(device=DEV).manual_seed(5)
+    psi = torch.randn(1 << n, dtype=torch.complex128, device=DEV, generator=g)
+    psi /= torch.linalg.vector_norm(psi)
+    out, info, st = fused_step(HamiltonianExpOperator(H, 0.005), psi, 1e-10, 1e-10, 100)
+    assert st == 0 and abs(info.output_norm - 1.0) < 1e-12
+    back, _, _ = fused_step(HamiltonianExpOperator(H, -0.005), out, 1e-10, 1e-10, 100)
+    assert torch.linalg.vector_norm(back - psi).item() < 1e-9
