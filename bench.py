@@ -44,6 +44,10 @@ def peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+def log(msg: str) -> None:
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi samples every 200 ms while the timed region runs."""
@@ -175,6 +179,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         dist.barrier()
     value = world * K / elapsed
     timed_iters = list(iters)
+    log(f"timed: {K} steps in {elapsed:.4f} s -> {value:.3f} steps/s, iterations {timed_iters}")
 
     # ---- profiled pass (not part of `value`): per-kernel device time by kind
     iters.clear()
@@ -194,6 +199,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     total_ms = pms.sum()
     kinds = ["hpsi", "orth", "small", "combine", "obs", "adjoint", "batch", "other"]
     shares = {kinds[i]: round(pms[i] / total_ms, 4) for i in range(8) if pl[i]}
+    log(f"profiled: ms by kind {pms.round(3).tolist()} launches {pl.tolist()}; "
+        f"hpsi {hpsi_avg_s * 1e3:.4f} ms/launch = {achieved:.1f} GB/s")
 
     # ---- H*psi alone (standalone launches, for the kernel roofline at both precisions)
     hstand = {}

@@ -1,5 +1,6 @@
 // C ABI: Hamiltonian diagonal, fused H*psi, energy moments, occupations, correlations.
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "hpsi_kernel.cuh"
@@ -87,9 +88,28 @@ static int launch_one(const HamParams &P, HpsiArgs A, int max_grid, cudaStream_t
     return EMUSV_OK;
 }
 
-// Dispatch on dtype / real coefficients / mode.
+int pass_min_qubits(int dtype);
+int launch_hpsi_passes(int dtype, int mode, const HamParams &H, const HpsiArgs &A,
+                       cudaStream_t s, int *grid_out);
+
+// EMUSV_HPSI_SINGLE_PASS=1 selects the single-pass tile kernel for every size (A/B checks).
+static bool single_pass_forced() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("EMUSV_HPSI_SINGLE_PASS");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v == 1;
+}
+
+// Dispatch on dtype / real coefficients / mode.  Registers of at least one pass-L tile
+// use the two-pass kernels for H*psi (store and Lanczos modes); the single-pass kernel
+// serves small registers, the energy reductions and the diagonal.
 int launch_hpsi(int dtype, int mode, const HamParams &P, HpsiArgs A, int max_grid,
                 cudaStream_t s, int *grid_out) {
+    if ((mode == HP_STORE || mode == HP_LANCZOS) && (dtype == EMUSV_C64 || dtype == EMUSV_C128) &&
+        P.n >= pass_min_qubits(dtype) && !single_pass_forced())
+        return launch_hpsi_passes(dtype, mode, P, A, s, grid_out);
 #define EMUSV_DISPATCH(R, M)                                                           \
     return P.real_coef ? launch_one<R, true, M>(P, A, max_grid, s, grid_out)           \
                        : launch_one<R, false, M>(P, A, max_grid, s, grid_out)

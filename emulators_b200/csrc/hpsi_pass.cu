@@ -1,0 +1,166 @@
+// Host side of the two-pass H*psi: layout choice, parameter tables, cluster launches.
+#include <string.h>
+
+#include "hpsi_kernel.cuh"
+#include "hpsi_pass.cuh"
+#include "profile.cuh"
+
+namespace emusv {
+
+// Tile shapes: 2^TB amplitudes per CTA (64 KiB of shared memory either way), 2^RB of them
+// in each thread's registers, 256 threads.
+template <typename R> struct PassShape;
+#ifndef PASS_RB64
+#define PASS_RB64 4
+#endif
+#ifndef PASS_RB128
+#define PASS_RB128 3
+#endif
+template <> struct PassShape<float> {
+    static constexpr int TB = 13, RB = PASS_RB64, PBMAX = 2, CMIN = 2;  // 32 B chunks in pass H
+};
+template <> struct PassShape<double> {
+    static constexpr int TB = 12, RB = PASS_RB128, PBMAX = 3, CMIN = 1;  // 32 B chunks in pass H
+};
+
+int pass_min_qubits(int dtype) {
+    return dtype == EMUSV_C64 ? PassShape<float>::TB : PassShape<double>::TB;
+}
+
+static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
+    memset(P, 0, sizeof(*P));
+    P->n = H.n;
+    P->real_coef = H.real_coef;
+    for (int p = 0; p < MAXQ; ++p) {
+        P->dup_re[p] = H.up_re[p];
+        P->dup_im[p] = H.up_im[p];
+        P->ddn_re[p] = H.dn_re[p];
+        P->ddn_im[p] = H.dn_im[p];
+        P->fup_re[p] = (float)H.up_re[p];
+        P->fup_im[p] = (float)H.up_im[p];
+        P->fdn_re[p] = (float)H.dn_re[p];
+        P->fdn_im[p] = (float)H.dn_im[p];
+        P->field[p] = H.field[p];
+    }
+    memcpy(P->U, H.U, sizeof(P->U));
+    const int SB = TB - RB;
+    for (int a = 0; a < (1 << RB); ++a) {  // fields and pairs of the register bits
+        double e = 0.0;
+        for (int k = 0; k < RB; ++k) {
+            if (!((a >> k) & 1)) continue;
+            e += H.field[SB + k];
+            for (int k2 = k + 1; k2 < RB; ++k2)
+                if ((a >> k2) & 1) e += H.U[(SB + k) * MAXQ + SB + k2];
+        }
+        P->ER[a] = e;
+    }
+    P->tb = TB;
+    P->rb = RB;
+}
+
+template <typename R, bool REALC, int EPI_L, int EPI_H>
+static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
+    typedef typename cvec<R>::T C;
+    constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
+    const int n = H.n;
+    PassParams P;
+    fill_params(H, TB, RB, &P);
+    int pb = n - TB;
+    if (pb > PassShape<R>::PBMAX) pb = PassShape<R>::PBMAX;
+    P.pb = pb;
+    const int rem = n - TB - pb;
+    int g = rem;
+    if (g > TB - PassShape<R>::CMIN) g = TB - PassShape<R>::CMIN;
+    P.hg = g;
+    P.hc = TB - g;
+    P.hpos = TB + pb;
+    P.xb_lo = TB + pb + g;
+    P.xb_hi = n;
+
+    PassArgs A = {};
+    A.u = HA.u;
+    A.su_dev = HA.su_dev;
+    A.su = HA.su;
+    A.up = HA.up;
+    A.sp_dev = HA.sp_dev;
+    A.sp = HA.sp;
+    A.out = HA.out;
+    A.partials = HA.partials;
+    A.gate = HA.gate;
+
+    const size_t smem = (sizeof(C) << TB) + 1024;
+    const int nsm = sm_count();
+    // ---- pass L
+    {
+        auto kern = (rem > 0) ? k_pass_low<R, REALC, TB, RB, EPI_L> : k_pass_low<R, REALC, TB, RB, EPI_H>;
+        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+        if (per_sm < 1) per_sm = 1;
+        const int CS = 1 << pb;
+        const int64_t ncta = int64_t(1) << (n - TB);
+        int64_t grid = (int64_t)nsm * per_sm;
+        if (grid > ncta) grid = ncta;
+        grid = grid / CS * CS;
+        if (grid < CS) grid = CS;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid, 1, 1);
+        cfg.blockDim = dim3(NT, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CS;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        {
+            ProfScope ps_(PROF_HPSI, s);
+            EMUSV_CHECK(cudaLaunchKernelEx(&cfg, kern, P, A));
+        }
+        if (rem == 0 && grid_out) *grid_out = (int)grid;
+    }
+    if (rem == 0) return EMUSV_OK;
+    // ---- pass H
+    {
+        auto kern = k_pass_high<R, REALC, TB, RB, EPI_H>;
+        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+        if (per_sm < 1) per_sm = 1;
+        const int64_t ntiles = int64_t(1) << (n - P.hc - P.hg);
+        int64_t grid = (int64_t)nsm * per_sm;
+        if (grid > ntiles) grid = ntiles;
+        {
+            ProfScope ps_(PROF_HPSI, s);
+            kern<<<(unsigned)grid, NT, smem, s>>>(P, A);
+        }
+        EMUSV_CHECK_LAUNCH();
+        if (grid_out) *grid_out = (int)grid;
+    }
+    return EMUSV_OK;
+}
+
+// mode: HP_STORE or HP_LANCZOS (values of HpsiMode)
+int launch_hpsi_passes(int dtype, int mode, const HamParams &H, const HpsiArgs &A,
+                       cudaStream_t s, int *grid_out) {
+    const bool lz = mode == HP_LANCZOS;
+    if (dtype == EMUSV_C64) {
+        if (H.real_coef)
+            return lz ? run_passes<float, true, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
+                      : run_passes<float, true, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
+        return lz ? run_passes<float, false, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
+                  : run_passes<float, false, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
+    }
+    if (dtype == EMUSV_C128) {
+        if (H.real_coef)
+            return lz ? run_passes<double, true, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
+                      : run_passes<double, true, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
+        return lz ? run_passes<double, false, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
+                  : run_passes<double, false, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
+    }
+    return EMUSV_BAD_ARGUMENT;
+}
+
+}  // namespace emusv

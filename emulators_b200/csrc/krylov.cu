@@ -283,7 +283,8 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
     for (int b = lane; b < nb_o; b += 32) v += part_o[(i64)b * NRED];
     v = warp_sum(v);
     const double r = sqrt(v);
-    const double n2 = dt * r;  // ||w|| of the operator -i dt H (krylov_exp.py:60)
+    const double adt = fabs(dt);
+    const double n2 = adt * r;  // ||w|| of the operator -i dt H (krylov_exp.py:60)
     if (!isfinite(r) || !isfinite(ks->hn[j]) || !isfinite(ks->a_re[j]) || !isfinite(ks->a_im[j]) ||
         !isfinite(ks->b_re[j]) || !isfinite(ks->b_im[j])) {
         if (lane == 0) {
@@ -325,7 +326,7 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
     const double2 x1 = make_double2(l.x * Z1.x - l.y * Z1.y, l.x * Z1.y + l.y * Z1.x);
     const double2 x2 = make_double2(l.x * Z2.x - l.y * Z2.y, l.x * Z2.y + l.y * Z2.x);
     const double err1 = hypot(x1.x, x1.y);                       // krylov_exp.py:81
-    const double err2 = hypot(x2.x, x2.y) * (dt * ks->hn[j]);   // krylov_exp.py:82
+    const double err2 = hypot(x2.x, x2.y) * (adt * ks->hn[j]);  // krylov_exp.py:82
     const double err = err1 < err2 ? err1 : (err1 * err2 / (err1 - err2));  // :84
     for (int k = lane; k < m; k += 32) {
         ks->c_re[k] = y[k + 1].x;

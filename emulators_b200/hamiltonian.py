@@ -92,7 +92,11 @@ class RydbergHamiltonian:
         assert isinstance(state, StateVector), \
             "Currently, only expectation values of StateVectors are supported"
         m = self._moments(state.data)
-        assert torch.allclose(m[1], torch.zeros_like(m[1]), atol=1e-8)
+        # H is Hermitian: the imaginary part is rounding only.  complex128 keeps the
+        # reference's absolute bound (hamiltonian.py:170-171); complex64 storage rounds
+        # H psi at ~6e-8 relative, so its bound scales with ||H psi||.
+        atol = 1e-8 if state.data.dtype == torch.complex128 else 1e-8 + 1e-6 * float(m[2].sqrt())
+        assert abs(float(m[1])) <= atol, f"imaginary energy {float(m[1])}"
         return m[0]
 
     def second_moment(self, state: StateVector) -> torch.Tensor:

@@ -40,11 +40,18 @@ def test_hpsi_c64_matches_reference_fixtures():
         np.testing.assert_allclose(out, c["hpsi"], atol=1e-6 * np.abs(c["hpsi"]).max(), rtol=0)
 
 
-@pytest.mark.parametrize("n,phase,dtype", [(14, False, torch.complex128), (16, True, torch.complex128),
-                                           (18, False, torch.complex64), (20, True, torch.complex128),
-                                           (21, False, torch.complex64)])
+C64, C128 = torch.complex64, torch.complex128
+
+
+@pytest.mark.parametrize("n,phase,dtype", [
+    # every layout of the two-pass kernel: single pass L with cluster sizes 1, 2, 4 (c64)
+    # and 1, 2, 4, 8 (c128), pass H with 1..11 group bits, and the global fallback bits
+    (12, True, C128), (13, False, C64), (13, True, C128), (14, True, C64), (14, False, C128),
+    (15, False, C64), (15, True, C128), (16, True, C64), (16, False, C128), (17, False, C64),
+    (18, True, C64), (20, True, C128), (21, False, C64), (23, True, C64), (24, False, C128),
+    (26, False, C64), (26, True, C128), (27, False, C128)])
 def test_hpsi_large_registers_vs_oracle(oracle, n, phase, dtype):
-    """Registers whose high bits take the global-partner path (tile bits < n)."""
+    """H*psi of every kernel layout against the oracle (c128: 1e-13, c64: 1e-6 relative)."""
     from emulators_b200 import RydbergHamiltonian
     from emulators_b200 import workloads as wl
 
