@@ -36,6 +36,7 @@ struct HpsiArgs {
     double *partials;  // [gridDim.x * NRED]
     int tile_bits;
     const int *gate;   // if non-null and *gate != 0 the kernel returns at once
+    void *part_buf;    // two-pass H*psi: buffer for the partial sum (null: in place in out)
 };
 
 struct SmemLayout {

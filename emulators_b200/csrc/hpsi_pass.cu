@@ -10,17 +10,14 @@ namespace emusv {
 // Tile shapes: 2^TB amplitudes per CTA (64 KiB of shared memory either way), 2^RB of them
 // in each thread's registers, 256 threads.
 template <typename R> struct PassShape;
-#ifndef PASS_RB64
-#define PASS_RB64 4
-#endif
-#ifndef PASS_RB128
-#define PASS_RB128 3
-#endif
+// c64: 4096-amplitude tiles (32 KiB), 16 amplitudes per thread; c128: 2048-amplitude
+// tiles (32 KiB), 8 per thread; 256 threads and two CTAs per SM either way.  Clusters of
+// up to 8 CTAs in pass L and pass H; pass H reads 32-byte chunks.
 template <> struct PassShape<float> {
-    static constexpr int TB = 13, RB = PASS_RB64, PBMAX = 2, CMIN = 2;  // 32 B chunks in pass H
+    static constexpr int TB = 12, RB = 4, PBMAX = 2, PBHMAX = 3, CMIN = 2;
 };
 template <> struct PassShape<double> {
-    static constexpr int TB = 12, RB = PASS_RB128, PBMAX = 3, CMIN = 1;  // 32 B chunks in pass H
+    static constexpr int TB = 11, RB = 3, PBMAX = 3, PBHMAX = 3, CMIN = 1;
 };
 
 int pass_min_qubits(int dtype) {
@@ -71,10 +68,13 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     const int rem = n - TB - pb;
     int g = rem;
     if (g > TB - PassShape<R>::CMIN) g = TB - PassShape<R>::CMIN;
+    int pbh = rem - g;
+    if (pbh > PassShape<R>::PBHMAX) pbh = PassShape<R>::PBHMAX;
     P.hg = g;
     P.hc = TB - g;
     P.hpos = TB + pb;
-    P.xb_lo = TB + pb + g;
+    P.pbh = pbh;
+    P.xb_lo = TB + pb + g + pbh;
     P.xb_hi = n;
 
     PassArgs A = {};
@@ -84,18 +84,19 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     A.up = HA.up;
     A.sp_dev = HA.sp_dev;
     A.sp = HA.sp;
-    A.out = HA.out;
+    A.out = rem > 0 && HA.part_buf ? HA.part_buf : HA.out;  // pass L output
+    A.part = nullptr;
     A.partials = HA.partials;
     A.gate = HA.gate;
 
-    const size_t smem = (sizeof(C) << TB) + 1024;
+    const size_t smem_l = pass_low_smem<C, TB>(), smem_h = pass_high_smem<C, TB>();
     const int nsm = sm_count();
     // ---- pass L
     {
         auto kern = (rem > 0) ? k_pass_low<R, REALC, TB, RB, EPI_L> : k_pass_low<R, REALC, TB, RB, EPI_H>;
-        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_l));
         int per_sm = 0;
-        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem_l));
         if (per_sm < 1) per_sm = 1;
         const int CS = 1 << pb;
         const int64_t ncta = int64_t(1) << (n - TB);
@@ -106,7 +107,7 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)grid, 1, 1);
         cfg.blockDim = dim3(NT, 1, 1);
-        cfg.dynamicSmemBytes = smem;
+        cfg.dynamicSmemBytes = smem_l;
         cfg.stream = s;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -122,21 +123,38 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
         if (rem == 0 && grid_out) *grid_out = (int)grid;
     }
     if (rem == 0) return EMUSV_OK;
-    // ---- pass H
+    // ---- pass H: partial from pass L's output, final into HA.out
+    A.part = A.out;
+    A.out = HA.out;
     {
-        auto kern = k_pass_high<R, REALC, TB, RB, EPI_H>;
-        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        auto kern = HA.part_buf ? k_pass_high<R, REALC, TB, RB, EPI_H, false>
+                                : k_pass_high<R, REALC, TB, RB, EPI_H, true>;
+        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_h));
         int per_sm = 0;
-        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem_h));
         if (per_sm < 1) per_sm = 1;
+        const int CS = 1 << pbh;
         const int64_t ntiles = int64_t(1) << (n - P.hc - P.hg);
         int64_t grid = (int64_t)nsm * per_sm;
         if (grid > ntiles) grid = ntiles;
+        grid = grid / CS * CS;
+        if (grid < CS) grid = CS;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid, 1, 1);
+        cfg.blockDim = dim3(NT, 1, 1);
+        cfg.dynamicSmemBytes = smem_h;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CS;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
         {
-            ProfScope ps_(PROF_HPSI, s);
-            kern<<<(unsigned)grid, NT, smem, s>>>(P, A);
+            ProfScope ps_(PROF_HPSI_HIGH, s);
+            EMUSV_CHECK(cudaLaunchKernelEx(&cfg, kern, P, A));
         }
-        EMUSV_CHECK_LAUNCH();
         if (grid_out) *grid_out = (int)grid;
     }
     return EMUSV_OK;

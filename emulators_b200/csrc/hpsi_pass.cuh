@@ -28,9 +28,6 @@ namespace emusv {
 
 namespace cg = cooperative_groups;
 
-#ifndef PASS_MIN_BLOCKS
-#define PASS_MIN_BLOCKS 1
-#endif
 
 enum PassEpi {
     EPI_PARTIAL = 0,  // store the partial sum (another pass follows)
@@ -50,8 +47,9 @@ struct PassParams {
     // layout
     int tb, rb;     // tile bits / register bits of the instantiation these tables are for
     int pb;         // pass L: cluster bits (cluster size 2^pb)
-    int hc, hg;     // pass H: chunk bits c and group bits g (group = bits n-hg .. n-1 minus extra)
+    int hc, hg;     // pass H: chunk bits c and group bits g
     int hpos;       // pass H: global position of the first group bit
+    int pbh;        // pass H: cluster bits (positions hpos+hg .. hpos+hg+pbh-1)
     int xb_lo, xb_hi;  // pass H: bits [xb_lo, xb_hi) applied from global memory (fallback)
 };
 
@@ -63,9 +61,28 @@ struct PassArgs {
     const double *sp_dev;
     double sp;
     void *out;              // partial / final output
+    const void *part;       // pass H: partial sum written by pass L (null: in place in out)
     double *partials;       // [gridDim.x * NRED]
     const int *gate;        // kernel returns at once when *gate != 0
 };
+
+// Map a local shared-memory address to the same offset in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t cluster_addr(const void *smem_ptr, uint32_t rank) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem_ptr);
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ float2 ld_cluster(uint32_t addr, const float2 *) {
+    float2 v;
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ double2 ld_cluster(uint32_t addr, const double2 *) {
+    double2 v;
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr));
+    return v;
+}
 
 template <typename R> struct Coef;
 template <> struct Coef<float> {
@@ -97,18 +114,18 @@ __device__ __forceinline__ void flip_acc(const PassParams &P, int p, bool bit, c
     }
 }
 
-// Epilogue shared by both passes: h = su * acc_total (+ su * d * u for pass L).
+// Epilogue shared by both passes: store h; Lanczos reductions with v and vp = sp * up[x].
 template <typename C, int EPI>
-__device__ __forceinline__ void epilogue(const PassArgs &A, int64_t x, double hr, double hi,
-                                         double vr, double vi, double sp, double (&red)[NRED]) {
-    C *out = reinterpret_cast<C *>(A.out);
+__device__ __forceinline__ void epilogue(C *__restrict__ out, const C *__restrict__ upv, int64_t x,
+                                         double hr, double hi, double vr, double vi, double sp,
+                                         double (&red)[NRED]) {
     out[x] = cmake<C>(hr, hi);
     if (EPI == EPI_LANCZOS) {
         red[0] += hr * hr + hi * hi;
         red[1] += vr * hr + vi * hi;
         red[2] += vr * hi - vi * hr;
-        if (A.up) {
-            const C q = reinterpret_cast<const C *>(A.up)[x];
+        if (upv) {
+            const C q = upv[x];
             const double pr = sp * double(q.x), pi = sp * double(q.y);
             red[3] += pr * hr + pi * hi;
             red[4] += pr * hi - pi * hr;
@@ -128,28 +145,51 @@ __device__ __forceinline__ void write_partials(const PassArgs &A, double (&red)[
     }
 }
 
+constexpr int PBMAX_ALL = 3;  // largest cluster (2^3 CTAs) either pass uses
+
 // ------------------------------------------------------------------------- pass L
+// Shared memory: tile [2^TB] | U [MAXQ*MAXQ] | field [MAXQ] | per-tile scalars | scratch
+template <typename C, int TB>
+__host__ __device__ constexpr size_t pass_low_smem() {
+    return (sizeof(C) << TB) + sizeof(double) * (MAXQ * MAXQ + MAXQ + 64 + 8 * NRED);
+}
+
 template <typename R, bool REALC, int TB, int RB, int EPI>
-__global__ void __launch_bounds__(1 << (TB - RB), PASS_MIN_BLOCKS)
+__global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_low(const PassParams P, PassArgs A) {
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
     if (A.gate && *A.gate != 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
     C *tile = reinterpret_cast<C *>(smem);
-    double *sh = reinterpret_cast<double *>(smem + (sizeof(C) << TB));  // per-tile scalars
-    double *crossT = sh;            // [SB]  sum_{p high set} U[q][p], q < SB
-    double *crossR = sh + SB;       // [RB]
-    double *eh = sh + SB + RB;      // [1]   energy of the high bits
-    double *red_scr = sh + 32;      // block reduction scratch
+    double *Ush = reinterpret_cast<double *>(smem + (sizeof(C) << TB));
+    double *fld = Ush + MAXQ * MAXQ;
+    double *crossT = fld + MAXQ;     // [SB] then crossR [RB] (lanes < TB)
+    double *crossR = crossT + SB;
+    double *eh = crossT + TB;
+    double *red_scr = crossT + 64;
 
-    cg::cluster_group cl = cg::this_cluster();
-    const int pb = P.pb;
-    const unsigned rank = pb ? cl.block_rank() : 0;
-    const int n = P.n;
+    const int n = P.n, pb = P.pb;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-
+    for (int k = tid; k < MAXQ * MAXQ; k += NT) Ush[k] = P.U[k];
+    for (int k = tid; k < MAXQ; k += NT) fld[k] = P.field[k];
+    uint32_t rank = 0;
+    if (pb) asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    // sibling tiles and the coefficients of the cluster bits (fixed per CTA)
+    uint32_t raddr[PBMAX_ALL];
+    R ccr[PBMAX_ALL], cci[PBMAX_ALL];
+#pragma unroll
+    for (int r = 0; r < PBMAX_ALL; ++r) {
+        raddr[r] = 0;
+        ccr[r] = cci[r] = R(0);
+        if (r < pb) {
+            raddr[r] = cluster_addr(tile, rank ^ (1u << r));
+            const bool bit = (rank >> r) & 1;
+            ccr[r] = bit ? Coef<R>::ure(P, TB + r) : Coef<R>::dre(P, TB + r);
+            cci[r] = bit ? Coef<R>::uim(P, TB + r) : Coef<R>::dim(P, TB + r);
+        }
+    }
     // per-thread constants: energy of the thread bits and thread x register crosses
     double ET = 0.0;
 #pragma unroll
@@ -164,58 +204,62 @@ k_pass_low(const PassParams P, PassArgs A) {
     double fR[RB];
 #pragma unroll
     for (int k = 0; k < RB; ++k) {
-        double s = 0.0;
+        double sacc = 0.0;
 #pragma unroll
         for (int q = 0; q < SB; ++q)
-            if ((tid >> q) & 1) s += P.U[(SB + k) * MAXQ + q];
-        fR[k] = s;
+            if ((tid >> q) & 1) sacc += P.U[(SB + k) * MAXQ + q];
+        fR[k] = sacc;
     }
+    __syncthreads();
 
     const double su = A.su_dev ? *A.su_dev : A.su;
-    const double sp = (EPI == EPI_LANCZOS && A.up) ? (A.sp_dev ? *A.sp_dev : A.sp) : 0.0;
+    const bool has_up = EPI == EPI_LANCZOS && A.up != nullptr;
+    const double sp = has_up ? (A.sp_dev ? *A.sp_dev : A.sp) : 0.0;
     const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
+    const C *__restrict__ upv = reinterpret_cast<const C *>(A.up);
+    C *__restrict__ out = reinterpret_cast<C *>(A.out);
     double red[NRED];
 #pragma unroll
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
 
-    const int CS = 1 << pb;
     const int64_t nsuper = int64_t(1) << (n - TB - pb);
     const int nclusters = gridDim.x >> pb;
     const int cid = blockIdx.x >> pb;
     for (int64_t s = cid; s < nsuper; s += nclusters) {
-        const int64_t t = (s << pb) | rank;
-        const int64_t base = t << TB;
-        // stage own amplitudes (coalesced) into registers and shared memory
+        const int64_t base = ((s << pb) | rank) << TB;
         C v[NA];
 #pragma unroll
         for (int a = 0; a < NA; ++a) v[a] = u[base + tid + a * NT];
         if (warp == 0) {
-            // per-tile high-bit energy and crosses (bits >= TB are fixed by `base`)
+            // energy of the tile's high bits and their crosses with the tile bits
             double e = 0.0;
             for (int p = TB + lane; p < n; p += 32) {
                 if (!((base >> p) & 1)) continue;
-                e += P.field[p];
+                e += fld[p];
                 for (int p2 = p + 1; p2 < n; ++p2)
-                    if ((base >> p2) & 1) e += P.U[p * MAXQ + p2];
+                    if ((base >> p2) & 1) e += Ush[p * MAXQ + p2];
             }
             e = warp_sum(e);
             if (lane == 0) eh[0] = e;
             if (lane < TB) {
-                double c = 0.0;
+                double cx = 0.0;
                 for (int p = TB; p < n; ++p)
-                    if ((base >> p) & 1) c += P.U[lane * MAXQ + p];
-                if (lane < SB) crossT[lane] = c;
-                else crossR[lane - SB] = c;
+                    if ((base >> p) & 1) cx += Ush[lane * MAXQ + p];
+                crossT[lane] = cx;  // lanes >= SB land in crossR
             }
         }
 #pragma unroll
         for (int a = 0; a < NA; ++a) tile[tid + a * NT] = v[a];
-        if (pb) cl.sync(); else __syncthreads();
-
+        if (pb) {
+            asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+        } else {
+            __syncthreads();
+        }
         double St = ET + eh[0];
 #pragma unroll
-        for (int q = 0; q < SB; ++q)
-            if ((tid >> q) & 1) St += crossT[q];
+        for (int k = 0; k < SB; ++k)
+            if ((tid >> k) & 1) St += crossT[k];
         double hR[RB];
 #pragma unroll
         for (int k = 0; k < RB; ++k) hR[k] = fR[k] + crossR[k];
@@ -224,49 +268,60 @@ k_pass_low(const PassParams P, PassArgs A) {
         for (int a = 0; a < NA; ++a) {
             const int l = tid + a * NT;
             R ar = R(0), ai = R(0);
-            // thread bits: partner in shared memory
 #pragma unroll
-            for (int q = 0; q < SB; ++q) {
-                const C w = tile[l ^ (1 << q)];
-                flip_acc<R, REALC>(P, q, (tid >> q) & 1, w, ar, ai);
-            }
-            // register bits: partner in registers
+            for (int k = 0; k < SB; ++k)  // thread bits: partner in shared memory
+                flip_acc<R, REALC>(P, k, (tid >> k) & 1, tile[l ^ (1 << k)], ar, ai);
 #pragma unroll
-            for (int k = 0; k < RB; ++k)
+            for (int k = 0; k < RB; ++k)  // register bits
                 flip_acc<R, REALC>(P, SB + k, (a >> k) & 1, v[a ^ (1 << k)], ar, ai);
-            // cluster bits: partner tile in a sibling CTA
-            for (int r = 0; r < pb; ++r) {
-                const C *rt = cl.map_shared_rank(tile, rank ^ (1u << r));
-                flip_acc<R, REALC>(P, TB + r, (rank >> r) & 1, rt[l], ar, ai);
+#pragma unroll
+            for (int r = 0; r < PBMAX_ALL; ++r) {  // cluster bits: sibling CTA's tile
+                if (r < pb) {
+                    const C w = ld_cluster(raddr[r] + (uint32_t)(l * sizeof(C)), (const C *)nullptr);
+                    if (REALC) {
+                        ar = fmar(ccr[r], w.x, ar);
+                        ai = fmar(ccr[r], w.y, ai);
+                    } else {
+                        ar = fmar(ccr[r], w.x, fmar(-cci[r], w.y, ar));
+                        ai = fmar(ccr[r], w.y, fmar(cci[r], w.x, ai));
+                    }
+                }
             }
-            // diagonal: St + E_R[a] + sum_{k in a} hR[k]
             double d = St + P.ER[a];
 #pragma unroll
             for (int k = 0; k < RB; ++k)
                 if ((a >> k) & 1) d += hR[k];
             const int64_t x = base + l;
             const double ur = double(v[a].x), ui = double(v[a].y);
-            const double hr = su * (double(ar) + d * ur), hi = su * (double(ai) + d * ui);
-            if (EPI == EPI_PARTIAL) {
-                // partial sum without the scale (pass H applies su once)
-                reinterpret_cast<C *>(A.out)[x] = cmake<C>(double(ar) + d * ur, double(ai) + d * ui);
-            } else {
-                epilogue<C, EPI>(A, x, hr, hi, su * ur, su * ui, sp, red);
-            }
+            const double tr = double(ar) + d * ur, ti = double(ai) + d * ui;
+            if (EPI == EPI_PARTIAL)
+                out[x] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
+            else
+                epilogue<C, EPI>(out, has_up ? upv : nullptr, x, su * tr, su * ti, su * ur, su * ui,
+                                 sp, red);
         }
-        if (pb) cl.sync(); else __syncthreads();  // siblings done reading this tile
+        if (pb) {
+            asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+        } else {
+            __syncthreads();
+        }
     }
     write_partials<EPI>(A, red, red_scr);
 }
 
 // ------------------------------------------------------------------------- pass H
-// Tile local index l = (j << c) | i, i < 2^c (contiguous low bits), j < 2^g (group bits
-// hpos..hpos+g-1, g = TB - c).  The thread owns l = tid + a*NT;
-// x = base + (l & cmask) + ((l >> c) << hpos), where base enumerates bits c..hpos-1 and
-// bits >= hpos+g.  Flips of local bits k >= c (global bit hpos + k - c) are applied;
-// the chunk bits were applied by pass L.
-template <typename R, bool REALC, int TB, int RB, int EPI>
-__global__ void __launch_bounds__(1 << (TB - RB), PASS_MIN_BLOCKS)
+// Tile local index l = (j << c) | i, i < 2^c (contiguous low bits, applied by pass L),
+// j < 2^g (group bits hpos..hpos+g-1).  A cluster of 2^pbh CTAs holds the tiles that
+// differ in bits hpos+g..hpos+g+pbh-1.  The thread owns l = tid + a*NT;
+// x = base + (l & cmask) + ((l >> c) << hpos).
+template <typename C, int TB>
+__host__ __device__ constexpr size_t pass_high_smem() {
+    return (sizeof(C) << TB) + sizeof(double) * 8 * NRED;
+}
+
+template <typename R, bool REALC, int TB, int RB, int EPI, bool INPL>
+__global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_high(const PassParams P, PassArgs A) {
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
@@ -274,12 +329,28 @@ k_pass_high(const PassParams P, PassArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     C *tile = reinterpret_cast<C *>(smem);
     double *red_scr = reinterpret_cast<double *>(smem + (sizeof(C) << TB));
-    const int n = P.n, c = P.hc, g = P.hg, hpos = P.hpos;
+    const int n = P.n, c = P.hc, g = P.hg, hpos = P.hpos, pbh = P.pbh;
     const int tid = threadIdx.x;
     const int64_t cmask = (int64_t(1) << c) - 1;
-    const int lowbits = hpos - c;  // base bits between the chunk and the group
-    const int64_t ntiles = int64_t(1) << (n - c - g);
+    const int lowbits = hpos - c;
+    const int64_t lowmask = (int64_t(1) << lowbits) - 1;
+    const int cpos = hpos + g;  // first cluster bit
 
+    uint32_t rank = 0;
+    if (pbh) asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    uint32_t raddr[PBMAX_ALL];
+    R ccr[PBMAX_ALL], cci[PBMAX_ALL];
+#pragma unroll
+    for (int r = 0; r < PBMAX_ALL; ++r) {
+        raddr[r] = 0;
+        ccr[r] = cci[r] = R(0);
+        if (r < pbh) {
+            raddr[r] = cluster_addr(tile, rank ^ (1u << r));
+            const bool bit = (rank >> r) & 1;
+            ccr[r] = bit ? Coef<R>::ure(P, cpos + r) : Coef<R>::dre(P, cpos + r);
+            cci[r] = bit ? Coef<R>::uim(P, cpos + r) : Coef<R>::dim(P, cpos + r);
+        }
+    }
     // coefficients of the shared-memory bits (direction fixed by the thread's own bits)
     R cr_s[SB], ci_s[SB];
 #pragma unroll
@@ -302,25 +373,40 @@ k_pass_high(const PassParams P, PassArgs A) {
         di_r[k] = ok ? Coef<R>::dim(P, p) : R(0);
     }
     const double su = A.su_dev ? *A.su_dev : A.su;
-    const double sp = (EPI == EPI_LANCZOS && A.up) ? (A.sp_dev ? *A.sp_dev : A.sp) : 0.0;
+    const bool has_up = EPI == EPI_LANCZOS && A.up != nullptr;
+    const double sp = has_up ? (A.sp_dev ? *A.sp_dev : A.sp) : 0.0;
     const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
-    C *outp = reinterpret_cast<C *>(A.out);
+    const C *__restrict__ upv = reinterpret_cast<const C *>(A.up);
+    C *__restrict__ outp = reinterpret_cast<C *>(A.out);
+    // INPL: the partial sum is read from `out` itself (all loads of a tile are issued
+    // before its stores); otherwise from a separate buffer.
+    const C *__restrict__ partp = reinterpret_cast<const C *>(INPL ? A.out : A.part);
     double red[NRED];
 #pragma unroll
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
 
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int64_t base = ((t & ((int64_t(1) << lowbits) - 1)) << c) |
-                             ((t >> lowbits) << (hpos + g));
-        C v[NA];
+    const int64_t nsuper = int64_t(1) << (n - c - g - pbh);
+    const int nclusters = gridDim.x >> pbh;
+    const int cid = blockIdx.x >> pbh;
+    for (int64_t s = cid; s < nsuper; s += nclusters) {
+        const int64_t base = ((s & lowmask) << c) | ((int64_t)rank << cpos) |
+                             ((s >> lowbits) << (cpos + pbh));
+        C v[NA], part[INPL ? NA : 1];
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
             const int64_t l = tid + a * NT;
-            v[a] = u[base + (l & cmask) + ((l >> c) << hpos)];
+            const int64_t x = base + (l & cmask) + ((l >> c) << hpos);
+            v[a] = u[x];
+            if (INPL) part[a] = partp[x];
         }
 #pragma unroll
         for (int a = 0; a < NA; ++a) tile[tid + a * NT] = v[a];
-        __syncthreads();
+        if (pbh) {
+            asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+        } else {
+            __syncthreads();
+        }
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
             const int l = tid + a * NT;
@@ -353,17 +439,36 @@ k_pass_high(const PassParams P, PassArgs A) {
                     ai = fmar(cr, w.y, fmar(ci, w.x, ai));
                 }
             }
-            // bits beyond both tiles (very large registers): partner from global memory
+#pragma unroll
+            for (int r = 0; r < PBMAX_ALL; ++r) {  // cluster bits: sibling CTA's tile
+                if (r < pbh) {
+                    const C w = ld_cluster(raddr[r] + (uint32_t)(l * sizeof(C)), (const C *)nullptr);
+                    if (REALC) {
+                        ar = fmar(ccr[r], w.x, ar);
+                        ai = fmar(ccr[r], w.y, ai);
+                    } else {
+                        ar = fmar(ccr[r], w.x, fmar(-cci[r], w.y, ar));
+                        ai = fmar(ccr[r], w.y, fmar(cci[r], w.x, ai));
+                    }
+                }
+            }
+            // bits beyond the tiles and the cluster (very large registers): global partner
             for (int p = P.xb_lo; p < P.xb_hi; ++p) {
                 const C w = u[x ^ (int64_t(1) << p)];
                 flip_acc<R, REALC>(P, p, (x >> p) & 1, w, ar, ai);
             }
-            const C part = outp[x];
-            const double hr = su * (double(part.x) + double(ar));
-            const double hi = su * (double(part.y) + double(ai));
-            epilogue<C, EPI>(A, x, hr, hi, su * double(v[a].x), su * double(v[a].y), sp, red);
+            const C pt = INPL ? part[INPL ? a : 0] : partp[x];
+            const double hr = su * (double(pt.x) + double(ar));
+            const double hi = su * (double(pt.y) + double(ai));
+            epilogue<C, EPI>(outp, has_up ? upv : nullptr, x, hr, hi, su * double(v[a].x),
+                             su * double(v[a].y), sp, red);
         }
-        __syncthreads();
+        if (pbh) {
+            asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+        } else {
+            __syncthreads();
+        }
     }
     write_partials<EPI>(A, red, red_scr);
 }

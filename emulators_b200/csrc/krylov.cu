@@ -372,7 +372,7 @@ k_combine(const KState *ks, const void *v0_, const unsigned char *basis, i64 D, 
         double re = cr[0] * double(a.x) - ci[0] * double(a.y);
         double im = cr[0] * double(a.y) + ci[0] * double(a.x);
         for (int k = 1; k < nv; ++k) {
-            const C b = bs[(i64)(k - 1) * D + x];
+            const C b = bs[(i64)k * D + x];
             re += cr[k] * double(b.x) - ci[k] * double(b.y);
             im += cr[k] * double(b.y) + ci[k] * double(b.x);
         }
@@ -493,7 +493,7 @@ extern "C" {
 size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity) {
     if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS || basis_capacity < 0) return 0;
     const size_t es = dtype == EMUSV_C128 ? 16 : 8;
-    return header_bytes() + (size_t)basis_capacity * (size_t(1) << nqubits) * es;
+    return header_bytes() + (size_t)(basis_capacity + 1) * (size_t(1) << nqubits) * es;
 }
 
 int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
@@ -515,10 +515,12 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
     const i64 D = i64(1) << nqubits;
     const size_t es = dtype == EMUSV_C128 ? 16 : 8;
     Workspace W = carve(workspace, workspace_bytes);
-    const int capacity = (int)(W.basis_bytes / (D * es));
+    // basis region: [partial-sum vector of the two-pass H*psi][stored_1][stored_2]...
+    const int capacity = (int)(W.basis_bytes / (D * es)) - 1;
     if (capacity < 1) return EMUSV_WORKSPACE_TOO_SMALL;
+    void *part_vec = W.basis;
     auto stored = [&](int k) -> const void * {
-        return k == 0 ? psi_in : (const void *)(W.basis + (size_t)(k - 1) * D * es);
+        return k == 0 ? psi_in : (const void *)(W.basis + (size_t)k * D * es);
     };
     const int sg = stream_grid(D);
 
@@ -556,6 +558,7 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
         A.partials = W.part_h;
         A.tile_bits = hpsi_tile_bits(nqubits);
         A.gate = &W.ks->status;
+        A.part_buf = part_vec;
         int gh = 0;
         int st = launch_hpsi(dtype, HP_LANCZOS, P, A, max_grid_blocks(), s, &gh);
         if (st) return st;

@@ -13,6 +13,7 @@ enum ProfKind {
     PROF_OBS = 4,      // observables
     PROF_ADJOINT = 5,  // adjoint contractions
     PROF_BATCH = 6,    // batched persistent evolution
+    PROF_HPSI_HIGH = 7,  // pass H of the two-pass H*psi
     PROF_KINDS = 8
 };
 

@@ -91,7 +91,8 @@ int emusv_correlation(int nqubits, int dtype, const void *psi, double *corr_dev,
                       size_t scratch_bytes, void *stream);
 
 /* Bytes of device workspace emusv_krylov_step needs for a basis of `basis_capacity`
- * stored Krylov vectors (the input vector is used in place and is not counted). */
+ * stored Krylov vectors (the input vector is used in place and is not counted; one more
+ * vector holds the partial sums of the two-pass H*psi). */
 size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity);
 
 /* One time step psi_out = exp(-i dt H) psi_in by Lanczos with the Expokit error
