@@ -35,6 +35,7 @@ class KrylovInfo(ctypes.Structure):
 SIGNATURES: dict[str, tuple] = {
     "emusv_build_arch": (_I, []),
     "emusv_status_string": (ctypes.c_char_p, [_I]),
+    "emusv_device_error": (_I, [_P]),
     "emusv_hamiltonian_diag": (_I, [_I, _P, _P, _P, _P]),
     "emusv_hpsi": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "emusv_scratch_bytes": (_SZ, [_I, _I]),

@@ -104,6 +104,7 @@ __device__ __forceinline__ void sum_partials(const double *partials, int nblocks
 // ---------------------------------------------------------------- host helpers
 int sm_count();                       // SMs of the current device (cached per device)
 int stream_status(cudaError_t e);     // map a CUDA error to emusv_status
+int *device_error_word();             // library-wide device error word (current device)
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 }  // namespace emusv

@@ -57,6 +57,15 @@ int sm_count() {
 
 int stream_status(cudaError_t e) { return e == cudaSuccess ? EMUSV_OK : EMUSV_CUDA_ERROR; }
 
+// Library-wide device word for errors of calls without a status word of their own.
+__device__ int g_device_error = 0;
+
+int *device_error_word() {
+    int *p = nullptr;
+    if (cudaGetSymbolAddress((void **)&p, g_device_error) != cudaSuccess) return nullptr;
+    return p;
+}
+
 int hpsi_tile_bits(int n) {
     int b = n - 8;
     if (b > 11) b = 11;
@@ -269,6 +278,17 @@ extern "C" {
 
 int emusv_build_arch(void) { return 100; }
 
+int emusv_device_error(void *stream) {
+    int *p = device_error_word();
+    if (!p) return EMUSV_CUDA_ERROR;
+    int h = 0;
+    cudaStream_t s = as_stream(stream);
+    EMUSV_CHECK(cudaMemcpyAsync(&h, p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    EMUSV_CHECK(cudaStreamSynchronize(s));
+    if (h) EMUSV_CHECK(cudaMemsetAsync(p, 0, sizeof(int), s));
+    return h;
+}
+
 const char *emusv_status_string(int status) {
     switch (status) {
     case EMUSV_OK: return "ok";
@@ -312,6 +332,8 @@ int emusv_hpsi(int nqubits, int dtype, const double *omegas, const double *delta
     A.u = psi;
     A.su = 1.0;
     A.out = out;
+    A.part_buf = out;  // the two-pass kernels keep their partial sums in place
+    A.err = device_error_word();
     A.tile_bits = hpsi_tile_bits(nqubits);
     return launch_hpsi(dtype, HP_STORE, P, A, 0, as_stream(stream), nullptr);
 }

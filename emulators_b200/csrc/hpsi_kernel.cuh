@@ -36,7 +36,8 @@ struct HpsiArgs {
     double *partials;  // [gridDim.x * NRED]
     int tile_bits;
     const int *gate;   // if non-null and *gate != 0 the kernel returns at once
-    void *part_buf;    // two-pass H*psi: buffer for the partial sum (null: in place in out)
+    void *part_buf;    // two-pass H*psi: buffer for the partial sums of pass L
+    int *err;          // device word receiving EMUSV_TIMEOUT if a bounded wait gives up
 };
 
 struct SmemLayout {

@@ -1,5 +1,8 @@
 // Host side of the two-pass H*psi: layout choice, parameter tables, cluster launches.
+#include <cudaTypedefs.h>
 #include <string.h>
+
+#include <mutex>
 
 #include "hpsi_kernel.cuh"
 #include "hpsi_pass.cuh"
@@ -19,6 +22,71 @@ template <> struct PassShape<float> {
 template <> struct PassShape<double> {
     static constexpr int TB = 11, RB = 3, PBMAX = 3, PBHMAX = 3, CMIN = 1;
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Tensor map of a 2^n vector of `es`-byte amplitudes for pass H (see hpsi_pass.cuh).
+static bool encode_pass_high(CUtensorMap *map, const void *base, int n, int es, const PassParams &P,
+                             int cm) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const int K = es / 8;
+    cuuint64_t dims[5], strides[4];
+    cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+    const int c = P.hc, g = P.hg, hpos = P.hpos, pbh = P.pbh;
+    if (P.hsplit == 0) {
+        dims[0] = (cuuint64_t(1) << c) * K;
+        dims[1] = cuuint64_t(1) << (hpos - c);
+        dims[2] = cuuint64_t(1) << g;
+        dims[3] = cuuint64_t(1) << pbh;
+        dims[4] = cuuint64_t(1) << (n - hpos - g - pbh);
+        strides[0] = (cuuint64_t(es) << c);
+        strides[1] = (cuuint64_t(es) << hpos);
+        strides[2] = (cuuint64_t(es) << (hpos + g));
+        strides[3] = (cuuint64_t(es) << (hpos + g + pbh));
+        box[0] = (cuuint32_t)dims[0];
+        box[1] = 1;
+        box[2] = (cuuint32_t)P.hbox_rows;
+        box[3] = 1;
+        box[4] = 1;
+    } else {
+        dims[0] = (cuuint64_t(1) << cm) * K;
+        dims[1] = cuuint64_t(1) << (c - cm);
+        dims[2] = cuuint64_t(1) << (hpos - c);
+        dims[3] = cuuint64_t(1) << g;
+        dims[4] = cuuint64_t(1) << (n - hpos - g);
+        strides[0] = (cuuint64_t(es) << cm);
+        strides[1] = (cuuint64_t(es) << c);
+        strides[2] = (cuuint64_t(es) << hpos);
+        strides[3] = (cuuint64_t(es) << (hpos + g));
+        box[0] = (cuuint32_t)dims[0];
+        box[1] = (cuuint32_t)dims[1];
+        box[2] = 1;
+        box[3] = (cuuint32_t)P.hbox_rows;
+        box[4] = 1;
+    }
+    const cuuint64_t chunk_bytes = (cuuint64_t(es) << c);
+    const CUtensorMapL2promotion promo =
+        chunk_bytes >= 256 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+                           : (chunk_bytes >= 128 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B
+                                                 : CU_TENSOR_MAP_L2_PROMOTION_NONE);
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void *>(base), dims,
+                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 
 int pass_min_qubits(int dtype) {
     return dtype == EMUSV_C64 ? PassShape<float>::TB : PassShape<double>::TB;
@@ -51,8 +119,6 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
         }
         P->ER[a] = e;
     }
-    P->tb = TB;
-    P->rb = RB;
 }
 
 template <typename R, bool REALC, int EPI_L, int EPI_H>
@@ -76,18 +142,23 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     P.pbh = pbh;
     P.xb_lo = TB + pb + g + pbh;
     P.xb_hi = n;
+    constexpr int K = sizeof(C) / 8;
+    // chunk rows wider than one 256-element TMA box dimension are split in two dims
+    int cm = 0;
+    while (((1 << (cm + 1)) * K) <= 256 && cm + 1 <= P.hc) ++cm;
+    P.hsplit = ((1 << P.hc) * K > 256) ? 1 : 0;
+    P.hbox_rows = g > 8 ? 256 : (1 << g);
+    if (P.hsplit && pbh) return EMUSV_BAD_ARGUMENT;  // not a layout the sizes above produce
 
     PassArgs A = {};
     A.u = HA.u;
     A.su_dev = HA.su_dev;
     A.su = HA.su;
-    A.up = HA.up;
-    A.sp_dev = HA.sp_dev;
-    A.sp = HA.sp;
-    A.out = rem > 0 && HA.part_buf ? HA.part_buf : HA.out;  // pass L output
-    A.part = nullptr;
+    A.out = rem > 0 ? (HA.part_buf ? HA.part_buf : HA.out) : HA.out;  // pass L output
     A.partials = HA.partials;
     A.gate = HA.gate;
+    A.err = HA.err;
+    if (rem > 0 && !HA.part_buf) return EMUSV_BAD_ARGUMENT;  // pass H needs its own buffer
 
     const size_t smem_l = pass_low_smem<C, TB>(), smem_h = pass_high_smem<C, TB>();
     const int nsm = sm_count();
@@ -123,12 +194,15 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
         if (rem == 0 && grid_out) *grid_out = (int)grid;
     }
     if (rem == 0) return EMUSV_OK;
-    // ---- pass H: partial from pass L's output, final into HA.out
-    A.part = A.out;
-    A.out = HA.out;
+    // ---- pass H: partial sums (pass L output) and values staged by TMA, final into HA.out
     {
-        auto kern = HA.part_buf ? k_pass_high<R, REALC, TB, RB, EPI_H, false>
-                                : k_pass_high<R, REALC, TB, RB, EPI_H, true>;
+        PassHighMaps M;
+        if (!encode_pass_high(&M.u, HA.u, n, (int)sizeof(C), P, cm) ||
+            !encode_pass_high(&M.part, HA.part_buf, n, (int)sizeof(C), P, cm))
+            return EMUSV_CUDA_ERROR;
+        PassArgs AH = A;
+        AH.out = HA.out;
+        auto kern = k_pass_high<R, REALC, TB, RB, EPI_H>;
         EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_h));
         int per_sm = 0;
         EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem_h));
@@ -153,7 +227,7 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
         cfg.numAttrs = 1;
         {
             ProfScope ps_(PROF_HPSI_HIGH, s);
-            EMUSV_CHECK(cudaLaunchKernelEx(&cfg, kern, P, A));
+            EMUSV_CHECK(cudaLaunchKernelEx(&cfg, kern, P, AH, M));
         }
         if (grid_out) *grid_out = (int)grid;
     }

@@ -1,39 +1,43 @@
-// Two-pass fused H*psi for large registers (sm_100a).
+// Two-pass fused H*psi for large registers (sm_100a), TMA-staged and double-buffered.
 //
-// H = D + sum_p X_p-terms.  The flip terms of every bit are applied on chip, split over
-// two streaming passes so that no amplitude is fetched more than once per pass:
+// H = D + sum_p (coefficient x flip of bit p).  Every flip is applied on chip, split over
+// two streaming passes so that each amplitude is read from HBM once per pass:
 //
-//  pass L  tile = 2^TB consecutive amplitudes (bits 0..TB-1) staged in shared memory;
-//          a cluster of 2^pb CTAs holds 2^pb neighbouring tiles, so the flips of bits
-//          TB..TB+pb-1 read the partner amplitude from a sibling CTA's shared memory
-//          (DSMEM).  The diagonal (detunings + C6/r^6 interactions) is rebuilt here from
-//          per-thread / per-tile FP64 partial energies.  Output: the partial sum (or the
-//          final H v when no bit is left).
-//  pass H  tile = 2^c contiguous amplitudes (the c low bits, already done by pass L) x
-//          2^g combinations of the g top bits, so the flips of the top bits are again
-//          shared-memory reads; adds them to the partial sum and runs the epilogue.
+//  pass L  tile = 2^TB consecutive amplitudes (bits 0..TB-1), brought into shared memory
+//          by one cp.async.bulk per tile; a cluster of 2^pb CTAs holds 2^pb neighbouring
+//          tiles, so the flips of bits TB..TB+pb-1 read the partner from a sibling CTA's
+//          shared memory (DSMEM).  The diagonal (detunings + C6/r^6 interactions) is
+//          rebuilt from per-thread / per-tile FP64 partial energies.  Output: the partial
+//          sum (or H v when no bit is left).
+//  pass H  tile = 2^c contiguous amplitudes (the c low bits, done by pass L) x 2^g
+//          combinations of the top bits, gathered by a 5-D TMA tensor-map load (rows of
+//          32 B or more); a cluster of 2^pbh CTAs covers the pbh bits above the group.
+//          Adds the flips of those bits to the partial sum (also TMA-staged) and runs the
+//          epilogue (store, Lanczos FP64 reductions).
+//
+// Both passes keep two tile buffers in flight: the load of tile i+1 is issued when tile
+// i starts computing.  mbarrier waits are bounded (about 2 s of clock): on a timeout the
+// kernel records status EMUSV_TIMEOUT in *A.err, skips the arithmetic and keeps taking
+// part in the cluster barriers so that no CTA is left waiting.
 //
 // Register blocking: each of the NT = 2^(TB-RB) threads owns NA = 2^RB amplitudes that
 // differ in the RB highest tile bits, so those flips are register-register; the other
-// tile bits are one shared-memory load per flip at an offset known at compile time.
-// Coefficients of compile-time bit positions are kernel-parameter (constant bank)
-// operands.
+// tile bits are one shared-memory load per flip at a compile-time offset.
 #pragma once
 
-#include <cooperative_groups.h>
+#include <cuda.h>
 
 #include "common.cuh"
 
 namespace emusv {
 
-namespace cg = cooperative_groups;
-
-
 enum PassEpi {
     EPI_PARTIAL = 0,  // store the partial sum (another pass follows)
     EPI_STORE = 1,    // store H v
-    EPI_LANCZOS = 2,  // store H v; ||Hv||^2, <v,Hv>, <vp,Hv>, <v,vp> partials
+    EPI_LANCZOS = 2,  // store H v; FP64 partials ||Hv||^2, <v,Hv>
 };
+
+constexpr int PBMAX_ALL = 3;  // largest cluster (2^3 CTAs) either pass uses
 
 struct PassParams {
     int n;
@@ -44,12 +48,12 @@ struct PassParams {
     double field[MAXQ];
     double U[MAXQ * MAXQ];
     double ER[32];  // energies of the register-bit patterns of pass L (fields + pairs)
-    // layout
-    int tb, rb;     // tile bits / register bits of the instantiation these tables are for
     int pb;         // pass L: cluster bits (cluster size 2^pb)
     int hc, hg;     // pass H: chunk bits c and group bits g
     int hpos;       // pass H: global position of the first group bit
     int pbh;        // pass H: cluster bits (positions hpos+hg .. hpos+hg+pbh-1)
+    int hsplit;     // pass H: tensor-map layout (0: 5-D with cluster dim, 1: chunk split)
+    int hbox_rows;  // pass H: group rows per TMA box (<= 256)
     int xb_lo, xb_hi;  // pass H: bits [xb_lo, xb_hi) applied from global memory (fallback)
 };
 
@@ -57,31 +61,85 @@ struct PassArgs {
     const void *u;          // stored input vector (raw); v = su * u
     const double *su_dev;   // device scale (or null: su)
     double su;
-    const void *up;         // previous Lanczos vector (EPI_LANCZOS, may be null)
-    const double *sp_dev;
-    double sp;
     void *out;              // partial / final output
-    const void *part;       // pass H: partial sum written by pass L (null: in place in out)
     double *partials;       // [gridDim.x * NRED]
     const int *gate;        // kernel returns at once when *gate != 0
+    int *err;               // receives EMUSV_TIMEOUT when a bounded wait gives up
 };
 
-// Map a local shared-memory address to the same offset in CTA `rank` of the cluster.
+// ------------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
 __device__ __forceinline__ uint32_t cluster_addr(const void *smem_ptr, uint32_t rank) {
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem_ptr);
     uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(smem_ptr)), "r"(rank));
     return r;
 }
 __device__ __forceinline__ float2 ld_cluster(uint32_t addr, const float2 *) {
     float2 v;
-    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
     return v;
 }
 __device__ __forceinline__ double2 ld_cluster(uint32_t addr, const double2 *) {
     double2 v;
-    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr));
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
     return v;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait (a few seconds of SM clock); false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > 4000000000LL) return false;
+    }
+    return true;
+}
+// 1-D bulk copy global -> own shared memory, completion on `bar`.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// 5-D tiled tensor-map load (no multicast), completion on `bar`.
+__device__ __forceinline__ void tmap_load5(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                           int c3, int c4, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+          "r"(smem_u32(bar))
+        : "memory");
 }
 
 template <typename R> struct Coef;
@@ -98,7 +156,8 @@ template <> struct Coef<double> {
     __device__ static double dim(const PassParams &P, int p) { return P.ddn_im[p]; }
 };
 
-// acc += c * w  with c = up (bit==1) or dn (bit==0) of bit position p
+// acc += c * w  with c = up (bit==1) or dn (bit==0) of bit position p (compile-time p:
+// the coefficient is a constant-bank operand).
 template <typename R, bool REALC, typename C>
 __device__ __forceinline__ void flip_acc(const PassParams &P, int p, bool bit, const C &w, R &ar,
                                          R &ai) {
@@ -113,25 +172,14 @@ __device__ __forceinline__ void flip_acc(const PassParams &P, int p, bool bit, c
         ai = fmar(cr, w.y, fmar(ci, w.x, ai));
     }
 }
-
-// Epilogue shared by both passes: store h; Lanczos reductions with v and vp = sp * up[x].
-template <typename C, int EPI>
-__device__ __forceinline__ void epilogue(C *__restrict__ out, const C *__restrict__ upv, int64_t x,
-                                         double hr, double hi, double vr, double vi, double sp,
-                                         double (&red)[NRED]) {
-    out[x] = cmake<C>(hr, hi);
-    if (EPI == EPI_LANCZOS) {
-        red[0] += hr * hr + hi * hi;
-        red[1] += vr * hr + vi * hi;
-        red[2] += vr * hi - vi * hr;
-        if (upv) {
-            const C q = upv[x];
-            const double pr = sp * double(q.x), pi = sp * double(q.y);
-            red[3] += pr * hr + pi * hi;
-            red[4] += pr * hi - pi * hr;
-            red[5] += vr * pr + vi * pi;
-            red[6] += vr * pi - vi * pr;
-        }
+template <typename R, bool REALC, typename C>
+__device__ __forceinline__ void flip_reg(R cr, R ci, const C &w, R &ar, R &ai) {
+    if (REALC) {
+        ar = fmar(cr, w.x, ar);
+        ai = fmar(cr, w.y, ai);
+    } else {
+        ar = fmar(cr, w.x, fmar(-ci, w.y, ar));
+        ai = fmar(cr, w.y, fmar(ci, w.x, ai));
     }
 }
 
@@ -145,13 +193,17 @@ __device__ __forceinline__ void write_partials(const PassArgs &A, double (&red)[
     }
 }
 
-constexpr int PBMAX_ALL = 3;  // largest cluster (2^3 CTAs) either pass uses
+__device__ __forceinline__ void report_timeout(const PassArgs &A) {
+    if (A.err) atomicExch(A.err, (int)EMUSV_TIMEOUT);
+}
 
 // ------------------------------------------------------------------------- pass L
-// Shared memory: tile [2^TB] | U [MAXQ*MAXQ] | field [MAXQ] | per-tile scalars | scratch
+// Shared memory: 2 tiles | mbarriers | U (padded rows) | field | per-tile scalars x2 | scratch
+constexpr int UPAD = MAXQ + 1;  // row stride of the shared U table (no bank conflicts)
+
 template <typename C, int TB>
 __host__ __device__ constexpr size_t pass_low_smem() {
-    return (sizeof(C) << TB) + sizeof(double) * (MAXQ * MAXQ + MAXQ + 64 + 8 * NRED);
+    return 2 * (sizeof(C) << TB) + 16 + sizeof(double) * (MAXQ * UPAD + MAXQ + 2 * 64 + 8 * NRED);
 }
 
 template <typename R, bool REALC, int TB, int RB, int EPI>
@@ -159,37 +211,40 @@ __global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_low(const PassParams P, PassArgs A) {
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
+    constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
     if (A.gate && *A.gate != 0) return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    C *tile = reinterpret_cast<C *>(smem);
-    double *Ush = reinterpret_cast<double *>(smem + (sizeof(C) << TB));
-    double *fld = Ush + MAXQ * MAXQ;
-    double *crossT = fld + MAXQ;     // [SB] then crossR [RB] (lanes < TB)
-    double *crossR = crossT + SB;
-    double *eh = crossT + TB;
-    double *red_scr = crossT + 64;
+    extern __shared__ __align__(128) unsigned char smem[];
+    C *tiles = reinterpret_cast<C *>(smem);                      // [2][2^TB]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * TILE_BYTES);  // [2]
+    double *Ush = reinterpret_cast<double *>(smem + 2 * TILE_BYTES + 16);
+    double *fld = Ush + MAXQ * UPAD;
+    double *scal = fld + MAXQ;       // [2][64]: crossT[SB] crossR[RB] eh
+    double *red_scr = scal + 2 * 64;
 
     const int n = P.n, pb = P.pb;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < MAXQ * MAXQ; k += NT) Ush[k] = P.U[k];
+    const uint32_t rank = pb ? cluster_rank() : 0;
+    const int64_t nsuper = int64_t(1) << (n - TB - pb);
+    const int nclusters = gridDim.x >> pb;
+    const int cid = blockIdx.x >> pb;
+    const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
+    C *__restrict__ out = reinterpret_cast<C *>(A.out);
+
+    for (int k = tid; k < MAXQ * MAXQ; k += NT) Ush[(k / MAXQ) * UPAD + (k % MAXQ)] = P.U[k];
     for (int k = tid; k < MAXQ; k += NT) fld[k] = P.field[k];
-    uint32_t rank = 0;
-    if (pb) asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-    // sibling tiles and the coefficients of the cluster bits (fixed per CTA)
-    uint32_t raddr[PBMAX_ALL];
-    R ccr[PBMAX_ALL], cci[PBMAX_ALL];
-#pragma unroll
-    for (int r = 0; r < PBMAX_ALL; ++r) {
-        raddr[r] = 0;
-        ccr[r] = cci[r] = R(0);
-        if (r < pb) {
-            raddr[r] = cluster_addr(tile, rank ^ (1u << r));
-            const bool bit = (rank >> r) & 1;
-            ccr[r] = bit ? Coef<R>::ure(P, TB + r) : Coef<R>::dre(P, TB + r);
-            cci[r] = bit ? Coef<R>::uim(P, TB + r) : Coef<R>::dim(P, TB + r);
-        }
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
     }
+    __syncthreads();
+    // prologue: first tile of this CTA into buffer 0
+    if (tid == 0 && cid < nsuper) {
+        mbar_expect_tx(&bars[0], TILE_BYTES);
+        bulk_load(tiles, u + ((((int64_t)cid << pb) | rank) << TB), TILE_BYTES, &bars[0]);
+    }
+
     // per-thread constants: energy of the thread bits and thread x register crosses
     double ET = 0.0;
 #pragma unroll
@@ -210,26 +265,32 @@ k_pass_low(const PassParams P, PassArgs A) {
             if ((tid >> q) & 1) sacc += P.U[(SB + k) * MAXQ + q];
         fR[k] = sacc;
     }
-    __syncthreads();
-
+    // sibling CTAs and the coefficients of the cluster bits (fixed per CTA)
+    uint32_t raddr[PBMAX_ALL];
+    R ccr[PBMAX_ALL], cci[PBMAX_ALL];
+#pragma unroll
+    for (int r = 0; r < PBMAX_ALL; ++r) {
+        raddr[r] = 0;
+        ccr[r] = cci[r] = R(0);
+        if (r < pb) {
+            raddr[r] = cluster_addr(tiles, rank ^ (1u << r));
+            const bool bit = (rank >> r) & 1;
+            ccr[r] = bit ? Coef<R>::ure(P, TB + r) : Coef<R>::dre(P, TB + r);
+            cci[r] = bit ? Coef<R>::uim(P, TB + r) : Coef<R>::dim(P, TB + r);
+        }
+    }
     const double su = A.su_dev ? *A.su_dev : A.su;
-    const bool has_up = EPI == EPI_LANCZOS && A.up != nullptr;
-    const double sp = has_up ? (A.sp_dev ? *A.sp_dev : A.sp) : 0.0;
-    const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
-    const C *__restrict__ upv = reinterpret_cast<const C *>(A.up);
-    C *__restrict__ out = reinterpret_cast<C *>(A.out);
     double red[NRED];
 #pragma unroll
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
+    bool ok = true;
 
-    const int64_t nsuper = int64_t(1) << (n - TB - pb);
-    const int nclusters = gridDim.x >> pb;
-    const int cid = blockIdx.x >> pb;
-    for (int64_t s = cid; s < nsuper; s += nclusters) {
+    int it = 0;
+    for (int64_t s = cid; s < nsuper; s += nclusters, ++it) {
+        const int buf = it & 1;
         const int64_t base = ((s << pb) | rank) << TB;
-        C v[NA];
-#pragma unroll
-        for (int a = 0; a < NA; ++a) v[a] = u[base + tid + a * NT];
+        C *tile = tiles + (buf << TB);
+        double *sc = scal + buf * 64;
         if (warp == 0) {
             // energy of the tile's high bits and their crosses with the tile bits
             double e = 0.0;
@@ -237,76 +298,80 @@ k_pass_low(const PassParams P, PassArgs A) {
                 if (!((base >> p) & 1)) continue;
                 e += fld[p];
                 for (int p2 = p + 1; p2 < n; ++p2)
-                    if ((base >> p2) & 1) e += Ush[p * MAXQ + p2];
+                    if ((base >> p2) & 1) e += Ush[p * UPAD + p2];
             }
             e = warp_sum(e);
-            if (lane == 0) eh[0] = e;
+            if (lane == 0) sc[TB] = e;
             if (lane < TB) {
                 double cx = 0.0;
                 for (int p = TB; p < n; ++p)
-                    if ((base >> p) & 1) cx += Ush[lane * MAXQ + p];
-                crossT[lane] = cx;  // lanes >= SB land in crossR
+                    if ((base >> p) & 1) cx += Ush[lane * UPAD + p];
+                sc[lane] = cx;  // crossT[0..SB) then crossR[0..RB)
             }
         }
-#pragma unroll
-        for (int a = 0; a < NA; ++a) tile[tid + a * NT] = v[a];
-        if (pb) {
-            asm volatile("barrier.cluster.arrive.release.aligned;\n"
-                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
-        } else {
-            __syncthreads();
+        if (ok && !mbar_wait(&bars[buf], (it >> 1) & 1)) {
+            ok = false;
+            report_timeout(A);
         }
-        double St = ET + eh[0];
+        // every CTA of the cluster has its tile; siblings are done with buffer buf^1
+        if (pb) cluster_sync_all(); else __syncthreads();
+        if (tid == 0 && s + nclusters < nsuper && ok) {
+            const int64_t nb = (((s + nclusters) << pb) | rank) << TB;
+            mbar_expect_tx(&bars[buf ^ 1], TILE_BYTES);
+            bulk_load(tiles + ((buf ^ 1) << TB), u + nb, TILE_BYTES, &bars[buf ^ 1]);
+        }
+        if (ok) {
+            double St = ET + sc[TB];
 #pragma unroll
-        for (int k = 0; k < SB; ++k)
-            if ((tid >> k) & 1) St += crossT[k];
-        double hR[RB];
+            for (int k = 0; k < SB; ++k)
+                if ((tid >> k) & 1) St += sc[k];
+            double hR[RB];
 #pragma unroll
-        for (int k = 0; k < RB; ++k) hR[k] = fR[k] + crossR[k];
-
+            for (int k = 0; k < RB; ++k) hR[k] = fR[k] + sc[SB + k];
+            const uint32_t boff = (uint32_t)buf * TILE_BYTES;
+            C v[NA];
 #pragma unroll
-        for (int a = 0; a < NA; ++a) {
-            const int l = tid + a * NT;
-            R ar = R(0), ai = R(0);
+            for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
 #pragma unroll
-            for (int k = 0; k < SB; ++k)  // thread bits: partner in shared memory
-                flip_acc<R, REALC>(P, k, (tid >> k) & 1, tile[l ^ (1 << k)], ar, ai);
+            for (int a = 0; a < NA; ++a) {
+                const int l = tid + a * NT;
+                R ar = R(0), ai = R(0);
 #pragma unroll
-            for (int k = 0; k < RB; ++k)  // register bits
-                flip_acc<R, REALC>(P, SB + k, (a >> k) & 1, v[a ^ (1 << k)], ar, ai);
+                for (int k = 0; k < SB; ++k)  // thread bits: partner in shared memory
+                    flip_acc<R, REALC>(P, k, (tid >> k) & 1, tile[l ^ (1 << k)], ar, ai);
 #pragma unroll
-            for (int r = 0; r < PBMAX_ALL; ++r) {  // cluster bits: sibling CTA's tile
-                if (r < pb) {
-                    const C w = ld_cluster(raddr[r] + (uint32_t)(l * sizeof(C)), (const C *)nullptr);
-                    if (REALC) {
-                        ar = fmar(ccr[r], w.x, ar);
-                        ai = fmar(ccr[r], w.y, ai);
-                    } else {
-                        ar = fmar(ccr[r], w.x, fmar(-cci[r], w.y, ar));
-                        ai = fmar(ccr[r], w.y, fmar(cci[r], w.x, ai));
+                for (int k = 0; k < RB; ++k)  // register bits
+                    flip_acc<R, REALC>(P, SB + k, (a >> k) & 1, v[a ^ (1 << k)], ar, ai);
+#pragma unroll
+                for (int r = 0; r < PBMAX_ALL; ++r)  // cluster bits: sibling CTA's tile
+                    if (r < pb)
+                        flip_reg<R, REALC>(ccr[r], cci[r],
+                                           ld_cluster(raddr[r] + boff + (uint32_t)(l * sizeof(C)),
+                                                      (const C *)nullptr), ar, ai);
+                double d = St + P.ER[a];
+#pragma unroll
+                for (int k = 0; k < RB; ++k)
+                    if ((a >> k) & 1) d += hR[k];
+                const int64_t x = base + l;
+                const double ur = double(v[a].x), ui = double(v[a].y);
+                const double tr = double(ar) + d * ur, ti = double(ai) + d * ui;
+                if (EPI == EPI_PARTIAL) {
+                    out[x] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
+                } else {
+                    const double hr = su * tr, hi = su * ti;
+                    out[x] = cmake<C>(hr, hi);
+                    if (EPI == EPI_LANCZOS) {
+                        const double vr = su * ur, vi = su * ui;
+                        red[0] += hr * hr + hi * hi;
+                        red[1] += vr * hr + vi * hi;
+                        red[2] += vr * hi - vi * hr;
                     }
                 }
             }
-            double d = St + P.ER[a];
-#pragma unroll
-            for (int k = 0; k < RB; ++k)
-                if ((a >> k) & 1) d += hR[k];
-            const int64_t x = base + l;
-            const double ur = double(v[a].x), ui = double(v[a].y);
-            const double tr = double(ar) + d * ur, ti = double(ai) + d * ui;
-            if (EPI == EPI_PARTIAL)
-                out[x] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
-            else
-                epilogue<C, EPI>(out, has_up ? upv : nullptr, x, su * tr, su * ti, su * ur, su * ui,
-                                 sp, red);
-        }
-        if (pb) {
-            asm volatile("barrier.cluster.arrive.release.aligned;\n"
-                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
-        } else {
-            __syncthreads();
         }
     }
+    // no CTA may leave while a sibling can still read its shared memory
+    if (pb) cluster_sync_all();
     write_partials<EPI>(A, red, red_scr);
 }
 
@@ -315,29 +380,69 @@ k_pass_low(const PassParams P, PassArgs A) {
 // j < 2^g (group bits hpos..hpos+g-1).  A cluster of 2^pbh CTAs holds the tiles that
 // differ in bits hpos+g..hpos+g+pbh-1.  The thread owns l = tid + a*NT;
 // x = base + (l & cmask) + ((l >> c) << hpos).
+// Tensor maps (8-byte elements, dims innermost first) describe the vector as
+//   hsplit 0: [2^c*K, 2^(hpos-c), 2^g, 2^pbh, rest]          (K = sizeof(C)/8)
+//   hsplit 1: [2^cm*K, 2^(c-cm), 2^(hpos-c), 2^g, rest]      (pbh = 0, wide chunks)
 template <typename C, int TB>
 __host__ __device__ constexpr size_t pass_high_smem() {
-    return (sizeof(C) << TB) + sizeof(double) * 8 * NRED;
+    return 4 * (sizeof(C) << TB) + 16 + sizeof(double) * 8 * NRED;
 }
 
-template <typename R, bool REALC, int TB, int RB, int EPI, bool INPL>
-__global__ void __launch_bounds__(1 << (TB - RB), 2)
-k_pass_high(const PassParams P, PassArgs A) {
+struct PassHighMaps {
+    CUtensorMap u;     // input vector
+    CUtensorMap part;  // partial sums of pass L
+};
+
+template <typename R, bool REALC, int TB, int RB, int EPI>
+__global__ void __launch_bounds__(1 << (TB - RB), 1)
+k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps M) {
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
+    constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
     if (A.gate && *A.gate != 0) return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    C *tile = reinterpret_cast<C *>(smem);
-    double *red_scr = reinterpret_cast<double *>(smem + (sizeof(C) << TB));
+    extern __shared__ __align__(128) unsigned char smem[];
+    C *tiles = reinterpret_cast<C *>(smem);  // [2][2^TB] values, then [2][2^TB] partials
+    C *parts = tiles + (2 << TB);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 4 * TILE_BYTES);
+    double *red_scr = reinterpret_cast<double *>(smem + 4 * TILE_BYTES + 16);
     const int n = P.n, c = P.hc, g = P.hg, hpos = P.hpos, pbh = P.pbh;
     const int tid = threadIdx.x;
     const int64_t cmask = (int64_t(1) << c) - 1;
     const int lowbits = hpos - c;
     const int64_t lowmask = (int64_t(1) << lowbits) - 1;
     const int cpos = hpos + g;  // first cluster bit
+    const uint32_t rank = pbh ? cluster_rank() : 0;
+    const int64_t nsuper = int64_t(1) << (n - c - g - pbh);
+    const int nclusters = gridDim.x >> pbh;
+    const int cid = blockIdx.x >> pbh;
+    const int rows = P.hbox_rows, nbox = (1 << g) / rows;
+    const uint32_t box_bytes = TILE_BYTES / nbox;
 
-    uint32_t rank = 0;
-    if (pbh) asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    // TMA loads of super-tile s into buffer buf (coordinates per the layouts above)
+    auto issue = [&](int64_t s, int buf) {
+        const int slo = (int)(s & lowmask);
+        const int shi = (int)(s >> lowbits);
+        mbar_expect_tx(&bars[buf], 2 * TILE_BYTES);
+        for (int b = 0; b < nbox; ++b) {
+            unsigned char *dv = reinterpret_cast<unsigned char *>(tiles + (buf << TB)) + b * box_bytes;
+            unsigned char *dp = reinterpret_cast<unsigned char *>(parts + (buf << TB)) + b * box_bytes;
+            if (P.hsplit == 0) {
+                tmap_load5(dv, &M.u, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
+                tmap_load5(dp, &M.part, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
+            } else {
+                tmap_load5(dv, &M.u, 0, 0, slo, b * rows, shi, &bars[buf]);
+                tmap_load5(dp, &M.part, 0, 0, slo, b * rows, shi, &bars[buf]);
+            }
+        }
+    };
+    if (tid == 0 && cid < nsuper) issue(cid, 0);
+
     uint32_t raddr[PBMAX_ALL];
     R ccr[PBMAX_ALL], cci[PBMAX_ALL];
 #pragma unroll
@@ -345,7 +450,7 @@ k_pass_high(const PassParams P, PassArgs A) {
         raddr[r] = 0;
         ccr[r] = cci[r] = R(0);
         if (r < pbh) {
-            raddr[r] = cluster_addr(tile, rank ^ (1u << r));
+            raddr[r] = cluster_addr(tiles, rank ^ (1u << r));
             const bool bit = (rank >> r) & 1;
             ccr[r] = bit ? Coef<R>::ure(P, cpos + r) : Coef<R>::dre(P, cpos + r);
             cci[r] = bit ? Coef<R>::uim(P, cpos + r) : Coef<R>::dim(P, cpos + r);
@@ -356,120 +461,88 @@ k_pass_high(const PassParams P, PassArgs A) {
 #pragma unroll
     for (int k = 0; k < SB; ++k) {
         const int p = hpos + k - c;
-        const bool ok = k >= c;
+        const bool okk = k >= c;
         const bool bit = (tid >> k) & 1;
-        cr_s[k] = ok ? (bit ? Coef<R>::ure(P, p) : Coef<R>::dre(P, p)) : R(0);
-        ci_s[k] = ok ? (bit ? Coef<R>::uim(P, p) : Coef<R>::dim(P, p)) : R(0);
+        cr_s[k] = okk ? (bit ? Coef<R>::ure(P, p) : Coef<R>::dre(P, p)) : R(0);
+        ci_s[k] = okk ? (bit ? Coef<R>::uim(P, p) : Coef<R>::dim(P, p)) : R(0);
     }
     // coefficients of the register bits (direction depends on the amplitude)
     R ur_r[RB], ui_r[RB], dr_r[RB], di_r[RB];
 #pragma unroll
     for (int k = 0; k < RB; ++k) {
         const int p = hpos + SB + k - c;
-        const bool ok = SB + k >= c;
-        ur_r[k] = ok ? Coef<R>::ure(P, p) : R(0);
-        ui_r[k] = ok ? Coef<R>::uim(P, p) : R(0);
-        dr_r[k] = ok ? Coef<R>::dre(P, p) : R(0);
-        di_r[k] = ok ? Coef<R>::dim(P, p) : R(0);
+        const bool okk = SB + k >= c;
+        ur_r[k] = okk ? Coef<R>::ure(P, p) : R(0);
+        ui_r[k] = okk ? Coef<R>::uim(P, p) : R(0);
+        dr_r[k] = okk ? Coef<R>::dre(P, p) : R(0);
+        di_r[k] = okk ? Coef<R>::dim(P, p) : R(0);
     }
     const double su = A.su_dev ? *A.su_dev : A.su;
-    const bool has_up = EPI == EPI_LANCZOS && A.up != nullptr;
-    const double sp = has_up ? (A.sp_dev ? *A.sp_dev : A.sp) : 0.0;
     const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
-    const C *__restrict__ upv = reinterpret_cast<const C *>(A.up);
     C *__restrict__ outp = reinterpret_cast<C *>(A.out);
-    // INPL: the partial sum is read from `out` itself (all loads of a tile are issued
-    // before its stores); otherwise from a separate buffer.
-    const C *__restrict__ partp = reinterpret_cast<const C *>(INPL ? A.out : A.part);
     double red[NRED];
 #pragma unroll
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
+    bool ok = true;
 
-    const int64_t nsuper = int64_t(1) << (n - c - g - pbh);
-    const int nclusters = gridDim.x >> pbh;
-    const int cid = blockIdx.x >> pbh;
-    for (int64_t s = cid; s < nsuper; s += nclusters) {
+    int it = 0;
+    for (int64_t s = cid; s < nsuper; s += nclusters, ++it) {
+        const int buf = it & 1;
         const int64_t base = ((s & lowmask) << c) | ((int64_t)rank << cpos) |
                              ((s >> lowbits) << (cpos + pbh));
-        C v[NA], part[INPL ? NA : 1];
-#pragma unroll
-        for (int a = 0; a < NA; ++a) {
-            const int64_t l = tid + a * NT;
-            const int64_t x = base + (l & cmask) + ((l >> c) << hpos);
-            v[a] = u[x];
-            if (INPL) part[a] = partp[x];
+        const C *tile = tiles + (buf << TB);
+        const C *ptile = parts + (buf << TB);
+        if (ok && !mbar_wait(&bars[buf], (it >> 1) & 1)) {
+            ok = false;
+            report_timeout(A);
         }
+        if (pbh) cluster_sync_all(); else __syncthreads();
+        if (tid == 0 && s + nclusters < nsuper && ok) issue(s + nclusters, buf ^ 1);
+        if (ok) {
+            const uint32_t boff = (uint32_t)buf * TILE_BYTES;
+            C v[NA];
 #pragma unroll
-        for (int a = 0; a < NA; ++a) tile[tid + a * NT] = v[a];
-        if (pbh) {
-            asm volatile("barrier.cluster.arrive.release.aligned;\n"
-                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
-        } else {
-            __syncthreads();
-        }
+            for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
 #pragma unroll
-        for (int a = 0; a < NA; ++a) {
-            const int l = tid + a * NT;
-            const int64_t x = base + (l & cmask) + ((int64_t)(l >> c) << hpos);
-            R ar = R(0), ai = R(0);
+            for (int a = 0; a < NA; ++a) {
+                const int l = tid + a * NT;
+                const int64_t x = base + (l & cmask) + ((int64_t)(l >> c) << hpos);
+                R ar = R(0), ai = R(0);
 #pragma unroll
-            for (int k = 0; k < SB; ++k) {
-                if (k < c) continue;  // uniform: chunk bits were applied by pass L
-                const C w = tile[l ^ (1 << k)];
-                if (REALC) {
-                    ar = fmar(cr_s[k], w.x, ar);
-                    ai = fmar(cr_s[k], w.y, ai);
-                } else {
-                    ar = fmar(cr_s[k], w.x, fmar(-ci_s[k], w.y, ar));
-                    ai = fmar(cr_s[k], w.y, fmar(ci_s[k], w.x, ai));
+                for (int k = 0; k < SB; ++k) {
+                    if (k < c) continue;  // uniform: chunk bits were applied by pass L
+                    flip_reg<R, REALC>(cr_s[k], ci_s[k], tile[l ^ (1 << k)], ar, ai);
+                }
+#pragma unroll
+                for (int k = 0; k < RB; ++k) {
+                    if (SB + k < c) continue;
+                    const bool bit = (a >> k) & 1;
+                    flip_reg<R, REALC>(bit ? ur_r[k] : dr_r[k], bit ? ui_r[k] : di_r[k],
+                                       v[a ^ (1 << k)], ar, ai);
+                }
+#pragma unroll
+                for (int r = 0; r < PBMAX_ALL; ++r)  // cluster bits: sibling CTA's tile
+                    if (r < pbh)
+                        flip_reg<R, REALC>(ccr[r], cci[r],
+                                           ld_cluster(raddr[r] + boff + (uint32_t)(l * sizeof(C)),
+                                                      (const C *)nullptr), ar, ai);
+                // bits beyond the tiles and the cluster (very large registers)
+                for (int p = P.xb_lo; p < P.xb_hi; ++p)
+                    flip_acc<R, REALC>(P, p, (x >> p) & 1, u[x ^ (int64_t(1) << p)], ar, ai);
+                const C pt = ptile[l];
+                const double hr = su * (double(pt.x) + double(ar));
+                const double hi = su * (double(pt.y) + double(ai));
+                outp[x] = cmake<C>(hr, hi);
+                if (EPI == EPI_LANCZOS) {
+                    const double vr = su * double(v[a].x), vi = su * double(v[a].y);
+                    red[0] += hr * hr + hi * hi;
+                    red[1] += vr * hr + vi * hi;
+                    red[2] += vr * hi - vi * hr;
                 }
             }
-#pragma unroll
-            for (int k = 0; k < RB; ++k) {
-                if (SB + k < c) continue;
-                const C w = v[a ^ (1 << k)];
-                const bool bit = (a >> k) & 1;
-                const R cr = bit ? ur_r[k] : dr_r[k];
-                if (REALC) {
-                    ar = fmar(cr, w.x, ar);
-                    ai = fmar(cr, w.y, ai);
-                } else {
-                    const R ci = bit ? ui_r[k] : di_r[k];
-                    ar = fmar(cr, w.x, fmar(-ci, w.y, ar));
-                    ai = fmar(cr, w.y, fmar(ci, w.x, ai));
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < PBMAX_ALL; ++r) {  // cluster bits: sibling CTA's tile
-                if (r < pbh) {
-                    const C w = ld_cluster(raddr[r] + (uint32_t)(l * sizeof(C)), (const C *)nullptr);
-                    if (REALC) {
-                        ar = fmar(ccr[r], w.x, ar);
-                        ai = fmar(ccr[r], w.y, ai);
-                    } else {
-                        ar = fmar(ccr[r], w.x, fmar(-cci[r], w.y, ar));
-                        ai = fmar(ccr[r], w.y, fmar(cci[r], w.x, ai));
-                    }
-                }
-            }
-            // bits beyond the tiles and the cluster (very large registers): global partner
-            for (int p = P.xb_lo; p < P.xb_hi; ++p) {
-                const C w = u[x ^ (int64_t(1) << p)];
-                flip_acc<R, REALC>(P, p, (x >> p) & 1, w, ar, ai);
-            }
-            const C pt = INPL ? part[INPL ? a : 0] : partp[x];
-            const double hr = su * (double(pt.x) + double(ar));
-            const double hi = su * (double(pt.y) + double(ai));
-            epilogue<C, EPI>(outp, has_up ? upv : nullptr, x, hr, hi, su * double(v[a].x),
-                             su * double(v[a].y), sp, red);
-        }
-        if (pbh) {
-            asm volatile("barrier.cluster.arrive.release.aligned;\n"
-                         "barrier.cluster.wait.acquire.aligned;" ::: "memory");
-        } else {
-            __syncthreads();
         }
     }
+    if (pbh) cluster_sync_all();
     write_partials<EPI>(A, red, red_scr);
 }
 

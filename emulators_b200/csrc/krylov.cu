@@ -28,16 +28,19 @@ int max_grid_blocks();
 
 constexpr int KMAX = 128;  // largest max_krylov_dim supported
 
-enum KStatus { KS_RUNNING = 0, KS_CONVERGED = 1, KS_HAPPY = 2, KS_MAXDIM = 3, KS_NONFINITE = 4 };
+// KS_TIMEOUT equals EMUSV_TIMEOUT: the streaming kernels write it on a bounded-wait timeout.
+enum KStatus { KS_RUNNING = 0, KS_CONVERGED = 1, KS_HAPPY = 2, KS_MAXDIM = 3, KS_NONFINITE = 4,
+               KS_TIMEOUT = EMUSV_TIMEOUT };
 
 struct KState {
     int status;
     int iters;
     int nvec;
-    int pad;
+    int kerr;  // error word of the streaming kernels (EMUSV_TIMEOUT), read by k_small
     double s0, err, outnorm2, pad2;
     double a_re[KMAX], a_im[KMAX];   // T_H[k][k]   = <v_k, H v_k> - b_k <v_k, v_{k-1}>
-    double b_re[KMAX], b_im[KMAX];   // T_H[k-1][k] = <v_{k-1}, H v_k>
+    double b_re[KMAX], b_im[KMAX];   // T_H[k-1][k] = ||w_{k-1}|| (= <v_{k-1}, H v_k> exactly)
+    double vv_re[KMAX + 2], vv_im[KMAX + 2];  // <v_k, v_{k-1}>: residual non-orthogonality
     double r[KMAX];                  // T_H[k+1][k] = ||w_k||
     double hn[KMAX];                 // ||H v_k||
     double scale[KMAX + 2];          // v_k = scale[k] * stored_k
@@ -110,12 +113,17 @@ __global__ void k_init(KState *ks, const double *partials, int nblocks) {
         ks->status = (isfinite(s0) && s0 > 0.0) ? KS_RUNNING : KS_NONFINITE;
         ks->iters = 0;
         ks->nvec = 0;
+        ks->kerr = 0;
         ks->err = 0.0;
         ks->outnorm2 = 0.0;
     }
 }
 
-// w <- w - b v_{j-1} - a v_j  (MGS order, krylov_exp.py:55-58), ||w||^2 partials.
+// Three-term recurrence w <- H v_j - b v_{j-1} - a v_j with b = ||w_{j-1}|| (which equals
+// <v_{j-1}, H v_j> in exact arithmetic) and a = <v_j, H v_j> - b <v_j, v_{j-1}>, the
+// modified Gram-Schmidt value of krylov_exp.py:55-58 with the measured non-orthogonality
+// <v_j, v_{j-1}> carried over from the previous iteration.  FP64 partials: ||w||^2 and
+// <v_j, w> (the next iteration's <v_{j+1}, v_j>).
 template <typename R>
 __global__ void __launch_bounds__(BLOCK)
 k_orth(KState *ks, int j, const double *part_h, int nb_h, const void *vj_, const void *vp_,
@@ -125,26 +133,22 @@ k_orth(KState *ks, int j, const double *part_h, int nb_h, const void *vj_, const
     __shared__ double red[(BLOCK / 32) * NRED];
     double s[NRED];
     sum_partials<NRED>(part_h, nb_h, NRED, s, red);
-    // s: 0 ||Hv||^2, 1-2 <v,Hv>, 3-4 <vp,Hv>, 5-6 <v,vp>
-    double br = 0.0, bi = 0.0;
-    if (j > 0) {
-        br = s[3];
-        bi = s[4];
-    }
-    // a = <v,Hv> - b <v,vp>
-    const double ar = s[1] - (j > 0 ? (br * s[5] - bi * s[6]) : 0.0);
-    const double ai = s[2] - (j > 0 ? (br * s[6] + bi * s[5]) : 0.0);
+    // s: 0 ||Hv||^2, 1-2 <v,Hv>
+    const double b = j > 0 ? ks->r[j - 1] : 0.0;
+    const double cr = j > 0 ? ks->vv_re[j] : 0.0, ci = j > 0 ? ks->vv_im[j] : 0.0;
+    const double ar = s[1] - b * cr;
+    const double ai = s[2] - b * ci;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ks->a_re[j] = ar;
         ks->a_im[j] = ai;
-        ks->b_re[j] = br;
-        ks->b_im[j] = bi;
+        ks->b_re[j] = b;
+        ks->b_im[j] = 0.0;
         ks->hn[j] = sqrt(s[0]);
     }
     const double sj = ks->scale[j];
     const double sp = j > 0 ? ks->scale[j - 1] : 0.0;
     // coefficients on the stored (unscaled) vectors
-    const double car = ar * sj, cai = ai * sj, cbr = br * sp, cbi = bi * sp;
+    const double car = ar * sj, cai = ai * sj, cb = b * sp;
     const C *vj = reinterpret_cast<const C *>(vj_);
     const C *vp = reinterpret_cast<const C *>(vp_);
     C *w = reinterpret_cast<C *>(w_);
@@ -158,12 +162,16 @@ k_orth(KState *ks, int j, const double *part_h, int nb_h, const void *vj_, const
         double wi = double(h.y) - (car * double(a.y) + cai * double(a.x));
         if (j > 0) {
             const C p = vp[x];
-            wr -= cbr * double(p.x) - cbi * double(p.y);
-            wi -= cbr * double(p.y) + cbi * double(p.x);
+            wr -= cb * double(p.x);
+            wi -= cb * double(p.y);
         }
         const C o = cmake<C>(wr, wi);
         w[x] = o;
-        acc[0] += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+        const double orr = double(o.x), oi = double(o.y);
+        const double vr = sj * double(a.x), vi = sj * double(a.y);
+        acc[0] += orr * orr + oi * oi;
+        acc[1] += vr * orr + vi * oi;  // <v_j, w>
+        acc[2] += vr * oi - vi * orr;
     }
     block_sum<NRED>(acc, red);
     if (threadIdx.x == 0)
@@ -275,13 +283,26 @@ __global__ void __launch_bounds__(32)
 k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp_tol,
         double norm_tol, int do_exp, int maxdim) {
     if (ks->status != KS_RUNNING) return;
+    if (ks->kerr) {  // a streaming kernel gave up on a bounded wait
+        if (threadIdx.x == 0) {
+            ks->status = KS_TIMEOUT;
+            ks->iters = j + 1;
+        }
+        return;
+    }
     __shared__ double2 d[KMAX + 2], up[KMAX + 2], lo[KMAX + 2];
     __shared__ double2 y[KMAX + 4], t[KMAX + 4], tn[KMAX + 4], acc[KMAX + 4];
     const int lane = threadIdx.x;
-    // deterministic sum of the ||w||^2 partials by one warp
-    double v = 0.0;
-    for (int b = lane; b < nb_o; b += 32) v += part_o[(i64)b * NRED];
+    // deterministic sums of the ||w||^2 and <v_j, w> partials by one warp
+    double v = 0.0, vr = 0.0, vi = 0.0;
+    for (int b = lane; b < nb_o; b += 32) {
+        v += part_o[(i64)b * NRED];
+        vr += part_o[(i64)b * NRED + 1];
+        vi += part_o[(i64)b * NRED + 2];
+    }
     v = warp_sum(v);
+    vr = warp_sum(vr);
+    vi = warp_sum(vi);
     const double r = sqrt(v);
     const double adt = fabs(dt);
     const double n2 = adt * r;  // ||w|| of the operator -i dt H (krylov_exp.py:60)
@@ -293,7 +314,11 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
         }
         return;
     }
-    if (lane == 0) ks->r[j] = r;
+    if (lane == 0) {
+        ks->r[j] = r;
+        ks->vv_re[j + 1] = vr / r;  // <v_{j+1}, v_j> = conj(<v_j, w>) / ||w||
+        ks->vv_im[j + 1] = -vi / r;
+    }
     const bool happy = n2 < norm_tol;  // krylov_exp.py:63
     if (!happy && !do_exp) {
         if (lane == 0) ks->scale[j + 1] = 1.0 / r;
@@ -552,12 +577,12 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
         HpsiArgs A = {};
         A.u = stored(j);
         A.su_dev = &W.ks->scale[j];
-        A.up = j > 0 ? stored(j - 1) : nullptr;
-        A.sp_dev = j > 0 ? &W.ks->scale[j - 1] : nullptr;
+        A.up = nullptr;  // b comes from the previous norm (see k_orth)
         A.out = const_cast<void *>(stored(j + 1));
         A.partials = W.part_h;
         A.tile_bits = hpsi_tile_bits(nqubits);
         A.gate = &W.ks->status;
+        A.err = &W.ks->kerr;
         A.part_buf = part_vec;
         int gh = 0;
         int st = launch_hpsi(dtype, HP_LANCZOS, P, A, max_grid_blocks(), s, &gh);
@@ -593,6 +618,10 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
     if (status == KS_RUNNING) {
         int st = read_status(W.ks, s, &status);
         if (st) return st;
+    }
+    if (status == KS_TIMEOUT) {
+        if (info) memset(info, 0, sizeof(*info));
+        return EMUSV_TIMEOUT;
     }
     if (status == KS_NONFINITE || status == KS_RUNNING) {
         if (info) memset(info, 0, sizeof(*info));

@@ -57,6 +57,10 @@ typedef struct {
 /* Library identification: returns the sm architecture compiled in (e.g. 100). */
 int emusv_build_arch(void);
 const char *emusv_status_string(int status);
+/* Reads and clears the device error word of calls that have no status output of their
+ * own (emusv_hpsi): EMUSV_OK, or EMUSV_TIMEOUT if a bounded device-side wait gave up.
+ * Synchronises the stream. */
+int emusv_device_error(void *stream);
 
 /* Diagonal of H, float64 [2^n] on the device.
  * Replaces RydbergHamiltonian._create_diagonal (emu_sv/hamiltonian.py:139-162). */
