@@ -121,10 +121,34 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
     }
 }
 
-template <typename R, bool REALC, int EPI_L, int EPI_H>
+// Kernel pointers by run-time layout (template arguments are compile-time).
+template <typename R, bool REALC, int TB, int RB, int EPI>
+static auto low_kernel(int pb) -> decltype(&k_pass_low<R, REALC, TB, RB, EPI, 0>) {
+    switch (pb) {
+    case 0: return k_pass_low<R, REALC, TB, RB, EPI, 0>;
+    case 1: return k_pass_low<R, REALC, TB, RB, EPI, 1>;
+    case 2: return k_pass_low<R, REALC, TB, RB, EPI, 2>;
+    default: return k_pass_low<R, REALC, TB, RB, EPI, 3>;
+    }
+}
+template <typename R, bool REALC, int TB, int RB, int EPI, int CMIN>
+static auto high_kernel(bool hot, int pbh) -> decltype(&k_pass_high<R, REALC, TB, RB, EPI, 0, 0>) {
+    if (hot) {
+        switch (pbh) {
+        case 0: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0>;
+        case 1: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 1>;
+        case 2: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 2>;
+        default: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 3>;
+        }
+    }
+    return pbh == 0 ? k_pass_high<R, REALC, TB, RB, EPI, 0, 0> : k_pass_high<R, REALC, TB, RB, EPI, 0, 3>;
+}
+
+template <typename R, bool REALC, int EPI_H>
 static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
+    constexpr int CMIN = PassShape<R>::CMIN;
     const int n = H.n;
     PassParams P;
     fill_params(H, TB, RB, &P);
@@ -133,7 +157,7 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     P.pb = pb;
     const int rem = n - TB - pb;
     int g = rem;
-    if (g > TB - PassShape<R>::CMIN) g = TB - PassShape<R>::CMIN;
+    if (g > TB - CMIN) g = TB - CMIN;
     int pbh = rem - g;
     if (pbh > PassShape<R>::PBHMAX) pbh = PassShape<R>::PBHMAX;
     P.hg = g;
@@ -149,22 +173,25 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     P.hsplit = ((1 << P.hc) * K > 256) ? 1 : 0;
     P.hbox_rows = g > 8 ? 256 : (1 << g);
     if (P.hsplit && pbh) return EMUSV_BAD_ARGUMENT;  // not a layout the sizes above produce
+    const bool hot = P.hc == CMIN && P.xb_lo == n;
+    if (!hot && pbh != 0 && pbh != 3) return EMUSV_BAD_ARGUMENT;
 
     PassArgs A = {};
     A.u = HA.u;
     A.su_dev = HA.su_dev;
     A.su = HA.su;
-    A.out = rem > 0 ? (HA.part_buf ? HA.part_buf : HA.out) : HA.out;  // pass L output
+    A.out = rem > 0 ? HA.part_buf : HA.out;  // pass L output
     A.partials = HA.partials;
     A.gate = HA.gate;
     A.err = HA.err;
-    if (rem > 0 && !HA.part_buf) return EMUSV_BAD_ARGUMENT;  // pass H needs its own buffer
+    if (rem > 0 && !HA.part_buf) return EMUSV_BAD_ARGUMENT;  // pass H needs the partial buffer
 
     const size_t smem_l = pass_low_smem<C, TB>(), smem_h = pass_high_smem<C, TB>();
     const int nsm = sm_count();
     // ---- pass L
     {
-        auto kern = (rem > 0) ? k_pass_low<R, REALC, TB, RB, EPI_L> : k_pass_low<R, REALC, TB, RB, EPI_H>;
+        auto kern = (rem > 0) ? low_kernel<R, REALC, TB, RB, EPI_PARTIAL>(pb)
+                              : low_kernel<R, REALC, TB, RB, EPI_H>(pb);
         EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_l));
         int per_sm = 0;
         EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem_l));
@@ -202,7 +229,7 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
             return EMUSV_CUDA_ERROR;
         PassArgs AH = A;
         AH.out = HA.out;
-        auto kern = k_pass_high<R, REALC, TB, RB, EPI_H>;
+        auto kern = high_kernel<R, REALC, TB, RB, EPI_H, CMIN>(hot, pbh);
         EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_h));
         int per_sm = 0;
         EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem_h));
@@ -240,17 +267,17 @@ int launch_hpsi_passes(int dtype, int mode, const HamParams &H, const HpsiArgs &
     const bool lz = mode == HP_LANCZOS;
     if (dtype == EMUSV_C64) {
         if (H.real_coef)
-            return lz ? run_passes<float, true, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
-                      : run_passes<float, true, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
-        return lz ? run_passes<float, false, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
-                  : run_passes<float, false, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
+            return lz ? run_passes<float, true, EPI_LANCZOS>(H, A, s, grid_out)
+                      : run_passes<float, true, EPI_STORE>(H, A, s, grid_out);
+        return lz ? run_passes<float, false, EPI_LANCZOS>(H, A, s, grid_out)
+                  : run_passes<float, false, EPI_STORE>(H, A, s, grid_out);
     }
     if (dtype == EMUSV_C128) {
         if (H.real_coef)
-            return lz ? run_passes<double, true, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
-                      : run_passes<double, true, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
-        return lz ? run_passes<double, false, EPI_PARTIAL, EPI_LANCZOS>(H, A, s, grid_out)
-                  : run_passes<double, false, EPI_PARTIAL, EPI_STORE>(H, A, s, grid_out);
+            return lz ? run_passes<double, true, EPI_LANCZOS>(H, A, s, grid_out)
+                      : run_passes<double, true, EPI_STORE>(H, A, s, grid_out);
+        return lz ? run_passes<double, false, EPI_LANCZOS>(H, A, s, grid_out)
+                  : run_passes<double, false, EPI_STORE>(H, A, s, grid_out);
     }
     return EMUSV_BAD_ARGUMENT;
 }

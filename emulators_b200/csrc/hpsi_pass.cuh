@@ -78,12 +78,12 @@ __device__ __forceinline__ uint32_t cluster_addr(const void *smem_ptr, uint32_t 
 }
 __device__ __forceinline__ float2 ld_cluster(uint32_t addr, const float2 *) {
     float2 v;
-    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
     return v;
 }
 __device__ __forceinline__ double2 ld_cluster(uint32_t addr, const double2 *) {
     double2 v;
-    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr));
     return v;
 }
 __device__ __forceinline__ void cluster_sync_all() {
@@ -156,31 +156,64 @@ template <> struct Coef<double> {
     __device__ static double dim(const PassParams &P, int p) { return P.ddn_im[p]; }
 };
 
+// Complex accumulator of the flip terms.  complex64 uses Blackwell's packed FP32x2 FMA
+// (one instruction per real coefficient and amplitude); complex128 uses two DFMA.
+__device__ __forceinline__ unsigned long long pk2(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+template <typename R> struct Acc;
+template <> struct Acc<float> {
+    unsigned long long a = 0ull;
+    __device__ __forceinline__ void real(float c, const float2 &w) { a = fma2(pk2(c, c), pk2(w.x, w.y), a); }
+    __device__ __forceinline__ void cplx(float cr, float ci, const float2 &w) {
+        a = fma2(pk2(cr, cr), pk2(w.x, w.y), a);
+        a = fma2(pk2(-ci, ci), pk2(w.y, w.x), a);
+    }
+    __device__ __forceinline__ double re() const { return double(upk2(a).x); }
+    __device__ __forceinline__ double im() const { return double(upk2(a).y); }
+};
+template <> struct Acc<double> {
+    double r = 0.0, i = 0.0;
+    __device__ __forceinline__ void real(double c, const double2 &w) {
+        r = fma(c, w.x, r);
+        i = fma(c, w.y, i);
+    }
+    __device__ __forceinline__ void cplx(double cr, double ci, const double2 &w) {
+        r = fma(cr, w.x, fma(-ci, w.y, r));
+        i = fma(cr, w.y, fma(ci, w.x, i));
+    }
+    __device__ __forceinline__ double re() const { return r; }
+    __device__ __forceinline__ double im() const { return i; }
+};
+
 // acc += c * w  with c = up (bit==1) or dn (bit==0) of bit position p (compile-time p:
-// the coefficient is a constant-bank operand).
+// the coefficient comes from the constant bank).
 template <typename R, bool REALC, typename C>
-__device__ __forceinline__ void flip_acc(const PassParams &P, int p, bool bit, const C &w, R &ar,
-                                         R &ai) {
+__device__ __forceinline__ void flip_acc(const PassParams &P, int p, bool bit, const C &w, Acc<R> &acc) {
     if (REALC) {
-        const R c = Coef<R>::ure(P, p);
-        ar = fmar(c, w.x, ar);
-        ai = fmar(c, w.y, ai);
+        acc.real(Coef<R>::ure(P, p), w);
     } else {
-        const R cr = bit ? Coef<R>::ure(P, p) : Coef<R>::dre(P, p);
-        const R ci = bit ? Coef<R>::uim(P, p) : Coef<R>::dim(P, p);
-        ar = fmar(cr, w.x, fmar(-ci, w.y, ar));
-        ai = fmar(cr, w.y, fmar(ci, w.x, ai));
+        acc.cplx(bit ? Coef<R>::ure(P, p) : Coef<R>::dre(P, p), bit ? Coef<R>::uim(P, p) : Coef<R>::dim(P, p), w);
     }
 }
 template <typename R, bool REALC, typename C>
-__device__ __forceinline__ void flip_reg(R cr, R ci, const C &w, R &ar, R &ai) {
-    if (REALC) {
-        ar = fmar(cr, w.x, ar);
-        ai = fmar(cr, w.y, ai);
-    } else {
-        ar = fmar(cr, w.x, fmar(-ci, w.y, ar));
-        ai = fmar(cr, w.y, fmar(ci, w.x, ai));
-    }
+__device__ __forceinline__ void flip_reg(R cr, R ci, const C &w, Acc<R> &acc) {
+    if (REALC) acc.real(cr, w);
+    else acc.cplx(cr, ci, w);
 }
 
 template <int EPI>
@@ -206,7 +239,7 @@ __host__ __device__ constexpr size_t pass_low_smem() {
     return 2 * (sizeof(C) << TB) + 16 + sizeof(double) * (MAXQ * UPAD + MAXQ + 2 * 64 + 8 * NRED);
 }
 
-template <typename R, bool REALC, int TB, int RB, int EPI>
+template <typename R, bool REALC, int TB, int RB, int EPI, int PB>
 __global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_low(const PassParams P, PassArgs A) {
     typedef typename cvec<R>::T C;
@@ -221,13 +254,13 @@ k_pass_low(const PassParams P, PassArgs A) {
     double *scal = fld + MAXQ;       // [2][64]: crossT[SB] crossR[RB] eh
     double *red_scr = scal + 2 * 64;
 
-    const int n = P.n, pb = P.pb;
+    const int n = P.n;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const uint32_t rank = pb ? cluster_rank() : 0;
-    const int64_t nsuper = int64_t(1) << (n - TB - pb);
-    const int nclusters = gridDim.x >> pb;
-    const int cid = blockIdx.x >> pb;
+    const uint32_t rank = PB ? cluster_rank() : 0;
+    const int64_t nsuper = int64_t(1) << (n - TB - PB);
+    const int nclusters = gridDim.x >> PB;
+    const int cid = blockIdx.x >> PB;
     const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
     C *__restrict__ out = reinterpret_cast<C *>(A.out);
 
@@ -242,7 +275,7 @@ k_pass_low(const PassParams P, PassArgs A) {
     // prologue: first tile of this CTA into buffer 0
     if (tid == 0 && cid < nsuper) {
         mbar_expect_tx(&bars[0], TILE_BYTES);
-        bulk_load(tiles, u + ((((int64_t)cid << pb) | rank) << TB), TILE_BYTES, &bars[0]);
+        bulk_load(tiles, u + ((((int64_t)cid << PB) | rank) << TB), TILE_BYTES, &bars[0]);
     }
 
     // per-thread constants: energy of the thread bits and thread x register crosses
@@ -266,18 +299,14 @@ k_pass_low(const PassParams P, PassArgs A) {
         fR[k] = sacc;
     }
     // sibling CTAs and the coefficients of the cluster bits (fixed per CTA)
-    uint32_t raddr[PBMAX_ALL];
-    R ccr[PBMAX_ALL], cci[PBMAX_ALL];
+    uint32_t raddr[PB > 0 ? PB : 1];
+    R ccr[PB > 0 ? PB : 1], cci[PB > 0 ? PB : 1];
 #pragma unroll
-    for (int r = 0; r < PBMAX_ALL; ++r) {
-        raddr[r] = 0;
-        ccr[r] = cci[r] = R(0);
-        if (r < pb) {
-            raddr[r] = cluster_addr(tiles, rank ^ (1u << r));
-            const bool bit = (rank >> r) & 1;
-            ccr[r] = bit ? Coef<R>::ure(P, TB + r) : Coef<R>::dre(P, TB + r);
-            cci[r] = bit ? Coef<R>::uim(P, TB + r) : Coef<R>::dim(P, TB + r);
-        }
+    for (int r = 0; r < PB; ++r) {
+        raddr[r] = cluster_addr(tiles, rank ^ (1u << r)) + (uint32_t)(tid * sizeof(C));
+        const bool bit = (rank >> r) & 1;
+        ccr[r] = bit ? Coef<R>::ure(P, TB + r) : Coef<R>::dre(P, TB + r);
+        cci[r] = bit ? Coef<R>::uim(P, TB + r) : Coef<R>::dim(P, TB + r);
     }
     const double su = A.su_dev ? *A.su_dev : A.su;
     double red[NRED];
@@ -288,7 +317,7 @@ k_pass_low(const PassParams P, PassArgs A) {
     int it = 0;
     for (int64_t s = cid; s < nsuper; s += nclusters, ++it) {
         const int buf = it & 1;
-        const int64_t base = ((s << pb) | rank) << TB;
+        const int64_t base = ((s << PB) | rank) << TB;
         C *tile = tiles + (buf << TB);
         double *sc = scal + buf * 64;
         if (warp == 0) {
@@ -314,9 +343,9 @@ k_pass_low(const PassParams P, PassArgs A) {
             report_timeout(A);
         }
         // every CTA of the cluster has its tile; siblings are done with buffer buf^1
-        if (pb) cluster_sync_all(); else __syncthreads();
+        if (PB) cluster_sync_all(); else __syncthreads();
         if (tid == 0 && s + nclusters < nsuper && ok) {
-            const int64_t nb = (((s + nclusters) << pb) | rank) << TB;
+            const int64_t nb = (((s + nclusters) << PB) | rank) << TB;
             mbar_expect_tx(&bars[buf ^ 1], TILE_BYTES);
             bulk_load(tiles + ((buf ^ 1) << TB), u + nb, TILE_BYTES, &bars[buf ^ 1]);
         }
@@ -332,34 +361,33 @@ k_pass_low(const PassParams P, PassArgs A) {
             C v[NA];
 #pragma unroll
             for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
+            C *out_t = out + base + tid;
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
                 const int l = tid + a * NT;
-                R ar = R(0), ai = R(0);
+                Acc<R> acc;
 #pragma unroll
                 for (int k = 0; k < SB; ++k)  // thread bits: partner in shared memory
-                    flip_acc<R, REALC>(P, k, (tid >> k) & 1, tile[l ^ (1 << k)], ar, ai);
+                    flip_acc<R, REALC>(P, k, (tid >> k) & 1, tile[l ^ (1 << k)], acc);
 #pragma unroll
                 for (int k = 0; k < RB; ++k)  // register bits
-                    flip_acc<R, REALC>(P, SB + k, (a >> k) & 1, v[a ^ (1 << k)], ar, ai);
+                    flip_acc<R, REALC>(P, SB + k, (a >> k) & 1, v[a ^ (1 << k)], acc);
 #pragma unroll
-                for (int r = 0; r < PBMAX_ALL; ++r)  // cluster bits: sibling CTA's tile
-                    if (r < pb)
-                        flip_reg<R, REALC>(ccr[r], cci[r],
-                                           ld_cluster(raddr[r] + boff + (uint32_t)(l * sizeof(C)),
-                                                      (const C *)nullptr), ar, ai);
+                for (int r = 0; r < PB; ++r)  // cluster bits: sibling CTA's tile
+                    flip_reg<R, REALC>(ccr[r], cci[r],
+                                       ld_cluster(raddr[r] + boff + (uint32_t)(a * NT * sizeof(C)),
+                                                  (const C *)nullptr), acc);
                 double d = St + P.ER[a];
 #pragma unroll
                 for (int k = 0; k < RB; ++k)
                     if ((a >> k) & 1) d += hR[k];
-                const int64_t x = base + l;
                 const double ur = double(v[a].x), ui = double(v[a].y);
-                const double tr = double(ar) + d * ur, ti = double(ai) + d * ui;
+                const double tr = acc.re() + d * ur, ti = acc.im() + d * ui;
                 if (EPI == EPI_PARTIAL) {
-                    out[x] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
+                    out_t[a * NT] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
                 } else {
                     const double hr = su * tr, hi = su * ti;
-                    out[x] = cmake<C>(hr, hi);
+                    out_t[a * NT] = cmake<C>(hr, hi);
                     if (EPI == EPI_LANCZOS) {
                         const double vr = su * ur, vi = su * ui;
                         red[0] += hr * hr + hi * hi;
@@ -371,7 +399,7 @@ k_pass_low(const PassParams P, PassArgs A) {
         }
     }
     // no CTA may leave while a sibling can still read its shared memory
-    if (pb) cluster_sync_all();
+    if (PB) cluster_sync_all();
     write_partials<EPI>(A, red, red_scr);
 }
 
@@ -393,7 +421,8 @@ struct PassHighMaps {
     CUtensorMap part;  // partial sums of pass L
 };
 
-template <typename R, bool REALC, int TB, int RB, int EPI>
+// CT: chunk bits c at compile time (0: taken from P at run time); PBH: cluster bits.
+template <typename R, bool REALC, int TB, int RB, int EPI, int CT, int PBH>
 __global__ void __launch_bounds__(1 << (TB - RB), 1)
 k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps M) {
     typedef typename cvec<R>::T C;
@@ -405,16 +434,16 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     C *parts = tiles + (2 << TB);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 4 * TILE_BYTES);
     double *red_scr = reinterpret_cast<double *>(smem + 4 * TILE_BYTES + 16);
-    const int n = P.n, c = P.hc, g = P.hg, hpos = P.hpos, pbh = P.pbh;
+    const int n = P.n, c = CT ? CT : P.hc, g = TB - c, hpos = P.hpos;
     const int tid = threadIdx.x;
     const int64_t cmask = (int64_t(1) << c) - 1;
     const int lowbits = hpos - c;
     const int64_t lowmask = (int64_t(1) << lowbits) - 1;
     const int cpos = hpos + g;  // first cluster bit
-    const uint32_t rank = pbh ? cluster_rank() : 0;
-    const int64_t nsuper = int64_t(1) << (n - c - g - pbh);
-    const int nclusters = gridDim.x >> pbh;
-    const int cid = blockIdx.x >> pbh;
+    const uint32_t rank = PBH ? cluster_rank() : 0;
+    const int64_t nsuper = int64_t(1) << (n - c - g - PBH);
+    const int nclusters = gridDim.x >> PBH;
+    const int cid = blockIdx.x >> PBH;
     const int rows = P.hbox_rows, nbox = (1 << g) / rows;
     const uint32_t box_bytes = TILE_BYTES / nbox;
 
@@ -443,18 +472,14 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     };
     if (tid == 0 && cid < nsuper) issue(cid, 0);
 
-    uint32_t raddr[PBMAX_ALL];
-    R ccr[PBMAX_ALL], cci[PBMAX_ALL];
+    uint32_t raddr[PBH > 0 ? PBH : 1];
+    R ccr[PBH > 0 ? PBH : 1], cci[PBH > 0 ? PBH : 1];
 #pragma unroll
-    for (int r = 0; r < PBMAX_ALL; ++r) {
-        raddr[r] = 0;
-        ccr[r] = cci[r] = R(0);
-        if (r < pbh) {
-            raddr[r] = cluster_addr(tiles, rank ^ (1u << r));
-            const bool bit = (rank >> r) & 1;
-            ccr[r] = bit ? Coef<R>::ure(P, cpos + r) : Coef<R>::dre(P, cpos + r);
-            cci[r] = bit ? Coef<R>::uim(P, cpos + r) : Coef<R>::dim(P, cpos + r);
-        }
+    for (int r = 0; r < PBH; ++r) {
+        raddr[r] = cluster_addr(tiles, rank ^ (1u << r)) + (uint32_t)(tid * sizeof(C));
+        const bool bit = (rank >> r) & 1;
+        ccr[r] = bit ? Coef<R>::ure(P, cpos + r) : Coef<R>::dre(P, cpos + r);
+        cci[r] = bit ? Coef<R>::uim(P, cpos + r) : Coef<R>::dim(P, cpos + r);
     }
     // coefficients of the shared-memory bits (direction fixed by the thread's own bits)
     R cr_s[SB], ci_s[SB];
@@ -484,19 +509,22 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
 #pragma unroll
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
     bool ok = true;
+    // x offset of amplitude a of this thread: (tid & cmask) + ((tid + a*NT) >> c) << hpos
+    const int64_t xt = (tid & cmask) + ((int64_t)(tid >> c) << hpos);
+    const int ash = hpos + SB - c;  // when c <= SB: x offset of a is a << ash
 
     int it = 0;
     for (int64_t s = cid; s < nsuper; s += nclusters, ++it) {
         const int buf = it & 1;
         const int64_t base = ((s & lowmask) << c) | ((int64_t)rank << cpos) |
-                             ((s >> lowbits) << (cpos + pbh));
+                             ((s >> lowbits) << (cpos + PBH));
         const C *tile = tiles + (buf << TB);
         const C *ptile = parts + (buf << TB);
         if (ok && !mbar_wait(&bars[buf], (it >> 1) & 1)) {
             ok = false;
             report_timeout(A);
         }
-        if (pbh) cluster_sync_all(); else __syncthreads();
+        if (PBH) cluster_sync_all(); else __syncthreads();
         if (tid == 0 && s + nclusters < nsuper && ok) issue(s + nclusters, buf ^ 1);
         if (ok) {
             const uint32_t boff = (uint32_t)buf * TILE_BYTES;
@@ -506,32 +534,33 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
                 const int l = tid + a * NT;
-                const int64_t x = base + (l & cmask) + ((int64_t)(l >> c) << hpos);
-                R ar = R(0), ai = R(0);
+                const int64_t x = (c <= SB) ? base + xt + ((int64_t)a << ash)
+                                            : base + (l & cmask) + ((int64_t)(l >> c) << hpos);
+                Acc<R> acc;
 #pragma unroll
                 for (int k = 0; k < SB; ++k) {
-                    if (k < c) continue;  // uniform: chunk bits were applied by pass L
-                    flip_reg<R, REALC>(cr_s[k], ci_s[k], tile[l ^ (1 << k)], ar, ai);
+                    if (k < c) continue;  // chunk bits were applied by pass L
+                    flip_reg<R, REALC>(cr_s[k], ci_s[k], tile[l ^ (1 << k)], acc);
                 }
 #pragma unroll
                 for (int k = 0; k < RB; ++k) {
                     if (SB + k < c) continue;
                     const bool bit = (a >> k) & 1;
                     flip_reg<R, REALC>(bit ? ur_r[k] : dr_r[k], bit ? ui_r[k] : di_r[k],
-                                       v[a ^ (1 << k)], ar, ai);
+                                       v[a ^ (1 << k)], acc);
                 }
 #pragma unroll
-                for (int r = 0; r < PBMAX_ALL; ++r)  // cluster bits: sibling CTA's tile
-                    if (r < pbh)
-                        flip_reg<R, REALC>(ccr[r], cci[r],
-                                           ld_cluster(raddr[r] + boff + (uint32_t)(l * sizeof(C)),
-                                                      (const C *)nullptr), ar, ai);
-                // bits beyond the tiles and the cluster (very large registers)
-                for (int p = P.xb_lo; p < P.xb_hi; ++p)
-                    flip_acc<R, REALC>(P, p, (x >> p) & 1, u[x ^ (int64_t(1) << p)], ar, ai);
+                for (int r = 0; r < PBH; ++r)  // cluster bits: sibling CTA's tile
+                    flip_reg<R, REALC>(ccr[r], cci[r],
+                                       ld_cluster(raddr[r] + boff + (uint32_t)(a * NT * sizeof(C)),
+                                                  (const C *)nullptr), acc);
+                if (CT == 0) {  // very large registers: bits beyond tiles and cluster
+                    for (int p = P.xb_lo; p < P.xb_hi; ++p)
+                        flip_acc<R, REALC>(P, p, (x >> p) & 1, u[x ^ (int64_t(1) << p)], acc);
+                }
                 const C pt = ptile[l];
-                const double hr = su * (double(pt.x) + double(ar));
-                const double hi = su * (double(pt.y) + double(ai));
+                const double hr = su * (double(pt.x) + acc.re());
+                const double hi = su * (double(pt.y) + acc.im());
                 outp[x] = cmake<C>(hr, hi);
                 if (EPI == EPI_LANCZOS) {
                     const double vr = su * double(v[a].x), vi = su * double(v[a].y);
@@ -542,7 +571,7 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
             }
         }
     }
-    if (pbh) cluster_sync_all();
+    if (PBH) cluster_sync_all();
     write_partials<EPI>(A, red, red_scr);
 }
 
