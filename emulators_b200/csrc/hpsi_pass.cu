@@ -118,6 +118,7 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
                 if ((a >> k2) & 1) e += H.U[(SB + k) * MAXQ + SB + k2];
         }
         P->ER[a] = e;
+        P->ERf[a] = (float)e;
     }
 }
 

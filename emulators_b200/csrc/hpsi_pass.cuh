@@ -27,6 +27,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace emusv {
@@ -48,6 +50,7 @@ struct PassParams {
     double field[MAXQ];
     double U[MAXQ * MAXQ];
     double ER[32];  // energies of the register-bit patterns of pass L (fields + pairs)
+    float ERf[32];  // the same, rounded to FP32 (complex64 path)
     int pb;         // pass L: cluster bits (cluster size 2^pb)
     int hc, hg;     // pass H: chunk bits c and group bits g
     int hpos;       // pass H: global position of the first group bit
@@ -185,6 +188,8 @@ template <> struct Acc<float> {
     }
     __device__ __forceinline__ double re() const { return double(upk2(a).x); }
     __device__ __forceinline__ double im() const { return double(upk2(a).y); }
+    // a += d * w (real d)
+    __device__ __forceinline__ void diag(float d, const float2 &w) { a = fma2(pk2(d, d), pk2(w.x, w.y), a); }
 };
 template <> struct Acc<double> {
     double r = 0.0, i = 0.0;
@@ -246,10 +251,10 @@ k_pass_low(const PassParams P, PassArgs A) {
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
     constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
     if (A.gate && *A.gate != 0) return;
-    extern __shared__ __align__(128) unsigned char smem[];
-    C *tiles = reinterpret_cast<C *>(smem);                      // [2][2^TB]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * TILE_BYTES);  // [2]
-    double *Ush = reinterpret_cast<double *>(smem + 2 * TILE_BYTES + 16);
+    extern __shared__ __align__(128) unsigned char smem_pass[];
+    C *tiles = reinterpret_cast<C *>(smem_pass);                      // [2][2^TB]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 2 * TILE_BYTES);  // [2]
+    double *Ush = reinterpret_cast<double *>(smem_pass + 2 * TILE_BYTES + 16);
     double *fld = Ush + MAXQ * UPAD;
     double *scal = fld + MAXQ;       // [2][64]: crossT[SB] crossR[RB] eh
     double *red_scr = scal + 2 * 64;
@@ -309,6 +314,7 @@ k_pass_low(const PassParams P, PassArgs A) {
         cci[r] = bit ? Coef<R>::uim(P, TB + r) : Coef<R>::dim(P, TB + r);
     }
     const double su = A.su_dev ? *A.su_dev : A.su;
+    const float suf = float(su);
     double red[NRED];
 #pragma unroll
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
@@ -357,6 +363,12 @@ k_pass_low(const PassParams P, PassArgs A) {
             double hR[RB];
 #pragma unroll
             for (int k = 0; k < RB; ++k) hR[k] = fR[k] + sc[SB + k];
+            // FP32 copies (complex64 path): one rounding per tile and thread
+            const float Stf = float(St);
+            float hRf[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) hRf[k] = float(hR[k]);
+            float rf[3] = {0.f, 0.f, 0.f};
             const uint32_t boff = (uint32_t)buf * TILE_BYTES;
             C v[NA];
 #pragma unroll
@@ -377,23 +389,52 @@ k_pass_low(const PassParams P, PassArgs A) {
                     flip_reg<R, REALC>(ccr[r], cci[r],
                                        ld_cluster(raddr[r] + boff + (uint32_t)(a * NT * sizeof(C)),
                                                   (const C *)nullptr), acc);
-                double d = St + P.ER[a];
+                if constexpr (std::is_same<R, float>::value) {
+                    // complex64: all per-amplitude arithmetic in FP32 / packed FP32x2 (the
+                    // FP64 <-> FP32 conversions would bound the kernel on the XU pipe)
+                    float d = Stf + P.ERf[a];
 #pragma unroll
-                for (int k = 0; k < RB; ++k)
-                    if ((a >> k) & 1) d += hR[k];
-                const double ur = double(v[a].x), ui = double(v[a].y);
-                const double tr = acc.re() + d * ur, ti = acc.im() + d * ui;
-                if (EPI == EPI_PARTIAL) {
-                    out_t[a * NT] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
-                } else {
-                    const double hr = su * tr, hi = su * ti;
-                    out_t[a * NT] = cmake<C>(hr, hi);
-                    if (EPI == EPI_LANCZOS) {
-                        const double vr = su * ur, vi = su * ui;
-                        red[0] += hr * hr + hi * hi;
-                        red[1] += vr * hr + vi * hi;
-                        red[2] += vr * hi - vi * hr;
+                    for (int k = 0; k < RB; ++k)
+                        if ((a >> k) & 1) d += hRf[k];
+                    acc.diag(d, v[a]);
+                    const float2 t = upk2(acc.a);
+                    if (EPI == EPI_PARTIAL) {
+                        out_t[a * NT] = t;  // unscaled partial; pass H applies su
+                    } else {
+                        const float2 h = make_float2(suf * t.x, suf * t.y);
+                        out_t[a * NT] = h;
+                        if (EPI == EPI_LANCZOS) {
+                            rf[0] = fmaf(h.x, h.x, fmaf(h.y, h.y, rf[0]));
+                            rf[1] = fmaf(v[a].x, h.x, fmaf(v[a].y, h.y, rf[1]));
+                            rf[2] = fmaf(v[a].x, h.y, fmaf(-v[a].y, h.x, rf[2]));
+                        }
                     }
+                } else {
+                    double d = St + P.ER[a];
+#pragma unroll
+                    for (int k = 0; k < RB; ++k)
+                        if ((a >> k) & 1) d += hR[k];
+                    const double ur = double(v[a].x), ui = double(v[a].y);
+                    const double tr = acc.re() + d * ur, ti = acc.im() + d * ui;
+                    if (EPI == EPI_PARTIAL) {
+                        out_t[a * NT] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
+                    } else {
+                        const double hr = su * tr, hi = su * ti;
+                        out_t[a * NT] = cmake<C>(hr, hi);
+                        if (EPI == EPI_LANCZOS) {
+                            const double vr = su * ur, vi = su * ui;
+                            red[0] += hr * hr + hi * hi;
+                            red[1] += vr * hr + vi * hi;
+                            red[2] += vr * hi - vi * hr;
+                        }
+                    }
+                }
+            }
+            if constexpr (std::is_same<R, float>::value) {
+                if (EPI == EPI_LANCZOS) {  // per-tile FP32 partial sums -> FP64 accumulators
+                    red[0] += double(rf[0]);
+                    red[1] += su * double(rf[1]);
+                    red[2] += su * double(rf[2]);
                 }
             }
         }
@@ -429,11 +470,11 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
     constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
     if (A.gate && *A.gate != 0) return;
-    extern __shared__ __align__(128) unsigned char smem[];
-    C *tiles = reinterpret_cast<C *>(smem);  // [2][2^TB] values, then [2][2^TB] partials
+    extern __shared__ __align__(128) unsigned char smem_pass[];
+    C *tiles = reinterpret_cast<C *>(smem_pass);  // [2][2^TB] values, then [2][2^TB] partials
     C *parts = tiles + (2 << TB);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 4 * TILE_BYTES);
-    double *red_scr = reinterpret_cast<double *>(smem + 4 * TILE_BYTES + 16);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 4 * TILE_BYTES);
+    double *red_scr = reinterpret_cast<double *>(smem_pass + 4 * TILE_BYTES + 16);
     const int n = P.n, c = CT ? CT : P.hc, g = TB - c, hpos = P.hpos;
     const int tid = threadIdx.x;
     const int64_t cmask = (int64_t(1) << c) - 1;
@@ -503,6 +544,7 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
         di_r[k] = okk ? Coef<R>::dim(P, p) : R(0);
     }
     const double su = A.su_dev ? *A.su_dev : A.su;
+    const float suf = float(su);
     const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
     C *__restrict__ outp = reinterpret_cast<C *>(A.out);
     double red[NRED];
@@ -528,6 +570,7 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
         if (tid == 0 && s + nclusters < nsuper && ok) issue(s + nclusters, buf ^ 1);
         if (ok) {
             const uint32_t boff = (uint32_t)buf * TILE_BYTES;
+            float rf[3] = {0.f, 0.f, 0.f};
             C v[NA];
 #pragma unroll
             for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
@@ -559,14 +602,32 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
                         flip_acc<R, REALC>(P, p, (x >> p) & 1, u[x ^ (int64_t(1) << p)], acc);
                 }
                 const C pt = ptile[l];
-                const double hr = su * (double(pt.x) + acc.re());
-                const double hi = su * (double(pt.y) + acc.im());
-                outp[x] = cmake<C>(hr, hi);
-                if (EPI == EPI_LANCZOS) {
-                    const double vr = su * double(v[a].x), vi = su * double(v[a].y);
-                    red[0] += hr * hr + hi * hi;
-                    red[1] += vr * hr + vi * hi;
-                    red[2] += vr * hi - vi * hr;
+                if constexpr (std::is_same<R, float>::value) {
+                    const float2 t = upk2(acc.a);
+                    const float2 h = make_float2(suf * (pt.x + t.x), suf * (pt.y + t.y));
+                    outp[x] = h;
+                    if (EPI == EPI_LANCZOS) {
+                        rf[0] = fmaf(h.x, h.x, fmaf(h.y, h.y, rf[0]));
+                        rf[1] = fmaf(v[a].x, h.x, fmaf(v[a].y, h.y, rf[1]));
+                        rf[2] = fmaf(v[a].x, h.y, fmaf(-v[a].y, h.x, rf[2]));
+                    }
+                } else {
+                    const double hr = su * (double(pt.x) + acc.re());
+                    const double hi = su * (double(pt.y) + acc.im());
+                    outp[x] = cmake<C>(hr, hi);
+                    if (EPI == EPI_LANCZOS) {
+                        const double vr = su * double(v[a].x), vi = su * double(v[a].y);
+                        red[0] += hr * hr + hi * hi;
+                        red[1] += vr * hr + vi * hi;
+                        red[2] += vr * hi - vi * hr;
+                    }
+                }
+            }
+            if constexpr (std::is_same<R, float>::value) {
+                if (EPI == EPI_LANCZOS) {  // per-tile FP32 partial sums -> FP64 accumulators
+                    red[0] += double(rf[0]);
+                    red[1] += su * double(rf[1]);
+                    red[2] += su * double(rf[2]);
                 }
             }
         }
