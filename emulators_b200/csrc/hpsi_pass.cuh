@@ -238,10 +238,12 @@ __device__ __forceinline__ void report_timeout(const PassArgs &A) {
 // ------------------------------------------------------------------------- pass L
 // Shared memory: 2 tiles | mbarriers | U (padded rows) | field | per-tile scalars x2 | scratch
 constexpr int UPAD = MAXQ + 1;  // row stride of the shared U table (no bank conflicts)
+constexpr int SL = 3;           // pass L pipeline stages (tiles in flight per CTA)
+constexpr int SH = 3;           // pass H pipeline stages
 
 template <typename C, int TB>
 __host__ __device__ constexpr size_t pass_low_smem() {
-    return 2 * (sizeof(C) << TB) + 16 + sizeof(double) * (MAXQ * UPAD + MAXQ + 2 * 64 + 8 * NRED);
+    return SL * (sizeof(C) << TB) + 8 * SL + sizeof(double) * (MAXQ * UPAD + MAXQ + SL * 64 + 8 * NRED);
 }
 
 template <typename R, bool REALC, int TB, int RB, int EPI, int PB>
@@ -252,12 +254,12 @@ k_pass_low(const PassParams P, PassArgs A) {
     constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
     if (A.gate && *A.gate != 0) return;
     extern __shared__ __align__(128) unsigned char smem_pass[];
-    C *tiles = reinterpret_cast<C *>(smem_pass);                      // [2][2^TB]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 2 * TILE_BYTES);  // [2]
-    double *Ush = reinterpret_cast<double *>(smem_pass + 2 * TILE_BYTES + 16);
+    C *tiles = reinterpret_cast<C *>(smem_pass);                      // [SL][2^TB]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + SL * TILE_BYTES);  // [SL]
+    double *Ush = reinterpret_cast<double *>(smem_pass + SL * TILE_BYTES + 8 * SL);
     double *fld = Ush + MAXQ * UPAD;
-    double *scal = fld + MAXQ;       // [2][64]: crossT[SB] crossR[RB] eh
-    double *red_scr = scal + 2 * 64;
+    double *scal = fld + MAXQ;       // [SL][64]: crossT[SB] crossR[RB] eh
+    double *red_scr = scal + SL * 64;
 
     const int n = P.n;
     const int tid = threadIdx.x;
@@ -272,15 +274,18 @@ k_pass_low(const PassParams P, PassArgs A) {
     for (int k = tid; k < MAXQ * MAXQ; k += NT) Ush[(k / MAXQ) * UPAD + (k % MAXQ)] = P.U[k];
     for (int k = tid; k < MAXQ; k += NT) fld[k] = P.field[k];
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int b = 0; b < SL; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
-    // prologue: first tile of this CTA into buffer 0
-    if (tid == 0 && cid < nsuper) {
-        mbar_expect_tx(&bars[0], TILE_BYTES);
-        bulk_load(tiles, u + ((((int64_t)cid << PB) | rank) << TB), TILE_BYTES, &bars[0]);
+    // prologue: the first SL-1 tiles of this CTA
+    if (tid == 0) {
+        for (int b = 0; b < SL - 1; ++b) {
+            const int64_t s0 = cid + (int64_t)b * nclusters;
+            if (s0 >= nsuper) break;
+            mbar_expect_tx(&bars[b], TILE_BYTES);
+            bulk_load(tiles + ((int64_t)b << TB), u + (((s0 << PB) | rank) << TB), TILE_BYTES, &bars[b]);
+        }
     }
 
     // per-thread constants: energy of the thread bits and thread x register crosses
@@ -320,11 +325,11 @@ k_pass_low(const PassParams P, PassArgs A) {
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
     bool ok = true;
 
-    int it = 0;
+    int it = 0, buf = 0;
+    uint32_t phase = 0;
     for (int64_t s = cid; s < nsuper; s += nclusters, ++it) {
-        const int buf = it & 1;
         const int64_t base = ((s << PB) | rank) << TB;
-        C *tile = tiles + (buf << TB);
+        C *tile = tiles + ((int64_t)buf << TB);
         double *sc = scal + buf * 64;
         if (warp == 0) {
             // energy of the tile's high bits and their crosses with the tile bits
@@ -344,16 +349,20 @@ k_pass_low(const PassParams P, PassArgs A) {
                 sc[lane] = cx;  // crossT[0..SB) then crossR[0..RB)
             }
         }
-        if (ok && !mbar_wait(&bars[buf], (it >> 1) & 1)) {
+        if (ok && !mbar_wait(&bars[buf], phase)) {
             ok = false;
             report_timeout(A);
         }
-        // every CTA of the cluster has its tile; siblings are done with buffer buf^1
+        // every CTA of the cluster has its tile; everyone is done with the previous buffer
         if (PB) cluster_sync_all(); else __syncthreads();
-        if (tid == 0 && s + nclusters < nsuper && ok) {
-            const int64_t nb = (((s + nclusters) << PB) | rank) << TB;
-            mbar_expect_tx(&bars[buf ^ 1], TILE_BYTES);
-            bulk_load(tiles + ((buf ^ 1) << TB), u + nb, TILE_BYTES, &bars[buf ^ 1]);
+        {
+            const int64_t sn = s + (int64_t)(SL - 1) * nclusters;  // refill the freed buffer
+            const int nbuf = buf == 0 ? SL - 1 : buf - 1;
+            if (tid == 0 && sn < nsuper && ok) {
+                mbar_expect_tx(&bars[nbuf], TILE_BYTES);
+                bulk_load(tiles + ((int64_t)nbuf << TB), u + (((sn << PB) | rank) << TB), TILE_BYTES,
+                          &bars[nbuf]);
+            }
         }
         if (ok) {
             double St = ET + sc[TB];
@@ -438,6 +447,10 @@ k_pass_low(const PassParams P, PassArgs A) {
                 }
             }
         }
+        if (++buf == SL) {
+            buf = 0;
+            phase ^= 1u;
+        }
     }
     // no CTA may leave while a sibling can still read its shared memory
     if (PB) cluster_sync_all();
@@ -454,7 +467,7 @@ k_pass_low(const PassParams P, PassArgs A) {
 //   hsplit 1: [2^cm*K, 2^(c-cm), 2^(hpos-c), 2^g, rest]      (pbh = 0, wide chunks)
 template <typename C, int TB>
 __host__ __device__ constexpr size_t pass_high_smem() {
-    return 4 * (sizeof(C) << TB) + 16 + sizeof(double) * 8 * NRED;
+    return 2 * SH * (sizeof(C) << TB) + 8 * SH + sizeof(double) * 8 * NRED;
 }
 
 struct PassHighMaps {
@@ -471,10 +484,10 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
     if (A.gate && *A.gate != 0) return;
     extern __shared__ __align__(128) unsigned char smem_pass[];
-    C *tiles = reinterpret_cast<C *>(smem_pass);  // [2][2^TB] values, then [2][2^TB] partials
-    C *parts = tiles + (2 << TB);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 4 * TILE_BYTES);
-    double *red_scr = reinterpret_cast<double *>(smem_pass + 4 * TILE_BYTES + 16);
+    C *tiles = reinterpret_cast<C *>(smem_pass);  // [SH][2^TB] values, then [SH][2^TB] partials
+    C *parts = tiles + ((int64_t)SH << TB);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 2 * SH * TILE_BYTES);
+    double *red_scr = reinterpret_cast<double *>(smem_pass + 2 * SH * TILE_BYTES + 8 * SH);
     const int n = P.n, c = CT ? CT : P.hc, g = TB - c, hpos = P.hpos;
     const int tid = threadIdx.x;
     const int64_t cmask = (int64_t(1) << c) - 1;
@@ -489,8 +502,7 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     const uint32_t box_bytes = TILE_BYTES / nbox;
 
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int b = 0; b < SH; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -500,8 +512,8 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
         const int shi = (int)(s >> lowbits);
         mbar_expect_tx(&bars[buf], 2 * TILE_BYTES);
         for (int b = 0; b < nbox; ++b) {
-            unsigned char *dv = reinterpret_cast<unsigned char *>(tiles + (buf << TB)) + b * box_bytes;
-            unsigned char *dp = reinterpret_cast<unsigned char *>(parts + (buf << TB)) + b * box_bytes;
+            unsigned char *dv = reinterpret_cast<unsigned char *>(tiles + ((int64_t)buf << TB)) + b * box_bytes;
+            unsigned char *dp = reinterpret_cast<unsigned char *>(parts + ((int64_t)buf << TB)) + b * box_bytes;
             if (P.hsplit == 0) {
                 tmap_load5(dv, &M.u, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
                 tmap_load5(dp, &M.part, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
@@ -511,7 +523,13 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
             }
         }
     };
-    if (tid == 0 && cid < nsuper) issue(cid, 0);
+    if (tid == 0) {
+        for (int b = 0; b < SH - 1; ++b) {
+            const int64_t s0 = cid + (int64_t)b * nclusters;
+            if (s0 >= nsuper) break;
+            issue(s0, b);
+        }
+    }
 
     uint32_t raddr[PBH > 0 ? PBH : 1];
     R ccr[PBH > 0 ? PBH : 1], cci[PBH > 0 ? PBH : 1];
@@ -555,19 +573,22 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     const int64_t xt = (tid & cmask) + ((int64_t)(tid >> c) << hpos);
     const int ash = hpos + SB - c;  // when c <= SB: x offset of a is a << ash
 
-    int it = 0;
+    int it = 0, buf = 0;
+    uint32_t phase = 0;
     for (int64_t s = cid; s < nsuper; s += nclusters, ++it) {
-        const int buf = it & 1;
         const int64_t base = ((s & lowmask) << c) | ((int64_t)rank << cpos) |
                              ((s >> lowbits) << (cpos + PBH));
-        const C *tile = tiles + (buf << TB);
-        const C *ptile = parts + (buf << TB);
-        if (ok && !mbar_wait(&bars[buf], (it >> 1) & 1)) {
+        const C *tile = tiles + ((int64_t)buf << TB);
+        const C *ptile = parts + ((int64_t)buf << TB);
+        if (ok && !mbar_wait(&bars[buf], phase)) {
             ok = false;
             report_timeout(A);
         }
         if (PBH) cluster_sync_all(); else __syncthreads();
-        if (tid == 0 && s + nclusters < nsuper && ok) issue(s + nclusters, buf ^ 1);
+        {
+            const int64_t sn = s + (int64_t)(SH - 1) * nclusters;  // refill the freed buffer
+            if (tid == 0 && sn < nsuper && ok) issue(sn, buf == 0 ? SH - 1 : buf - 1);
+        }
         if (ok) {
             const uint32_t boff = (uint32_t)buf * TILE_BYTES;
             float rf[3] = {0.f, 0.f, 0.f};
@@ -630,6 +651,10 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
                     red[2] += su * double(rf[2]);
                 }
             }
+        }
+        if (++buf == SH) {
+            buf = 0;
+            phase ^= 1u;
         }
     }
     if (PBH) cluster_sync_all();
