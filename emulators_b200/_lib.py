@@ -15,7 +15,8 @@ import numpy as np
 import torch
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libemusv_b200.so")
+# EMUSV_LIB selects another build of the same library (e.g. an instrumented one)
+LIB_PATH = os.environ.get("EMUSV_LIB") or os.path.join(PKG, "libemusv_b200.so")
 
 OK, NOT_CONVERGED, NONFINITE, BAD_ARGUMENT, WORKSPACE_TOO_SMALL, CUDA_ERROR, TIMEOUT = range(7)
 C128, C64 = 0, 1

@@ -14,13 +14,15 @@ namespace emusv {
 // in each thread's registers, 256 threads.
 template <typename R> struct PassShape;
 // c64: 4096-amplitude tiles (32 KiB), 16 amplitudes per thread; c128: 2048-amplitude
-// tiles (32 KiB), 8 per thread; 256 threads and two CTAs per SM either way.  Clusters of
-// up to 8 CTAs in pass L and pass H; pass H reads 32-byte chunks.
+// tiles (32 KiB), 8 per thread; 256 threads.  Pass H reads rows of at least 32 bytes.
+// No thread-block clusters: measured on B200, reading partner amplitudes from a sibling
+// CTA's shared memory amplitude by amplitude (and the per-tile cluster barrier) cost more
+// than a further streaming pass, so every pass keeps its flips inside one CTA's tile.
 template <> struct PassShape<float> {
-    static constexpr int TB = 12, RB = 4, PBMAX = 2, PBHMAX = 3, CMIN = 2;
+    static constexpr int TB = 12, RB = 4, CMIN = 2;
 };
 template <> struct PassShape<double> {
-    static constexpr int TB = 11, RB = 3, PBMAX = 3, PBHMAX = 3, CMIN = 1;
+    static constexpr int TB = 11, RB = 3, CMIN = 1;
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
@@ -122,144 +124,106 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
     }
 }
 
-// Kernel pointers by run-time layout (template arguments are compile-time).
-template <typename R, bool REALC, int TB, int RB, int EPI>
-static auto low_kernel(int pb) -> decltype(&k_pass_low<R, REALC, TB, RB, EPI, 0>) {
-    switch (pb) {
-    case 0: return k_pass_low<R, REALC, TB, RB, EPI, 0>;
-    case 1: return k_pass_low<R, REALC, TB, RB, EPI, 1>;
-    case 2: return k_pass_low<R, REALC, TB, RB, EPI, 2>;
-    default: return k_pass_low<R, REALC, TB, RB, EPI, 3>;
-    }
-}
-template <typename R, bool REALC, int TB, int RB, int EPI, int CMIN>
-static auto high_kernel(bool hot, int pbh) -> decltype(&k_pass_high<R, REALC, TB, RB, EPI, 0, 0>) {
-    if (hot) {
-        switch (pbh) {
-        case 0: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0>;
-        case 1: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 1>;
-        case 2: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 2>;
-        default: return k_pass_high<R, REALC, TB, RB, EPI, CMIN, 3>;
-        }
-    }
-    return pbh == 0 ? k_pass_high<R, REALC, TB, RB, EPI, 0, 0> : k_pass_high<R, REALC, TB, RB, EPI, 0, 3>;
-}
-
-template <typename R, bool REALC, int EPI_H>
-static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
+template <typename R, bool REALC, int EPI>
+static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
-    constexpr int CMIN = PassShape<R>::CMIN;
-    const int n = H.n;
-    PassParams P;
-    fill_params(H, TB, RB, &P);
-    int pb = n - TB;
-    if (pb > PassShape<R>::PBMAX) pb = PassShape<R>::PBMAX;
-    P.pb = pb;
-    const int rem = n - TB - pb;
-    int g = rem;
-    if (g > TB - CMIN) g = TB - CMIN;
-    int pbh = rem - g;
-    if (pbh > PassShape<R>::PBHMAX) pbh = PassShape<R>::PBHMAX;
+    auto kern = k_pass_low<R, REALC, TB, RB, EPI, 0>;
+    const size_t smem = pass_low_smem<C, TB>();
+    EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int64_t ntiles = int64_t(1) << (P.n - TB);
+    int64_t grid = (int64_t)sm_count() * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    {
+        ProfScope ps_(PROF_HPSI, s);
+        kern<<<(unsigned)grid, NT, smem, s>>>(P, A);
+    }
+    EMUSV_CHECK_LAUNCH();
+    if (grid_out) *grid_out = (int)grid;
+    return EMUSV_OK;
+}
+
+// One strided pass over the group bits [hpos, hpos + g); chunk c = TB - g low bits.
+template <typename R, bool REALC, int EPI>
+static int launch_high(PassParams P, int hpos, int g, const PassArgs &A, const void *part,
+                       cudaStream_t s, int *grid_out) {
+    typedef typename cvec<R>::T C;
+    constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
+    constexpr int CMIN = PassShape<R>::CMIN, K = sizeof(C) / 8;
+    const int n = P.n;
     P.hg = g;
     P.hc = TB - g;
-    P.hpos = TB + pb;
-    P.pbh = pbh;
-    P.xb_lo = TB + pb + g + pbh;
-    P.xb_hi = n;
-    constexpr int K = sizeof(C) / 8;
-    // chunk rows wider than one 256-element TMA box dimension are split in two dims
-    int cm = 0;
+    P.hpos = hpos;
+    P.pbh = 0;
+    P.xb_lo = P.xb_hi = n;
+    int cm = 0;  // chunk rows wider than one 256-element TMA box dimension are split
     while (((1 << (cm + 1)) * K) <= 256 && cm + 1 <= P.hc) ++cm;
     P.hsplit = ((1 << P.hc) * K > 256) ? 1 : 0;
     P.hbox_rows = g > 8 ? 256 : (1 << g);
-    if (P.hsplit && pbh) return EMUSV_BAD_ARGUMENT;  // not a layout the sizes above produce
-    const bool hot = P.hc == CMIN && P.xb_lo == n;
-    if (!hot && pbh != 0 && pbh != 3) return EMUSV_BAD_ARGUMENT;
+    PassHighMaps M;
+    if (!encode_pass_high(&M.u, A.u, n, (int)sizeof(C), P, cm) ||
+        !encode_pass_high(&M.part, part, n, (int)sizeof(C), P, cm))
+        return EMUSV_CUDA_ERROR;
+    auto kern = (P.hc == CMIN) ? k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0>
+                               : k_pass_high<R, REALC, TB, RB, EPI, 0, 0>;
+    const size_t smem = pass_high_smem<C, TB>();
+    EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int64_t ntiles = int64_t(1) << (n - TB);
+    int64_t grid = (int64_t)sm_count() * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    {
+        ProfScope ps_(PROF_HPSI_HIGH, s);
+        kern<<<(unsigned)grid, NT, smem, s>>>(P, A, M);
+    }
+    EMUSV_CHECK_LAUNCH();
+    if (grid_out) *grid_out = (int)grid;
+    return EMUSV_OK;
+}
+
+// H v in two or three streaming passes: L (bits 0..TB-1, diagonal), then strided passes
+// over groups of at most TB - CMIN bits.  The partial sums live in HA.part_buf (which may
+// be HA.out: every pass reads a tile before writing it).
+template <typename R, bool REALC, int EPI_F>
+static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
+    constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, CMIN = PassShape<R>::CMIN;
+    const int n = H.n;
+    PassParams P;
+    fill_params(H, TB, RB, &P);
+    P.pb = 0;
+    const int rem = n - TB;
+    const int g1 = rem < TB - CMIN ? rem : TB - CMIN;
+    const int g2 = rem - g1;
+    if (g2 > TB - CMIN) return EMUSV_BAD_ARGUMENT;  // more than three passes: n too large
+    if (rem > 0 && !HA.part_buf) return EMUSV_BAD_ARGUMENT;
 
     PassArgs A = {};
     A.u = HA.u;
     A.su_dev = HA.su_dev;
     A.su = HA.su;
-    A.out = rem > 0 ? HA.part_buf : HA.out;  // pass L output
     A.partials = HA.partials;
     A.gate = HA.gate;
     A.err = HA.err;
-    if (rem > 0 && !HA.part_buf) return EMUSV_BAD_ARGUMENT;  // pass H needs the partial buffer
-
-    const size_t smem_l = pass_low_smem<C, TB>(), smem_h = pass_high_smem<C, TB>();
-    const int nsm = sm_count();
-    // ---- pass L
-    {
-        auto kern = (rem > 0) ? low_kernel<R, REALC, TB, RB, EPI_PARTIAL>(pb)
-                              : low_kernel<R, REALC, TB, RB, EPI_H>(pb);
-        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_l));
-        int per_sm = 0;
-        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem_l));
-        if (per_sm < 1) per_sm = 1;
-        const int CS = 1 << pb;
-        const int64_t ncta = int64_t(1) << (n - TB);
-        int64_t grid = (int64_t)nsm * per_sm;
-        if (grid > ncta) grid = ncta;
-        grid = grid / CS * CS;
-        if (grid < CS) grid = CS;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)grid, 1, 1);
-        cfg.blockDim = dim3(NT, 1, 1);
-        cfg.dynamicSmemBytes = smem_l;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = CS;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        {
-            ProfScope ps_(PROF_HPSI, s);
-            EMUSV_CHECK(cudaLaunchKernelEx(&cfg, kern, P, A));
-        }
-        if (rem == 0 && grid_out) *grid_out = (int)grid;
+    int st;
+    if (rem == 0) {
+        A.out = HA.out;
+        return launch_low<R, REALC, EPI_F>(P, A, s, grid_out);
     }
-    if (rem == 0) return EMUSV_OK;
-    // ---- pass H: partial sums (pass L output) and values staged by TMA, final into HA.out
-    {
-        PassHighMaps M;
-        if (!encode_pass_high(&M.u, HA.u, n, (int)sizeof(C), P, cm) ||
-            !encode_pass_high(&M.part, HA.part_buf, n, (int)sizeof(C), P, cm))
-            return EMUSV_CUDA_ERROR;
-        PassArgs AH = A;
-        AH.out = HA.out;
-        auto kern = high_kernel<R, REALC, TB, RB, EPI_H, CMIN>(hot, pbh);
-        EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_h));
-        int per_sm = 0;
-        EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem_h));
-        if (per_sm < 1) per_sm = 1;
-        const int CS = 1 << pbh;
-        const int64_t ntiles = int64_t(1) << (n - P.hc - P.hg);
-        int64_t grid = (int64_t)nsm * per_sm;
-        if (grid > ntiles) grid = ntiles;
-        grid = grid / CS * CS;
-        if (grid < CS) grid = CS;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)grid, 1, 1);
-        cfg.blockDim = dim3(NT, 1, 1);
-        cfg.dynamicSmemBytes = smem_h;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = CS;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        {
-            ProfScope ps_(PROF_HPSI_HIGH, s);
-            EMUSV_CHECK(cudaLaunchKernelEx(&cfg, kern, P, AH, M));
-        }
-        if (grid_out) *grid_out = (int)grid;
+    A.out = HA.part_buf;
+    if ((st = launch_low<R, REALC, EPI_PARTIAL>(P, A, s, nullptr))) return st;
+    if (g2 == 0) {
+        A.out = HA.out;
+        return launch_high<R, REALC, EPI_F>(P, TB, g1, A, HA.part_buf, s, grid_out);
     }
-    return EMUSV_OK;
+    A.out = HA.part_buf;
+    if ((st = launch_high<R, REALC, EPI_PARTIAL>(P, TB, g1, A, HA.part_buf, s, nullptr))) return st;
+    A.out = HA.out;
+    return launch_high<R, REALC, EPI_F>(P, TB + g1, g2, A, HA.part_buf, s, grid_out);
 }
 
 // mode: HP_STORE or HP_LANCZOS (values of HpsiMode)

@@ -118,14 +118,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait (a few seconds of SM clock); false on timeout.
+// Bounded wait (a few seconds of SM clock); false on timeout.  The clock is read once
+// per 1024 polls so that waiting warps do not crowd the issue slots.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > 4000000000LL) return false;
+    for (uint32_t i = 1;; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 1023u) == 0 && clock64() - t0 > 4000000000LL) return false;
     }
-    return true;
 }
 // 1-D bulk copy global -> own shared memory, completion on `bar`.
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
@@ -623,7 +624,14 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
                         flip_acc<R, REALC>(P, p, (x >> p) & 1, u[x ^ (int64_t(1) << p)], acc);
                 }
                 const C pt = ptile[l];
-                if constexpr (std::is_same<R, float>::value) {
+                if (EPI == EPI_PARTIAL) {  // another pass follows: unscaled running sum
+                    if constexpr (std::is_same<R, float>::value) {
+                        const float2 t = upk2(acc.a);
+                        outp[x] = make_float2(pt.x + t.x, pt.y + t.y);
+                    } else {
+                        outp[x] = cmake<C>(double(pt.x) + acc.re(), double(pt.y) + acc.im());
+                    }
+                } else if constexpr (std::is_same<R, float>::value) {
                     const float2 t = upk2(acc.a);
                     const float2 h = make_float2(suf * (pt.x + t.x), suf * (pt.y + t.y));
                     outp[x] = h;
