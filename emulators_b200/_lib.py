@@ -41,6 +41,7 @@ SIGNATURES: dict[str, tuple] = {
     "emusv_hpsi": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "emusv_scratch_bytes": (_SZ, [_I, _I]),
     "emusv_expect": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
+    "emusv_expect_noalloc": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "emusv_occupation": (_I, [_I, _I, _P, _P, _P, _SZ, _P]),
     "emusv_correlation": (_I, [_I, _I, _P, _P, _P, _SZ, _P]),
     "emusv_krylov_workspace_bytes": (_SZ, [_I, _I, _I]),

@@ -84,6 +84,19 @@ int emusv_expect(int nqubits, int dtype, const double *omegas, const double *del
                  const double *phis, const double *interaction, const void *psi,
                  double *result_dev, void *scratch, size_t scratch_bytes, void *stream);
 
+/* The same energy moments as emusv_expect with no scratch argument and no allocation:
+ * the partial sums go to a static device array inside the library (about 66 KB per GPU,
+ * kept until the process exits).  For callers that cannot allocate device memory at the
+ * call site (graph-recording code, external memory managers, host runtimes without a
+ * device allocator).  Registers up to EMUSV_MAX_QUBITS; larger ones give
+ * EMUSV_BAD_ARGUMENT.  The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the
+ * array, so calls that overlap on the GPU race.  No counterpart in the reference: it has
+ * no C interface. */
+int emusv_expect_noalloc(int nqubits, int dtype, const double *omegas, const double *deltas,
+                         const double *phis, const double *interaction, const void *psi,
+                         double *result_dev, void *stream);
+
 /* occ_dev[i] = sum_x |psi_x|^2 x_i (device float64 [n]), one pass over psi.
  * Replaces qubit_occupation_sv_impl (emu_sv/custom_callback_implementations.py:30-47). */
 int emusv_occupation(int nqubits, int dtype, const void *psi, double *occ_dev, void *scratch,
