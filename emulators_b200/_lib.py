@@ -47,6 +47,9 @@ SIGNATURES: dict[str, tuple] = {
     "emusv_krylov_workspace_bytes": (_SZ, [_I, _I, _I]),
     "emusv_krylov_step": (_I, [_I, _I, _D, _P, _P, _P, _P, _P, _P, _D, _D, _I, _I, _P, _SZ,
                                ctypes.POINTER(KrylovInfo), _P]),
+    "emusv_adjoint_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "emusv_adjoint_step": (_I, [_I, _I, _D, _P, _P, _P, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _SZ,
+                                _P]),
     "emusv_vec_dot": (_I, [_I64, _I, _P, _P, _P, _P, _SZ, _P]),
     "emusv_vec_axpy": (_I, [_I64, _I, _P, _P, _P, _P]),
     "emusv_vec_combine": (_I, [_I64, _I, _I, _P, _P, _P, _P]),

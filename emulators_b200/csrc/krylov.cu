@@ -16,7 +16,7 @@
 // convergence.
 #include <string.h>
 
-#include "hpsi_kernel.cuh"
+#include "krylov_internal.cuh"
 #include "profile.cuh"
 
 namespace emusv {
@@ -25,27 +25,6 @@ int hpsi_tile_bits(int n);
 int launch_hpsi(int dtype, int mode, const HamParams &P, HpsiArgs A, int max_grid,
                 cudaStream_t s, int *grid_out);
 int max_grid_blocks();
-
-constexpr int KMAX = 128;  // largest max_krylov_dim supported
-
-// KS_TIMEOUT equals EMUSV_TIMEOUT: the streaming kernels write it on a bounded-wait timeout.
-enum KStatus { KS_RUNNING = 0, KS_CONVERGED = 1, KS_HAPPY = 2, KS_MAXDIM = 3, KS_NONFINITE = 4,
-               KS_TIMEOUT = EMUSV_TIMEOUT };
-
-struct KState {
-    int status;
-    int iters;
-    int nvec;
-    int kerr;  // error word of the streaming kernels (EMUSV_TIMEOUT), read by k_small
-    double s0, err, outnorm2, pad2;
-    double a_re[KMAX], a_im[KMAX];   // T_H[k][k]   = <v_k, H v_k> - b_k <v_k, v_{k-1}>
-    double b_re[KMAX], b_im[KMAX];   // T_H[k-1][k] = ||w_{k-1}|| (= <v_{k-1}, H v_k> exactly)
-    double vv_re[KMAX + 2], vv_im[KMAX + 2];  // <v_k, v_{k-1}>: residual non-orthogonality
-    double r[KMAX];                  // T_H[k+1][k] = ||w_k||
-    double hn[KMAX];                 // ||H v_k||
-    double scale[KMAX + 2];          // v_k = scale[k] * stored_k
-    double c_re[KMAX + 2], c_im[KMAX + 2];  // result coefficients
-};
 
 struct Workspace {
     KState *ks;
@@ -496,8 +475,10 @@ __global__ void __launch_bounds__(32) k_tridiag_expm(int m, const TriArgs *A, do
 
 using namespace emusv;
 
+namespace emusv {
 namespace {
 thread_local int *pinned_status = nullptr;
+}  // namespace
 
 int read_status(KState *ks, cudaStream_t s, int *out) {
     if (!pinned_status) {
@@ -511,43 +492,26 @@ int read_status(KState *ks, cudaStream_t s, int *out) {
     *out = pinned_status[0];
     return EMUSV_OK;
 }
-}  // namespace
+}  // namespace emusv
 
-extern "C" {
+namespace emusv {
 
-size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity) {
-    if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS || basis_capacity < 0) return 0;
-    const size_t es = dtype == EMUSV_C128 ? 16 : 8;
-    return header_bytes() + (size_t)(basis_capacity + 1) * (size_t(1) << nqubits) * es;
-}
-
-int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
-                      const double *deltas, const double *phis, const double *interaction,
-                      const void *psi_in, void *psi_out, double exp_tolerance,
-                      double norm_tolerance, int max_krylov_dim, int krylov_dim_hint,
-                      void *workspace, size_t workspace_bytes, emusv_krylov_info *info,
-                      void *stream) {
-    HamParams P;
-    if (!psi_in || !psi_out || !workspace || (dtype != EMUSV_C128 && dtype != EMUSV_C64) ||
-        max_krylov_dim < 1 || max_krylov_dim > KMAX - 2 || !isfinite(dt) ||
-        !make_params(nqubits, omegas, deltas, phis, interaction, &P))
-        return EMUSV_BAD_ARGUMENT;
-    if (workspace_bytes < header_bytes()) return EMUSV_WORKSPACE_TOO_SMALL;
-    if ((reinterpret_cast<uintptr_t>(workspace) & 255) || (reinterpret_cast<uintptr_t>(psi_in) & 15) ||
-        (reinterpret_cast<uintptr_t>(psi_out) & 15))
-        return EMUSV_BAD_ARGUMENT;
-    cudaStream_t s = as_stream(stream);
+int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState *ks,
+                double *part_h, double *part_o, unsigned char *basis, int capacity,
+                double exp_tol, double norm_tol, int maxdim, int hint, cudaStream_t s,
+                int *status_out) {
+    const int nqubits = P.n;
     const i64 D = i64(1) << nqubits;
     const size_t es = dtype == EMUSV_C128 ? 16 : 8;
-    Workspace W = carve(workspace, workspace_bytes);
-    // basis region: [partial-sum vector of the two-pass H*psi][stored_1][stored_2]...
-    const int capacity = (int)(W.basis_bytes / (D * es)) - 1;
-    if (capacity < 1) return EMUSV_WORKSPACE_TOO_SMALL;
-    void *part_vec = W.basis;
+    void *part_vec = basis;
     auto stored = [&](int k) -> const void * {
-        return k == 0 ? psi_in : (const void *)(W.basis + (size_t)k * D * es);
+        return k == 0 ? v0 : (const void *)(basis + (size_t)k * D * es);
     };
     const int sg = stream_grid(D);
+    const double exp_tolerance = exp_tol, norm_tolerance = norm_tol;
+    const int max_krylov_dim = maxdim, krylov_dim_hint = hint;
+    const void *psi_in = v0;
+    struct { KState *ks; double *part_h, *part_o; } W = {ks, part_h, part_o};
 
     if (dtype == EMUSV_C128)
         {
@@ -617,6 +581,51 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
     }
     if (status == KS_RUNNING) {
         int st = read_status(W.ks, s, &status);
+        if (st) return st;
+    }
+    *status_out = status;
+    return EMUSV_OK;
+}
+
+}  // namespace emusv
+
+extern "C" {
+
+size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity) {
+    if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS || basis_capacity < 0) return 0;
+    const size_t es = dtype == EMUSV_C128 ? 16 : 8;
+    return header_bytes() + (size_t)(basis_capacity + 1) * (size_t(1) << nqubits) * es;
+}
+
+int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
+                      const double *deltas, const double *phis, const double *interaction,
+                      const void *psi_in, void *psi_out, double exp_tolerance,
+                      double norm_tolerance, int max_krylov_dim, int krylov_dim_hint,
+                      void *workspace, size_t workspace_bytes, emusv_krylov_info *info,
+                      void *stream) {
+    HamParams P;
+    if (!psi_in || !psi_out || !workspace || (dtype != EMUSV_C128 && dtype != EMUSV_C64) ||
+        max_krylov_dim < 1 || max_krylov_dim > KMAX - 2 || !isfinite(dt) ||
+        !make_params(nqubits, omegas, deltas, phis, interaction, &P))
+        return EMUSV_BAD_ARGUMENT;
+    if (workspace_bytes < header_bytes()) return EMUSV_WORKSPACE_TOO_SMALL;
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) || (reinterpret_cast<uintptr_t>(psi_in) & 15) ||
+        (reinterpret_cast<uintptr_t>(psi_out) & 15))
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    const i64 D = i64(1) << nqubits;
+    const size_t es = dtype == EMUSV_C128 ? 16 : 8;
+    Workspace W = carve(workspace, workspace_bytes);
+    // basis region: [partial-sum vector of the two-pass H*psi][stored_1][stored_2]...
+    const int capacity = (int)(W.basis_bytes / (D * es)) - 1;
+    if (capacity < 1) return EMUSV_WORKSPACE_TOO_SMALL;
+    const int sg = stream_grid(D);
+
+    int status = KS_RUNNING;
+    {
+        const int st = lanczos_run(P, dtype, dt, psi_in, W.ks, W.part_h, W.part_o, W.basis, capacity,
+                                   exp_tolerance, norm_tolerance, max_krylov_dim, krylov_dim_hint, s,
+                                   &status);
         if (st) return st;
     }
     if (status == KS_TIMEOUT) {

@@ -1,0 +1,41 @@
+// Shared state of the Lanczos iteration (krylov.cu) and the adjoint (adjoint.cu).
+#pragma once
+
+#include "hpsi_kernel.cuh"
+
+namespace emusv {
+
+constexpr int KMAX = 128;  // largest max_krylov_dim supported
+
+// KS_TIMEOUT equals EMUSV_TIMEOUT: the streaming kernels write it on a bounded-wait timeout.
+enum KStatus { KS_RUNNING = 0, KS_CONVERGED = 1, KS_HAPPY = 2, KS_MAXDIM = 3, KS_NONFINITE = 4,
+               KS_TIMEOUT = EMUSV_TIMEOUT };
+
+struct KState {
+    int status;
+    int iters;
+    int nvec;
+    int kerr;  // error word of the streaming kernels (EMUSV_TIMEOUT), read by k_small
+    double s0, err, outnorm2, pad2;
+    double a_re[KMAX], a_im[KMAX];   // T_H[k][k]   = <v_k, H v_k> - b_k <v_k, v_{k-1}>
+    double b_re[KMAX], b_im[KMAX];   // T_H[k-1][k] = ||w_{k-1}|| (= <v_{k-1}, H v_k> exactly)
+    double vv_re[KMAX + 2], vv_im[KMAX + 2];  // <v_k, v_{k-1}>: residual non-orthogonality
+    double r[KMAX];                  // T_H[k+1][k] = ||w_k||
+    double hn[KMAX];                 // ||H v_k||
+    double scale[KMAX + 2];          // v_k = scale[k] * stored_k
+    double c_re[KMAX + 2], c_im[KMAX + 2];  // result coefficients
+};
+
+
+// One Lanczos run on the device: v0 (with scale 1/||v0||) is basis vector 0, basis
+// vectors 1.. are stored unnormalised at basis + k*vec_bytes (k >= 1; slot 0 of `basis`
+// holds the partial sums of the two-pass H*psi).  Stops like krylov_exp.py:49-106 (and
+// double_krylov.py:79-110, which has the same tests).  Returns an emusv status; the
+// run's own outcome is in ks->status.
+int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState *ks,
+                double *part_h, double *part_o, unsigned char *basis, int capacity,
+                double exp_tol, double norm_tol, int maxdim, int hint, cudaStream_t s,
+                int *status_out);
+int read_status(KState *ks, cudaStream_t s, int *out);
+
+}  // namespace emusv

@@ -130,6 +130,27 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
                       void *workspace, size_t workspace_bytes, emusv_krylov_info *info,
                       void *stream);
 
+/* Bytes of device workspace emusv_adjoint_step needs when each of its two Lanczos bases
+ * may hold `basis_capacity` vectors (3 * (capacity + 1) + 1 vectors of 2^n amplitudes
+ * plus small tables); 0 for registers above 20 qubits. */
+size_t emusv_adjoint_workspace_bytes(int nqubits, int dtype, int basis_capacity);
+
+/* Adjoint of one time step psi_out = exp(-i dt H) state: given grad_out = dL/dpsi_out
+ * (torch's convention for complex tensors), writes dL/dOmega_i, dL/ddelta_i, dL/dphi_i
+ * and dL/dU_ij (i < j; host float64 arrays, any of them may be NULL to skip it).
+ * Replaces DifferentiableStateVectorEvolution.backward (emu_sv/time_evolution/torch.py:
+ * 223-353) with double_krylov (emu_base/math/double_krylov.py:5-113); the state gradient
+ * exp(+i dt H) grad_out (torch.py:355-366) is a separate emusv_krylov_step with -dt.
+ * Returns EMUSV_NOT_CONVERGED (RecursionError, double_krylov.py:107-110) or
+ * EMUSV_WORKSPACE_TOO_SMALL (retry with a larger capacity).  Registers up to 20 qubits.
+ * Synchronises the stream. */
+int emusv_adjoint_step(int nqubits, int dtype, double dt, const double *omegas,
+                       const double *deltas, const double *phis, const double *interaction,
+                       const void *state, const void *grad_out, double tolerance,
+                       int max_krylov_dim, double *g_omegas, double *g_deltas, double *g_phis,
+                       double *g_interaction, void *workspace, size_t workspace_bytes,
+                       void *stream);
+
 /* ---- building blocks of the generic krylov_exp(op, v, ...) (krylov_exp.py:23-106) ----
  * For an arbitrary operator applied by the caller, these give the FP64-accumulated
  * Lanczos arithmetic and the on-device exponential of the extended Krylov matrix. */
