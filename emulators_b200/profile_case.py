@@ -1,6 +1,7 @@
 """A small, self-contained run of the hot path for profilers (ncu) and quick timing.
 
     python -m emulators_b200.profile_case [--n 25] [--dtype c64] [--steps 2] [--hpsi 3]
+                                          [--max-krylov-dim 100]
 
 Builds the 2 x n/2 ladder at 5.5 um with the ladder_n26 drive, runs `--hpsi` standalone
 H*psi launches and `--steps` Krylov time steps from |g...g>, prints device times.  Sized
@@ -26,6 +27,8 @@ def main(argv=None) -> int:
     ap.add_argument("--dtype", choices=["c64", "c128"], default="c64")
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--hpsi", type=int, default=3)
+    ap.add_argument("--max-krylov-dim", type=int, default=100,
+                    help="bounds the Krylov basis the step allocates")
     a = ap.parse_args(argv)
     dev = torch.device("cuda", 0)
     dt_ = torch.complex64 if a.dtype == "c64" else torch.complex128
@@ -53,7 +56,8 @@ def main(argv=None) -> int:
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(a.steps):
-        v, info, st = fused_step(HamiltonianExpOperator(H, 0.005), v, 1e-10, 1e-10, 100)
+        v, info, st = fused_step(HamiltonianExpOperator(H, 0.005), v, 1e-10, 1e-10,
+                                  a.max_krylov_dim)
         _lib.check(st, "step")
         iters.append(info.iterations)
     e1.record()
