@@ -40,45 +40,27 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // Tensor map of a 2^n vector of `es`-byte amplitudes for pass H (see hpsi_pass.cuh).
-static bool encode_pass_high(CUtensorMap *map, const void *base, int n, int es, const PassParams &P,
-                             int cm) {
+static bool encode_pass_high(CUtensorMap *map, const void *base, int n, int es, const PassParams &P) {
     auto fn = encode_fn();
     if (!fn) return false;
     const int K = es / 8;
     cuuint64_t dims[5], strides[4];
     cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
     const int c = P.hc, g = P.hg, hpos = P.hpos, pbh = P.pbh;
-    if (P.hsplit == 0) {
-        dims[0] = (cuuint64_t(1) << c) * K;
-        dims[1] = cuuint64_t(1) << (hpos - c);
-        dims[2] = cuuint64_t(1) << g;
-        dims[3] = cuuint64_t(1) << pbh;
-        dims[4] = cuuint64_t(1) << (n - hpos - g - pbh);
-        strides[0] = (cuuint64_t(es) << c);
-        strides[1] = (cuuint64_t(es) << hpos);
-        strides[2] = (cuuint64_t(es) << (hpos + g));
-        strides[3] = (cuuint64_t(es) << (hpos + g + pbh));
-        box[0] = (cuuint32_t)dims[0];
-        box[1] = 1;
-        box[2] = (cuuint32_t)P.hbox_rows;
-        box[3] = 1;
-        box[4] = 1;
-    } else {
-        dims[0] = (cuuint64_t(1) << cm) * K;
-        dims[1] = cuuint64_t(1) << (c - cm);
-        dims[2] = cuuint64_t(1) << (hpos - c);
-        dims[3] = cuuint64_t(1) << g;
-        dims[4] = cuuint64_t(1) << (n - hpos - g);
-        strides[0] = (cuuint64_t(es) << cm);
-        strides[1] = (cuuint64_t(es) << c);
-        strides[2] = (cuuint64_t(es) << hpos);
-        strides[3] = (cuuint64_t(es) << (hpos + g));
-        box[0] = (cuuint32_t)dims[0];
-        box[1] = (cuuint32_t)dims[1];
-        box[2] = 1;
-        box[3] = (cuuint32_t)P.hbox_rows;
-        box[4] = 1;
-    }
+    dims[0] = (cuuint64_t(1) << c) * K;
+    dims[1] = cuuint64_t(1) << (hpos - c);
+    dims[2] = cuuint64_t(1) << g;
+    dims[3] = cuuint64_t(1) << pbh;
+    dims[4] = cuuint64_t(1) << (n - hpos - g - pbh);
+    strides[0] = (cuuint64_t(es) << c);
+    strides[1] = (cuuint64_t(es) << hpos);
+    strides[2] = (cuuint64_t(es) << (hpos + g));
+    strides[3] = (cuuint64_t(es) << (hpos + g + pbh));
+    box[0] = (cuuint32_t)dims[0];
+    box[1] = 1;
+    box[2] = (cuuint32_t)P.hbox_rows;
+    box[3] = 1;
+    box[4] = 1;
     const cuuint64_t chunk_bytes = (cuuint64_t(es) << c);
     const CUtensorMapL2promotion promo =
         chunk_bytes >= 256 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B
@@ -146,29 +128,27 @@ static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, in
     return EMUSV_OK;
 }
 
-// One strided pass over the group bits [hpos, hpos + g); chunk c = TB - g low bits.
+// One strided pass over the group bits [hpos, hpos + TB - CMIN) with CMIN chunk bits;
+// group bits below TB were applied by pass L and are skipped.
 template <typename R, bool REALC, int EPI>
-static int launch_high(PassParams P, int hpos, int g, const PassArgs &A, const void *part,
+static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *part,
                        cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
-    constexpr int CMIN = PassShape<R>::CMIN, K = sizeof(C) / 8;
-    const int n = P.n;
+    constexpr int CMIN = PassShape<R>::CMIN;
+    const int n = P.n, g = TB - CMIN;
+    if (hpos < CMIN || hpos + g > n) return EMUSV_BAD_ARGUMENT;
     P.hg = g;
-    P.hc = TB - g;
+    P.hc = CMIN;
     P.hpos = hpos;
     P.pbh = 0;
-    P.xb_lo = P.xb_hi = n;
-    int cm = 0;  // chunk rows wider than one 256-element TMA box dimension are split
-    while (((1 << (cm + 1)) * K) <= 256 && cm + 1 <= P.hc) ++cm;
-    P.hsplit = ((1 << P.hc) * K > 256) ? 1 : 0;
+    P.hskip = TB;
     P.hbox_rows = g > 8 ? 256 : (1 << g);
     PassHighMaps M;
-    if (!encode_pass_high(&M.u, A.u, n, (int)sizeof(C), P, cm) ||
-        !encode_pass_high(&M.part, part, n, (int)sizeof(C), P, cm))
+    if (!encode_pass_high(&M.u, A.u, n, (int)sizeof(C), P) ||
+        !encode_pass_high(&M.part, part, n, (int)sizeof(C), P))
         return EMUSV_CUDA_ERROR;
-    auto kern = (P.hc == CMIN) ? k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0>
-                               : k_pass_high<R, REALC, TB, RB, EPI, 0, 0>;
+    auto kern = k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0>;
     const size_t smem = pass_high_smem<C, TB>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -187,8 +167,11 @@ static int launch_high(PassParams P, int hpos, int g, const PassArgs &A, const v
 }
 
 // H v in two or three streaming passes: L (bits 0..TB-1, diagonal), then strided passes
-// over groups of at most TB - CMIN bits.  The partial sums live in HA.part_buf (which may
-// be HA.out: every pass reads a tile before writing it).
+// over groups of G = TB - CMIN bits: the final one over the top G bits [n - G, n), and,
+// when n - TB > G, one before it over [n - 2G, n - G).  Group bits below TB (covered by
+// pass L) are skipped, so every H pass keeps the compile-time chunk of CMIN bits.  The
+// partial sums live in HA.part_buf (which may be HA.out: every pass reads a tile before
+// writing it).
 template <typename R, bool REALC, int EPI_F>
 static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, CMIN = PassShape<R>::CMIN;
@@ -196,10 +179,8 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     PassParams P;
     fill_params(H, TB, RB, &P);
     P.pb = 0;
-    const int rem = n - TB;
-    const int g1 = rem < TB - CMIN ? rem : TB - CMIN;
-    const int g2 = rem - g1;
-    if (g2 > TB - CMIN) return EMUSV_BAD_ARGUMENT;  // more than three passes: n too large
+    const int rem = n - TB, G = TB - CMIN;
+    if (rem > 2 * G) return EMUSV_BAD_ARGUMENT;  // more than three passes: n too large
     if (rem > 0 && !HA.part_buf) return EMUSV_BAD_ARGUMENT;
 
     PassArgs A = {};
@@ -216,14 +197,12 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     }
     A.out = HA.part_buf;
     if ((st = launch_low<R, REALC, EPI_PARTIAL>(P, A, s, nullptr))) return st;
-    if (g2 == 0) {
-        A.out = HA.out;
-        return launch_high<R, REALC, EPI_F>(P, TB, g1, A, HA.part_buf, s, grid_out);
+    if (rem > G) {
+        if ((st = launch_high<R, REALC, EPI_PARTIAL>(P, n - 2 * G, A, HA.part_buf, s, nullptr)))
+            return st;
     }
-    A.out = HA.part_buf;
-    if ((st = launch_high<R, REALC, EPI_PARTIAL>(P, TB, g1, A, HA.part_buf, s, nullptr))) return st;
     A.out = HA.out;
-    return launch_high<R, REALC, EPI_F>(P, TB + g1, g2, A, HA.part_buf, s, grid_out);
+    return launch_high<R, REALC, EPI_F>(P, n - G, A, HA.part_buf, s, grid_out);
 }
 
 // mode: HP_STORE or HP_LANCZOS (values of HpsiMode)

@@ -1,24 +1,27 @@
-// Two-pass fused H*psi for large registers (sm_100a), TMA-staged and double-buffered.
+// Multi-pass fused H*psi for large registers (sm_100a), TMA-staged, three tiles in flight.
 //
 // H = D + sum_p (coefficient x flip of bit p).  Every flip is applied on chip, split over
-// two streaming passes so that each amplitude is read from HBM once per pass:
+// streaming passes so that each amplitude is read from HBM once per pass:
 //
 //  pass L  tile = 2^TB consecutive amplitudes (bits 0..TB-1), brought into shared memory
-//          by one cp.async.bulk per tile; a cluster of 2^pb CTAs holds 2^pb neighbouring
-//          tiles, so the flips of bits TB..TB+pb-1 read the partner from a sibling CTA's
-//          shared memory (DSMEM).  The diagonal (detunings + C6/r^6 interactions) is
-//          rebuilt from per-thread / per-tile FP64 partial energies.  Output: the partial
-//          sum (or H v when no bit is left).
+//          by one cp.async.bulk per tile.  The diagonal (detunings + C6/r^6 interactions)
+//          is rebuilt from per-thread / per-tile FP64 partial energies.  Output: the
+//          partial sum (or H v when no bit is left).
 //  pass H  tile = 2^c contiguous amplitudes (the c low bits, done by pass L) x 2^g
-//          combinations of the top bits, gathered by a 5-D TMA tensor-map load (rows of
-//          32 B or more); a cluster of 2^pbh CTAs covers the pbh bits above the group.
-//          Adds the flips of those bits to the partial sum (also TMA-staged) and runs the
-//          epilogue (store, Lanczos FP64 reductions).
+//          combinations of g higher bits, gathered by a 5-D TMA tensor-map load (rows of
+//          32 B or more).  Adds the flips of those bits to the partial sum (also
+//          TMA-staged) and runs the epilogue (partial, store, Lanczos FP64 reductions).
+//          Registers with more than TB + (TB - c) qubits take two H passes.
 //
-// Both passes keep two tile buffers in flight: the load of tile i+1 is issued when tile
-// i starts computing.  mbarrier waits are bounded (about 2 s of clock): on a timeout the
-// kernel records status EMUSV_TIMEOUT in *A.err, skips the arithmetic and keeps taking
-// part in the cluster barriers so that no CTA is left waiting.
+// Both kernels are templated on a thread-block-cluster size (PB, PBH bits) whose sibling
+// CTAs would serve the next bits from distributed shared memory; the library instantiates
+// PB = PBH = 0 only, because on B200 the per-element DSMEM loads made both passes about
+// twice as slow as one more streaming pass.
+//
+// Each pass keeps SL (SH) = 3 tile buffers in flight: the load of tile i+2 is issued when
+// tile i starts computing.  mbarrier waits are bounded (about 2 s of clock): on a timeout
+// the kernel records status EMUSV_TIMEOUT in *A.err, skips the arithmetic and keeps taking
+// part in the block barriers so that no thread is left waiting.
 //
 // Register blocking: each of the NT = 2^(TB-RB) threads owns NA = 2^RB amplitudes that
 // differ in the RB highest tile bits, so those flips are register-register; the other
@@ -55,9 +58,8 @@ struct PassParams {
     int hc, hg;     // pass H: chunk bits c and group bits g
     int hpos;       // pass H: global position of the first group bit
     int pbh;        // pass H: cluster bits (positions hpos+hg .. hpos+hg+pbh-1)
-    int hsplit;     // pass H: tensor-map layout (0: 5-D with cluster dim, 1: chunk split)
     int hbox_rows;  // pass H: group rows per TMA box (<= 256)
-    int xb_lo, xb_hi;  // pass H: bits [xb_lo, xb_hi) applied from global memory (fallback)
+    int hskip;      // pass H: group bits below this position were applied by pass L
 };
 
 struct PassArgs {
@@ -462,10 +464,10 @@ k_pass_low(const PassParams P, PassArgs A) {
 // Tile local index l = (j << c) | i, i < 2^c (contiguous low bits, applied by pass L),
 // j < 2^g (group bits hpos..hpos+g-1).  A cluster of 2^pbh CTAs holds the tiles that
 // differ in bits hpos+g..hpos+g+pbh-1.  The thread owns l = tid + a*NT;
-// x = base + (l & cmask) + ((l >> c) << hpos).
-// Tensor maps (8-byte elements, dims innermost first) describe the vector as
-//   hsplit 0: [2^c*K, 2^(hpos-c), 2^g, 2^pbh, rest]          (K = sizeof(C)/8)
-//   hsplit 1: [2^cm*K, 2^(c-cm), 2^(hpos-c), 2^g, rest]      (pbh = 0, wide chunks)
+// x = base + (l & cmask) + ((l >> c) << hpos).  Group bits below P.hskip (already applied
+// by pass L when the group overlaps the pass-L tile) are skipped.
+// Tensor map (8-byte elements, dims innermost first): [2^c*K, 2^(hpos-c), 2^g, 2^pbh, rest]
+// with K = sizeof(C)/8.
 template <typename C, int TB>
 __host__ __device__ constexpr size_t pass_high_smem() {
     return 2 * SH * (sizeof(C) << TB) + 8 * SH + sizeof(double) * 8 * NRED;
@@ -476,7 +478,7 @@ struct PassHighMaps {
     CUtensorMap part;  // partial sums of pass L
 };
 
-// CT: chunk bits c at compile time (0: taken from P at run time); PBH: cluster bits.
+// CT: chunk bits c (compile time); PBH: cluster bits.
 template <typename R, bool REALC, int TB, int RB, int EPI, int CT, int PBH>
 __global__ void __launch_bounds__(1 << (TB - RB), 1)
 k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps M) {
@@ -489,7 +491,9 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     C *parts = tiles + ((int64_t)SH << TB);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 2 * SH * TILE_BYTES);
     double *red_scr = reinterpret_cast<double *>(smem_pass + 2 * SH * TILE_BYTES + 8 * SH);
-    const int n = P.n, c = CT ? CT : P.hc, g = TB - c, hpos = P.hpos;
+    static_assert(CT >= 1 && CT <= TB - RB, "chunk bits must lie below the register bits");
+    const int n = P.n, hpos = P.hpos;
+    constexpr int c = CT, g = TB - CT;
     const int tid = threadIdx.x;
     const int64_t cmask = (int64_t(1) << c) - 1;
     const int lowbits = hpos - c;
@@ -515,13 +519,8 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
         for (int b = 0; b < nbox; ++b) {
             unsigned char *dv = reinterpret_cast<unsigned char *>(tiles + ((int64_t)buf << TB)) + b * box_bytes;
             unsigned char *dp = reinterpret_cast<unsigned char *>(parts + ((int64_t)buf << TB)) + b * box_bytes;
-            if (P.hsplit == 0) {
-                tmap_load5(dv, &M.u, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
-                tmap_load5(dp, &M.part, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
-            } else {
-                tmap_load5(dv, &M.u, 0, 0, slo, b * rows, shi, &bars[buf]);
-                tmap_load5(dp, &M.part, 0, 0, slo, b * rows, shi, &bars[buf]);
-            }
+            tmap_load5(dv, &M.u, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
+            tmap_load5(dp, &M.part, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
         }
     };
     if (tid == 0) {
@@ -541,6 +540,10 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
         ccr[r] = bit ? Coef<R>::ure(P, cpos + r) : Coef<R>::dre(P, cpos + r);
         cci[r] = bit ? Coef<R>::uim(P, cpos + r) : Coef<R>::dim(P, cpos + r);
     }
+    // tile bits whose flips this pass applies: group bits at or above P.hskip
+    uint32_t apply = 0;
+    for (int k = c; k < TB; ++k)
+        if (hpos + k - c >= P.hskip) apply |= 1u << k;
     // coefficients of the shared-memory bits (direction fixed by the thread's own bits)
     R cr_s[SB], ci_s[SB];
 #pragma unroll
@@ -564,7 +567,6 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     }
     const double su = A.su_dev ? *A.su_dev : A.su;
     const float suf = float(su);
-    const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
     C *__restrict__ outp = reinterpret_cast<C *>(A.out);
     double red[NRED];
 #pragma unroll
@@ -572,7 +574,7 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     bool ok = true;
     // x offset of amplitude a of this thread: (tid & cmask) + ((tid + a*NT) >> c) << hpos
     const int64_t xt = (tid & cmask) + ((int64_t)(tid >> c) << hpos);
-    const int ash = hpos + SB - c;  // when c <= SB: x offset of a is a << ash
+    const int ash = hpos + SB - c;  // c <= SB: the x offset of amplitude a is a << ash
 
     int it = 0, buf = 0;
     uint32_t phase = 0;
@@ -599,17 +601,17 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
                 const int l = tid + a * NT;
-                const int64_t x = (c <= SB) ? base + xt + ((int64_t)a << ash)
-                                            : base + (l & cmask) + ((int64_t)(l >> c) << hpos);
+                const int64_t x = base + xt + ((int64_t)a << ash);
                 Acc<R> acc;
 #pragma unroll
                 for (int k = 0; k < SB; ++k) {
                     if (k < c) continue;  // chunk bits were applied by pass L
+                    if (!((apply >> k) & 1)) continue;
                     flip_reg<R, REALC>(cr_s[k], ci_s[k], tile[l ^ (1 << k)], acc);
                 }
 #pragma unroll
                 for (int k = 0; k < RB; ++k) {
-                    if (SB + k < c) continue;
+                    if (!((apply >> (SB + k)) & 1)) continue;
                     const bool bit = (a >> k) & 1;
                     flip_reg<R, REALC>(bit ? ur_r[k] : dr_r[k], bit ? ui_r[k] : di_r[k],
                                        v[a ^ (1 << k)], acc);
@@ -619,10 +621,6 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
                     flip_reg<R, REALC>(ccr[r], cci[r],
                                        ld_cluster(raddr[r] + boff + (uint32_t)(a * NT * sizeof(C)),
                                                   (const C *)nullptr), acc);
-                if (CT == 0) {  // very large registers: bits beyond tiles and cluster
-                    for (int p = P.xb_lo; p < P.xb_hi; ++p)
-                        flip_acc<R, REALC>(P, p, (x >> p) & 1, u[x ^ (int64_t(1) << p)], acc);
-                }
                 const C pt = ptile[l];
                 if (EPI == EPI_PARTIAL) {  // another pass follows: unscaled running sum
                     if constexpr (std::is_same<R, float>::value) {

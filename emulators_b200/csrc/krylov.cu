@@ -189,6 +189,9 @@ __device__ void warp_expm_col(int m, const double2 *d, const double2 *up, const 
     int s = 1;
     if (nrm > THETA) s = nrm < THETA * (1 << 20) ? (int)ceil(nrm / THETA) : (1 << 20);
     const double h = 1.0 / s;
+    // reciprocals 1/q (q < 84) by the warp in parallel: no FP64 division in the series
+    __shared__ double inv[84];
+    for (int q = lane; q < 84; q += 32) inv[q] = q ? 1.0 / q : 0.0;
     // padded vectors: index k+1 holds entry k; pads stay zero
     for (int k = lane; k < m + 2; k += 32) {
         y[k] = make_double2(k == 1 ? 1.0 : 0.0, 0.0);
@@ -208,7 +211,7 @@ __device__ void warp_expm_col(int m, const double2 *d, const double2 *up, const 
         double2 S1 = tl, S2 = make_double2(0.5 * tl.x, 0.5 * tl.y);
         double2 *cur = t, *nxt = tn;
         for (int q = 1; q < 80; ++q) {
-            const double f = h / q;
+            const double f = h * inv[q];
             double tmax = 0.0, amax = 0.0;
             for (int k = lane; k < m; k += 32) {
                 const double2 a0 = cur[k + 1], am = cur[k], ap = cur[k + 2];
@@ -232,10 +235,8 @@ __device__ void warp_expm_col(int m, const double2 *d, const double2 *up, const 
                 amax = fmax(amax, fmax(fabs(ac.x), fabs(ac.y)));
             }
             __syncwarp();
-            tmax = warp_max(tmax);
-            amax = warp_max(amax);
             const double2 last = nxt[m];
-            const double w1 = 1.0 / (q + 1), w2 = 1.0 / ((double)(q + 1) * (q + 2));
+            const double w1 = inv[q + 1], w2 = inv[q + 1] * inv[q + 2];
             S1.x += w1 * last.x;
             S1.y += w1 * last.y;
             S2.x += w2 * last.x;
@@ -243,7 +244,11 @@ __device__ void warp_expm_col(int m, const double2 *d, const double2 *up, const 
             double2 *tmp = cur;
             cur = nxt;
             nxt = tmp;
-            if (tmax <= 1e-18 * fmax(amax, 1e-300)) break;
+            if ((q & 3) == 0) {  // test the term size every fourth term (warp shuffles)
+                tmax = warp_max(tmax);
+                amax = warp_max(amax);
+                if (tmax <= 1e-18 * fmax(amax, 1e-300)) break;
+            }
         }
         z2.x += h * z1.x + h * h * S2.x;
         z2.y += h * z1.y + h * h * S2.y;
@@ -256,11 +261,49 @@ __device__ void warp_expm_col(int m, const double2 *d, const double2 *up, const 
     *Z2 = z2;
 }
 
-// Decide iteration j: ||w_j||, happy breakdown, extended exponential, error estimate.
-// do_exp = 0 skips the exponential (convergence is not tested at this j).
+// Extended exponential of iteration jj (the matrix A = -i dt T_H of size jj+1 with the
+// extension entry lo[jj] = -i dt r_jj): writes the coefficients c[0..jj+1] and returns the
+// Expokit error estimate (krylov_exp.py:77-84).  One warp.
+__device__ double krylov_eval(KState *ks, int jj, double dt, double2 *d, double2 *up,
+                              double2 *lo, double2 *y, double2 *t, double2 *tn, double2 *acc) {
+    const int lane = threadIdx.x & 31;
+    const int m = jj + 1;
+    for (int k = lane; k < m; k += 32) {
+        d[k] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
+        up[k] = k > 0 ? make_double2(dt * ks->b_im[k], -dt * ks->b_re[k]) : make_double2(0.0, 0.0);
+        lo[k] = make_double2(0.0, -dt * ks->r[k]);
+    }
+    __syncwarp();
+    double2 Z1, Z2;
+    warp_expm_col(m, d, up, lo, y, t, tn, acc, &Z1, &Z2);
+    // extension: x_{jj+1} = l Z1, x_{jj+2} = l Z2 with l = A[jj+1][jj] = -i dt r_jj
+    const double2 l = lo[jj];
+    const double2 x1 = make_double2(l.x * Z1.x - l.y * Z1.y, l.x * Z1.y + l.y * Z1.x);
+    const double2 x2 = make_double2(l.x * Z2.x - l.y * Z2.y, l.x * Z2.y + l.y * Z2.x);
+    const double err1 = hypot(x1.x, x1.y);                             // krylov_exp.py:81
+    const double err2 = hypot(x2.x, x2.y) * (fabs(dt) * ks->hn[jj]);  // krylov_exp.py:82
+    for (int k = lane; k < m; k += 32) {
+        ks->c_re[k] = y[k + 1].x;
+        ks->c_im[k] = y[k + 1].y;
+    }
+    if (lane == 0) {
+        ks->c_re[m] = x1.x;  // expd[j+1, 0] multiplies v_{j+1} (krylov_exp.py:88-90)
+        ks->c_im[m] = x1.y;
+    }
+    __syncwarp();
+    return err1 < err2 ? err1 : (err1 * err2 / (err1 - err2));  // krylov_exp.py:84
+}
+
+// Decide iteration j: ||w_j||, happy breakdown (every iteration), and, when the host
+// polls (`poll`), the extended exponential and the error estimate.  Iterations the host
+// did not poll are not tested, so on the first poll of a step that finds convergence the
+// kernel walks back over the earlier iterations while they also converge, and stops at
+// the earliest of that run -- the iteration where the reference, which tests every
+// iteration, would have stopped (the estimate decreases with j).  Later kernels of the
+// step return at once once the status leaves KS_RUNNING.
 __global__ void __launch_bounds__(32)
 k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp_tol,
-        double norm_tol, int do_exp, int maxdim) {
+        double norm_tol, int poll, int first_poll, int maxdim) {
     if (ks->status != KS_RUNNING) return;
     if (ks->kerr) {  // a streaming kernel gave up on a bounded wait
         if (threadIdx.x == 0) {
@@ -297,23 +340,19 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
         ks->r[j] = r;
         ks->vv_re[j + 1] = vr / r;  // <v_{j+1}, v_j> = conj(<v_j, w>) / ||w||
         ks->vv_im[j + 1] = -vi / r;
-    }
-    const bool happy = n2 < norm_tol;  // krylov_exp.py:63
-    if (!happy && !do_exp) {
-        if (lane == 0) ks->scale[j + 1] = 1.0 / r;
-        return;
-    }
-    // A = -i dt T_H (complex tridiagonal, size j+1)
-    const int m = j + 1;
-    for (int k = lane; k < m; k += 32) {
-        d[k] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
-        up[k] = k > 0 ? make_double2(dt * ks->b_im[k], -dt * ks->b_re[k]) : make_double2(0.0, 0.0);
-        lo[k] = make_double2(0.0, -dt * (k == j ? r : ks->r[k]));  // lo[j]: extension entry
+        ks->scale[j + 1] = 1.0 / r;
     }
     __syncwarp();
-    double2 Z1, Z2;
-    warp_expm_col(m, d, up, lo, y, t, tn, acc, &Z1, &Z2);
-    if (happy) {  // krylov_exp.py:65-71: exp(T[:j+1,:j+1]) e_0 over j+1 vectors
+    const int m = j + 1;
+    if (n2 < norm_tol) {  // krylov_exp.py:63-71: exp(T[:j+1,:j+1]) e_0 over j+1 vectors
+        for (int k = lane; k < m; k += 32) {
+            d[k] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
+            up[k] = k > 0 ? make_double2(dt * ks->b_im[k], -dt * ks->b_re[k]) : make_double2(0.0, 0.0);
+            lo[k] = make_double2(0.0, -dt * ks->r[k]);
+        }
+        __syncwarp();
+        double2 Z1, Z2;
+        warp_expm_col(m, d, up, lo, y, t, tn, acc, &Z1, &Z2);
         for (int k = lane; k < m; k += 32) {
             ks->c_re[k] = y[k + 1].x;
             ks->c_im[k] = y[k + 1].y;
@@ -325,24 +364,22 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
         }
         return;
     }
-    // extension: x_{j+1} = l Z1, x_{j+2} = l Z2 with l = A[j+1][j] = -i dt r_j
-    const double2 l = lo[j];
-    const double2 x1 = make_double2(l.x * Z1.x - l.y * Z1.y, l.x * Z1.y + l.y * Z1.x);
-    const double2 x2 = make_double2(l.x * Z2.x - l.y * Z2.y, l.x * Z2.y + l.y * Z2.x);
-    const double err1 = hypot(x1.x, x1.y);                       // krylov_exp.py:81
-    const double err2 = hypot(x2.x, x2.y) * (adt * ks->hn[j]);  // krylov_exp.py:82
-    const double err = err1 < err2 ? err1 : (err1 * err2 / (err1 - err2));  // :84
-    for (int k = lane; k < m; k += 32) {
-        ks->c_re[k] = y[k + 1].x;
-        ks->c_im[k] = y[k + 1].y;
+    if (!poll) return;
+    double err = krylov_eval(ks, j, dt, d, up, lo, y, t, tn, acc);
+    int jc = j;  // iteration whose coefficients are in ks->c
+    if (err < exp_tol && first_poll) {
+        for (int jj = j - 1; jj >= 0; --jj) {
+            const double e = krylov_eval(ks, jj, dt, d, up, lo, y, t, tn, acc);
+            if (!(e < exp_tol)) break;
+            err = e;
+            jc = jj;
+        }
+        if (jc != j) krylov_eval(ks, jc, dt, d, up, lo, y, t, tn, acc);  // its coefficients
     }
     if (lane == 0) {
-        ks->c_re[m] = x1.x;  // expd[j+1, 0] multiplies v_{j+1} (krylov_exp.py:88-90)
-        ks->c_im[m] = x1.y;
-        ks->scale[j + 1] = 1.0 / r;
         ks->err = err;
-        ks->nvec = m + 1;
-        ks->iters = j + 1;
+        ks->nvec = jc + 2;
+        ks->iters = jc + 1;
         if (err < exp_tol)
             ks->status = KS_CONVERGED;
         else if (j + 1 >= maxdim)
@@ -531,6 +568,7 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
     EMUSV_CHECK_LAUNCH();
 
     int status = KS_RUNNING;
+    bool polled = false;
     for (int j = 0; j < max_krylov_dim; ++j) {
         if (j + 1 > capacity) {
             int st = read_status(W.ks, s, &status);
@@ -566,14 +604,17 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
                                                    const_cast<void *>(stored(j + 1)), D, W.part_o);
             }
         EMUSV_CHECK_LAUNCH();
-        const int do_exp = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
+        // convergence is tested from the hint on; the first test of the step also looks
+        // back over the untested iterations (k_small)
+        const int poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
         {
             ProfScope ps_(PROF_SMALL, s);
-            k_small<<<1, 32, 0, s>>>(W.ks, j, W.part_o, sg, dt, exp_tolerance, norm_tolerance, do_exp,
-                                     max_krylov_dim);
+            k_small<<<1, 32, 0, s>>>(W.ks, j, W.part_o, sg, dt, exp_tolerance, norm_tolerance,
+                                     poll, poll && !polled, max_krylov_dim);
         }
         EMUSV_CHECK_LAUNCH();
-        if (do_exp) {
+        if (poll) {
+            polled = true;
             st = read_status(W.ks, s, &status);
             if (st) return st;
             if (status != KS_RUNNING) break;

@@ -59,8 +59,9 @@ class _StepCache:
 
 
 _caches: dict = {}
-# When true, convergence is first tested one iteration before the previous step's count
-# (a hint only adds iterations, so results stay within tolerance of the reference).
+# When true, convergence is first tested one iteration before the previous step's count;
+# a first test that converges looks back over the untested iterations (emusv_krylov_step),
+# so the hint saves host synchronisations without moving the stopping iteration.
 use_iteration_hint: bool = True
 
 

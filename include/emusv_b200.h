@@ -118,7 +118,9 @@ size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity);
  * (emu_sv/time_evolution/torch.py:143-219) with krylov_exp
  * (emu_base/math/krylov_exp.py:23-131) and RydbergHamiltonian.__mul__ as the operator.
  * Convergence is tested from iteration `krylov_dim_hint` on (0: every iteration, as the
- * reference does; a hint only ever adds iterations, never removes one).
+ * reference does); when the first test already converges, the earlier iterations are
+ * tested backwards while they converge too, so the step stops where the reference stops
+ * whenever the error estimate decreases with the iteration count.
  * psi_out may equal psi_in.  Returns EMUSV_NOT_CONVERGED (result still written, as
  * krylov_exp_impl does) or EMUSV_WORKSPACE_TOO_SMALL (nothing written; retry with a
  * larger basis).  `info` (host) may be NULL.  Synchronises the stream at every

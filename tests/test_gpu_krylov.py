@@ -111,3 +111,27 @@ def test_in_place_and_unitarity_large():
     assert st == 0 and abs(info.output_norm - 1.0) < 1e-12
     back, _, _ = fused_step(HamiltonianExpOperator(H, -0.005), out, 1e-10, 1e-10, 100)
     assert torch.linalg.vector_norm(back - psi).item() < 1e-9
+
+
+def test_stale_iteration_hint_keeps_the_stopping_iteration():
+    """A hint far above the needed iteration count (left by another problem of the same
+    size) must not change the step: the first convergence test looks back over the
+    iterations it skipped."""
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian, krylov
+    from emulators_b200 import workloads as wl
+
+    w = wl.lattice_n20()
+    H = RydbergHamiltonian(*(torch.as_tensor(a) for a in (w.omega[0], w.delta[0], w.phi[0], w.U)),
+                           DEV)
+    psi = torch.zeros(1 << w.nqubits, dtype=torch.complex128, device=DEV)
+    psi[0] = 1.0
+    op = HamiltonianExpOperator(H, w.dt)
+    outs = []
+    for stale in (0, 60):
+        krylov.release_workspaces()
+        c = krylov._cache(psi.device, w.nqubits, 0)
+        c.last_iters = stale
+        out, info, st = krylov.fused_step(op, psi, w.tolerance, w.tolerance, 100)
+        outs.append((out.cpu().numpy(), info.iterations))
+    assert outs[0][1] == outs[1][1]
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
