@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import re
 import os
 import statistics
 import subprocess
@@ -42,6 +43,18 @@ def peaks() -> tuple[float, str]:
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def ncu_traffic() -> int | None:
+    """DRAM bytes (read + write) of one H*psi at N=26 from the committed ncu summary
+    (profiles/hpsi_passes_ladder_n25_c64.md: a capture at N=25 scaled by 2)."""
+    p = os.path.join(REPO, "profiles", "hpsi_passes_ladder_n25_c64.md")
+    try:
+        with open(p) as f:
+            m = re.search(r"traffic_bytes_per_hpsi_at_n26:\s*(\d+)", f.read())
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
 
 
 def log(msg: str) -> None:
@@ -263,7 +276,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                                "and diagonal on chip, Lanczos reductions fused), per Lanczos "
                                "iteration; achieved = 2*D*8 algorithmic bytes / H*psi time",
                      "achieved": round(achieved, 1), "peak": hbm, "peak_source": which,
-                     "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                     "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                     "traffic": ncu_traffic() if n == 26 and es == 8 else None,
+                     "traffic_source": "ncu --set full of the three passes at N=25, x2 "
+                                       "(profiles/hpsi_passes_ladder_n25_c64.md)",
                      "algorithmic_bytes_per_launch": alg_hpsi,
                      "avg_launch_ms": round(hpsi_avg_s * 1e3, 4),
                      "per_kernel": per_pass,
@@ -273,6 +289,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "secondary": {"hpsi_standalone": hstand},
         "e2e": e2e,
     }
+    if not args.no_plain and world == 1:
+        plain = plain_torch_c128(w, dev)
+        plain["ours_c64_over_plain"] = round(value / world / plain["steps_per_s"], 2)
+        result["secondary"]["plain_torch_c128_gpu"] = plain
+        log(f"plain complex128 torch path: {plain}")
+    if not args.no_precision and world == 1:
+        result["secondary"]["precision"] = precision_check(w, dev)
+        log(f"precision: {result['secondary']['precision']}")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
     if dist:
@@ -325,6 +349,134 @@ def run_e2e(w, W, K, dev, dist, world) -> dict:
             "d2h_bytes_per_step": int(d2h), "wall_s": round(wall, 3),
             "api": "SVBackendImpl(SVConfig(precision='c64'), SequenceData)._run()",
             "observations": n_obs}
+
+
+# ------------------------------------------------------------------ precision form check
+def precision_check(w, dev) -> dict:
+    """The whole workload (all steps) in complex64/FP64 and in complex128 through the same
+    kernels, from |g...g>: infidelity and state error of the complex64 run every 100
+    steps against the complex128 run (itself checked against the oracle in the tests)."""
+    import torch
+
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian, krylov
+    from emulators_b200.krylov import fused_step
+
+    n, D = w.nqubits, 1 << w.nqubits
+    U = torch.as_tensor(w.U)
+    states = {}
+    rates = {}
+    snaps = {torch.complex64: [], torch.complex128: []}
+    for dt_ in (torch.complex64, torch.complex128):
+        krylov.release_workspaces()
+        a = torch.zeros(D, dtype=dt_, device=dev)
+        a[0] = 1.0
+        b = torch.empty_like(a)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(w.nsteps):
+            H = RydbergHamiltonian(torch.as_tensor(w.omega[k]), torch.as_tensor(w.delta[k]),
+                                   torch.as_tensor(w.phi[k]), U, dev)
+            _, info, st = fused_step(HamiltonianExpOperator(H, w.dt), a, w.tolerance,
+                                     w.tolerance, w.max_krylov_dim, out=b)
+            a, b = b, a
+            if (k + 1) % 100 == 0 or k + 1 == w.nsteps:
+                snaps[dt_].append(a.to(torch.complex128).cpu())
+        torch.cuda.synchronize()
+        rates[dt_] = w.nsteps / (time.perf_counter() - t0)
+        states[dt_] = a
+        del b
+    krylov.release_workspaces()
+    infid, errs = [], []
+    for x, y in zip(snaps[torch.complex64], snaps[torch.complex128]):
+        ov = abs(torch.vdot(y, x).item()) ** 2 / (torch.vdot(x, x).real.item() * torch.vdot(y, y).real.item())
+        infid.append(float(f"{1 - ov:.3e}"))
+        errs.append(float(f"{torch.linalg.vector_norm(x - y).item():.3e}"))
+    return {"steps": w.nsteps, "every": 100, "infidelity_c64_vs_c128": infid,
+            "state_error_c64_vs_c128": errs,
+            "c64_steps_per_s_untimed_loop": round(rates[torch.complex64], 3),
+            "c128_steps_per_s_untimed_loop": round(rates[torch.complex128], 3)}
+
+
+# ------------------------------------------------------------------ plain complex128 GPU path
+def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1) -> dict:
+    """The plain complex128 GPU path: the reference's algorithm written with plain torch
+    tensor ops (the reference modules themselves are not on the GPU machine) -- per-qubit
+    strided-view flips, the diagonal rebuilt every step from view slices, the Lanczos loop
+    with the tridiagonal matrix, its exponential and the error estimate on the host and one
+    host synchronisation per reduction (emu_sv/hamiltonian.py:69-162,
+    emu_base/math/krylov_exp.py:23-131).  Timed over `steps` steps after `warm`."""
+    import scipy.linalg
+    import torch
+
+    n, D = w.nqubits, 1 << w.nqubits
+    U = np.asarray(w.U)
+
+    def diagonal(de):
+        d = torch.zeros(D, dtype=torch.complex128, device=dev)
+        for i in range(n):
+            d.view(2 ** i, 2, -1)[:, 1] -= float(de[i])
+            for j in range(i + 1, n):
+                if U[i, j] != 0.0:
+                    d.view(2 ** i, 2, 2 ** (j - i - 1), 2, -1)[:, 1, :, 1] += float(U[i, j])
+        return d
+
+    def hpsi(v, d, coef):
+        out = d * v
+        for i in range(n):
+            vv, oo = v.view(2 ** i, 2, -1), out.view(2 ** i, 2, -1)
+            oo[:, 1] += coef[i] * vv[:, 0]
+            oo[:, 0] += np.conj(coef[i]) * vv[:, 1]
+        return out
+
+    def step(k, psi):
+        coef = 0.5 * np.asarray(w.omega[k]) * np.exp(1j * np.asarray(w.phi[k]))
+        d = diagonal(w.delta[k])
+        dt, tol, mk = w.dt, w.tolerance, w.max_krylov_dim
+        nrm = torch.linalg.vector_norm(psi).item()
+        V = [psi / nrm]
+        T = np.zeros((mk + 2, mk + 2), dtype=np.complex128)
+        for j in range(mk):
+            wv = (-1j * dt) * hpsi(V[-1], d, coef)
+            nn = torch.linalg.vector_norm(wv).item()
+            for kk in range(max(0, j - 1), j + 1):
+                ov = torch.vdot(V[kk], wv).item()
+                T[kk, j] = ov
+                wv -= ov * V[kk]
+            n2 = torch.linalg.vector_norm(wv).item()
+            T[j + 1, j] = n2
+            if n2 < tol:
+                e = scipy.linalg.expm(T[:j + 1, :j + 1])[:, 0]
+                return nrm * sum(complex(e[i]) * V[i] for i in range(j + 1))
+            V.append(wv / n2)
+            T[j + 2, j + 1] = 1.0
+            e = scipy.linalg.expm(T[:j + 3, :j + 3])[:, 0]
+            err1, err2 = abs(e[j + 1]), abs(e[j + 2] * nn)
+            err = err1 if err1 < err2 else err1 * err2 / (err1 - err2)
+            if err < tol:
+                return nrm * sum(complex(e[i]) * V[i] for i in range(j + 2))
+        raise RecursionError("plain path did not converge")
+
+    psi = torch.zeros(D, dtype=torch.complex128, device=dev)
+    psi[0] = 1.0
+    for k in range(warm):
+        psi = step(k, psi)
+    if dev.type != "cuda":  # host run (checks of this function only)
+        for k in range(warm, warm + steps):
+            psi = step(k, psi)
+        return {"state": psi}
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(warm, warm + steps):
+        psi = step(k, psi)
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    del psi
+    torch.cuda.empty_cache()
+    return {"steps_per_s": round(steps / el, 4), "unit": UNIT,
+            "sample": f"steps {warm}..{warm + steps - 1} of ladder_n26 in complex128 after "
+                      f"{warm} warm-up step(s); CUDA events"}
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
@@ -386,6 +538,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=30.0)
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain complex128 torch GPU path")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the complex64-vs-complex128 run of the whole workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
