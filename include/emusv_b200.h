@@ -153,6 +153,40 @@ int emusv_adjoint_step(int nqubits, int dtype, double dt, const double *omegas,
                        double *g_interaction, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/* ---- batched evolution: many registers in one persistent launch ----
+ * Replaces running the reference's time loop (emu_sv/sv_backend_impl.py:197-209, one
+ * krylov_exp per step, krylov_exp.py:23-131) once per register: every register of the
+ * batch (its own size up to emusv_batch_max_qubits(), pulse and step count) takes all its
+ * steps inside ONE cooperative persistent kernel.  States are packed back to back in
+ * instance order (2^n_i amplitudes each) in one device buffer and evolved in place.
+ * Host arrays, packed in instance order: omegas/deltas/phis [sum_i nsteps_i * n_i]
+ * (step-major per instance, qubit order), interactions [sum_i n_i * n_i] (row-major,
+ * upper triangle read), dt [ninst] (us).  tile_bits T (8-10 for complex64, 8-9 for
+ * complex128, T <= every n_i) and blocks_per_sm are launch shapes (autotuned by the
+ * Python layer); basis_capacity bounds the Krylov basis of every instance. */
+int emusv_batch_max_qubits(void);
+size_t emusv_batch_workspace_bytes(int ninst, const int *nqubits, const int *nsteps, int dtype,
+                                   int tile_bits, int basis_capacity);
+/* Uploads the tables (coefficients, interaction tables, per-instance layout) into the
+ * workspace and records `states`; synchronises the stream. */
+int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const double *dt,
+                        int dtype, const double *omegas, const double *deltas, const double *phis,
+                        const double *interactions, void *states, double exp_tolerance,
+                        double norm_tolerance, int max_krylov_dim, int tile_bits,
+                        int basis_capacity, void *workspace, size_t workspace_bytes,
+                        void *stream);
+/* One memset and one cooperative launch (stream-ordered only, so it can be captured in a
+ * CUDA graph and replayed): evolves every instance through all its steps. */
+int emusv_batch_launch(int dtype, int tile_bits, int blocks_per_sm, void *workspace, void *stream);
+/* CTAs per SM the persistent kernel can keep resident for this shape (0: no such shape). */
+int emusv_batch_max_blocks_per_sm(int dtype, int tile_bits);
+/* Per-instance emusv_status (EMUSV_NOT_CONVERGED = RecursionError of that instance,
+ * EMUSV_WORKSPACE_TOO_SMALL = basis_capacity too small) and the Krylov iteration count of
+ * every step [ninst][max_steps] into host arrays; returns the worst status, or
+ * EMUSV_TIMEOUT if a grid barrier gave up.  Synchronises the stream. */
+int emusv_batch_results(int ninst, int max_steps, void *workspace, int *status_out,
+                        int *iterations_out, void *stream);
+
 /* ---- building blocks of the generic krylov_exp(op, v, ...) (krylov_exp.py:23-106) ----
  * For an arbitrary operator applied by the caller, these give the FP64-accumulated
  * Lanczos arithmetic and the on-device exponential of the extended Krylov matrix. */

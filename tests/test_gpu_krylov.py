@@ -135,3 +135,35 @@ def test_stale_iteration_hint_keeps_the_stopping_iteration():
         outs.append((out.cpu().numpy(), info.iterations))
     assert outs[0][1] == outs[1][1]
     np.testing.assert_array_equal(outs[0][0], outs[1][0])
+
+
+def test_iteration_hint_matches_testing_every_iteration():
+    """A chain whose iteration count goes up and down by one between steps: the first
+    convergence test of a step that already converges must keep the stopping iteration's
+    coefficients, so the hinted run equals the run that tests every iteration."""
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian, krylov
+    from emulators_b200 import workloads as wl
+
+    rng = np.random.default_rng(3)
+    n, steps = 13, 12
+    U = wl.interaction_matrix(wl.random_box(n, 27.0, 5.0, rng))
+    om = rng.uniform(0, 2 * np.pi, steps)
+    de = rng.uniform(-20, 20, steps)
+    ph = rng.normal(size=(steps, n))
+    runs = []
+    for hint in (False, True):
+        krylov.use_iteration_hint = hint
+        krylov.release_workspaces()
+        s = torch.zeros(1 << n, dtype=torch.complex128, device=DEV)
+        s[0] = 1.0
+        its = []
+        for k in range(steps):
+            H = RydbergHamiltonian(torch.full((n,), om[k]), torch.full((n,), de[k]),
+                                   torch.as_tensor(ph[k]), torch.as_tensor(U), DEV)
+            s, info, st = krylov.fused_step(HamiltonianExpOperator(H, 0.01), s, 1e-10, 1e-10, 100)
+            its.append(info.iterations)
+        runs.append((s.cpu().numpy(), its))
+    krylov.use_iteration_hint = True
+    assert runs[0][1] == runs[1][1]
+    assert len(set(np.diff(runs[0][1]).tolist()) & {-1}) == 1  # a count drops by one
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
