@@ -55,6 +55,12 @@ SIGNATURES: dict[str, tuple] = {
     "emusv_batch_prepare": (_I, [_I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _D, _I, _I, _I, _P,
                                  _SZ, _P]),
     "emusv_batch_launch": (_I, [_I, _I, _I, _P, _P]),
+    "emusv_batch_launch_steps": (_I, [_I, _I, _I, _I, _I, _P, _P, _I, _P, _P]),
+    "emusv_batch_adjoint_workspace_bytes": (_SZ, [_I, _P, _P, _I, _I, _I]),
+    "emusv_batch_adjoint_prepare": (_I, [_I, _P, _P, _P, _I, _P, _P, _P, _P, _D, _I, _I, _I, _P,
+                                         _SZ, _P]),
+    "emusv_batch_adjoint_launch": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "emusv_batch_adjoint_iterations": (_I, [_I, _P, _P, _P]),
     "emusv_batch_max_blocks_per_sm": (_I, [_I, _I]),
     "emusv_batch_results": (_I, [_I, _I, _P, _P, _P, _P]),
     "emusv_vec_dot": (_I, [_I64, _I, _P, _P, _P, _P, _SZ, _P]),

@@ -25,12 +25,13 @@
 //  * grid barriers are an arrival counter plus a generation word; every wait is bounded
 //    (about a second of SM clock): on a timeout the kernel records EMUSV_TIMEOUT and
 //    every CTA returns.  The launch is cooperative, so all CTAs are co-resident.
-//  * convergence is tested from a per-instance hint (the previous step's count - 1), and
-//    the first test of a step looks back over the untested iterations (krylov_decide), so
-//    each instance stops where the reference would.
+//  * convergence is tested from a per-instance hint (the previous step's count - 3); a
+//    first test that already converges tests the skipped iterations in order
+//    (krylov_decide), so each instance stops where the reference would.
 #include <math.h>
 #include <string.h>
 
+#include <initializer_list>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -46,11 +47,16 @@ constexpr int BS_IDLE = 16;      // instance has no step left
 constexpr int BS_CAPACITY = 17;  // Krylov basis larger than the workspace's capacity
 constexpr long long BAR_LIMIT = 2000000000LL;  // clock cycles a barrier waits at most
 
+// One Lanczos "job": an instance's state (the forward evolution, or the state half of an
+// adjoint step) or an adjoint step's incoming gradient.
 struct BInst {
     int n, nsteps, tile0, ntiles;
-    long long off;  // amplitude offset of this instance in every slot
+    long long off;   // amplitude offset of this job in every stored-vector slot
+    long long off0;  // offset of its vector 0 in the buffer v0[src]
     double dt;
-    int coef0;      // index of this instance's step-0 record in the coefficient array
+    int coef0;       // index of the instance's step-0 record in the coefficient array
+    int pidx;        // instance index (interaction tables)
+    int src;         // vector 0 lives in v0[src]
     int pad;
 };
 
@@ -58,6 +64,7 @@ struct BInst {
 struct BCoef {
     double up_re[BMAXQ], up_im[BMAXQ];  // coefficient of |1><0| on bit p (Omega/2 e^{i phi})
     double field[BMAXQ];                // -delta
+    double om[BMAXQ], ph[BMAXQ];        // Omega and phi (the adjoint's derivative operators)
     float fup_re[BMAXQ], fup_im[BMAXQ];
 };
 
@@ -82,11 +89,32 @@ struct BArgs {
     double *sumA, *sumB, *sumN;     // [ninst][4] their per-instance totals
     unsigned *cnt;                  // [3][ninst] tiles done per phase kind (A, B, N)
     int *ranB;                      // [ninst] 1 + last round whose phase B ran the instance
-    void *states;         // slot 0 (the caller's packed states, in place)
+    void *v0[2];          // buffers holding every job's vector 0 (forward: the packed states,
+                          // evolved in place; adjoint: states and incoming gradients)
     unsigned char *slots;  // slots 1..capacity
     long long slot_amps;
     BCtl *ctl;
+    // set per launch
+    int first_step;       // absolute index of the launch's first step
+    int run_steps;        // steps this launch takes
+    void *hist;           // optional: states after every hist_every-th step
+    int hist_every;
+    long long hist_stride;  // amplitudes per history slot
 };
+
+// Adjoint step (k_batch_adj): jobs 2i (state psi_i) and 2i+1 (gradient g_i) of instance i.
+struct BAdj {
+    int ninst, step, mmax;  // instances, absolute step, largest basis (scratch sizing)
+    double2 *dS;            // [ninst][mmax*mmax]: dS[r][k] at r*mmax + k
+    unsigned char *E;       // E_k of every instance: [mmax][inst_amps]
+    long long inst_amps;
+    double *partC;          // [total job tiles][NCP] contraction partials
+    double *grads;          // [ninst][3][BMAXQ] dL/dOmega, dL/ddelta, dL/dphi by qubit
+    void *gout;             // packed state gradient exp(+i dt H) g
+    unsigned *cntC;         // [ninst]
+    int *astatus;           // [ninst] emusv status of the instance's adjoint
+};
+constexpr int NCP = 6 * BMAXQ;  // per bit: T_re, T_im, U_re, U_im, S_re, S_im
 
 // ---------------------------------------------------------------- grid barrier
 // Arrival counter + generation; the last arriver also clears the tile counter of the
@@ -184,9 +212,16 @@ __device__ __forceinline__ double3 ld_sum(const double *sum, int i) {
                         __ldcg(sum + 4 * (size_t)i + 2));
 }
 
+// |o|^2 added to an FP64 sum with explicit fused operations, so the norm of a vector
+// written by a combination and the norm of the same vector read back agree to the bit.
+template <typename C>
+__device__ __forceinline__ void add_sq(double &acc, C o) {
+    acc = fma(double(o.x), double(o.x), fma(double(o.y), double(o.y), acc));
+}
+
 template <typename C>
 __device__ __forceinline__ C *vec_ptr(const BArgs &A, int k, const BInst &I) {
-    if (k == 0) return reinterpret_cast<C *>(A.states) + I.off;
+    if (k == 0) return reinterpret_cast<C *>(A.v0[I.src]) + I.off0;
     return reinterpret_cast<C *>(A.slots + (size_t)(k - 1) * (size_t)A.slot_amps * sizeof(C)) + I.off;
 }
 
@@ -216,8 +251,8 @@ __device__ void tile_hpsi(const BArgs &A, const BInst &I, int i, int t, int step
     const int lane = threadIdx.x & 31;
     const int n = I.n;
     const long long base = (long long)(t - I.tile0) << T;
-    const BCoef &cf = A.coef[I.coef0 + step];
-    const double *Ub = A.Ubits + (size_t)i * BMAXQ * BMAXQ;
+    const BCoef &cf = A.coef[I.coef0 + step];  // step: absolute
+    const double *Ub = A.Ubits + (size_t)I.pidx * BMAXQ * BMAXQ;
     const C *u = vec_ptr<C>(A, j, I);
     C *out = vec_ptr<C>(A, j + 1, I);
     // per-tile diagonal terms: fields of the low bits including the high bits' pairs
@@ -246,7 +281,7 @@ __device__ void tile_hpsi(const BArgs &A, const BInst &I, int i, int t, int step
     double freg[T - 5];
 #pragma unroll
     for (int k = 0; k < T - 5; ++k) freg[k] = __shfl_sync(0xffffffffu, fl, 5 + k);
-    const double *El = A.Elow + ((size_t)i << T);
+    const double *El = A.Elow + ((size_t)I.pidx << T);
 
     C v[AMP];
     R ar[AMP], ai[AMP];
@@ -378,10 +413,7 @@ __device__ void tile_norm(const BArgs &A, const BInst &I, int i, int t) {
     const C *u = vec_ptr<C>(A, 0, I);
     double nrm = 0.0;
 #pragma unroll 8
-    for (int a = 0; a < AMP; ++a) {
-        const C o = ldcg(u + base + lane + 32 * a);
-        nrm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
-    }
+    for (int a = 0; a < AMP; ++a) add_sq(nrm, ldcg(u + base + lane + 32 * a));
     nrm = warp_sum(nrm);
     if (lane == 0) A.partN[4 * (size_t)t] = nrm;
     tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
@@ -392,364 +424,685 @@ __device__ __forceinline__ int ld_status(const KState *ks) {
 }
 __device__ __forceinline__ int ld_vol(const int *p) { return *(volatile const int *)p; }
 
-// ---------------------------------------------------------------- the persistent kernel
-// Phase bookkeeping keeps every instance's tiles either all processed or all skipped in a
-// phase (so the per-instance tile counters complete): phase A_j runs an instance if its
-// step starts (j = 0) or if phase B of the previous round ran it (ranB), never from a
-// status that the decisions of the same phase may be changing.
-template <typename R, int T, int MINB>
-__global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch(const BArgs A) {
-    typedef typename cvec<R>::T C;
-    __shared__ KSmem S;
-    __shared__ int s_flag;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned ph = 0;
-    int round = 0;  // phase-B rounds so far (the same in every CTA)
+// ---------------------------------------------------------------- phases
+// Phase bookkeeping keeps every job's tiles either all processed or all skipped in a
+// phase (so the per-job tile counters complete): phase A_j runs a job if its step starts
+// (j = 0) or if phase B of the previous round ran it (ranB), never from a status that the
+// decisions of the same phase may be changing.
 
-    // initial norms
+// Norms of every job's vector 0 (into sumN).
+template <typename R, int T>
+__device__ void norm_phase(const BArgs &A, unsigned ph) {
     for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
         const int i = inst_of_tile(A, t);
         tile_norm<R, T>(A, A.inst[i], i, t);
     }
-    if (!grid_sync(A.ctl, ph)) return;
+}
 
-    for (int step = 0; step < A.max_steps; ++step) {
-        for (int j = 0;; ++j) {
-            // ---------------- phase A_j: decisions for j-1 (init at j = 0), tiles H v_j
-            if (warp == 0) {
-                for (int i = blockIdx.x; i < A.ninst; i += gridDim.x) {
-                    const BInst I = A.inst[i];
-                    KState *ks = A.ks + i;
-                    if (j == 0) {
-                        if (lane == 0) {
-                            const double s0 = sqrt(__ldcg(A.sumN + 4 * (size_t)i));
-                            int st = KS_RUNNING;
-                            const int f = ld_vol(&A.fail[i]);
-                            if (f) st = f;
-                            else if (step >= I.nsteps) st = BS_IDLE;
-                            else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
-                            ks->s0 = s0;
-                            ks->scale[0] = 1.0 / s0;
-                            ks->iters = 0;
-                            ks->nvec = 0;
-                            ks->kerr = 0;
-                            ks->err = 0.0;
-                            A.polled[i] = 0;
-                            ks->status = st;
-                            if (st == KS_NONFINITE) A.fail[i] = st;
-                        }
-                        __syncwarp();
-                        continue;
-                    }
-                    if (ld_status(ks) != KS_RUNNING) continue;
-                    const int jj = j - 1;
-                    const double3 sb = ld_sum(A.sumB, i);
-                    const int hint = A.hint[i];
-                    const bool poll = (jj + 1 >= hint) || (jj + 1 >= A.maxdim);
-                    const bool first = poll && !A.polled[i];
-                    __syncwarp();
-                    if (lane == 0 && poll) A.polled[i] = 1;
-                    krylov_decide(ks, jj, sb.x, sb.y, sb.z, I.dt, A.exp_tol, A.norm_tol, poll,
-                                  first, A.maxdim, S);
-                    if (lane == 0) {
-                        int st = ks->status;
-                        if (st == KS_RUNNING && jj + 2 > A.capacity) {
-                            st = BS_CAPACITY;
-                            ks->status = st;
-                        }
-                        if (st == KS_NONFINITE || st == BS_CAPACITY) A.fail[i] = st;
-                        if (st != KS_RUNNING) {
-                            A.iters_out[(size_t)i * A.max_steps + step] = ks->iters;
-                            A.hint[i] = ks->iters > 1 ? ks->iters - 1 : 0;
-                        }
-                    }
-                    __syncwarp();
-                }
-            }
-            if (j < A.maxdim && j + 1 <= A.capacity) {
-                for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
-                    const int i = inst_of_tile(A, t);
-                    const BInst I = A.inst[i];
-                    double sj;
-                    if (j == 0) {
-                        if (step >= I.nsteps || ld_vol(&A.fail[i])) continue;
-                        sj = 1.0 / sqrt(__ldcg(A.sumN + 4 * (size_t)i));
-                    } else {
-                        if (ld_vol(&A.ranB[i]) != round) continue;  // B ran it last round
-                        sj = 1.0 / sqrt(__ldcg(A.sumB + 4 * (size_t)i));
-                    }
-                    if (!isfinite(sj) || sj <= 0.0) continue;  // the same for all its tiles
-                    tile_hpsi<R, T>(A, I, i, t, step, j, sj);
-                }
-            }
-            if (!grid_sync(A.ctl, ph)) return;
-            // does any instance still iterate?
-            if (warp == 0) {
-                int any = 0;
-                for (int i = lane; i < A.ninst; i += 32) any |= ld_status(A.ks + i) == KS_RUNNING;
-                any = __any_sync(0xffffffffu, any);
-                if (lane == 0) s_flag = any;
-            }
-            __syncthreads();
-            if (!s_flag) break;
-            // ---------------- phase B_j: w = H v_j - a v_j - b v_{j-1}
-            {
-                int ci = -1;
-                double car = 0, cai = 0, cb = 0, sj = 0;
-                for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
-                    const int i = inst_of_tile(A, t);
-                    KState *ks = A.ks + i;
-                    if (ld_status(ks) != KS_RUNNING) continue;
-                    const BInst I = A.inst[i];
-                    if (i != ci) {
-                        const double3 s = ld_sum(A.sumA, i);
-                        const double b = j > 0 ? __ldcg(&ks->r[j - 1]) : 0.0;
-                        const double vr = j > 0 ? __ldcg(&ks->vv_re[j]) : 0.0;
-                        const double vi = j > 0 ? __ldcg(&ks->vv_im[j]) : 0.0;
-                        const double ar = s.y - b * vr, ai = s.z - b * vi;
-                        sj = __ldcg(&ks->scale[j]);
-                        const double sp = j > 0 ? __ldcg(&ks->scale[j - 1]) : 0.0;
-                        car = ar * sj;
-                        cai = ai * sj;
-                        cb = b * sp;
-                        ci = i;
-                        // the warp of the instance's first tile records T_H's column j (a warp
-                        // meets a given instance's first tile before any other of its tiles)
-                        if (t == I.tile0 && lane == 0) {
-                            ks->a_re[j] = ar;
-                            ks->a_im[j] = ai;
-                            ks->b_re[j] = b;
-                            ks->b_im[j] = 0.0;
-                            ks->hn[j] = sqrt(s.x);
-                            A.ranB[i] = round + 1;  // 0 (cleared at launch) = never
-                        }
-                    }
-                    tile_orth<R, T>(A, I, i, t, j, car, cai, cb, sj);
-                }
-            }
-            if (!grid_sync(A.ctl, ph)) return;
-            ++round;
-        }
-        // ---------------- combination of every instance that took this step
-        {
-            int ci = -1, nvec = 0;
-            double cr0 = 0, ci0 = 0, cr1 = 0, ci1 = 0, cr2 = 0, ci2 = 0, cr3 = 0, ci3 = 0;
-            for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
-                const int i = inst_of_tile(A, t);
-                const KState *ks = A.ks + i;
-                const int st = ld_status(ks);
+// All Lanczos iterations of one step of every job (krylov_exp.py:49-106 per job).
+// gstep: absolute step (coefficients, whether the job still has this step); rstep: the
+// launch-relative step (iteration record).  Returns false if a barrier gave up.
+template <typename R, int T>
+__device__ bool krylov_rounds(const BArgs &A, int gstep, int rstep, unsigned &ph, int &round,
+                              int &s_flag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = 0;; ++j) {
+        // ---------------- phase A_j: decisions for j-1 (init at j = 0), tiles H v_j
+        if (warp == 0) {
+            for (int i = blockIdx.x; i < A.ninst; i += gridDim.x) {
                 const BInst I = A.inst[i];
-                if (st != KS_CONVERGED && st != KS_HAPPY && st != KS_MAXDIM) {
-                    // idle or failed: keep the state, refresh its norm for the next step
-                    tile_norm<R, T>(A, I, i, t);
+                KState *ks = A.ks + i;
+                if (j == 0) {
+                    if (lane == 0) {
+                        const double s0 = sqrt(__ldcg(A.sumN + 4 * (size_t)i));
+                        int st = KS_RUNNING;
+                        const int f = ld_vol(&A.fail[i]);
+                        if (f) st = f;
+                        else if (gstep >= I.nsteps) st = BS_IDLE;
+                        else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
+                        ks->s0 = s0;
+                        ks->scale[0] = 1.0 / s0;
+                        ks->iters = 0;
+                        ks->nvec = 0;
+                        ks->kerr = 0;
+                        ks->err = 0.0;
+                        A.polled[i] = 0;
+                        ks->status = st;
+                        if (st == KS_NONFINITE) A.fail[i] = st;
+                    }
+                    __syncwarp();
                     continue;
                 }
-                if (i != ci) {
-                    // coefficients s0 scale_k c_k (k < nvec <= 128): lane k % 32 holds block
-                    // k / 32 in registers; the combination reads them by shuffles
-                    nvec = __ldcg(&ks->nvec);
-                    const double s0 = __ldcg(&ks->s0);
-                    double *cr[4] = {&cr0, &cr1, &cr2, &cr3}, *cim[4] = {&ci0, &ci1, &ci2, &ci3};
-#pragma unroll
-                    for (int blk = 0; blk < 4; ++blk) {
-                        const int k = lane + 32 * blk;
-                        double a = 0.0, b = 0.0;
-                        if (k < nvec) {
-                            const double f = s0 * __ldcg(&ks->scale[k]);
-                            a = f * __ldcg(&ks->c_re[k]);
-                            b = f * __ldcg(&ks->c_im[k]);
-                        }
-                        *cr[blk] = a;
-                        *cim[blk] = b;
+                if (ld_status(ks) != KS_RUNNING) continue;
+                const int jj = j - 1;
+                const double3 sb = ld_sum(A.sumB, i);
+                const int hint = A.hint[i];
+                const bool poll = (jj + 1 >= hint) || (jj + 1 >= A.maxdim);
+                const bool first = poll && !A.polled[i];
+                __syncwarp();
+                if (lane == 0 && poll) A.polled[i] = 1;
+                krylov_decide(ks, jj, sb.x, sb.y, sb.z, I.dt, A.exp_tol, A.norm_tol, poll, first,
+                              A.maxdim);
+                if (lane == 0) {
+                    int st = ks->status;
+                    if (st == KS_RUNNING && jj + 2 > A.capacity) {
+                        st = BS_CAPACITY;
+                        ks->status = st;
                     }
-                    ci = i;
-                }
-                constexpr int AMP = 1 << (T - 5);
-                constexpr int CH = AMP < 4 ? AMP : 4;
-                const long long base = (long long)(t - I.tile0) << T;
-                C *out = vec_ptr<C>(A, 0, I);
-                double nrm = 0.0;
-                for (int a0 = 0; a0 < AMP; a0 += CH) {
-                    double re[CH], im[CH];
-#pragma unroll
-                    for (int c = 0; c < CH; ++c) re[c] = im[c] = 0.0;
-                    for (int k = 0; k < nvec; ++k) {
-                        const int src = k & 31, blk = k >> 5;
-                        const double vr = blk == 0 ? cr0 : blk == 1 ? cr1 : blk == 2 ? cr2 : cr3;
-                        const double vi = blk == 0 ? ci0 : blk == 1 ? ci1 : blk == 2 ? ci2 : ci3;
-                        const double c_r = __shfl_sync(0xffffffffu, vr, src);
-                        const double c_i = __shfl_sync(0xffffffffu, vi, src);
-                        const C *vk = vec_ptr<C>(A, k, I) + base + lane;
-                        C b[CH];
-#pragma unroll
-                        for (int c = 0; c < CH; ++c) b[c] = ldcg(vk + 32 * (a0 + c));
-#pragma unroll
-                        for (int c = 0; c < CH; ++c) {
-                            re[c] += c_r * double(b[c].x) - c_i * double(b[c].y);
-                            im[c] += c_r * double(b[c].y) + c_i * double(b[c].x);
-                        }
-                    }
-#pragma unroll
-                    for (int c = 0; c < CH; ++c) {
-                        const C o = cmake<C>(re[c], im[c]);
-                        out[base + lane + 32 * (a0 + c)] = o;
-                        nrm += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+                    if (st == KS_NONFINITE || st == BS_CAPACITY) A.fail[i] = st;
+                    if (st != KS_RUNNING) {
+                        A.iters_out[(size_t)i * A.max_steps + rstep] = ks->iters;
+                        A.hint[i] = ks->iters > 3 ? ks->iters - 3 : 0;  // poll a little early
                     }
                 }
-                nrm = warp_sum(nrm);
-                if (lane == 0) A.partN[4 * (size_t)t] = nrm;
-                tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
+                __syncwarp();
             }
         }
+        if (j < A.maxdim && j + 1 <= A.capacity) {
+            for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+                const int i = inst_of_tile(A, t);
+                const BInst I = A.inst[i];
+                double sj;
+                if (j == 0) {
+                    if (gstep >= I.nsteps || ld_vol(&A.fail[i])) continue;
+                    sj = 1.0 / sqrt(__ldcg(A.sumN + 4 * (size_t)i));
+                } else {
+                    if (ld_vol(&A.ranB[i]) != round) continue;  // B ran it last round
+                    sj = 1.0 / sqrt(__ldcg(A.sumB + 4 * (size_t)i));
+                }
+                if (!isfinite(sj) || sj <= 0.0) continue;  // the same for all its tiles
+                tile_hpsi<R, T>(A, I, i, t, gstep, j, sj);
+            }
+        }
+        if (!grid_sync(A.ctl, ph)) return false;
+        // does any job still iterate?
+        if (warp == 0) {
+            int any = 0;
+            for (int i = lane; i < A.ninst; i += 32) any |= ld_status(A.ks + i) == KS_RUNNING;
+            any = __any_sync(0xffffffffu, any);
+            if (lane == 0) s_flag = any;
+        }
+        __syncthreads();
+        if (!s_flag) return true;
+        // ---------------- phase B_j: w = H v_j - a v_j - b v_{j-1}
+        {
+            int ci = -1;
+            double car = 0, cai = 0, cb = 0, sj = 0;
+            for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+                const int i = inst_of_tile(A, t);
+                KState *ks = A.ks + i;
+                if (ld_status(ks) != KS_RUNNING) continue;
+                const BInst I = A.inst[i];
+                if (i != ci) {
+                    const double3 sa = ld_sum(A.sumA, i);
+                    const double b = j > 0 ? __ldcg(&ks->r[j - 1]) : 0.0;
+                    const double vr = j > 0 ? __ldcg(&ks->vv_re[j]) : 0.0;
+                    const double vi = j > 0 ? __ldcg(&ks->vv_im[j]) : 0.0;
+                    const double ar = sa.y - b * vr, ai = sa.z - b * vi;
+                    sj = __ldcg(&ks->scale[j]);
+                    const double sp = j > 0 ? __ldcg(&ks->scale[j - 1]) : 0.0;
+                    car = ar * sj;
+                    cai = ai * sj;
+                    cb = b * sp;
+                    ci = i;
+                    // the warp of the job's first tile records T_H's column j (a warp meets a
+                    // given job's first tile before any other of its tiles)
+                    if (t == I.tile0 && lane == 0) {
+                        ks->a_re[j] = ar;
+                        ks->a_im[j] = ai;
+                        ks->b_re[j] = b;
+                        ks->b_im[j] = 0.0;
+                        ks->hn[j] = sqrt(sa.x);
+                        A.ranB[i] = round + 1;  // 0 (cleared at launch) = never
+                    }
+                }
+                tile_orth<R, T>(A, I, i, t, j, car, cai, cb, sj);
+            }
+        }
+        if (!grid_sync(A.ctl, ph)) return false;
+        ++round;
+    }
+}
+
+// Lane k % 32 holds coefficient block k / 32 (k < 128): f * c_k with f = s0 scale_k, or
+// the conjugate of c_k (exp(+i dt H) from the same basis).
+__device__ __forceinline__ void load_coefs(const KState *ks, int nvec, bool conj_c, double (&cr)[4],
+                                           double (&cim)[4]) {
+    const int lane = threadIdx.x & 31;
+    const double s0 = __ldcg(&ks->s0);
+#pragma unroll
+    for (int blk = 0; blk < 4; ++blk) {
+        const int k = lane + 32 * blk;
+        double a = 0.0, b = 0.0;
+        if (k < nvec) {
+            const double f = s0 * __ldcg(&ks->scale[k]);
+            a = f * __ldcg(&ks->c_re[k]);
+            b = f * __ldcg(&ks->c_im[k]);
+            if (conj_c) b = -b;
+        }
+        cr[blk] = a;
+        cim[blk] = b;
+    }
+}
+
+// out(tile) = sum_k coef_k stored_k(tile) over k < nvec; returns the tile's ||out||^2.
+template <typename R, int T>
+__device__ double tile_lincomb(const BArgs &A, const BInst &I, int t, int nvec, const double (&cr)[4],
+                               const double (&cim)[4], typename cvec<R>::T *out) {
+    typedef typename cvec<R>::T C;
+    constexpr int AMP = 1 << (T - 5);
+    constexpr int CH = AMP < 4 ? AMP : 4;
+    const int lane = threadIdx.x & 31;
+    const long long base = (long long)(t - I.tile0) << T;
+    double nrm = 0.0;
+    for (int a0 = 0; a0 < AMP; a0 += CH) {
+        double re[CH], im[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) re[c] = im[c] = 0.0;
+        for (int k = 0; k < nvec; ++k) {
+            const int src = k & 31, blk = k >> 5;
+            const double vr = blk == 0 ? cr[0] : blk == 1 ? cr[1] : blk == 2 ? cr[2] : cr[3];
+            const double vi = blk == 0 ? cim[0] : blk == 1 ? cim[1] : blk == 2 ? cim[2] : cim[3];
+            const double c_r = __shfl_sync(0xffffffffu, vr, src);
+            const double c_i = __shfl_sync(0xffffffffu, vi, src);
+            const C *vk = vec_ptr<C>(A, k, I) + base + lane;
+            C b[CH];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) b[c] = ldcg(vk + 32 * (a0 + c));
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                re[c] += c_r * double(b[c].x) - c_i * double(b[c].y);
+                im[c] += c_r * double(b[c].y) + c_i * double(b[c].x);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const C o = cmake<C>(re[c], im[c]);
+            out[base + lane + 32 * (a0 + c)] = o;
+            add_sq(nrm, o);
+        }
+    }
+    return warp_sum(nrm);
+}
+
+// psi' = s0 sum_k c_k v_k for every job that took the step (norm partials for the next
+// step), optionally also into the history buffer.
+template <typename R, int T>
+__device__ void combine_phase(const BArgs &A, int rstep, unsigned ph) {
+    typedef typename cvec<R>::T C;
+    const int lane = threadIdx.x & 31;
+    int ci = -1, nvec = 0;
+    double cr[4], cim[4];
+    const bool hist = A.hist && ((rstep + 1) % A.hist_every) == 0;
+    for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+        const int i = inst_of_tile(A, t);
+        const KState *ks = A.ks + i;
+        const int st = ld_status(ks);
+        const BInst I = A.inst[i];
+        if (st != KS_CONVERGED && st != KS_HAPPY && st != KS_MAXDIM) {
+            tile_norm<R, T>(A, I, i, t);  // idle or failed: keep the state, refresh its norm
+            continue;
+        }
+        if (i != ci) {
+            nvec = __ldcg(&ks->nvec);
+            load_coefs(ks, nvec, false, cr, cim);
+            ci = i;
+        }
+        C *out = vec_ptr<C>(A, 0, I);
+        const double nrm = tile_lincomb<R, T>(A, I, t, nvec, cr, cim, out);
+        if (hist) {  // copy the new tile into the history slot
+            constexpr int AMP = 1 << (T - 5);
+            const long long base = (long long)(t - I.tile0) << T;
+            C *h = reinterpret_cast<C *>(A.hist) +
+                   (size_t)((rstep + 1) / A.hist_every - 1) * (size_t)A.hist_stride + I.off0;
+            __syncwarp();
+            for (int a = 0; a < AMP; ++a) h[base + lane + 32 * a] = out[base + lane + 32 * a];
+        }
+        if (lane == 0) A.partN[4 * (size_t)t] = nrm;
+        tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
+    }
+}
+
+// ---------------------------------------------------------------- forward kernel
+template <typename R, int T, int MINB>
+__global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch(const BArgs A) {
+    __shared__ int s_flag;
+    const int lane = threadIdx.x & 31;
+    unsigned ph = 0;
+    int round = 0;  // phase-B rounds so far (the same in every CTA)
+    norm_phase<R, T>(A, ph);
+    if (!grid_sync(A.ctl, ph)) return;
+    for (int step = 0; step < A.run_steps; ++step) {
+        if (!krylov_rounds<R, T>(A, A.first_step + step, step, ph, round, s_flag)) return;
+        combine_phase<R, T>(A, step, ph);
         if (!grid_sync(A.ctl, ph)) return;
     }
-    // final statuses
-    if (threadIdx.x < 32) {
+    if (threadIdx.x < 32) {  // final statuses
         for (int i = blockIdx.x * 32 + lane; i < A.ninst; i += gridDim.x * 32) {
             const int st = ld_status(A.ks + i);
-            A.status_out[i] = A.fail[i] ? A.fail[i] : (st == BS_IDLE ? KS_CONVERGED : st);
+            const int f = A.fail[i];
+            A.status_out[i] = f ? f : (st == BS_IDLE ? KS_CONVERGED : st);
         }
+    }
+}
+
+// ---------------------------------------------------------------- adjoint kernel
+// Basis size of a finished Lanczos job (double_krylov.py:100-113).
+__device__ __forceinline__ int basis_size(const KState *ks) {
+    const int st = ld_status(ks);
+    const int it = __ldcg(&ks->iters);
+    return st == KS_HAPPY ? it : it + 1;
+}
+
+__device__ __forceinline__ bool job_ok(const KState *ks) {
+    const int st = ld_status(ks);
+    return st == KS_CONVERGED || st == KS_HAPPY;
+}
+
+// dS column `col` of instance i: y = exp(B) e_{ms+col} for the block matrix
+// B = [[A_s, e0 e0^T], [0, A_g]] (A = -i dt T of each basis, the coupling taken as 1:
+// double_krylov.py:54-57 scales it by |state||grad| afterwards), rows 0..ms-1 of y.
+// One warp per column, Chebyshev form (the spectrum of B is that of the two blocks).
+__device__ __forceinline__ void block_row(const KState *ks, int kk, int m, double dt, double2 &d,
+                                          double2 &l, double2 &u, double &td, double &tr) {
+    const int jj = __ldcg(&ks->iters) - 1;  // last Lanczos column; row jj+1 is the appended one
+    d = l = u = make_double2(0.0, 0.0);
+    td = tr = 0.0;
+    if (kk <= jj) {
+        const double ar = __ldcg(&ks->a_re[kk]), ai = __ldcg(&ks->a_im[kk]);
+        d = make_double2(dt * ai, -dt * ar);
+        td = ar;
+        tr = fabs(ai);
+    }
+    if (kk >= 1) {
+        const double r = __ldcg(&ks->r[kk - 1]);
+        l = make_double2(0.0, -dt * r);
+        tr += fabs(r);
+    }
+    if (kk + 1 <= jj && kk + 1 < m) {
+        const double br = __ldcg(&ks->b_re[kk + 1]), bi = __ldcg(&ks->b_im[kk + 1]);
+        u = make_double2(dt * bi, -dt * br);
+        tr += hypot(br, bi);
+    }
+}
+
+constexpr int DS_NE = 8;  // block matrices up to 256 rows
+
+__global__ void __launch_bounds__(BWARPS * 32) k_batch_dS(const BArgs A, const BAdj D) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.y, col = blockIdx.x * BWARPS + warp;
+    const KState *kss = A.ks + 2 * i, *ksg = A.ks + 2 * i + 1;
+    if (!job_ok(kss) || !job_ok(ksg)) return;
+    const int ms = basis_size(kss), mg = basis_size(ksg), M = ms + mg;
+    if (col >= mg || M > 32 * DS_NE || ms > D.mmax || mg > D.mmax) return;
+    const double dt = A.inst[2 * i].dt;
+    double2 d[DS_NE], l[DS_NE], u[DS_NE], y[DS_NE];
+    double td[DS_NE], tr[DS_NE];
+#pragma unroll
+    for (int e = 0; e < DS_NE; ++e) {
+        const int k = lane * DS_NE + e;
+        d[e] = l[e] = u[e] = make_double2(0.0, 0.0);
+        td[e] = tr[e] = 0.0;
+        if (k < ms) block_row(kss, k, ms, dt, d[e], l[e], u[e], td[e], tr[e]);
+        else if (k < M) block_row(ksg, k - ms, mg, dt, d[e], l[e], u[e], td[e], tr[e]);
+        if (k == 0) tr[e] += 1.0 / fabs(dt);  // the coupling entry 1 in T units
+    }
+    cheb_expm<DS_NE>(d, l, u, ms, make_double2(1.0, 0.0), ms + col, dt, td, tr, M, y);
+    double2 *out = D.dS + (size_t)i * D.mmax * D.mmax;
+#pragma unroll
+    for (int e = 0; e < DS_NE; ++e) {
+        const int r = lane * DS_NE + e;
+        if (r < ms) out[r * D.mmax + col] = y[e];
+    }
+}
+
+template <typename R, int T, int MINB>
+__global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_rounds(const BArgs A, const BAdj D) {
+    __shared__ int s_flag;
+    unsigned ph = 0;
+    int round = 0;
+    norm_phase<R, T>(A, ph);
+    if (!grid_sync(A.ctl, ph)) return;
+    krylov_rounds<R, T>(A, D.step, 0, ph, round, s_flag);
+}
+
+template <typename R, int T, int MINB>
+__global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_post(const BArgs A, const BAdj D) {
+    typedef typename cvec<R>::T C;
+    constexpr int AMP = 1 << (T - 5);
+    const int lane = threadIdx.x & 31;
+    unsigned ph = 0;
+
+    // ---------------- E_k = sum_r dS[r][k] v^s_r (state tiles); g_out (gradient tiles)
+    for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+        const int J = inst_of_tile(A, t), i = J >> 1;
+        const KState *kss = A.ks + 2 * i, *ksg = A.ks + 2 * i + 1;
+        const BInst I = A.inst[J];
+        const long long base = (long long)(t - I.tile0) << T;
+        if (!job_ok(kss) || !job_ok(ksg)) {
+            if ((J & 1) && __ldcg(&ksg->s0) == 0.0) {  // exp(+i dt H) 0 = 0
+                C *o = reinterpret_cast<C *>(D.gout) + I.off0 + base + lane;
+                for (int a = 0; a < AMP; ++a) o[32 * a] = cmake<C>(0.0, 0.0);
+            }
+            continue;
+        }
+        const int ms = basis_size(kss), mg = basis_size(ksg);
+        if (J & 1) {  // state gradient from the gradient basis
+            double cr[4], cim[4];
+            const int nvec = __ldcg(&ksg->nvec);
+            load_coefs(ksg, nvec, true, cr, cim);
+            tile_lincomb<R, T>(A, I, t, nvec, cr, cim, reinterpret_cast<C *>(D.gout) + I.off0);
+            continue;
+        }
+        const double2 *dS = D.dS + (size_t)i * D.mmax * D.mmax;
+        constexpr int KC = 4, CH = AMP < 4 ? AMP : 4;
+        for (int k0 = 0; k0 < mg; k0 += KC) {
+            for (int a0 = 0; a0 < AMP; a0 += CH) {
+                double er[KC][CH], ei[KC][CH];
+#pragma unroll
+                for (int kk = 0; kk < KC; ++kk)
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) er[kk][c] = ei[kk][c] = 0.0;
+                for (int r = 0; r < ms; ++r) {
+                    const double sc = __ldcg(&kss->scale[r]);
+                    const C *vr = vec_ptr<C>(A, r, I) + base + lane;
+                    C v[CH];
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) v[c] = ldcg(vr + 32 * (a0 + c));
+#pragma unroll
+                    for (int kk = 0; kk < KC; ++kk) {
+                        if (k0 + kk >= mg) break;
+                        const double2 d = dS[r * D.mmax + k0 + kk];
+                        const double dr = sc * d.x, di = sc * d.y;
+#pragma unroll
+                        for (int c = 0; c < CH; ++c) {
+                            er[kk][c] += dr * double(v[c].x) - di * double(v[c].y);
+                            ei[kk][c] += dr * double(v[c].y) + di * double(v[c].x);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int kk = 0; kk < KC; ++kk) {
+                    if (k0 + kk >= mg) break;
+                    C *Ek = reinterpret_cast<C *>(D.E + (size_t)(k0 + kk) * D.inst_amps * sizeof(C)) + I.off0;
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) Ek[base + lane + 32 * (a0 + c)] = cmake<C>(er[kk][c], ei[kk][c]);
+                }
+            }
+        }
+    }
+    if (!grid_sync(A.ctl, ph)) return;
+
+    // ---------------- contractions over state tiles; the last tile of an instance turns
+    // its sums into the step's gradients (torch.py:324-353)
+    for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+        const int J = inst_of_tile(A, t), i = J >> 1;
+        if (J & 1) continue;
+        const KState *kss = A.ks + 2 * i, *ksg = A.ks + 2 * i + 1;
+        const BInst I = A.inst[J], IG = A.inst[J + 1];
+        const int n = I.n;
+        const long long base = (long long)(t - I.tile0) << T;
+        double acc[6] = {0, 0, 0, 0, 0, 0};  // lane p: T, U, S sums of bit p
+        const bool ok = job_ok(kss) && job_ok(ksg);
+        if (ok) {
+            const int mg = basis_size(ksg);
+            double rr[AMP], ri[AMP];
+#pragma unroll
+            for (int a = 0; a < AMP; ++a) rr[a] = ri[a] = 0.0;
+            for (int k = 0; k < mg; ++k) {
+                const double gs = __ldcg(&ksg->scale[k]);
+                const C *gk = vec_ptr<C>(A, k, IG) + base + lane;
+                const C *Ek = reinterpret_cast<const C *>(D.E + (size_t)k * D.inst_amps * sizeof(C)) + I.off0;
+                double gr[AMP], gi[AMP];
+                C e[AMP];
+#pragma unroll
+                for (int a = 0; a < AMP; ++a) {
+                    const C g = ldcg(gk + 32 * a);
+                    gr[a] = gs * double(g.x);
+                    gi[a] = -gs * double(g.y);  // conj
+                    e[a] = ldcg(Ek + base + lane + 32 * a);
+                    rr[a] += gr[a] * double(e[a].x) - gi[a] * double(e[a].y);
+                    ri[a] += gr[a] * double(e[a].y) + gi[a] * double(e[a].x);
+                }
+                for (int p = 0; p < n; ++p) {
+                    double tr = 0, ti = 0, ur = 0, ui = 0;
+#pragma unroll
+                    for (int a = 0; a < AMP; ++a) {
+                        C w;
+                        int bit;
+                        if (p < 5) {
+                            w = shfl_c(e[a], 1 << p);
+                            bit = (lane >> p) & 1;
+                        } else if (p < T) {
+                            w = e[a ^ (1 << (p - 5))];
+                            bit = (a >> (p - 5)) & 1;
+                        } else {
+                            w = ldcg(Ek + (base ^ (1LL << p)) + lane + 32 * a);
+                            bit = (int)((base >> p) & 1);
+                        }
+                        const double pr = gr[a] * double(w.x) - gi[a] * double(w.y);
+                        const double pi = gr[a] * double(w.y) + gi[a] * double(w.x);
+                        tr += pr;
+                        ti += pi;
+                        if (bit) {
+                            ur += pr;
+                            ui += pi;
+                        }
+                    }
+                    tr = warp_sum(tr);
+                    ti = warp_sum(ti);
+                    ur = warp_sum(ur);
+                    ui = warp_sum(ui);
+                    if (lane == p) {
+                        acc[0] += tr;
+                        acc[1] += ti;
+                        acc[2] += ur;
+                        acc[3] += ui;
+                    }
+                }
+            }
+            for (int p = 0; p < n; ++p) {  // S_pp = sum over x with bit p of rho(x)
+                double sr = 0, si = 0;
+#pragma unroll
+                for (int a = 0; a < AMP; ++a) {
+                    const long long x = base + lane + 32 * a;
+                    if ((x >> p) & 1) {
+                        sr += rr[a];
+                        si += ri[a];
+                    }
+                }
+                sr = warp_sum(sr);
+                si = warp_sum(si);
+                if (lane == p) {
+                    acc[4] += sr;
+                    acc[5] += si;
+                }
+            }
+        }
+        double *pc = D.partC + (size_t)t * NCP;
+        if (lane < n)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) pc[6 * lane + c] = acc[c];
+        // count the tile; the instance's last tile finalises
+        unsigned old = 0;
+        if (lane == 0) {
+            __threadfence();
+            old = atomicAdd(&D.cntC[i], 1u);
+        }
+        old = __shfl_sync(0xffffffffu, old, 0);
+        if (old != (unsigned)I.ntiles - 1) continue;
+        __threadfence();
+        if (lane == 0) D.cntC[i] = 0;
+        double *g = D.grads + (size_t)i * 3 * BMAXQ;
+        if (!ok) {  // a zero gradient (or a failed basis): no parameter gradient
+            const bool zero = __ldcg(&ksg->s0) == 0.0;
+            if (lane < n) g[lane] = g[BMAXQ + lane] = g[2 * BMAXQ + lane] = 0.0;
+            if (lane == 0) {
+                int e = EMUSV_OK;
+                if (!zero) {
+                    e = EMUSV_NONFINITE;
+                    for (const KState *k2 : {kss, ksg}) {
+                        const int st = ld_status(k2);
+                        if (st == KS_MAXDIM) e = EMUSV_NOT_CONVERGED;  // double_krylov.py:107-110
+                        if (st == BS_CAPACITY) e = EMUSV_WORKSPACE_TOO_SMALL;
+                    }
+                }
+                D.astatus[i] = e;
+            }
+            continue;
+        }
+        double sum[6] = {0, 0, 0, 0, 0, 0};  // lane p: instance sums of bit p
+        if (lane < n)
+            for (int tt = 0; tt < I.ntiles; ++tt)
+#pragma unroll
+                for (int c = 0; c < 6; ++c) sum[c] += __ldcg(D.partC + (size_t)(I.tile0 + tt) * NCP + 6 * lane + c);
+        if (lane < n) {
+            const int p = lane, q = n - 1 - p;  // bit p is qubit q
+            const BCoef &cf = A.coef[I.coef0 + D.step];
+            const double dt = I.dt, c = __ldcg(&kss->s0) * __ldcg(&ksg->s0);
+            const double Ure = sum[2], Uim = sum[3], Dre = sum[0] - sum[2], Dim = sum[1] - sum[3];
+            // Re(-i dt c <.>) for a flip with coefficient a on |1><0| and conj(a) on |0><1|
+            auto flip = [&](double ar, double ai) {
+                const double im = ar * Uim + ai * Ure + ar * Dim - ai * Dre;
+                return dt * c * im;
+            };
+            const double om = cf.om[p], phv = cf.ph[p];
+            g[q] = flip(0.5 * cos(phv), 0.5 * sin(phv));                     // DHDOmegaSparse
+            g[BMAXQ + q] = dt * c * (-sum[5]);                              // DHDDeltaSparse: -n
+            g[2 * BMAXQ + q] = flip(-0.5 * om * sin(phv), 0.5 * om * cos(phv));  // DHDPhiSparse
+        }
+        if (lane == 0) D.astatus[i] = EMUSV_OK;
     }
 }
 
 // ---------------------------------------------------------------- host side
 static size_t al256(size_t v) { return (v + 255) / 256 * 256; }
 
+// Workspace layout.  Forward: one job per instance.  Adjoint: jobs 2i (state) and 2i+1
+// (gradient) per instance, plus the adjoint's own arrays.
 struct BLayout {
-    size_t args, ctl, ints, inst, coef, ubits, elow, ks, sums, iters, partA, partB, partN, slots,
-        total;
-    int total_tiles;
-    long long slot_amps;
-    int coef_count;
+    size_t args, ctl, ints, inst, coef, ubits, elow, ks, sums, iters, partA, partB, partN, slots;
+    size_t dS, escr, E, partC, total;
+    int njobs, total_tiles, coef_count, max_steps, mmax, escr_warps;
+    long long inst_amps, slot_amps;
 };
 
+
 static bool layout(int ninst, const int *nq, const int *nsteps, int es, int T, int capacity,
-                   int max_steps, BLayout *L) {
+                   bool adjoint, BLayout *L) {
     long long amps = 0;
-    int tiles = 0, coefs = 0;
+    int tiles = 0, coefs = 0, max_steps = 0;
     for (int i = 0; i < ninst; ++i) {
         if (nq[i] < T || nq[i] > BMAXQ || nsteps[i] < 0) return false;
         amps += 1LL << nq[i];
         tiles += 1 << (nq[i] - T);
-        coefs += nsteps[i] > 0 ? nsteps[i] : 0;
+        coefs += nsteps[i];
+        max_steps = nsteps[i] > max_steps ? nsteps[i] : max_steps;
     }
+    const int nj = adjoint ? 2 * ninst : ninst;
+    L->njobs = nj;
+    L->inst_amps = amps;
+    L->slot_amps = adjoint ? 2 * amps : amps;
+    L->total_tiles = adjoint ? 2 * tiles : tiles;
+    L->coef_count = coefs;
+    L->max_steps = adjoint ? 1 : max_steps;
+    L->mmax = capacity + 1;
     size_t off = 0;
     auto take = [&](size_t b) { const size_t o = off; off += al256(b); return o; };
     L->args = take(sizeof(BArgs));
-    // control block and per-instance integer flags, contiguous: cleared by every launch
+    // control block and integer flags, contiguous so that a launch clears them in one go:
+    // hint, polled, fail, status, ranB, cnt[3] per job, then the adjoint's counters
     L->ctl = off;
     off += sizeof(BCtl);
     L->ints = off;
-    off += sizeof(int) * 8 * ninst;  // hint, polled, fail, status, ranB, cnt[3]
+    off += sizeof(int) * (8 * (size_t)nj + ninst);
     off = al256(off);
-    L->inst = take(sizeof(BInst) * ninst);
+    L->inst = take(sizeof(BInst) * nj);
     L->coef = take(sizeof(BCoef) * (coefs > 0 ? coefs : 1));
     L->ubits = take(sizeof(double) * BMAXQ * BMAXQ * ninst);
     L->elow = take(sizeof(double) * ((size_t)ninst << T));
-    L->ks = take(sizeof(KState) * ninst);
-    L->sums = take(sizeof(double) * 12 * ninst);
-    L->iters = take(sizeof(int) * (size_t)ninst * (max_steps > 0 ? max_steps : 1));
-    L->partA = take(sizeof(double) * 4 * tiles);
-    L->partB = take(sizeof(double) * 4 * tiles);
-    L->partN = take(sizeof(double) * 4 * tiles);
-    L->slots = take((size_t)capacity * (size_t)amps * es);
+    L->ks = take(sizeof(KState) * nj);
+    L->sums = take(sizeof(double) * 12 * nj);
+    L->iters = take(sizeof(int) * (size_t)nj * (L->max_steps > 0 ? L->max_steps : 1));
+    L->partA = take(sizeof(double) * 4 * L->total_tiles);
+    L->partB = take(sizeof(double) * 4 * L->total_tiles);
+    L->partN = take(sizeof(double) * 4 * L->total_tiles);
+    L->slots = take((size_t)capacity * (size_t)L->slot_amps * es);
+    L->dS = L->escr = L->E = L->partC = off;
+    L->escr_warps = 0;
+    if (adjoint) {
+        L->dS = take(sizeof(double2) * ninst * (size_t)L->mmax * L->mmax);
+        L->E = take((size_t)L->mmax * (size_t)amps * es);
+        L->partC = take(sizeof(double) * NCP * (size_t)L->total_tiles);
+    }
     L->total = off;
-    L->total_tiles = tiles;
-    L->slot_amps = amps;
-    L->coef_count = coefs;
     return true;
 }
 
-// Register-heavy shapes (32 complex64 or 16 complex128 amplitudes per lane) keep one CTA
-// per SM; the smaller ones are compiled for two.
 template <typename R, int T>
-static void *kernel_ptr() {
-    constexpr int MINB = (sizeof(R) == 4 ? T >= 10 : T >= 9) ? 1 : 2;
-    return reinterpret_cast<void *>(k_batch<R, T, MINB>);
-}
+struct Shape {
+    // register-heavy shapes (32 complex64 or 16 complex128 amplitudes per lane) keep one
+    // CTA per SM; the smaller ones are compiled for two
+    static constexpr int MINB = (sizeof(R) == 4 ? T >= 10 : T >= 9) ? 1 : 2;
+};
 
-// Host copies of the argument blocks prepared per workspace (the launch passes the block
-// by value, so the kernel reads it from the parameter bank).
-static std::mutex g_args_mu;
-static std::unordered_map<const void *, BArgs> g_args;
-
-static void *pick_kernel(int dtype, int T) {
+// kind 0: forward; 1: adjoint rounds; 2: adjoint post-processing
+static void *pick_kernel(int dtype, int T, int kind) {
+#define EMUSV_K(R, TT)                                                                   \
+    (kind == 1   ? reinterpret_cast<void *>(k_batch_adj_rounds<R, TT, Shape<R, TT>::MINB>) \
+     : kind == 2 ? reinterpret_cast<void *>(k_batch_adj_post<R, TT, Shape<R, TT>::MINB>)   \
+                 : reinterpret_cast<void *>(k_batch<R, TT, Shape<R, TT>::MINB>))
     if (dtype == EMUSV_C64) {
-        if (T == 8) return kernel_ptr<float, 8>();
-        if (T == 9) return kernel_ptr<float, 9>();
-        if (T == 10) return kernel_ptr<float, 10>();
+        if (T == 8) return EMUSV_K(float, 8);
+        if (T == 9) return EMUSV_K(float, 9);
+        if (T == 10) return EMUSV_K(float, 10);
     } else if (dtype == EMUSV_C128) {
-        if (T == 8) return kernel_ptr<double, 8>();
-        if (T == 9) return kernel_ptr<double, 9>();
+        if (T == 8) return EMUSV_K(double, 8);
+        if (T == 9) return EMUSV_K(double, 9);
     }
+#undef EMUSV_K
     return nullptr;
 }
 
-}  // namespace emusv
-
-using namespace emusv;
-
-extern "C" {
-
-int emusv_batch_max_qubits(void) { return BMAXQ; }
-
-size_t emusv_batch_workspace_bytes(int ninst, const int *nqubits, const int *nsteps, int dtype,
-                                   int tile_bits, int basis_capacity) {
-    if (ninst < 1 || !nqubits || !nsteps || basis_capacity < 1 || !pick_kernel(dtype, tile_bits))
-        return 0;
-    int max_steps = 0;
-    for (int i = 0; i < ninst; ++i) max_steps = nsteps[i] > max_steps ? nsteps[i] : max_steps;
+// Host copies of the argument blocks prepared per workspace (launches pass them by value,
+// so the kernel reads them from the parameter bank).
+struct Prepared {
+    BArgs A;
+    BAdj D;
     BLayout L;
-    if (!layout(ninst, nqubits, nsteps, dtype == EMUSV_C128 ? 16 : 8, tile_bits, basis_capacity,
-                max_steps, &L))
-        return 0;
-    return L.total;
-}
+    bool adjoint;
+};
+static std::mutex g_args_mu;
+static std::unordered_map<const void *, Prepared> g_args;
 
-int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const double *dt,
-                        int dtype, const double *omegas, const double *deltas, const double *phis,
-                        const double *interactions, void *states, double exp_tolerance,
-                        double norm_tolerance, int max_krylov_dim, int tile_bits,
-                        int basis_capacity, void *workspace, size_t workspace_bytes,
-                        void *stream) {
+static int prepare_common(int ninst, const int *nqubits, const int *nsteps, const double *dt,
+                          int dtype, const double *omegas, const double *deltas, const double *phis,
+                          const double *interactions, void *states, double exp_tolerance,
+                          double norm_tolerance, int max_krylov_dim, int T, int capacity,
+                          bool adjoint, void *workspace, size_t workspace_bytes, cudaStream_t s) {
     if (ninst < 1 || !nqubits || !nsteps || !dt || !omegas || !deltas || !phis || !interactions ||
-        !states || (reinterpret_cast<uintptr_t>(states) & 15) ||
-        !workspace || max_krylov_dim < 1 || max_krylov_dim > KMAX - 2 || basis_capacity < 1 ||
-        !pick_kernel(dtype, tile_bits) || (reinterpret_cast<uintptr_t>(workspace) & 255))
+        !workspace || max_krylov_dim < 1 || max_krylov_dim > KMAX - 2 || capacity < 1 ||
+        capacity > KMAX - 2 || !pick_kernel(dtype, T, adjoint ? 1 : 0) ||
+        (reinterpret_cast<uintptr_t>(workspace) & 255) || (reinterpret_cast<uintptr_t>(states) & 15))
         return EMUSV_BAD_ARGUMENT;
-    const int T = tile_bits;
-    int max_steps = 0;
-    for (int i = 0; i < ninst; ++i) {
+    for (int i = 0; i < ninst; ++i)
         if (!isfinite(dt[i])) return EMUSV_BAD_ARGUMENT;
-        max_steps = nsteps[i] > max_steps ? nsteps[i] : max_steps;
-    }
     const int es = dtype == EMUSV_C128 ? 16 : 8;
     BLayout L;
-    if (!layout(ninst, nqubits, nsteps, es, T, basis_capacity, max_steps, &L))
-        return EMUSV_BAD_ARGUMENT;
+    if (!layout(ninst, nqubits, nsteps, es, T, capacity, adjoint, &L)) return EMUSV_BAD_ARGUMENT;
     if (workspace_bytes < L.total) return EMUSV_WORKSPACE_TOO_SMALL;
     unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
-    cudaStream_t s = as_stream(stream);
+    const int nj = L.njobs;
 
-    // host tables
-    std::vector<BInst> inst(ninst);
+    std::vector<BInst> inst(nj);
     std::vector<BCoef> coef(L.coef_count > 0 ? L.coef_count : 1);
     std::vector<double> ub((size_t)BMAXQ * BMAXQ * ninst, 0.0);
     std::vector<double> elow((size_t)ninst << T, 0.0);
     long long off = 0;
-    int tile = 0, c0 = 0;
+    int c0 = 0;
     size_t pofs = 0, uofs = 0;  // offsets into the packed parameter arrays
     for (int i = 0; i < ninst; ++i) {
         const int n = nqubits[i];
-        BInst &I = inst[i];
-        I.n = n;
-        I.nsteps = nsteps[i];
-        I.tile0 = tile;
-        I.ntiles = 1 << (n - T);
-        I.off = off;
-        I.dt = dt[i];
-        I.coef0 = c0;
-        I.pad = 0;
         for (int k = 0; k < nsteps[i]; ++k) {
             BCoef &C = coef[c0 + k];
             memset(&C, 0, sizeof(C));
@@ -760,9 +1113,10 @@ int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const 
                 const double ph = phis[pofs + (size_t)k * n + q];
                 if (!isfinite(om) || !isfinite(de) || !isfinite(ph)) return EMUSV_BAD_ARGUMENT;
                 C.up_re[p] = 0.5 * om * cos(ph);  // hamiltonian.py:52,62-64
-                C.up_im[p] = 0.5 * om * sin(ph);
-                if (ph == 0.0) C.up_im[p] = 0.0;
+                C.up_im[p] = ph == 0.0 ? 0.0 : 0.5 * om * sin(ph);
                 C.field[p] = -de;
+                C.om[p] = om;
+                C.ph[p] = ph;
                 C.fup_re[p] = (float)C.up_re[p];
                 C.fup_im[p] = (float)C.up_im[p];
             }
@@ -785,20 +1139,43 @@ int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const 
                         if ((l >> q) & 1) e += U[p * BMAXQ + q];
             E[l] = e;
         }
+        const int per = adjoint ? 2 : 1;
+        for (int r = 0; r < per; ++r) {
+            BInst &I = inst[per * i + r];
+            I.n = n;
+            I.nsteps = adjoint ? (1 << 30) : nsteps[i];
+            I.ntiles = 1 << (n - T);
+            I.off0 = off;
+            I.dt = dt[i];
+            I.coef0 = c0;
+            I.pidx = i;
+            I.src = r;
+            I.pad = 0;
+        }
         off += 1LL << n;
-        tile += 1 << (n - T);
-        c0 += nsteps[i] > 0 ? nsteps[i] : 0;
-        pofs += (size_t)(nsteps[i] > 0 ? nsteps[i] : 0) * n;
+        c0 += nsteps[i];
+        pofs += (size_t)nsteps[i] * n;
         uofs += (size_t)n * n;
     }
-    BArgs A;
-    memset(&A, 0, sizeof(A));
-    A.ninst = ninst;
+    long long joff = 0;
+    int tile = 0;
+    for (int J = 0; J < nj; ++J) {  // stored-vector offsets and tiles, jobs back to back
+        inst[J].off = joff;
+        inst[J].tile0 = tile;
+        joff += 1LL << inst[J].n;
+        tile += inst[J].ntiles;
+    }
+    Prepared P;
+    memset(&P, 0, sizeof(P));
+    P.L = L;
+    P.adjoint = adjoint;
+    BArgs &A = P.A;
+    A.ninst = nj;
     A.T = T;
     A.total_tiles = L.total_tiles;
     A.maxdim = max_krylov_dim;
-    A.capacity = basis_capacity;
-    A.max_steps = max_steps;
+    A.capacity = capacity;
+    A.max_steps = L.max_steps;
     A.exp_tol = exp_tolerance;
     A.norm_tol = norm_tolerance;
     A.inst = reinterpret_cast<BInst *>(ws + L.inst);
@@ -808,80 +1185,152 @@ int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const 
     A.ks = reinterpret_cast<KState *>(ws + L.ks);
     int *ints = reinterpret_cast<int *>(ws + L.ints);
     A.hint = ints;
-    A.polled = ints + ninst;
-    A.fail = ints + 2 * ninst;
-    A.status_out = ints + 3 * ninst;
-    A.ranB = ints + 4 * ninst;
-    A.cnt = reinterpret_cast<unsigned *>(ints + 5 * ninst);
+    A.polled = ints + nj;
+    A.fail = ints + 2 * nj;
+    A.status_out = ints + 3 * nj;
+    A.ranB = ints + 4 * nj;
+    A.cnt = reinterpret_cast<unsigned *>(ints + 5 * nj);
     double *sums = reinterpret_cast<double *>(ws + L.sums);
     A.sumA = sums;
-    A.sumB = sums + 4 * ninst;
-    A.sumN = sums + 8 * ninst;
+    A.sumB = sums + 4 * nj;
+    A.sumN = sums + 8 * nj;
     A.iters_out = reinterpret_cast<int *>(ws + L.iters);
     A.partA = reinterpret_cast<double *>(ws + L.partA);
     A.partB = reinterpret_cast<double *>(ws + L.partB);
     A.partN = reinterpret_cast<double *>(ws + L.partN);
-    A.states = states;
+    A.v0[0] = states;
+    A.v0[1] = nullptr;
     A.slots = ws + L.slots;
     A.slot_amps = L.slot_amps;
     A.ctl = reinterpret_cast<BCtl *>(ws + L.ctl);
+    A.first_step = 0;
+    A.run_steps = L.max_steps;
+    A.hist = nullptr;
+    A.hist_every = 1;
+    A.hist_stride = L.inst_amps;
+    if (adjoint) {
+        BAdj &D = P.D;
+        D.ninst = ninst;
+        D.mmax = L.mmax;
+        D.dS = reinterpret_cast<double2 *>(ws + L.dS);
+        D.E = ws + L.E;
+        D.inst_amps = L.inst_amps;
+        D.partC = reinterpret_cast<double *>(ws + L.partC);
+        D.cntC = reinterpret_cast<unsigned *>(ints + 8 * nj);
+    }
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.args, &A, sizeof(A), cudaMemcpyHostToDevice, s));
-    EMUSV_CHECK(cudaMemcpyAsync(ws + L.inst, inst.data(), sizeof(BInst) * ninst, cudaMemcpyHostToDevice, s));
+    EMUSV_CHECK(cudaMemcpyAsync(ws + L.inst, inst.data(), sizeof(BInst) * nj, cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.coef, coef.data(), sizeof(BCoef) * coef.size(), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.ubits, ub.data(), sizeof(double) * ub.size(), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.elow, elow.data(), sizeof(double) * elow.size(), cudaMemcpyHostToDevice, s));
+    EMUSV_CHECK(cudaMemsetAsync(ws + L.ctl, 0, sizeof(BCtl) + sizeof(int) * (8 * (size_t)nj + ninst), s));
     EMUSV_CHECK(cudaStreamSynchronize(s));  // the host tables go out of scope
     {
         std::lock_guard<std::mutex> g(g_args_mu);
-        g_args[workspace] = A;
+        g_args[workspace] = P;
     }
     return EMUSV_OK;
 }
 
-// Clears the control block and launches the persistent kernel on the states given to
-// emusv_batch_prepare.  Issues only stream-ordered device work (one memset and one
-// cooperative launch), so the call can be recorded into a CUDA graph and replayed.
-int emusv_batch_launch(int dtype, int tile_bits, int blocks_per_sm, void *workspace, void *stream) {
-    void *kern = pick_kernel(dtype, tile_bits);
-    if (!kern || !workspace || blocks_per_sm < 1) return EMUSV_BAD_ARGUMENT;
-    cudaStream_t s = as_stream(stream);
-    unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
+static int lookup(const void *workspace, bool adjoint, Prepared *out) {
+    std::lock_guard<std::mutex> g(g_args_mu);
+    auto it = g_args.find(workspace);
+    if (it == g_args.end() || it->second.adjoint != adjoint) return EMUSV_BAD_ARGUMENT;
+    *out = it->second;
+    return EMUSV_OK;
+}
+
+static int cooperative_launch(void *kern, int blocks_per_sm, void **args, cudaStream_t s,
+                              int *grid_out) {
     int per_sm = 0;
     EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BWARPS * 32, 0));
     if (per_sm < 1) return EMUSV_CUDA_ERROR;
     const int bps = blocks_per_sm < per_sm ? blocks_per_sm : per_sm;
     const int grid = bps * sm_count();
-    BArgs A;
-    {
-        std::lock_guard<std::mutex> g(g_args_mu);
-        auto it = g_args.find(workspace);
-        if (it == g_args.end()) return EMUSV_BAD_ARGUMENT;  // not prepared
-        A = it->second;
-    }
-    // control block, flags, hints and tile counters start at zero
-    const size_t clr = sizeof(BCtl) + sizeof(int) * 8 * (size_t)A.ninst;
-    EMUSV_CHECK(cudaMemsetAsync(ws + al256(sizeof(BArgs)), 0, clr, s));
-    void *args[] = {(void *)&A};
-    {
-        ProfScope ps_(PROF_BATCH, s);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3(BWARPS * 32);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        EMUSV_CHECK(cudaLaunchKernelExC(&cfg, kern, args));
-    }
+    if (grid_out) *grid_out = grid;
+    ProfScope ps_(PROF_BATCH, s);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(BWARPS * 32);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    EMUSV_CHECK(cudaLaunchKernelExC(&cfg, kern, args));
     return EMUSV_OK;
 }
 
-// Largest CTAs per SM the persistent kernel can keep resident (the cooperative limit).
+}  // namespace emusv
+
+using namespace emusv;
+
+extern "C" {
+
+int emusv_batch_max_qubits(void) { return BMAXQ; }
+
+size_t emusv_batch_workspace_bytes(int ninst, const int *nqubits, const int *nsteps, int dtype,
+                                   int tile_bits, int basis_capacity) {
+    if (ninst < 1 || !nqubits || !nsteps || basis_capacity < 1 || basis_capacity > KMAX - 2 ||
+        !pick_kernel(dtype, tile_bits, 0))
+        return 0;
+    BLayout L;
+    if (!layout(ninst, nqubits, nsteps, dtype == EMUSV_C128 ? 16 : 8, tile_bits, basis_capacity,
+                false, &L))
+        return 0;
+    return L.total;
+}
+
+int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const double *dt,
+                        int dtype, const double *omegas, const double *deltas, const double *phis,
+                        const double *interactions, void *states, double exp_tolerance,
+                        double norm_tolerance, int max_krylov_dim, int tile_bits,
+                        int basis_capacity, void *workspace, size_t workspace_bytes,
+                        void *stream) {
+    if (!states) return EMUSV_BAD_ARGUMENT;
+    return prepare_common(ninst, nqubits, nsteps, dt, dtype, omegas, deltas, phis, interactions,
+                          states, exp_tolerance, norm_tolerance, max_krylov_dim, tile_bits,
+                          basis_capacity, false, workspace, workspace_bytes, as_stream(stream));
+}
+
+int emusv_batch_launch_steps(int dtype, int tile_bits, int blocks_per_sm, int first_step,
+                             int steps, void *states, void *history, int history_every,
+                             void *workspace, void *stream) {
+    void *kern = pick_kernel(dtype, tile_bits, 0);
+    Prepared P;
+    if (!kern || !workspace || blocks_per_sm < 1 || lookup(workspace, false, &P)) return EMUSV_BAD_ARGUMENT;
+    BArgs A = P.A;
+    if (first_step < 0 || steps < 0 || first_step + steps > P.L.max_steps || history_every < 1 ||
+        (states && (reinterpret_cast<uintptr_t>(states) & 15)))
+        return EMUSV_BAD_ARGUMENT;
+    if (A.T != tile_bits) return EMUSV_BAD_ARGUMENT;
+    if (states) A.v0[0] = states;
+    A.first_step = first_step;
+    A.run_steps = steps;
+    A.hist = history;
+    A.hist_every = history_every;
+    cudaStream_t s = as_stream(stream);
+    unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
+    // control block, flags, hints and tile counters start at zero
+    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * 8 * (size_t)A.ninst, s));
+    void *args[] = {(void *)&A};
+    return cooperative_launch(kern, blocks_per_sm, args, s, nullptr);
+}
+
+// Clears the control block and launches the persistent kernel over every step on the
+// states given to emusv_batch_prepare.  Issues only stream-ordered device work (one memset
+// and one cooperative launch), so the call can be recorded into a CUDA graph and replayed.
+int emusv_batch_launch(int dtype, int tile_bits, int blocks_per_sm, void *workspace, void *stream) {
+    Prepared P;
+    if (!workspace || lookup(workspace, false, &P)) return EMUSV_BAD_ARGUMENT;
+    return emusv_batch_launch_steps(dtype, tile_bits, blocks_per_sm, 0, P.L.max_steps, nullptr,
+                                    nullptr, 1, workspace, stream);
+}
+
 int emusv_batch_max_blocks_per_sm(int dtype, int tile_bits) {
-    void *kern = pick_kernel(dtype, tile_bits);
+    void *kern = pick_kernel(dtype, tile_bits, 0);
     if (!kern) return 0;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BWARPS * 32, 0) != cudaSuccess)
@@ -889,23 +1338,19 @@ int emusv_batch_max_blocks_per_sm(int dtype, int tile_bits) {
     return per_sm;
 }
 
-// Statuses (emusv_status per instance) and Krylov iteration counts [ninst][max_steps]
-// to host arrays; returns EMUSV_TIMEOUT if a grid barrier gave up.  Synchronises.
 int emusv_batch_results(int ninst, int max_steps, void *workspace, int *status_out,
                         int *iterations_out, void *stream) {
-    if (!workspace || ninst < 1) return EMUSV_BAD_ARGUMENT;
+    Prepared P;
+    if (!workspace || ninst < 1 || lookup(workspace, false, &P)) return EMUSV_BAD_ARGUMENT;
+    if (P.A.ninst != ninst || P.A.max_steps != max_steps) return EMUSV_BAD_ARGUMENT;
     cudaStream_t s = as_stream(stream);
     unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
-    BArgs A;
     BCtl C;
-    EMUSV_CHECK(cudaMemcpyAsync(&A, ws, sizeof(A), cudaMemcpyDeviceToHost, s));
-    EMUSV_CHECK(cudaMemcpyAsync(&C, ws + al256(sizeof(BArgs)), sizeof(C), cudaMemcpyDeviceToHost, s));
-    EMUSV_CHECK(cudaStreamSynchronize(s));
-    if (A.ninst != ninst || A.max_steps != max_steps) return EMUSV_BAD_ARGUMENT;
     std::vector<int> st(ninst);
-    EMUSV_CHECK(cudaMemcpyAsync(st.data(), A.status_out, sizeof(int) * ninst, cudaMemcpyDeviceToHost, s));
+    EMUSV_CHECK(cudaMemcpyAsync(&C, ws + P.L.ctl, sizeof(C), cudaMemcpyDeviceToHost, s));
+    EMUSV_CHECK(cudaMemcpyAsync(st.data(), P.A.status_out, sizeof(int) * ninst, cudaMemcpyDeviceToHost, s));
     if (iterations_out && max_steps > 0)
-        EMUSV_CHECK(cudaMemcpyAsync(iterations_out, A.iters_out, sizeof(int) * (size_t)ninst * max_steps,
+        EMUSV_CHECK(cudaMemcpyAsync(iterations_out, P.A.iters_out, sizeof(int) * (size_t)ninst * max_steps,
                                     cudaMemcpyDeviceToHost, s));
     EMUSV_CHECK(cudaStreamSynchronize(s));
     if (C.err) return C.err;
@@ -922,6 +1367,80 @@ int emusv_batch_results(int ninst, int max_steps, void *workspace, int *status_o
         if (e != EMUSV_OK && (worst == EMUSV_OK || e == EMUSV_WORKSPACE_TOO_SMALL)) worst = e;
     }
     return worst;
+}
+
+// ---- batched adjoint steps
+size_t emusv_batch_adjoint_workspace_bytes(int ninst, const int *nqubits, const int *nsteps,
+                                           int dtype, int tile_bits, int basis_capacity) {
+    if (ninst < 1 || !nqubits || !nsteps || basis_capacity < 1 || basis_capacity > KMAX - 2 ||
+        !pick_kernel(dtype, tile_bits, 1))
+        return 0;
+    BLayout L;
+    if (!layout(ninst, nqubits, nsteps, dtype == EMUSV_C128 ? 16 : 8, tile_bits, basis_capacity,
+                true, &L))
+        return 0;
+    return L.total;
+}
+
+int emusv_batch_adjoint_prepare(int ninst, const int *nqubits, const int *nsteps, const double *dt,
+                                int dtype, const double *omegas, const double *deltas,
+                                const double *phis, const double *interactions, double tolerance,
+                                int max_krylov_dim, int tile_bits, int basis_capacity,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+    return prepare_common(ninst, nqubits, nsteps, dt, dtype, omegas, deltas, phis, interactions,
+                          nullptr, tolerance, tolerance, max_krylov_dim, tile_bits, basis_capacity,
+                          true, workspace, workspace_bytes, as_stream(stream));
+}
+
+int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int step,
+                               const void *states, const void *grad_in, void *grad_out,
+                               double *grads_dev, int *status_dev, void *workspace, void *stream) {
+    void *k1 = pick_kernel(dtype, tile_bits, 1), *k3 = pick_kernel(dtype, tile_bits, 2);
+    Prepared P;
+    if (!k1 || !workspace || !states || !grad_in || !grad_out || !grads_dev || !status_dev ||
+        blocks_per_sm < 1 || lookup(workspace, true, &P))
+        return EMUSV_BAD_ARGUMENT;
+    if (P.A.T != tile_bits || step < 0) return EMUSV_BAD_ARGUMENT;
+    for (const void *q : {states, grad_in, (const void *)grad_out})
+        if (reinterpret_cast<uintptr_t>(q) & 15) return EMUSV_BAD_ARGUMENT;
+    BArgs A = P.A;
+    BAdj D = P.D;
+    A.v0[0] = const_cast<void *>(states);
+    A.v0[1] = const_cast<void *>(grad_in);
+    D.step = step;
+    D.grads = grads_dev;
+    D.gout = grad_out;
+    D.astatus = status_dev;
+    cudaStream_t s = as_stream(stream);
+    unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
+    // clear the control block and everything after the hints and polled flags (the
+    // hints carry from one step to the next)
+    const int nj = A.ninst;
+    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl), s));
+    EMUSV_CHECK(cudaMemsetAsync(A.fail, 0, sizeof(int) * (6 * (size_t)nj + D.ninst), s));
+    void *args[] = {(void *)&A, (void *)&D};
+    int st = cooperative_launch(k1, blocks_per_sm, args, s, nullptr);
+    if (st) return st;
+    {
+        ProfScope ps_(PROF_ADJOINT, s);
+        dim3 grid((D.mmax + BWARPS - 1) / BWARPS, D.ninst);
+        k_batch_dS<<<grid, BWARPS * 32, 0, s>>>(A, D);
+    }
+    EMUSV_CHECK_LAUNCH();
+    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl), s));
+    return cooperative_launch(k3, blocks_per_sm, args, s, nullptr);
+}
+
+// Krylov iteration counts of the last adjoint launch: [ninst][2] (state, gradient basis).
+int emusv_batch_adjoint_iterations(int ninst, void *workspace, int *iterations_out, void *stream) {
+    Prepared P;
+    if (!workspace || !iterations_out || lookup(workspace, true, &P) || P.D.ninst != ninst)
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    EMUSV_CHECK(cudaMemcpyAsync(iterations_out, P.A.iters_out, sizeof(int) * 2 * (size_t)ninst,
+                                cudaMemcpyDeviceToHost, s));
+    EMUSV_CHECK(cudaStreamSynchronize(s));
+    return EMUSV_OK;
 }
 
 }  // extern "C"

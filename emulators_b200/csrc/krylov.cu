@@ -170,7 +170,6 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
         }
         return;
     }
-    __shared__ KSmem S;
     const int lane = threadIdx.x;
     // deterministic sums of the ||w||^2 and <v_j, w> partials by one warp
     double v = 0.0, vr = 0.0, vi = 0.0;
@@ -182,7 +181,7 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
     v = warp_sum(v);
     vr = warp_sum(vr);
     vi = warp_sum(vi);
-    krylov_decide(ks, j, v, vr, vi, dt, exp_tol, norm_tol, poll != 0, first_poll != 0, maxdim, S);
+    krylov_decide(ks, j, v, vr, vi, dt, exp_tol, norm_tol, poll != 0, first_poll != 0, maxdim);
 }
 
 // out = s0 * sum_k c_k scale_k stored_k ;  ||out||^2 partials.
@@ -366,7 +365,6 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
     EMUSV_CHECK_LAUNCH();
 
     int status = KS_RUNNING;
-    bool polled = false;
     for (int j = 0; j < max_krylov_dim; ++j) {
         if (j + 1 > capacity) {
             int st = read_status(W.ks, s, &status);
@@ -402,17 +400,17 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
                                                    const_cast<void *>(stored(j + 1)), D, W.part_o);
             }
         EMUSV_CHECK_LAUNCH();
-        // convergence is tested from the hint on; the first test of the step also looks
-        // back over the untested iterations (k_small)
+        // the device tests convergence at every iteration, as the reference does; the host
+        // reads the status (one synchronisation) from the hint on, and kernels launched
+        // after the device converged return at once
         const int poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
         {
             ProfScope ps_(PROF_SMALL, s);
-            k_small<<<1, 32, 0, s>>>(W.ks, j, W.part_o, sg, dt, exp_tolerance, norm_tolerance,
-                                     poll, poll && !polled, max_krylov_dim);
+            k_small<<<1, 32, 0, s>>>(W.ks, j, W.part_o, sg, dt, exp_tolerance, norm_tolerance, 1,
+                                     j == 0, max_krylov_dim);
         }
         EMUSV_CHECK_LAUNCH();
         if (poll) {
-            polled = true;
             st = read_status(W.ks, s, &status);
             if (st) return st;
             if (status != KS_RUNNING) break;

@@ -114,52 +114,337 @@ static __device__ __noinline__ void warp_expm_col(int m, const double2 *d, const
 // Extended exponential of iteration jj (the matrix A = -i dt T_H of size jj+1 with the
 // extension entry lo[jj] = -i dt r_jj): writes the coefficients c[0..jj+1] and returns the
 // Expokit error estimate (krylov_exp.py:77-84).  One warp.
-static __device__ __noinline__ double krylov_eval(KState *ks, int jj, double dt, double2 *d, double2 *up,
-                              double2 *lo, double2 *y, double2 *t, double2 *tn, double2 *acc) {
+// ---------------------------------------------------------------- register form
+// One warp, exp(A) e_col for a complex tridiagonal M x M matrix A (plus, optionally, one
+// coupling entry A[0][cpl] = 1), with the vectors in registers: lane L owns the entries
+// k = L * NE + e (e < NE), so the tridiagonal products need two lane shuffles per term.
+// Row form: A[k][k] = d[e], A[k][k-1] = l[e], A[k][k+1] = u[e] (zero outside the matrix).
+// Method: Taylor series of exp(hA) on the vector, h = 1/s with ||hA||_inf <= 2, s times;
+// when zlast >= 0 the Expokit integrals Z1 = int_0^1 y_zlast, Z2 = int_0^1 (1-s) y_zlast
+// come from the same series term by term (as warp_expm_col).
+template <int NE>
+__device__ __forceinline__ double2 reg_pick(const double2 (&v)[NE], int k) {
+    const int owner = k / NE, e = k - owner * NE;
+    double2 r = v[0];
+#pragma unroll
+    for (int q = 1; q < NE; ++q)
+        if (q == e) r = v[q];
+    r.x = __shfl_sync(0xffffffffu, r.x, owner);
+    r.y = __shfl_sync(0xffffffffu, r.y, owner);
+    return r;
+}
+
+template <int NE>
+static __device__ void reg_expm(int M, const double2 (&d)[NE], const double2 (&l)[NE],
+                                const double2 (&u)[NE], int cpl, int col, double2 (&y)[NE],
+                                int zlast, double2 *Z1, double2 *Z2) {
     const int lane = threadIdx.x & 31;
-    const int m = jj + 1;
-    for (int k = lane; k < m; k += 32) {
-        d[k] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
-        up[k] = k > 0 ? make_double2(dt * ks->b_im[k], -dt * ks->b_re[k]) : make_double2(0.0, 0.0);
-        lo[k] = make_double2(0.0, -dt * ks->r[k]);
+    double nrm = 0.0;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        double c = hypot(d[e].x, d[e].y) + hypot(l[e].x, l[e].y) + hypot(u[e].x, u[e].y);
+        if (cpl >= 0 && lane * NE + e == 0) c += 1.0;
+        nrm = fmax(nrm, c);
     }
-    __syncwarp();
-    double2 Z1, Z2;
-    warp_expm_col(m, d, up, lo, y, t, tn, acc, &Z1, &Z2);
-    // extension: x_{jj+1} = l Z1, x_{jj+2} = l Z2 with l = A[jj+1][jj] = -i dt r_jj
-    const double2 l = lo[jj];
-    const double2 x1 = make_double2(l.x * Z1.x - l.y * Z1.y, l.x * Z1.y + l.y * Z1.x);
-    const double2 x2 = make_double2(l.x * Z2.x - l.y * Z2.y, l.x * Z2.y + l.y * Z2.x);
+    nrm = warp_max(nrm);
+    int s = 1;
+    if (nrm > 2.0) s = nrm < 2.0 * (1 << 20) ? (int)ceil(nrm / 2.0) : (1 << 20);
+    const double h = 1.0 / s;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) y[e] = make_double2(lane * NE + e == col ? 1.0 : 0.0, 0.0);
+    double2 z1 = make_double2(0.0, 0.0), z2 = make_double2(0.0, 0.0);
+    for (int st = 0; st < s; ++st) {
+        double2 t[NE], acc[NE];
+#pragma unroll
+        for (int e = 0; e < NE; ++e) t[e] = acc[e] = y[e];
+        double2 S1 = make_double2(0.0, 0.0), S2 = S1;
+        if (zlast >= 0) {
+            S1 = reg_pick(t, zlast);
+            S2 = make_double2(0.5 * S1.x, 0.5 * S1.y);
+        }
+        for (int q = 1; q < 90; ++q) {
+            const double f = h / q;
+            // neighbours across the lane boundary
+            double2 prev, next;
+            prev.x = __shfl_up_sync(0xffffffffu, t[NE - 1].x, 1);
+            prev.y = __shfl_up_sync(0xffffffffu, t[NE - 1].y, 1);
+            next.x = __shfl_down_sync(0xffffffffu, t[0].x, 1);
+            next.y = __shfl_down_sync(0xffffffffu, t[0].y, 1);
+            if (lane == 0) prev = make_double2(0.0, 0.0);
+            if (lane == 31) next = make_double2(0.0, 0.0);
+            double2 cp = make_double2(0.0, 0.0);
+            if (cpl >= 0) cp = reg_pick(t, cpl);
+            double2 nt[NE];
+            double tmax = 0.0;
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                const double2 a0 = t[e];
+                const double2 am = e > 0 ? t[e - 1] : prev;
+                const double2 ap = e < NE - 1 ? t[e + 1] : next;
+                double re = d[e].x * a0.x - d[e].y * a0.y + l[e].x * am.x - l[e].y * am.y +
+                            u[e].x * ap.x - u[e].y * ap.y;
+                double im = d[e].x * a0.y + d[e].y * a0.x + l[e].x * am.y + l[e].y * am.x +
+                            u[e].x * ap.y + u[e].y * ap.x;
+                if (cpl >= 0 && lane == 0 && e == 0) {
+                    re += cp.x;
+                    im += cp.y;
+                }
+                nt[e] = make_double2(f * re, f * im);
+                acc[e].x += nt[e].x;
+                acc[e].y += nt[e].y;
+                tmax = fmax(tmax, fmax(fabs(nt[e].x), fabs(nt[e].y)));
+            }
+#pragma unroll
+            for (int e = 0; e < NE; ++e) t[e] = nt[e];
+            if (zlast >= 0) {
+                const double2 last = reg_pick(t, zlast);
+                const double w1 = 1.0 / (q + 1), w2 = w1 / (q + 2);
+                S1.x += w1 * last.x;
+                S1.y += w1 * last.y;
+                S2.x += w2 * last.x;
+                S2.y += w2 * last.y;
+            }
+            if ((q & 3) == 0) {
+                double amax = 0.0;
+#pragma unroll
+                for (int e = 0; e < NE; ++e) amax = fmax(amax, fmax(fabs(acc[e].x), fabs(acc[e].y)));
+                tmax = warp_max(tmax);
+                amax = warp_max(amax);
+                if (tmax <= 1e-18 * fmax(amax, 1e-300)) break;
+            }
+        }
+        z2.x += h * z1.x + h * h * S2.x;
+        z2.y += h * z1.y + h * h * S2.y;
+        z1.x += h * S1.x;
+        z1.y += h * S1.y;
+#pragma unroll
+        for (int e = 0; e < NE; ++e) y[e] = acc[e];
+    }
+    if (Z1) *Z1 = z1;
+    if (Z2) *Z2 = z2;
+}
+
+// ---------------------------------------------------------------- Chebyshev form
+// One warp, y = exp(A) e_col for A = -i dt T with T tridiagonal (plus optionally one
+// coupling entry A[0][cpl] = cplv, plus any non-symmetric rows whose eigenvalues are
+// inside T's Gershgorin interval), held in rows by the lanes as in reg_expm.  With
+// T's spectrum in [c - R, c + R] (Gershgorin), A = -i dt (c + R X) and
+//   exp(-i z x) = J_0(z) + 2 sum_{k>=1} (-i)^k J_k(z) T_k(x),   z = dt R,
+// so exp(A) e_col = e^{-i dt c} sum_k coef_k T_k(X) e_col, summed by Clenshaw's
+// recurrence from the top term down while Miller's backward recurrence produces the
+// Bessel values J_k(|z|) in the same order (normalised at the end by
+// J_0 + 2 sum J_2k = 1).  About |z| + 40 tridiagonal products instead of the Taylor
+// form's ~12 |z|.  `Tdiag[e]` is T's (real) diagonal centre of row e and `Trad[e]` its
+// Gershgorin radius (|row| off-diagonal sum of T).
+template <int NE>
+static __device__ void cheb_expm(const double2 (&d)[NE], const double2 (&l)[NE], const double2 (&u)[NE],
+                                 int cpl, double2 cplv, int col, double dt, const double (&Tdiag)[NE],
+                                 const double (&Trad)[NE], int M, double2 (&y)[NE]) {
+    const int lane = threadIdx.x & 31;
+    double lo = 1e300, hi = -1e300;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        if (lane * NE + e < M) {
+            lo = fmin(lo, Tdiag[e] - Trad[e]);
+            hi = fmax(hi, Tdiag[e] + Trad[e]);
+        }
+    }
+    lo = -warp_max(-lo);
+    hi = warp_max(hi);
+    const double c = 0.5 * (lo + hi);
+    // radius at least 1/|dt| (z >= 1): keeps X = (T - c)/R bounded when T's own spread is
+    // tiny, and Miller's recurrence (factors 2k/z) far from overflow
+    const double R = fmax(0.5 * (hi - lo), 1.0 / fabs(dt));
+    const double z = fabs(dt) * R;
+    const double sgn = dt >= 0.0 ? 1.0 : -1.0;
+    // X = (A - alpha) / beta,  alpha = -i dt c,  beta = -i dt R;  1/beta = i / (dt R)
+    const double2 ib = make_double2(0.0, 1.0 / (dt * R));
+    const double2 alpha = make_double2(0.0, -dt * c);
+    auto cm = [](double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+    double2 xd[NE], xl[NE], xu[NE];
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        xd[e] = cm(make_double2(d[e].x - alpha.x, d[e].y - alpha.y), ib);
+        xl[e] = cm(l[e], ib);
+        xu[e] = cm(u[e], ib);
+        if (lane * NE + e >= M) xd[e] = make_double2(0.0, 0.0);
+    }
+    const double2 xc = cm(cplv, ib);
+    // X v for a vector held in the row layout
+    auto xmul = [&](const double2 (&v)[NE], double2 (&out)[NE]) {
+        double2 prev, next;
+        prev.x = __shfl_up_sync(0xffffffffu, v[NE - 1].x, 1);
+        prev.y = __shfl_up_sync(0xffffffffu, v[NE - 1].y, 1);
+        next.x = __shfl_down_sync(0xffffffffu, v[0].x, 1);
+        next.y = __shfl_down_sync(0xffffffffu, v[0].y, 1);
+        if (lane == 0) prev = make_double2(0.0, 0.0);
+        if (lane == 31) next = make_double2(0.0, 0.0);
+        double2 cp = make_double2(0.0, 0.0);
+        if (cpl >= 0) cp = reg_pick(v, cpl);
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const double2 am = e > 0 ? v[e - 1] : prev;
+            const double2 ap = e < NE - 1 ? v[e + 1] : next;
+            double2 o = cm(xd[e], v[e]);
+            const double2 t1 = cm(xl[e], am), t2 = cm(xu[e], ap);
+            o.x += t1.x + t2.x;
+            o.y += t1.y + t2.y;
+            if (cpl >= 0 && lane == 0 && e == 0) {
+                const double2 t3 = cm(xc, cp);
+                o.x += t3.x;
+                o.y += t3.y;
+            }
+            out[e] = o;
+        }
+    };
+    const int N = (int)ceil(1.1 * z) + 40;  // terms kept
+    const int K = N + 30;                   // Miller's start
+    double2 b1[NE], b2[NE];  // b_{k+1}, b_{k+2}
+#pragma unroll
+    for (int e = 0; e < NE; ++e) b1[e] = b2[e] = make_double2(0.0, 0.0);
+    double jk1 = 0.0, jk = 1e-280, S = 0.0;  // J~_{k+1}, J~_k, normalisation sum
+    // (-i sgn)^k at k = K, stepped down by multiplying with (i sgn)
+    double2 ph;
+    {
+        const int r = K & 3;
+        const double2 base = make_double2(0.0, -sgn);
+        ph = make_double2(1.0, 0.0);
+        for (int q = 0; q < r; ++q) ph = cm(ph, base);
+    }
+    const double2 up_step = make_double2(0.0, sgn);
+    for (int k = K; k >= 1; --k) {
+        if ((k & 1) == 0) S += 2.0 * jk;
+        if (k <= N) {  // b_k = coef_k e_col + 2 X b_{k+1} - b_{k+2}
+            double2 xb[NE];
+            xmul(b1, xb);
+            const double2 ck = make_double2(2.0 * jk * ph.x, 2.0 * jk * ph.y);
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                double2 nb = make_double2(2.0 * xb[e].x - b2[e].x, 2.0 * xb[e].y - b2[e].y);
+                if (lane * NE + e == col) {
+                    nb.x += ck.x;
+                    nb.y += ck.y;
+                }
+                b2[e] = b1[e];
+                b1[e] = nb;
+            }
+        }
+        // J~_{k-1} = (2k / z) J~_k - J~_{k+1}
+        const double jm = (z > 0.0 ? (2.0 * k / z) : 0.0) * jk - jk1;
+        jk1 = jk;
+        jk = jm;
+        ph = cm(ph, up_step);
+        if (fabs(jk) > 1e250) {  // rescale everything linear in the J~
+            const double f = 1e-250;
+            jk *= f;
+            jk1 *= f;
+            S *= f;
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                b1[e].x *= f;
+                b1[e].y *= f;
+                b2[e].x *= f;
+                b2[e].y *= f;
+            }
+        }
+    }
+    // now jk = J~_0, b1 = b_1, b2 = b_2:  sum = J~_0 e_col + X b_1 - b_2
+    S += jk;
+    double2 xb[NE];
+    xmul(b1, xb);
+    const double2 ea = make_double2(cos(alpha.y), sin(alpha.y));  // e^{alpha}, alpha imaginary
+    const double inv = z > 0.0 ? 1.0 / S : 1.0;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        double2 v = make_double2(xb[e].x - b2[e].x, xb[e].y - b2[e].y);
+        if (lane * NE + e == col) v.x += jk;
+        if (z == 0.0) v = make_double2(lane * NE + e == col ? 1.0 : 0.0, 0.0);
+        v.x *= inv;
+        v.y *= inv;
+        y[e] = cm(ea, v);
+    }
+}
+
+// Rows of A = -i dt T_H (the first m rows of a Lanczos run) in the register layout.
+template <int NE>
+__device__ __forceinline__ void load_rows(const KState *ks, int m, double dt, double2 (&d)[NE],
+                                          double2 (&l)[NE], double2 (&u)[NE], double (&td)[NE],
+                                          double (&tr)[NE]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        const int k = lane * NE + e;
+        d[e] = l[e] = u[e] = make_double2(0.0, 0.0);
+        td[e] = tr[e] = 0.0;
+        if (k < m) {
+            d[e] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
+            td[e] = ks->a_re[k];
+            if (k > 0) {
+                l[e] = make_double2(0.0, -dt * ks->r[k - 1]);  // A[k][k-1]
+                tr[e] += fabs(ks->r[k - 1]);
+            }
+            if (k + 1 < m) {
+                u[e] = make_double2(dt * ks->b_im[k + 1], -dt * ks->b_re[k + 1]);  // A[k][k+1]
+                tr[e] += hypot(ks->b_re[k + 1], ks->b_im[k + 1]);
+            }
+            tr[e] += fabs(ks->a_im[k]);
+        }
+    }
+}
+
+// Extended exponential of iteration jj: exp of the (jj+3) x (jj+3) matrix
+// [[A, 0, 0], [l e_jj^T, 0, 0], [0, 1, 0]] (A = -i dt T_H of size jj+1, l = -i dt r_jj)
+// applied to e_0 = (y, x1, x2) (krylov_exp.py:77-78); writes the coefficients
+// c[0..jj+1] = (y, x1) and returns the Expokit error estimate (krylov_exp.py:81-84).
+// One warp, Chebyshev form.
+static __device__ __noinline__ double krylov_eval(KState *ks, int jj, double dt) {
+    constexpr int NE = (KMAX + 2 + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const int m = jj + 1, M = m + 2;
+    double2 d[NE], l[NE], u[NE], y[NE];
+    double td[NE], tr[NE];
+    load_rows<NE>(ks, m, dt, d, l, u, td, tr);
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {  // the two extension rows (eigenvalue 0 of T)
+        const int k = lane * NE + e;
+        if (k == m) {  // T units: centre 0, the entry r_jj
+            l[e] = make_double2(0.0, -dt * ks->r[jj]);
+            td[e] = 0.0;
+            tr[e] = fabs(ks->r[jj]);
+        }
+        if (k == m + 1) {  // the entry 1 of A is 1/|dt| in T units
+            l[e] = make_double2(1.0, 0.0);
+            td[e] = 0.0;
+            tr[e] = 1.0 / fabs(dt);
+        }
+    }
+    cheb_expm<NE>(d, l, u, -1, make_double2(0.0, 0.0), 0, dt, td, tr, M, y);
+    const double2 x1 = reg_pick(y, m), x2 = reg_pick(y, m + 1);
     const double err1 = hypot(x1.x, x1.y);                             // krylov_exp.py:81
     const double err2 = hypot(x2.x, x2.y) * (fabs(dt) * ks->hn[jj]);  // krylov_exp.py:82
-    for (int k = lane; k < m; k += 32) {
-        ks->c_re[k] = y[k + 1].x;
-        ks->c_im[k] = y[k + 1].y;
-    }
-    if (lane == 0) {
-        ks->c_re[m] = x1.x;  // expd[j+1, 0] multiplies v_{j+1} (krylov_exp.py:88-90)
-        ks->c_im[m] = x1.y;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        const int k = lane * NE + e;
+        if (k <= m) {  // c[m] = x1 multiplies v_{jj+1} (krylov_exp.py:88-90)
+            ks->c_re[k] = y[e].x;
+            ks->c_im[k] = y[e].y;
+        }
     }
     __syncwarp();
     return err1 < err2 ? err1 : (err1 * err2 / (err1 - err2));  // krylov_exp.py:84
 }
 
-// Scratch of the one-warp tridiagonal exponential (shared memory).
-struct KSmem {
-    double2 d[KMAX + 2], up[KMAX + 2], lo[KMAX + 2];
-    double2 y[KMAX + 4], t[KMAX + 4], tn[KMAX + 4], acc[KMAX + 4];
-};
-
 // Decide iteration j of a Lanczos run from the FP64 sums v = ||w_j||^2 and
 // (vr, vi) = <v_j, w_j>: ||w_j||, happy breakdown (every iteration), and, when `poll`, the
 // extended exponential and the error estimate.  Iterations that were not polled are not
-// tested, so on the first poll (`first_poll`) that finds convergence the warp walks back
-// over the earlier iterations while they also converge, and stops at the earliest of that
-// run -- the iteration where the reference, which tests every iteration, would have
-// stopped (the estimate decreases with j).  One warp; ks->status must be KS_RUNNING.
+// tested, so when the first poll (`first_poll`) already converges the warp tests the
+// earlier iterations in order and stops at the first that converges -- where the
+// reference, which tests every iteration, stops.  Callers start polling a few iterations
+// before the expected count, so that scan is rare.  One warp; ks->status must be
+// KS_RUNNING.
 static __device__ void krylov_decide(KState *ks, int j, double v, double vr, double vi, double dt,
                               double exp_tol, double norm_tol, bool poll, bool first_poll,
-                              int maxdim, KSmem &S) {
+                              int maxdim) {
     const int lane = threadIdx.x & 31;
     const double r = sqrt(v);
     const double adt = fabs(dt);
@@ -182,17 +467,18 @@ static __device__ void krylov_decide(KState *ks, int j, double v, double vr, dou
     __syncwarp();
     const int m = j + 1;
     if (n2 < norm_tol) {  // krylov_exp.py:63-71: exp(T[:j+1,:j+1]) e_0 over j+1 vectors
-        for (int k = lane; k < m; k += 32) {
-            S.d[k] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
-            S.up[k] = k > 0 ? make_double2(dt * ks->b_im[k], -dt * ks->b_re[k]) : make_double2(0.0, 0.0);
-            S.lo[k] = make_double2(0.0, -dt * ks->r[k]);
-        }
-        __syncwarp();
-        double2 Z1, Z2;
-        warp_expm_col(m, S.d, S.up, S.lo, S.y, S.t, S.tn, S.acc, &Z1, &Z2);
-        for (int k = lane; k < m; k += 32) {
-            ks->c_re[k] = S.y[k + 1].x;
-            ks->c_im[k] = S.y[k + 1].y;
+        constexpr int NE = (KMAX + 2 + 31) / 32;
+        double2 d[NE], l[NE], u[NE], y[NE];
+        double td[NE], tr[NE];
+        load_rows<NE>(ks, m, dt, d, l, u, td, tr);
+        cheb_expm<NE>(d, l, u, -1, make_double2(0.0, 0.0), 0, dt, td, tr, m, y);
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const int k = lane * NE + e;
+            if (k < m) {
+                ks->c_re[k] = y[e].x;
+                ks->c_im[k] = y[e].y;
+            }
         }
         if (lane == 0) {
             ks->nvec = m;
@@ -203,18 +489,20 @@ static __device__ void krylov_decide(KState *ks, int j, double v, double vr, dou
         return;
     }
     if (!poll) return;
-    double err = krylov_eval(ks, j, dt, S.d, S.up, S.lo, S.y, S.t, S.tn, S.acc);
+    double err = krylov_eval(ks, j, dt);
     int jc = j;  // the stopping iteration
-    if (err < exp_tol && first_poll) {
-        int last = j;  // iteration whose coefficients are in ks->c
-        for (int jj = j - 1; jj >= 0; --jj) {
-            const double e = krylov_eval(ks, jj, dt, S.d, S.up, S.lo, S.y, S.t, S.tn, S.acc);
-            last = jj;
-            if (!(e < exp_tol)) break;
-            err = e;
-            jc = jj;
+    if (err < exp_tol && first_poll && j > 0) {
+        // the untested iterations, in order: the first that converges is where the
+        // reference (testing every iteration) stops
+        for (int jj = 0; jj < j; ++jj) {
+            const double e = krylov_eval(ks, jj, dt);
+            if (e < exp_tol) {
+                err = e;
+                jc = jj;
+                break;
+            }
         }
-        if (last != jc) krylov_eval(ks, jc, dt, S.d, S.up, S.lo, S.y, S.t, S.tn, S.acc);
+        if (jc == j) krylov_eval(ks, j, dt);  // its coefficients again
     }
     if (lane == 0) {
         ks->err = err;

@@ -59,9 +59,9 @@ class _StepCache:
 
 
 _caches: dict = {}
-# When true, convergence is first tested one iteration before the previous step's count;
-# a first test that converges looks back over the untested iterations (emusv_krylov_step),
-# so the hint saves host synchronisations without moving the stopping iteration.
+# When true, the host first reads the device's convergence decision three iterations
+# before the previous step's count (the device tests every iteration), so the hint saves
+# host synchronisations without moving the stopping iteration.
 use_iteration_hint: bool = True
 
 
@@ -91,7 +91,7 @@ def fused_step(op: HamiltonianExpOperator, v: torch.Tensor, exp_tolerance: float
     c = _cache(v.device, n, code)
     out = torch.empty_like(v) if out is None else out
     info = _lib.KrylovInfo()
-    hint = max(0, c.last_iters - 1) if use_iteration_hint else 0
+    hint = max(0, c.last_iters - 3) if use_iteration_hint else 0
     if c.buf is None:
         c.capacity = min(max_krylov_dim + 1, 32)
     while True:

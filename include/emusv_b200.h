@@ -117,10 +117,10 @@ size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity);
  * Replaces DifferentiableStateVectorEvolution.forward/evolve
  * (emu_sv/time_evolution/torch.py:143-219) with krylov_exp
  * (emu_base/math/krylov_exp.py:23-131) and RydbergHamiltonian.__mul__ as the operator.
- * Convergence is tested from iteration `krylov_dim_hint` on (0: every iteration, as the
- * reference does); when the first test already converges, the earlier iterations are
- * tested backwards while they converge too, so the step stops where the reference stops
- * whenever the error estimate decreases with the iteration count.
+ * Convergence is tested on the device at every iteration, as the reference does; the
+ * host reads the device's decision from iteration `krylov_dim_hint` on (0: every
+ * iteration), so the hint only saves host synchronisations and never moves the stopping
+ * iteration.
  * psi_out may equal psi_in.  Returns EMUSV_NOT_CONVERGED (result still written, as
  * krylov_exp_impl does) or EMUSV_WORKSPACE_TOO_SMALL (nothing written; retry with a
  * larger basis).  `info` (host) may be NULL.  Synchronises the stream at every
@@ -178,6 +178,14 @@ int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const 
 /* One memset and one cooperative launch (stream-ordered only, so it can be captured in a
  * CUDA graph and replayed): evolves every instance through all its steps. */
 int emusv_batch_launch(int dtype, int tile_bits, int blocks_per_sm, void *workspace, void *stream);
+/* Steps [first_step, first_step + steps) of the prepared batch on `states` (NULL: the
+ * prepared states), in place; when `history` is given, the packed states after every
+ * `history_every`-th step of the launch are also written to history slot
+ * (k + 1) / history_every - 1 (slots of sum_i 2^n_i amplitudes): the checkpoints of a
+ * checkpointed adjoint and the states it recomputes between them.  Capturable. */
+int emusv_batch_launch_steps(int dtype, int tile_bits, int blocks_per_sm, int first_step,
+                             int steps, void *states, void *history, int history_every,
+                             void *workspace, void *stream);
 /* CTAs per SM the persistent kernel can keep resident for this shape (0: no such shape). */
 int emusv_batch_max_blocks_per_sm(int dtype, int tile_bits);
 /* Per-instance emusv_status (EMUSV_NOT_CONVERGED = RecursionError of that instance,
@@ -186,6 +194,29 @@ int emusv_batch_max_blocks_per_sm(int dtype, int tile_bits);
  * EMUSV_TIMEOUT if a grid barrier gave up.  Synchronises the stream. */
 int emusv_batch_results(int ninst, int max_steps, void *workspace, int *status_out,
                         int *iterations_out, void *stream);
+
+/* ---- batched adjoint steps: DifferentiableStateVectorEvolution.backward
+ * (emu_sv/time_evolution/torch.py:223-378, double_krylov.py:5-113) for every instance of a
+ * batch in one persistent launch.  Prepared like a batch (all steps' pulses); each launch
+ * takes step `step` of every instance: states (psi_step, packed) and grad_in (dL/dpsi
+ * after the step, packed) in, grad_out (dL/dpsi before the step = exp(+i dt H) grad_in)
+ * and grads_dev [ninst][3][20] (dL/dOmega_q, dL/ddelta_q, dL/dphi_q by qubit q; FP64,
+ * device) out, plus an emusv status per instance in status_dev [ninst] (device).  The
+ * interaction-matrix gradient is not formed here (emusv_adjoint_step has it).
+ * Capturable: a launch issues two memsets and one cooperative kernel. */
+size_t emusv_batch_adjoint_workspace_bytes(int ninst, const int *nqubits, const int *nsteps,
+                                           int dtype, int tile_bits, int basis_capacity);
+int emusv_batch_adjoint_prepare(int ninst, const int *nqubits, const int *nsteps, const double *dt,
+                                int dtype, const double *omegas, const double *deltas,
+                                const double *phis, const double *interactions, double tolerance,
+                                int max_krylov_dim, int tile_bits, int basis_capacity,
+                                void *workspace, size_t workspace_bytes, void *stream);
+int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int step,
+                               const void *states, const void *grad_in, void *grad_out,
+                               double *grads_dev, int *status_dev, void *workspace, void *stream);
+/* Krylov iteration counts of the last adjoint launch, [ninst][2] (state basis, gradient
+ * basis), to a host array.  Synchronises the stream. */
+int emusv_batch_adjoint_iterations(int ninst, void *workspace, int *iterations_out, void *stream);
 
 /* ---- building blocks of the generic krylov_exp(op, v, ...) (krylov_exp.py:23-106) ----
  * For an arbitrary operator applied by the caller, these give the FP64-accumulated
