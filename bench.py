@@ -294,6 +294,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         plain["ours_c64_over_plain"] = round(value / world / plain["steps_per_s"], 2)
         result["secondary"]["plain_torch_c128_gpu"] = plain
         log(f"plain complex128 torch path: {plain}")
+    if not args.no_batch and world == 1:
+        result["secondary"]["batch_256_c64"] = batch_c4(dev)
+        log(f"batch: {result['secondary']['batch_256_c64']}")
+        result["secondary"]["ring_n16_gradients_c128"] = grads_c5(dev)
+        log(f"gradients: {result['secondary']['ring_n16_gradients_c128']}")
     if not args.no_precision and world == 1:
         result["secondary"]["precision"] = precision_check(w, dev)
         log(f"precision: {result['secondary']['precision']}")
@@ -479,6 +484,130 @@ def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1) -> dict:
                       f"{warm} warm-up step(s); CUDA events"}
 
 
+# ------------------------------------------------------------------ batched workloads
+def batch_c4(dev, per_instance_sample: int = 8) -> dict:
+    """The 256-register batch (N in 12..18, 150 steps each, complex64/FP64) in one
+    persistent launch replayed from a CUDA graph, with the autotuned launch shape, next to
+    the same registers stepped one at a time through the single-register API."""
+    import torch
+
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian, _lib
+    from emulators_b200 import workloads as wl
+    from emulators_b200.batch import BatchEvolution, autotune
+    from emulators_b200.krylov import fused_step
+
+    regs = wl.batch_256()
+    b = BatchEvolution(regs, precision="c64")
+    t = autotune(b)
+    b.reset()
+    b.prepare(t.tile_bits, t.capacity)
+    b.capture(t.blocks_per_sm)
+    times = []
+    for _ in range(3):  # first replay warms up
+        b.reset()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    status, iters = b.results()
+    el = min(times[1:])
+    total = int(b.nsteps.sum())
+    # per-instance path: the first registers, every step, one fused step call each
+    per = regs[:per_instance_sample]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    nst = 0
+    for w in per:
+        n = w.nqubits
+        s = torch.zeros(1 << n, dtype=torch.complex64, device=dev)
+        s[0] = 1.0
+        for k in range(w.nsteps):
+            H = RydbergHamiltonian(torch.as_tensor(w.omega[k]), torch.as_tensor(w.delta[k]),
+                                   torch.as_tensor(w.phi[k]), torch.as_tensor(w.U), dev)
+            s, _, st = fused_step(HamiltonianExpOperator(H, w.dt), s, w.tolerance, w.tolerance, 100)
+            _lib.check(st, "step")
+            nst += 1
+    e1.record()
+    torch.cuda.synchronize()
+    el1 = e0.elapsed_time(e1) / 1e3
+    # scale the sample's time by its share of the batch's amplitude-steps
+    amp = lambda ws: sum((1 << w.nqubits) * w.nsteps for w in ws)  # noqa: E731
+    per_rate = nst / el1
+    per_rate_weighted = total / (el1 * amp(regs) / amp(per))
+    return {"instances": len(regs), "instance_steps": total,
+            "ms": round(el * 1e3, 2), "instance_steps_per_s": round(total / el, 1),
+            "launch": {"tile_bits": t.tile_bits, "blocks_per_sm": t.blocks_per_sm,
+                       "krylov_capacity": t.capacity, "autotune_ms": t.ms,
+                       "graph": "one cooperative persistent kernel replayed from a CUDA graph"},
+            "krylov_iterations_mean": round(float(iters[iters > 0].mean()), 2),
+            "all_converged": bool((status == 0).all()),
+            "per_instance_api": {"sample": f"first {len(per)} registers, all steps, one "
+                                           f"emusv_krylov_step each",
+                                 "instance_steps_per_s": round(per_rate, 1),
+                                 "batch_equivalent_instance_steps_per_s": round(per_rate_weighted, 1)},
+            "speedup_vs_per_instance": round((total / el) / per_rate_weighted, 1)}
+
+
+def grads_c5(dev) -> dict:
+    """Neel-loss gradients of the 64 parameter sets of the N=16 ring (20 segments x 10
+    steps, complex128, checkpoints every 16 steps) through the batched forward and adjoint,
+    next to one set through the per-step autograd.Function chain (the reference's way)."""
+    import torch
+
+    from emulators_b200 import DifferentiableStateVectorEvolution as DSE
+    from emulators_b200 import workloads as wl
+    from emulators_b200.gradients import PulseGradientBatch
+
+    gw = wl.ring_n16_grad()
+    kd = 120  # some steps of some sets need more than 100 Krylov vectors
+    b = PulseGradientBatch(gw.U, gw.dt, gw.omega_seg, gw.delta_seg, gw.steps_per_segment,
+                           gw.target, precision="c128", checkpoint_every=16,
+                           tolerance=gw.tolerance, max_krylov_dim=kd)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    loss, go, gd, _ = b.loss_and_grad()
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    # one set, per-step Function chain
+    n = gw.nqubits
+    p = 0
+    om = torch.tensor(gw.omega_seg[p], device=dev, requires_grad=True)
+    de = torch.tensor(gw.delta_seg[p], device=dev, requires_grad=True)
+    U = torch.tensor(gw.U, device=dev)
+    zeros = torch.zeros(n, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    e0.record()
+    s = torch.zeros(1 << n, dtype=torch.complex128, device=dev)
+    s[0] = 1.0
+    for seg in range(gw.nsegments):
+        for _ in range(gw.steps_per_segment):
+            s, _ = DSE.apply(gw.dt, om[seg].expand(n), de[seg].expand(n), zeros, U, s,
+                             gw.tolerance, kd)
+    occ = torch.stack([torch.linalg.vector_norm(s.view(2**i, 2, -1)[:, 1]) ** 2 for i in range(n)])
+    L1 = torch.mean((occ - torch.tensor(gw.target, device=dev)) ** 2)
+    g_om, g_de = torch.autograd.grad(L1, (om, de))
+    e1.record()
+    torch.cuda.synchronize()
+    el1 = e0.elapsed_time(e1) / 1e3
+    rel = max(float(np.abs(g_om.cpu().numpy() - go[p]).max() / np.abs(go[p]).max()),
+              float(np.abs(g_de.cpu().numpy() - gd[p]).max() / np.abs(gd[p]).max()))
+    return {"sets": b.nsets, "steps": b.nsteps, "s": round(el, 3),
+            "grads_per_s": round(b.nsets / el, 3), "max_krylov_dim": kd,
+            "per_instance_autograd": {"sample": "set 0, all steps, the per-step autograd "
+                                                "Function (fused step forward, adjoint step "
+                                                "backward), every step's state kept",
+                                      "s": round(el1, 3), "grads_per_s": round(1.0 / el1, 4),
+                                      "max_rel_diff_vs_batched": rel},
+            "speedup_vs_per_instance": round((b.nsets / el) * el1, 1)}
+
+
 # ------------------------------------------------------------------ CPU baseline (oracle)
 def cpu_baseline(w, budget_s: float) -> dict:
     """The oracle (C/OpenMP restatement of the reference path, FP64/complex128) timed on
@@ -540,6 +669,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=30.0)
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain complex128 torch GPU path")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched evolution and batched gradient workloads")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the complex64-vs-complex128 run of the whole workload")
     args = ap.parse_args()

@@ -20,7 +20,7 @@
 
 #include <initializer_list>
 
-#include "krylov_internal.cuh"
+#include "krylov_device.cuh"
 #include "profile.cuh"
 
 namespace emusv {
@@ -84,109 +84,60 @@ static bool carve_adj(void *ws, size_t bytes, int64_t D, size_t es, AdjWorkspace
 }
 
 // ------------------------------------------------------------------ dS = exp(B) block
-// B (size M = ms + mg) is tridiagonal per block (d, up, lo) plus B[0][ms] = 1.
-// y = exp(B) e_{col}; Taylor series of exp(hB) applied to the vector, ||hB||_1 <= 2.
-__device__ void warp_expm_vec(int M, int ms, const double2 *d, const double2 *up,
-                              const double2 *lo, int col, double2 *y, double2 *t, double2 *tn,
-                              double2 *acc) {
-    const int lane = threadIdx.x & 31;
-    double nrm = 0.0;
-    for (int k = lane; k < M; k += 32) {
-        double c = hypot(d[k].x, d[k].y);
-        if (k > 0) c += hypot(up[k].x, up[k].y);
-        if (k < M - 1) c += hypot(lo[k].x, lo[k].y);
-        if (k == ms) c += 1.0;  // the coupling entry B[0][ms]
-        nrm = fmax(nrm, c);
+// Column col of dS: y = exp(B) e_{ms+col} for B = [[A_s, e0 e0^T], [0, A_g]] (A = -i dt T
+// of each basis, coupling 1; double_krylov.py:54-57), rows 0..ms-1.  T (double_krylov.py:
+// 100-113) has size m = j+2 after convergence (last row: T[j+1][j] = ||w_j||, T[j+1][j+1]
+// = 0) or j+1 after a happy breakdown.  One warp per column, Chebyshev form
+// (cheb_expm: the spectrum of B is that of its two blocks).
+__device__ __forceinline__ void adj_block_row(const KState *ks, int kk, int m, double dt,
+                                              double2 &d, double2 &l, double2 &u, double &td,
+                                              double &tr) {
+    const int jj = ks->iters - 1;
+    d = l = u = make_double2(0.0, 0.0);
+    td = tr = 0.0;
+    if (kk <= jj) {
+        d = make_double2(dt * ks->a_im[kk], -dt * ks->a_re[kk]);
+        td = ks->a_re[kk];
+        tr = fabs(ks->a_im[kk]);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nrm = fmax(nrm, __shfl_xor_sync(0xffffffffu, nrm, o));
-    int s = 1;
-    if (nrm > 2.0) s = nrm < 2.0 * (1 << 20) ? (int)ceil(nrm / 2.0) : (1 << 20);
-    const double h = 1.0 / s;
-    for (int k = lane; k < M + 2; k += 32) {
-        y[k] = make_double2(k == col + 1 ? 1.0 : 0.0, 0.0);
-        t[k] = tn[k] = acc[k] = make_double2(0.0, 0.0);
+    if (kk >= 1) {
+        l = make_double2(0.0, -dt * ks->r[kk - 1]);
+        tr += fabs(ks->r[kk - 1]);
     }
-    __syncwarp();
-    for (int step = 0; step < s; ++step) {
-        for (int k = lane; k < M; k += 32) t[k + 1] = acc[k + 1] = y[k + 1];
-        __syncwarp();
-        double2 *cur = t, *nxt = tn;
-        for (int q = 1; q < 80; ++q) {
-            const double f = h / q;
-            double tmax = 0.0, amax = 0.0;
-            for (int k = lane; k < M; k += 32) {
-                const double2 a0 = cur[k + 1], am = cur[k], ap = cur[k + 2];
-                double re = d[k].x * a0.x - d[k].y * a0.y;
-                double im = d[k].x * a0.y + d[k].y * a0.x;
-                if (k > 0) {
-                    re += lo[k - 1].x * am.x - lo[k - 1].y * am.y;
-                    im += lo[k - 1].x * am.y + lo[k - 1].y * am.x;
-                }
-                if (k < M - 1) {
-                    re += up[k + 1].x * ap.x - up[k + 1].y * ap.y;
-                    im += up[k + 1].x * ap.y + up[k + 1].y * ap.x;
-                }
-                if (k == 0) {  // B[0][ms] = 1
-                    re += cur[ms + 1].x;
-                    im += cur[ms + 1].y;
-                }
-                const double2 o = make_double2(f * re, f * im);
-                nxt[k + 1] = o;
-                double2 ac = acc[k + 1];
-                ac.x += o.x;
-                ac.y += o.y;
-                acc[k + 1] = ac;
-                tmax = fmax(tmax, fmax(fabs(o.x), fabs(o.y)));
-                amax = fmax(amax, fmax(fabs(ac.x), fabs(ac.y)));
-            }
-            __syncwarp();
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-                amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-            }
-            double2 *tmp = cur;
-            cur = nxt;
-            nxt = tmp;
-            if (tmax <= 1e-18 * fmax(amax, 1e-300)) break;
-        }
-        for (int k = lane; k < M; k += 32) y[k + 1] = acc[k + 1];
-        __syncwarp();
+    if (kk + 1 <= jj && kk + 1 < m) {
+        u = make_double2(dt * ks->b_im[kk + 1], -dt * ks->b_re[kk + 1]);
+        tr += hypot(ks->b_re[kk + 1], ks->b_im[kk + 1]);
     }
 }
 
-constexpr int DS_WARPS = 2;  // 2 x 33 KB of per-warp series buffers + 12 KB of matrix
+constexpr int DS_WARPS = 4;
+constexpr int ADS_NE = (2 * KMAX + 31) / 32;
 
-// Fill the block matrix (op = -i dt H in this package's Lanczos basis) and compute the
-// columns of dS, one warp per column.  T (double_krylov.py:100-113): size m = j+2 after
-// convergence (last row: T[j+1][j] = ||w_j||, T[j+1][j+1] = 0) or j+1 after a happy
-// breakdown.
 __global__ void __launch_bounds__(32 * DS_WARPS)
 k_dS(const KState *ks_s, const KState *ks_g, double dt, double2 *dS) {
-    __shared__ double2 d[2 * KMAX + 2], up[2 * KMAX + 2], lo[2 * KMAX + 2];
-    __shared__ double2 buf[DS_WARPS][4][2 * KMAX + 4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ms = ks_s->status == 2 ? ks_s->iters : ks_s->iters + 1;
     const int mg = ks_g->status == 2 ? ks_g->iters : ks_g->iters + 1;
     const int M = ms + mg;
-    for (int k = threadIdx.x; k < M; k += blockDim.x) {
-        const KState *ks = k < ms ? ks_s : ks_g;
-        const int kk = k < ms ? k : k - ms, m = k < ms ? ms : mg, jj = ks->iters - 1;
-        // diagonal -i dt a_k, zero for the appended last vector
-        d[k] = kk <= jj ? make_double2(dt * ks->a_im[kk], -dt * ks->a_re[kk]) : make_double2(0.0, 0.0);
-        // upper T[kk-1][kk] = -i dt b_kk (kk = 1..jj), zero at the block start and the end
-        up[k] = (kk >= 1 && kk <= jj) ? make_double2(dt * ks->b_im[kk], -dt * ks->b_re[kk])
-                                      : make_double2(0.0, 0.0);
-        // lower T[kk+1][kk] = -i dt ||w_kk|| inside the block
-        lo[k] = (kk < m - 1) ? make_double2(0.0, -dt * ks->r[kk]) : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col = blockIdx.x * DS_WARPS + warp;
-    if (col >= mg) return;
-    double2 *y = buf[warp][0], *t = buf[warp][1], *tn = buf[warp][2], *acc = buf[warp][3];
-    warp_expm_vec(M, ms, d, up, lo, ms + col, y, t, tn, acc);
-    for (int i = lane; i < ms; i += 32) dS[i * KMAX + col] = y[i + 1];
+    if (col >= mg || M > 32 * ADS_NE) return;
+    double2 d[ADS_NE], l[ADS_NE], u[ADS_NE], y[ADS_NE];
+    double td[ADS_NE], tr[ADS_NE];
+#pragma unroll
+    for (int e = 0; e < ADS_NE; ++e) {
+        const int k = lane * ADS_NE + e;
+        d[e] = l[e] = u[e] = make_double2(0.0, 0.0);
+        td[e] = tr[e] = 0.0;
+        if (k < ms) adj_block_row(ks_s, k, ms, dt, d[e], l[e], u[e], td[e], tr[e]);
+        else if (k < M) adj_block_row(ks_g, k - ms, mg, dt, d[e], l[e], u[e], td[e], tr[e]);
+        if (k == 0) tr[e] += 1.0 / fabs(dt);  // the coupling entry 1 in T units
+    }
+    cheb_expm<ADS_NE>(d, l, u, ms, make_double2(1.0, 0.0), ms + col, dt, td, tr, M, y);
+#pragma unroll
+    for (int e = 0; e < ADS_NE; ++e) {
+        const int r = lane * ADS_NE + e;
+        if (r < ms) dS[r * KMAX + col] = y[e];
+    }
 }
 
 // ------------------------------------------------------------------ E = dS^T V_s
