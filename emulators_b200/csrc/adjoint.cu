@@ -96,8 +96,8 @@ __device__ __forceinline__ void adj_block_row(const KState *ks, int kk, int m, d
     d = l = u = make_double2(0.0, 0.0);
     td = tr = 0.0;
     if (kk <= jj) {
-        d = make_double2(dt * ks->a_im[kk], -dt * ks->a_re[kk]);
-        td = ks->a_re[kk];
+        d = make_double2(dt * ks->a_im[kk], -dt * (ks->a_re[kk] + ks->shift));
+        td = ks->a_re[kk] + ks->shift;
         tr = fabs(ks->a_im[kk]);
     }
     if (kk >= 1) {
@@ -391,11 +391,11 @@ int emusv_adjoint_step(int nqubits, int dtype, double dt, const double *omegas,
     // 1. the two Lanczos bases (double_krylov.py:51-52), both tolerances = tolerance
     int st_s = 0, st_g = 0;
     int st = lanczos_run(P, dtype, dt, state, W.ks_s, W.part_h, W.part_o, W.basis_s, W.capacity,
-                         tolerance, tolerance, max_krylov_dim, 0, s, &st_s);
+                         tolerance, tolerance, max_krylov_dim, 0, false, s, &st_s);
     if (st) return st;
     if (st_s == 0) return EMUSV_WORKSPACE_TOO_SMALL;
     st = lanczos_run(P, dtype, dt, grad_out, W.ks_g, W.part_h, W.part_o, W.basis_g, W.capacity,
-                     tolerance, tolerance, max_krylov_dim, 0, s, &st_g);
+                     tolerance, tolerance, max_krylov_dim, 0, false, s, &st_g);
     if (st) return st;
     if (st_g == 0) return EMUSV_WORKSPACE_TOO_SMALL;
     int hg[2];

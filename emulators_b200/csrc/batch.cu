@@ -461,6 +461,7 @@ __device__ bool krylov_rounds(const BArgs &A, int gstep, int rstep, unsigned &ph
                         else if (gstep >= I.nsteps) st = BS_IDLE;
                         else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
                         ks->s0 = s0;
+                        ks->shift = 0.0;
                         ks->scale[0] = 1.0 / s0;
                         ks->iters = 0;
                         ks->nvec = 0;
@@ -709,7 +710,7 @@ __device__ __forceinline__ void block_row(const KState *ks, int kk, int m, doubl
     d = l = u = make_double2(0.0, 0.0);
     td = tr = 0.0;
     if (kk <= jj) {
-        const double ar = __ldcg(&ks->a_re[kk]), ai = __ldcg(&ks->a_im[kk]);
+        const double ar = __ldcg(&ks->a_re[kk]) + __ldcg(&ks->shift), ai = __ldcg(&ks->a_im[kk]);
         d = make_double2(dt * ai, -dt * ar);
         td = ar;
         tr = fabs(ai);

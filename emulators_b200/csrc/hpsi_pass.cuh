@@ -70,6 +70,7 @@ struct PassArgs {
     double *partials;       // [gridDim.x * NRED]
     const int *gate;        // kernel returns at once when *gate != 0
     int *err;               // receives EMUSV_TIMEOUT when a bounded wait gives up
+    const double *eshift;   // pass L: if non-null, the diagonal is taken minus *eshift
 };
 
 // ------------------------------------------------------------------ PTX helpers
@@ -252,6 +253,7 @@ __host__ __device__ constexpr size_t pass_low_smem() {
 template <typename R, bool REALC, int TB, int RB, int EPI, int PB>
 __global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_low(const PassParams P, PassArgs A) {
+    const double eshift = A.eshift ? *A.eshift : 0.0;
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
     constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
@@ -344,7 +346,7 @@ k_pass_low(const PassParams P, PassArgs A) {
                     if ((base >> p2) & 1) e += Ush[p * UPAD + p2];
             }
             e = warp_sum(e);
-            if (lane == 0) sc[TB] = e;
+            if (lane == 0) sc[TB] = e - eshift;
             if (lane < TB) {
                 double cx = 0.0;
                 for (int p = TB; p < n; ++p)

@@ -81,11 +81,23 @@ __global__ void __launch_bounds__(BLOCK) k_norm2(const void *v_, i64 D, double *
         for (int k = 0; k < NRED; ++k) partials[(i64)blockIdx.x * NRED + k] = acc[k];
 }
 
-__global__ void k_init(KState *ks, const double *partials, int nblocks) {
+// Start of a run: the input norm, and sigma, the energy the run subtracts from H.  With
+// energy_shift, sigma = the previous run's <v_0, H v_0> (sigma_prev + a_0) when that run
+// finished, else 0.  The Lanczos recurrence of H - sigma has the same basis and the
+// tridiagonal matrix minus sigma (a_k is stored shifted); the exponentials add sigma back
+// (load_rows), so coefficients and error estimates are those of H itself -- only the
+// complex64 rounding of the diagonal inside H*psi shrinks.
+__global__ void k_init(KState *ks, const double *partials, int nblocks, int energy_shift) {
     __shared__ double red[(BLOCK / 32) * NRED];
     double v[NRED];
     sum_partials<NRED>(partials, nblocks, NRED, v, red);
     if (threadIdx.x == 0) {
+        double sh = 0.0;
+        if (energy_shift && (ks->status == KS_CONVERGED || ks->status == KS_HAPPY) && ks->iters > 0) {
+            sh = ks->shift + ks->a_re[0];
+            if (!isfinite(sh) || fabs(sh) > 1e12) sh = 0.0;
+        }
+        ks->shift = sh;
         const double s0 = sqrt(v[0]);  // krylov_exp.py:43
         ks->s0 = s0;
         ks->scale[0] = 1.0 / s0;       // krylov_exp.py:44 (applied on load)
@@ -122,7 +134,9 @@ k_orth(KState *ks, int j, const double *part_h, int nb_h, const void *vj_, const
         ks->a_im[j] = ai;
         ks->b_re[j] = b;
         ks->b_im[j] = 0.0;
-        ks->hn[j] = sqrt(s[0]);
+        // ||H v||^2 = ||(H - sigma) v||^2 + 2 sigma Re<v,(H - sigma) v> + sigma^2
+        const double sg = ks->shift;
+        ks->hn[j] = sqrt(fmax(0.0, s[0] + 2.0 * sg * s[1] + sg * sg));
     }
     const double sj = ks->scale[j];
     const double sp = j > 0 ? ks->scale[j - 1] : 0.0;
@@ -332,8 +346,8 @@ namespace emusv {
 
 int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState *ks,
                 double *part_h, double *part_o, unsigned char *basis, int capacity,
-                double exp_tol, double norm_tol, int maxdim, int hint, cudaStream_t s,
-                int *status_out) {
+                double exp_tol, double norm_tol, int maxdim, int hint, bool energy_shift,
+                cudaStream_t s, int *status_out) {
     const int nqubits = P.n;
     const i64 D = i64(1) << nqubits;
     const size_t es = dtype == EMUSV_C128 ? 16 : 8;
@@ -360,7 +374,7 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
     EMUSV_CHECK_LAUNCH();
     {
         ProfScope ps_(PROF_SMALL, s);
-        k_init<<<1, BLOCK, 0, s>>>(W.ks, W.part_h, sg);
+        k_init<<<1, BLOCK, 0, s>>>(W.ks, W.part_h, sg, energy_shift ? 1 : 0);
     }
     EMUSV_CHECK_LAUNCH();
 
@@ -382,6 +396,7 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
         A.gate = &W.ks->status;
         A.err = &W.ks->kerr;
         A.part_buf = part_vec;
+        A.eshift = &W.ks->shift;
         int gh = 0;
         int st = launch_hpsi(dtype, HP_LANCZOS, P, A, max_grid_blocks(), s, &gh);
         if (st) return st;
@@ -461,8 +476,8 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
     int status = KS_RUNNING;
     {
         const int st = lanczos_run(P, dtype, dt, psi_in, W.ks, W.part_h, W.part_o, W.basis, capacity,
-                                   exp_tolerance, norm_tolerance, max_krylov_dim, krylov_dim_hint, s,
-                                   &status);
+                                   exp_tolerance, norm_tolerance, max_krylov_dim, krylov_dim_hint,
+                                   true, s, &status);
         if (st) return st;
     }
     if (status == KS_TIMEOUT) {

@@ -377,8 +377,9 @@ __device__ __forceinline__ void load_rows(const KState *ks, int m, double dt, do
         d[e] = l[e] = u[e] = make_double2(0.0, 0.0);
         td[e] = tr[e] = 0.0;
         if (k < m) {
-            d[e] = make_double2(dt * ks->a_im[k], -dt * ks->a_re[k]);
-            td[e] = ks->a_re[k];
+            const double ar = ks->a_re[k] + ks->shift;  // a_k of H (the run may use H - sigma)
+            d[e] = make_double2(dt * ks->a_im[k], -dt * ar);
+            td[e] = ar;
             if (k > 0) {
                 l[e] = make_double2(0.0, -dt * ks->r[k - 1]);  // A[k][k-1]
                 tr[e] += fabs(ks->r[k - 1]);

@@ -16,7 +16,8 @@ struct KState {
     int iters;
     int nvec;
     int kerr;  // error word of the streaming kernels (EMUSV_TIMEOUT), read by k_small
-    double s0, err, outnorm2, pad2;
+    double s0, err, outnorm2;
+    double shift;  // sigma: the run works on H - sigma (the previous step's energy), see k_init
     double a_re[KMAX], a_im[KMAX];   // T_H[k][k]   = <v_k, H v_k> - b_k <v_k, v_{k-1}>
     double b_re[KMAX], b_im[KMAX];   // T_H[k-1][k] = ||w_{k-1}|| (= <v_{k-1}, H v_k> exactly)
     double vv_re[KMAX + 2], vv_im[KMAX + 2];  // <v_k, v_{k-1}>: residual non-orthogonality
@@ -34,8 +35,8 @@ struct KState {
 // run's own outcome is in ks->status.
 int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState *ks,
                 double *part_h, double *part_o, unsigned char *basis, int capacity,
-                double exp_tol, double norm_tol, int maxdim, int hint, cudaStream_t s,
-                int *status_out);
+                double exp_tol, double norm_tol, int maxdim, int hint, bool energy_shift,
+                cudaStream_t s, int *status_out);
 int read_status(KState *ks, cudaStream_t s, int *out);
 
 }  // namespace emusv

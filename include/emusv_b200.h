@@ -121,6 +121,9 @@ size_t emusv_krylov_workspace_bytes(int nqubits, int dtype, int basis_capacity);
  * host reads the device's decision from iteration `krylov_dim_hint` on (0: every
  * iteration), so the hint only saves host synchronisations and never moves the stopping
  * iteration.
+ * The workspace carries one value from call to call: the previous step's energy, which
+ * the next step subtracts from H inside H*psi (same basis and coefficients; less
+ * complex64 rounding of the diagonal).  Zero the workspace once before its first call.
  * psi_out may equal psi_in.  Returns EMUSV_NOT_CONVERGED (result still written, as
  * krylov_exp_impl does) or EMUSV_WORKSPACE_TOO_SMALL (nothing written; retry with a
  * larger basis).  `info` (host) may be NULL.  Synchronises the stream at every
