@@ -796,38 +796,36 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_post(const BArg
             continue;
         }
         const double2 *dS = D.dS + (size_t)i * D.mmax * D.mmax;
-        constexpr int KC = 4, CH = AMP < 4 ? AMP : 4;
+        // KC outputs per pass over the state basis: every loaded amplitude feeds KC MACs
+        constexpr int KC = 16;
         for (int k0 = 0; k0 < mg; k0 += KC) {
-            for (int a0 = 0; a0 < AMP; a0 += CH) {
-                double er[KC][CH], ei[KC][CH];
+            const int kn = mg - k0 < KC ? mg - k0 : KC;
+            for (int a = 0; a < AMP; ++a) {
+                double er[KC], ei[KC];
 #pragma unroll
-                for (int kk = 0; kk < KC; ++kk)
-#pragma unroll
-                    for (int c = 0; c < CH; ++c) er[kk][c] = ei[kk][c] = 0.0;
+                for (int kk = 0; kk < KC; ++kk) er[kk] = ei[kk] = 0.0;
+                const long long x = base + lane + 32 * a;
+#pragma unroll 4
                 for (int r = 0; r < ms; ++r) {
                     const double sc = __ldcg(&kss->scale[r]);
-                    const C *vr = vec_ptr<C>(A, r, I) + base + lane;
-                    C v[CH];
-#pragma unroll
-                    for (int c = 0; c < CH; ++c) v[c] = ldcg(vr + 32 * (a0 + c));
+                    const C v = ldcg(vec_ptr<C>(A, r, I) + x);
+                    const double vx = sc * double(v.x), vy = sc * double(v.y);
+                    const double2 *drow = dS + (size_t)r * D.mmax + k0;
 #pragma unroll
                     for (int kk = 0; kk < KC; ++kk) {
-                        if (k0 + kk >= mg) break;
-                        const double2 d = dS[r * D.mmax + k0 + kk];
-                        const double dr = sc * d.x, di = sc * d.y;
-#pragma unroll
-                        for (int c = 0; c < CH; ++c) {
-                            er[kk][c] += dr * double(v[c].x) - di * double(v[c].y);
-                            ei[kk][c] += dr * double(v[c].y) + di * double(v[c].x);
+                        if (kk < kn) {
+                            const double2 d = drow[kk];
+                            er[kk] += d.x * vx - d.y * vy;
+                            ei[kk] += d.x * vy + d.y * vx;
                         }
                     }
                 }
 #pragma unroll
                 for (int kk = 0; kk < KC; ++kk) {
-                    if (k0 + kk >= mg) break;
-                    C *Ek = reinterpret_cast<C *>(D.E + (size_t)(k0 + kk) * D.inst_amps * sizeof(C)) + I.off0;
-#pragma unroll
-                    for (int c = 0; c < CH; ++c) Ek[base + lane + 32 * (a0 + c)] = cmake<C>(er[kk][c], ei[kk][c]);
+                    if (kk < kn) {
+                        C *Ek = reinterpret_cast<C *>(D.E + (size_t)(k0 + kk) * D.inst_amps * sizeof(C)) + I.off0;
+                        Ek[x] = cmake<C>(er[kk], ei[kk]);
+                    }
                 }
             }
         }
@@ -1242,14 +1240,14 @@ static int lookup(const void *workspace, bool adjoint, Prepared *out) {
 }
 
 static int cooperative_launch(void *kern, int blocks_per_sm, void **args, cudaStream_t s,
-                              int *grid_out) {
+                              int *grid_out, int prof_kind = PROF_BATCH) {
     int per_sm = 0;
     EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BWARPS * 32, 0));
     if (per_sm < 1) return EMUSV_CUDA_ERROR;
     const int bps = blocks_per_sm < per_sm ? blocks_per_sm : per_sm;
     const int grid = bps * sm_count();
     if (grid_out) *grid_out = grid;
-    ProfScope ps_(PROF_BATCH, s);
+    ProfScope ps_(prof_kind, s);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(BWARPS * 32);
@@ -1429,7 +1427,7 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
     }
     EMUSV_CHECK_LAUNCH();
     EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl), s));
-    return cooperative_launch(k3, blocks_per_sm, args, s, nullptr);
+    return cooperative_launch(k3, blocks_per_sm, args, s, nullptr, PROF_ADJOINT);
 }
 
 // Krylov iteration counts of the last adjoint launch: [ninst][2] (state, gradient basis).

@@ -213,24 +213,69 @@ k_combine(const KState *ks, const void *v0_, const unsigned char *basis, i64 D, 
         ci[k] = f * ks->c_im[k];
     }
     __syncthreads();
-    const C *v0 = reinterpret_cast<const C *>(v0_);
-    const C *bs = reinterpret_cast<const C *>(basis);
+    const C *v0 = reinterpret_cast<const C *>(v0_);  // may equal out (in place, per element)
+    const C *__restrict__ bs = reinterpret_cast<const C *>(basis);
     C *out = reinterpret_cast<C *>(out_);
     double acc[NRED];
 #pragma unroll
     for (int k = 0; k < NRED; ++k) acc[k] = 0.0;
-    for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < D; x += (i64)gridDim.x * blockDim.x) {
-        const C a = v0[x];
-        double re = cr[0] * double(a.x) - ci[0] * double(a.y);
-        double im = cr[0] * double(a.y) + ci[0] * double(a.x);
-        for (int k = 1; k < nv; ++k) {
-            const C b = bs[(i64)k * D + x];
-            re += cr[k] * double(b.x) - ci[k] * double(b.y);
-            im += cr[k] * double(b.y) + ci[k] * double(b.x);
+    // XA amplitudes per thread (grid-strided, so every load instruction is coalesced) and
+    // KU basis vectors per step: XA * KU independent loads in flight per thread
+    constexpr int XA = 4, KU = 4;
+    const i64 G = (i64)gridDim.x * blockDim.x;
+    for (i64 x0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; x0 < D; x0 += XA * G) {
+        double re[XA], im[XA];
+#pragma unroll
+        for (int a = 0; a < XA; ++a) {
+            const i64 x = x0 + a * G;
+            re[a] = im[a] = 0.0;
+            if (x < D) {
+                const C v = __ldcs(v0 + x);
+                re[a] = cr[0] * double(v.x) - ci[0] * double(v.y);
+                im[a] = cr[0] * double(v.y) + ci[0] * double(v.x);
+            }
         }
-        const C o = cmake<C>(re, im);
-        out[x] = o;
-        acc[0] += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+        int k = 1;
+        for (; k + KU <= nv; k += KU) {
+            C b[KU][XA];
+#pragma unroll
+            for (int u = 0; u < KU; ++u)
+#pragma unroll
+                for (int a = 0; a < XA; ++a) {
+                    const i64 x = x0 + a * G;
+                    b[u][a] = x < D ? __ldcs(bs + (i64)(k + u) * D + x) : cmake<C>(0.0, 0.0);
+                }
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                const double r_ = cr[k + u], i_ = ci[k + u];
+#pragma unroll
+                for (int a = 0; a < XA; ++a) {
+                    re[a] += r_ * double(b[u][a].x) - i_ * double(b[u][a].y);
+                    im[a] += r_ * double(b[u][a].y) + i_ * double(b[u][a].x);
+                }
+            }
+        }
+        for (; k < nv; ++k) {
+            const double r_ = cr[k], i_ = ci[k];
+#pragma unroll
+            for (int a = 0; a < XA; ++a) {
+                const i64 x = x0 + a * G;
+                if (x < D) {
+                    const C b = __ldcs(bs + (i64)k * D + x);
+                    re[a] += r_ * double(b.x) - i_ * double(b.y);
+                    im[a] += r_ * double(b.y) + i_ * double(b.x);
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < XA; ++a) {
+            const i64 x = x0 + a * G;
+            if (x < D) {
+                const C o = cmake<C>(re[a], im[a]);
+                out[x] = o;
+                acc[0] += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+            }
+        }
     }
     block_sum<NRED>(acc, red);
     if (threadIdx.x == 0)
