@@ -118,6 +118,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------------ replicas
+def replica_rate(elapsed_s: float, steps: int, world: int, dist, device) -> tuple[float, float]:
+    """Whole-job rate of `world` independent replicas that each took `steps` steps: the
+    time is the maximum over ranks (one all-reduce after the timed region, nothing inside
+    it), the rate world * steps / that time."""
+    if dist is not None and world > 1:
+        import torch
+
+        t = torch.tensor([float(elapsed_s)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_s = float(t.item())
+    return elapsed_s, world * steps / elapsed_s
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     import torch
@@ -184,13 +198,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     ms_by = (np.zeros(8)).astype(np.float64)
     launches = np.zeros(8, dtype=np.int64)
     L.emusv_profile_end(ms_by.ctypes.data, launches.ctypes.data, 8)
-    elapsed = e0.elapsed_time(e1) / 1e3
+    elapsed, value = replica_rate(e0.elapsed_time(e1) / 1e3, K, world, dist, dev)
     if dist:
-        t = torch.tensor([elapsed], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = t.item()
         dist.barrier()
-    value = world * K / elapsed
     timed_iters = list(iters)
     log(f"timed: {K} steps in {elapsed:.4f} s -> {value:.3f} steps/s, iterations {timed_iters}")
 
@@ -341,16 +351,12 @@ def run_e2e(w, W, K, dev, dist, world) -> dict:
     host_out.copy_(impl.state.data, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
-    el = e0.elapsed_time(e1) / 1e3
     wall = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([el], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el = t.item()
+    el, rate = replica_rate(e0.elapsed_time(e1) / 1e3, K, world, dist, dev)
     n_obs = len(res.get("occupation"))
     h2d = (D * 8 + K * (3 * n + n * n) * 8) / K
     d2h = (D * 8 + K * 8 + n_obs * (n + 1) * 8) / K
-    return {"value": round(world * K / el, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+    return {"value": round(rate, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "wall_s": round(wall, 3),
             "api": "SVBackendImpl(SVConfig(precision='c64'), SequenceData)._run()",
             "observations": n_obs}
