@@ -15,6 +15,8 @@ from typing import Sequence
 
 import torch
 
+from . import _lib
+
 dtype = torch.complex128
 
 
@@ -74,17 +76,13 @@ class StateVector:
         return StateVector(scalar * self.data, eigenstates=self.eigenstates)
 
     def sample(self, num_shots: int = 1000) -> Counter:
-        """Bitstring counts drawn from |psi|^2 (dense_state.py:40-95)."""
-        p = (self.data.real.double() ** 2 + self.data.imag.double() ** 2)
-        if p.numel() <= 2**24:
-            idx = torch.multinomial(p, num_shots, replacement=True)
-        else:
-            cdf = torch.cumsum(p, 0)
-            cdf /= cdf[-1].clone()
-            idx = torch.searchsorted(cdf, torch.rand(num_shots, dtype=torch.float64,
-                                                     device=cdf.device), right=True)
-            idx.clamp_(max=p.numel() - 1)
-        n = self.n_qudits
+        """Bitstring counts drawn from |psi|^2 (dense_state.py:40-95) by inverting the
+        cumulative distribution on the GPU (emusv_sample; the reference's path for
+        registers above 2^24 amplitudes, emu_sv/utils.py:17-49, used here at every size)."""
+        psi = _lib.require_cuda_vector(self.data, "state")
+        n = _lib.nqubits_of(psi)
+        u = torch.rand(num_shots, dtype=torch.float64, device=psi.device)
+        idx = sample_indices(psi, u)
         return Counter(format(i, f"0{n}b") for i in idx.tolist())
 
     def __repr__(self) -> str:
@@ -93,3 +91,20 @@ class StateVector:
 
 def inner(left: StateVector, right: StateVector) -> torch.Tensor:
     return left.inner(right)
+
+
+def sample_indices(psi: torch.Tensor, uniforms: torch.Tensor) -> torch.Tensor:
+    """Indices drawn from |psi|^2 for the given uniforms in [0, 1): the first index whose
+    cumulative probability exceeds u * total (emu_sv/utils.py:40-49), on the GPU."""
+    psi = _lib.require_cuda_vector(psi, "state")
+    n = _lib.nqubits_of(psi)
+    u = uniforms.to(device=psi.device, dtype=torch.float64).contiguous()
+    out = torch.empty(u.numel(), dtype=torch.int64, device=psi.device)
+    L = _lib.load()
+    sc = _lib.scratch(psi.device, L.emusv_sample_scratch_bytes(n))
+    st = L.emusv_sample(n, _lib.dtype_code(psi.dtype), psi.data_ptr(), u.numel(), u.data_ptr(),
+                        out.data_ptr(), sc.data_ptr(), sc.numel(), _lib.stream_of(psi))
+    if st == _lib.NONFINITE:  # torch.multinomial's exception and message
+        raise RuntimeError("invalid multinomial distribution (sum of probabilities <= 0)")
+    _lib.check(st, "sample")
+    return out

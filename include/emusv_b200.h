@@ -156,6 +156,16 @@ int emusv_adjoint_step(int nqubits, int dtype, double dt, const double *omegas,
                        double *g_interaction, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/* Bitstring sampling (emu_sv/utils.py:17-49 sample_indices, its inverse-CDF path for
+ * every size): indices[k] = the first index whose FP64 cumulative |psi|^2 exceeds
+ * uniforms[k] * sum|psi|^2 (searchsorted right=True), clamped to 2^n - 1.  uniforms
+ * (device, [num_shots], in [0,1)) and indices (device int64) are caller-owned; the CDF is
+ * never formed (block sums, their prefix, one warp per draw).  EMUSV_NONFINITE when the
+ * total probability is not positive (the reference raises RuntimeError).  Synchronises. */
+size_t emusv_sample_scratch_bytes(int nqubits);
+int emusv_sample(int nqubits, int dtype, const void *psi, int num_shots, const double *uniforms,
+                 long long *indices, void *scratch, size_t scratch_bytes, void *stream);
+
 /* ---- batched evolution: many registers in one persistent launch ----
  * Replaces running the reference's time loop (emu_sv/sv_backend_impl.py:197-209, one
  * krylov_exp per step, krylov_exp.py:23-131) once per register: every register of the

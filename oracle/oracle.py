@@ -311,6 +311,18 @@ def step_backward(dt, omegas, deltas, phis, U, state, grad_out, tol, max_krylov_
     return g_om, g_de, g_ph, g_U, g_st
 
 
+# ----------------------------------------------------------------------- sampling
+def sample_indices(p: np.ndarray, uniforms: np.ndarray) -> np.ndarray:
+    """emu_sv/utils.py:40-49: cdf = cumsum(p) in FP64, normalised by its last value,
+    searchsorted(cdf, u, right=True), clamped to the last index."""
+    cdf = np.cumsum(np.asarray(p, dtype=np.float64))
+    total = cdf[-1]
+    if not total > 0:
+        raise RuntimeError("invalid multinomial distribution (sum of probabilities <= 0)")
+    idx = np.searchsorted(cdf / total, np.asarray(uniforms, dtype=np.float64), side="right")
+    return np.minimum(idx, len(cdf) - 1)
+
+
 # ----------------------------------------------------------------------- observables
 def occupation(psi: np.ndarray) -> np.ndarray:
     """custom_callback_implementations.py:30-47."""

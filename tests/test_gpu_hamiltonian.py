@@ -113,3 +113,27 @@ def test_empty_and_edge_registers():
     H0 = RydbergHamiltonian(torch.zeros(2), torch.zeros(2), torch.zeros(2), torch.zeros(2, 2), DEV)
     psi = torch.randn(4, dtype=torch.complex128, device=DEV)
     assert torch.count_nonzero(H0 * psi).item() == 0
+
+
+@pytest.mark.parametrize("n,dtype", [(5, torch.complex128), (13, torch.complex64),
+                                     (25, torch.complex128)])
+def test_sample_indices_vs_oracle(oracle, n, dtype):
+    """emusv_sample equals the inverse-CDF draw of emu_sv/utils.py:40-49 (restated by the
+    oracle) for the same uniforms, below and above the reference's 2^24 switch, including
+    draws near 0 and 1 and zero-probability amplitudes."""
+    from emulators_b200.state_vector import sample_indices
+
+    rng = np.random.default_rng(n)
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi[rng.random(1 << n) < 0.3] = 0.0  # zero-probability indices are never drawn
+    psi /= np.linalg.norm(psi)
+    u = np.concatenate([rng.random(4000), [0.0, 1e-300, 1 - 1e-16]])
+    t = torch.as_tensor(psi).to(DEV, dtype)
+    got = sample_indices(t, torch.as_tensor(u)).cpu().numpy()
+    p = np.abs(t.cpu().numpy().astype(np.complex128)) ** 2
+    want = oracle.sample_indices(p, u)
+    # identical draws except where u * total falls within rounding of a cumulative boundary
+    assert (got != want).sum() <= 2, (got != want).sum()
+    assert np.all((p[got] > 0) | (got == (1 << n) - 1))  # the clamp may land anywhere
+    with pytest.raises(RuntimeError):
+        sample_indices(torch.zeros_like(t), torch.as_tensor(u[:4]))
