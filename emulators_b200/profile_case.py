@@ -2,6 +2,8 @@
 
     python -m emulators_b200.profile_case [--n 25] [--dtype c64] [--steps 2] [--hpsi 3]
                                           [--max-krylov-dim 100]
+    python -m emulators_b200.profile_case --batch 64 --steps 3        # batched engine
+    python -m emulators_b200.profile_case --adjoint 8 --dtype c128    # batched adjoint
 
 Builds the 2 x n/2 ladder at 5.5 um with the ladder_n26 drive, runs `--hpsi` standalone
 H*psi launches and `--steps` Krylov time steps from |g...g>, prints device times.  Sized
@@ -29,7 +31,18 @@ def main(argv=None) -> int:
     ap.add_argument("--hpsi", type=int, default=3)
     ap.add_argument("--max-krylov-dim", type=int, default=100,
                     help="bounds the Krylov basis the step allocates")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instead: the first BATCH registers of the 256-register batch "
+                         "workload for --steps steps in one persistent launch")
+    ap.add_argument("--adjoint", type=int, default=0,
+                    help="instead: ADJOINT parameter sets of the N=16 ring gradient "
+                         "workload, 4 segments: forward, one checkpoint-segment "
+                         "recomputation and two batched adjoint steps")
     a = ap.parse_args(argv)
+    if a.batch:
+        return _batch_case(a)
+    if a.adjoint:
+        return _adjoint_case(a)
     dev = torch.device("cuda", 0)
     dt_ = torch.complex64 if a.dtype == "c64" else torch.complex128
     n = a.n
@@ -66,6 +79,52 @@ def main(argv=None) -> int:
                 "iterations": iters, "norm": float(torch.linalg.vector_norm(v))})
     print(json.dumps(out))
     assert np.isfinite(out["norm"])
+    return 0
+
+
+def _batch_case(a) -> int:
+    import dataclasses
+
+    from .batch import BatchEvolution
+
+    k = a.steps
+    regs = [dataclasses.replace(w, omega=w.omega[:k], delta=w.delta[:k], phi=w.phi[:k])
+            for w in wl.batch_256()[:a.batch]]
+    b = BatchEvolution(regs, precision=a.dtype)
+    tb = 9 if a.dtype == "c64" else 8
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b.reset()
+    b.prepare(tb, 40)
+    e0.record()
+    b.launch(2)
+    e1.record()
+    status, iters = b.results()
+    print(json.dumps({"registers": a.batch, "steps": k, "ms": e0.elapsed_time(e1),
+                      "iterations_mean": float(iters[iters > 0].mean()),
+                      "failed": int((status != 0).sum())}))
+    return 0
+
+
+def _adjoint_case(a) -> int:
+    from .gradients import PulseGradientBatch
+
+    gw = wl.ring_n16_grad()
+    S = a.adjoint
+    b = PulseGradientBatch(gw.U, gw.dt, gw.omega_seg[:S, :4], gw.delta_seg[:S, :4],
+                           gw.steps_per_segment, gw.target, precision=a.dtype, tile_bits=9,
+                           blocks_per_sm=1, max_krylov_dim=120)
+    b.forward()
+    occ = b.occupations()
+    n = b.nsets << b.n
+    b.g.copy_(b._seed(occ).reshape(-1))
+    first, length = 32, 8
+    b.work.copy_(b.hist.view(-1, n)[1])
+    b._launch_f(first, length - 1, b.work, b.rec, 1)
+    for k in (7, 6):
+        b._launch_a(first + k, b.rec.view(-1, n)[k - 1], b.g, b.g2)
+        b.g, b.g2 = b.g2, b.g
+    torch.cuda.synchronize()
+    print(json.dumps({"sets": S, "status": b.status[first + 6].tolist()}))
     return 0
 
 
