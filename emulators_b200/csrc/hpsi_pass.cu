@@ -13,13 +13,15 @@ namespace emusv {
 // Tile shapes: 2^TB amplitudes per CTA (64 KiB of shared memory either way), 2^RB of them
 // in each thread's registers, 256 threads.
 template <typename R> struct PassShape;
-// c64: 4096-amplitude tiles (32 KiB), 16 amplitudes per thread; c128: 2048-amplitude
-// tiles (32 KiB), 8 per thread; 256 threads.  Pass H reads rows of at least 32 bytes.
+// c64: 4096-amplitude tiles (32 KiB), 16 amplitudes per thread, pass H rows of 8
+// amplitudes (64 bytes: measured on B200, 32-byte rows made the N=26 Krylov step 9 %
+// slower); c128: 2048-amplitude tiles (32 KiB), 8 per thread, rows of 2 amplitudes
+// (32 bytes); 256 threads.
 // No thread-block clusters: measured on B200, reading partner amplitudes from a sibling
 // CTA's shared memory amplitude by amplitude (and the per-tile cluster barrier) cost more
 // than a further streaming pass, so every pass keeps its flips inside one CTA's tile.
 template <> struct PassShape<float> {
-    static constexpr int TB = 12, RB = 4, CMIN = 2;
+    static constexpr int TB = 12, RB = 4, CMIN = 3;
 };
 template <> struct PassShape<double> {
     static constexpr int TB = 11, RB = 3, CMIN = 1;
