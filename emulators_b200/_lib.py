@@ -50,6 +50,13 @@ SIGNATURES: dict[str, tuple] = {
     "emusv_adjoint_workspace_bytes": (_SZ, [_I, _I, _I]),
     "emusv_adjoint_step": (_I, [_I, _I, _D, _P, _P, _P, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _SZ,
                                 _P]),
+    "emusv_hpsi_noisy": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "emusv_arnoldi_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "emusv_arnoldi_step": (_I, [_I, _I, _D, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I, _I, _P, _SZ,
+                                ctypes.POINTER(KrylovInfo), _P]),
+    "emusv_qubit_densities_scratch_bytes": (_SZ, [_I]),
+    "emusv_qubit_densities": (_I, [_I, _I, _P, _P, _P, _SZ, _P]),
+    "emusv_apply_1q": (_I, [_I, _I, _P, _I, _P, _P]),
     "emusv_sample_scratch_bytes": (_SZ, [_I]),
     "emusv_sample": (_I, [_I, _I, _P, _I, _P, _P, _P, _SZ, _P]),
     "emusv_batch_max_qubits": (_I, []),

@@ -40,14 +40,23 @@ struct HamParams {
     double up_im[MAXQ];
     double dn_re[MAXQ];        // coefficient of |g><r| (target bit 0)
     double dn_im[MAXQ];
-    double field[MAXQ];        // -delta
+    double field[MAXQ];        // -delta (plus the real part of the noise per excitation)
     double U[MAXQ * MAXQ];     // symmetric U by bit positions, zero diagonal
+    // non-Hermitian noise term -0.5i sum_j L_j^dag L_j (the same 2x2 matrix on every
+    // qubit, hamiltonian.py:61-67,147-151): its off-diagonal entries are added to up/dn,
+    // the real part of its diagonal to field[] and dc_re; the imaginary part of the
+    // diagonal of x is dc_im + dg_im * popcount(x)
+    int noisy;
+    double dc_re, dc_im, dg_im;
 };
 
 // Build a HamParams from host arrays in reference (qubit) order.
 // Returns false on a bad argument.
 bool make_params(int n, const double *omegas, const double *deltas, const double *phis,
                  const double *interaction, HamParams *P);
+// Add the noise matrix `noise` (2x2 complex, row-major, re/im interleaved: 8 doubles) to
+// P.  Returns false on a non-finite entry.
+bool add_noise(const double *noise, HamParams *P);
 
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ double warp_sum(double v) {

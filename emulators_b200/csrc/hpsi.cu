@@ -42,6 +42,28 @@ bool make_params(int n, const double *omegas, const double *deltas, const double
     return true;
 }
 
+bool add_noise(const double *noise, HamParams *P) {
+    if (!noise) return true;
+    for (int k = 0; k < 8; ++k)
+        if (!isfinite(noise[k])) return false;
+    // noise[a][b] at (2a + b) * 2 (re) and + 1 (im)
+    const double n00r = noise[0], n00i = noise[1], n01r = noise[2], n01i = noise[3];
+    const double n10r = noise[4], n10i = noise[5], n11r = noise[6], n11i = noise[7];
+    for (int p = 0; p < P->n; ++p) {
+        P->up_re[p] += n10r;  // |1><0| (hamiltonian.py:66)
+        P->up_im[p] += n10i;
+        P->dn_re[p] += n01r;  // |0><1| (hamiltonian.py:67)
+        P->dn_im[p] += n01i;
+        P->field[p] += n11r - n00r;  // diagonal noise per excitation (hamiltonian.py:147-151)
+    }
+    P->real_coef = 0;
+    P->noisy = 1;
+    P->dc_re = P->n * n00r;
+    P->dc_im = P->n * n00i;
+    P->dg_im = n11i - n00i;
+    return true;
+}
+
 int sm_count() {
     static int cached[64] = {0};
     int dev = 0;
@@ -333,6 +355,24 @@ int emusv_hpsi(int nqubits, int dtype, const double *omegas, const double *delta
     A.su = 1.0;
     A.out = out;
     A.part_buf = out;  // the two-pass kernels keep their partial sums in place
+    A.err = device_error_word();
+    A.tile_bits = hpsi_tile_bits(nqubits);
+    return launch_hpsi(dtype, HP_STORE, P, A, 0, as_stream(stream), nullptr);
+}
+
+// H psi with the noise term (2x2 complex matrix on every qubit, 8 doubles row-major).
+int emusv_hpsi_noisy(int nqubits, int dtype, const double *omegas, const double *deltas,
+                     const double *phis, const double *interaction, const double *noise,
+                     const void *psi, void *out, void *stream) {
+    HamParams P;
+    if (!psi || !out || psi == out || !noise ||
+        !make_params(nqubits, omegas, deltas, phis, interaction, &P) || !add_noise(noise, &P))
+        return EMUSV_BAD_ARGUMENT;
+    HpsiArgs A = {};
+    A.u = psi;
+    A.su = 1.0;
+    A.out = out;
+    A.part_buf = out;
     A.err = device_error_word();
     A.tile_bits = hpsi_tile_bits(nqubits);
     return launch_hpsi(dtype, HP_STORE, P, A, 0, as_stream(stream), nullptr);

@@ -159,7 +159,8 @@ k_hpsi(const HamParams P, HpsiArgs A) {
             }
         }
         __syncthreads();
-        const double ehigh = gv[MAXQ] - (MODE == HP_LANCZOS && A.eshift ? *A.eshift : 0.0);
+        const double ehigh = gv[MAXQ] - (MODE == HP_LANCZOS && A.eshift ? *A.eshift : 0.0) +
+                             (MODE == HP_DIAG ? 0.0 : P.dc_re);
 
         for (int k = tid; k < TILE; k += BLOCK) {
             const i64 x = base + k;
@@ -199,9 +200,17 @@ k_hpsi(const HamParams P, HpsiArgs A) {
                     ai = fmar(cr, w.y, fmar(ci, w.x, ai));
                 }
             }
-            // H v = su * (flip sum + diag * u), diagonal product in FP64
-            const double hr = su * (double(ar) + d * double(v.x));
-            const double hi = su * (double(ai) + d * double(v.y));
+            // H v = su * (flip sum + diag * u), diagonal product in FP64; with the noise
+            // term the diagonal has the imaginary part dc_im + dg_im * popcount(x)
+            double hr, hi;
+            if (P.noisy) {
+                const double dI = P.dc_im + P.dg_im * __popcll((unsigned long long)x);
+                hr = su * (double(ar) + d * double(v.x) - dI * double(v.y));
+                hi = su * (double(ai) + d * double(v.y) + dI * double(v.x));
+            } else {
+                hr = su * (double(ar) + d * double(v.x));
+                hi = su * (double(ai) + d * double(v.y));
+            }
             const double vr = su * double(v.x), vi = su * double(v.y);
             if (MODE == HP_STORE || MODE == HP_LANCZOS)
                 reinterpret_cast<C *>(A.out)[x] = cmake<C>(hr, hi);

@@ -13,10 +13,11 @@ namespace emusv {
 // Tile shapes: 2^TB amplitudes per CTA (64 KiB of shared memory either way), 2^RB of them
 // in each thread's registers, 256 threads.
 template <typename R> struct PassShape;
-// c64: 4096-amplitude tiles (32 KiB), 16 amplitudes per thread, pass H rows of 8
-// amplitudes (64 bytes: measured on B200, 32-byte rows made the N=26 Krylov step 9 %
-// slower); c128: 2048-amplitude tiles (32 KiB), 8 per thread, rows of 2 amplitudes
-// (32 bytes); 256 threads.
+// c64: 4096-amplitude tiles (32 KiB), 16 amplitudes per thread; c128: 2048-amplitude
+// tiles (32 KiB), 8 per thread; 256 threads.  CMIN: chunk bits of the pass H rows, 64
+// bytes (measured on B200, 32-byte rows made the N=26 complex64 Krylov step 9 % slower);
+// complex128 registers whose high bits do not fit two 64-byte-row passes (n > 29) use
+// 32-byte rows (CMIN - 1).
 // No thread-block clusters: measured on B200, reading partner amplitudes from a sibling
 // CTA's shared memory amplitude by amplitude (and the per-tile cluster barrier) cost more
 // than a further streaming pass, so every pass keeps its flips inside one CTA's tile.
@@ -24,7 +25,7 @@ template <> struct PassShape<float> {
     static constexpr int TB = 12, RB = 4, CMIN = 3;
 };
 template <> struct PassShape<double> {
-    static constexpr int TB = 11, RB = 3, CMIN = 1;
+    static constexpr int TB = 11, RB = 3, CMIN = 2;
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
@@ -94,6 +95,9 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
         P->field[p] = H.field[p];
     }
     memcpy(P->U, H.U, sizeof(P->U));
+    P->dc_re = H.dc_re;
+    P->dc_im = H.dc_im;
+    P->dg_im = H.dg_im;
     const int SB = TB - RB;
     for (int a = 0; a < (1 << RB); ++a) {  // fields and pairs of the register bits
         double e = 0.0;
@@ -108,11 +112,11 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
     }
 }
 
-template <typename R, bool REALC, int EPI>
+template <typename R, bool REALC, int EPI, bool NOISY>
 static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
-    auto kern = k_pass_low<R, REALC, TB, RB, EPI, 0>;
+    auto kern = k_pass_low<R, REALC, TB, RB, EPI, 0, NOISY>;
     const size_t smem = pass_low_smem<C, TB>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -132,12 +136,11 @@ static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, in
 
 // One strided pass over the group bits [hpos, hpos + TB - CMIN) with CMIN chunk bits;
 // group bits below TB were applied by pass L and are skipped.
-template <typename R, bool REALC, int EPI>
+template <typename R, bool REALC, int EPI, int CMIN>
 static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *part,
                        cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
-    constexpr int CMIN = PassShape<R>::CMIN;
     const int n = P.n, g = TB - CMIN;
     if (hpos < CMIN || hpos + g > n) return EMUSV_BAD_ARGUMENT;
     P.hg = g;
@@ -174,9 +177,9 @@ static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *pa
 // pass L) are skipped, so every H pass keeps the compile-time chunk of CMIN bits.  The
 // partial sums live in HA.part_buf (which may be HA.out: every pass reads a tile before
 // writing it).
-template <typename R, bool REALC, int EPI_F>
+template <typename R, bool REALC, int EPI_F, int CMIN, bool NOISY>
 static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
-    constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, CMIN = PassShape<R>::CMIN;
+    constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB;
     const int n = H.n;
     PassParams P;
     fill_params(H, TB, RB, &P);
@@ -196,22 +199,37 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     int st;
     if (rem == 0) {
         A.out = HA.out;
-        return launch_low<R, REALC, EPI_F>(P, A, s, grid_out);
+        return launch_low<R, REALC, EPI_F, NOISY>(P, A, s, grid_out);
     }
     A.out = HA.part_buf;
-    if ((st = launch_low<R, REALC, EPI_PARTIAL>(P, A, s, nullptr))) return st;
+    if ((st = launch_low<R, REALC, EPI_PARTIAL, NOISY>(P, A, s, nullptr))) return st;
     if (rem > G) {
-        if ((st = launch_high<R, REALC, EPI_PARTIAL>(P, n - 2 * G, A, HA.part_buf, s, nullptr)))
+        if ((st = launch_high<R, REALC, EPI_PARTIAL, CMIN>(P, n - 2 * G, A, HA.part_buf, s, nullptr)))
             return st;
     }
     A.out = HA.out;
-    return launch_high<R, REALC, EPI_F>(P, n - G, A, HA.part_buf, s, grid_out);
+    return launch_high<R, REALC, EPI_F, CMIN>(P, n - G, A, HA.part_buf, s, grid_out);
+}
+
+// 64-byte rows (PassShape CMIN) where two H passes cover the bits above pass L, else
+// 32-byte rows
+template <typename R, bool REALC, int EPI_F, bool NOISY = false>
+static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
+    constexpr int TB = PassShape<R>::TB, CMIN = PassShape<R>::CMIN;
+    if (H.n - TB <= 2 * (TB - CMIN))
+        return run_passes<R, REALC, EPI_F, CMIN, NOISY>(H, HA, s, grid_out);
+    return run_passes<R, REALC, EPI_F, CMIN - 1, NOISY>(H, HA, s, grid_out);
 }
 
 // mode: HP_STORE or HP_LANCZOS (values of HpsiMode)
 int launch_hpsi_passes(int dtype, int mode, const HamParams &H, const HpsiArgs &A,
                        cudaStream_t s, int *grid_out) {
     const bool lz = mode == HP_LANCZOS;
+    if (H.noisy) {  // the non-Hermitian noise term: store mode only (Arnoldi, H*psi)
+        if (lz) return EMUSV_BAD_ARGUMENT;
+        return dtype == EMUSV_C64 ? run_passes<float, false, EPI_STORE, true>(H, A, s, grid_out)
+                                  : run_passes<double, false, EPI_STORE, true>(H, A, s, grid_out);
+    }
     if (dtype == EMUSV_C64) {
         if (H.real_coef)
             return lz ? run_passes<float, true, EPI_LANCZOS>(H, A, s, grid_out)

@@ -60,6 +60,7 @@ struct PassParams {
     int pbh;        // pass H: cluster bits (positions hpos+hg .. hpos+hg+pbh-1)
     int hbox_rows;  // pass H: group rows per TMA box (<= 256)
     int hskip;      // pass H: group bits below this position were applied by pass L
+    double dc_re, dc_im, dg_im;  // noise term of the diagonal (HamParams)
 };
 
 struct PassArgs {
@@ -250,7 +251,8 @@ __host__ __device__ constexpr size_t pass_low_smem() {
     return SL * (sizeof(C) << TB) + 8 * SL + sizeof(double) * (MAXQ * UPAD + MAXQ + SL * 64 + 8 * NRED);
 }
 
-template <typename R, bool REALC, int TB, int RB, int EPI, int PB>
+// NOISY: the diagonal has the imaginary part dc_im + dg_im * popcount(x) (noise term)
+template <typename R, bool REALC, int TB, int RB, int EPI, int PB, bool NOISY = false>
 __global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_low(const PassParams P, PassArgs A) {
     const double eshift = A.eshift ? *A.eshift : 0.0;
@@ -346,7 +348,7 @@ k_pass_low(const PassParams P, PassArgs A) {
                     if ((base >> p2) & 1) e += Ush[p * UPAD + p2];
             }
             e = warp_sum(e);
-            if (lane == 0) sc[TB] = e - eshift;
+            if (lane == 0) sc[TB] = e - eshift + P.dc_re;
             if (lane < TB) {
                 double cx = 0.0;
                 for (int p = TB; p < n; ++p)
@@ -388,6 +390,10 @@ k_pass_low(const PassParams P, PassArgs A) {
 #pragma unroll
             for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
             C *out_t = out + base + tid;
+            // noise: imaginary diagonal of x = base + tid + a*NT (disjoint bit fields)
+            const double dI0 = NOISY ? P.dc_im + P.dg_im * double(__popcll((unsigned long long)base) +
+                                                                  __popc((unsigned)tid))
+                                     : 0.0;
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
                 const int l = tid + a * NT;
@@ -411,6 +417,10 @@ k_pass_low(const PassParams P, PassArgs A) {
                     for (int k = 0; k < RB; ++k)
                         if ((a >> k) & 1) d += hRf[k];
                     acc.diag(d, v[a]);
+                    if (NOISY) {  // + i dI v
+                        const float dI = float(dI0 + P.dg_im * double(__popc((unsigned)a)));
+                        acc.a = fma2(pk2(-dI, dI), pk2(v[a].y, v[a].x), acc.a);
+                    }
                     const float2 t = upk2(acc.a);
                     if (EPI == EPI_PARTIAL) {
                         out_t[a * NT] = t;  // unscaled partial; pass H applies su
@@ -429,7 +439,12 @@ k_pass_low(const PassParams P, PassArgs A) {
                     for (int k = 0; k < RB; ++k)
                         if ((a >> k) & 1) d += hR[k];
                     const double ur = double(v[a].x), ui = double(v[a].y);
-                    const double tr = acc.re() + d * ur, ti = acc.im() + d * ui;
+                    double tr = acc.re() + d * ur, ti = acc.im() + d * ui;
+                    if (NOISY) {
+                        const double dI = dI0 + P.dg_im * double(__popc((unsigned)a));
+                        tr -= dI * ui;
+                        ti += dI * ur;
+                    }
                     if (EPI == EPI_PARTIAL) {
                         out_t[a * NT] = cmake<C>(tr, ti);  // unscaled partial; pass H applies su
                     } else {

@@ -373,6 +373,44 @@ namespace {
 thread_local int *pinned_status = nullptr;
 }  // namespace
 
+// Input norm and KState reset (no energy shift), as the start of lanczos_run.
+int krylov_begin(int dtype, const void *psi_in, i64 D, KState *ks, double *partials, cudaStream_t s) {
+    const int sg = stream_grid(D);
+    {
+        ProfScope ps_(PROF_ORTH, s);
+        if (dtype == EMUSV_C128) k_norm2<double><<<sg, BLOCK, 0, s>>>(psi_in, D, partials);
+        else k_norm2<float><<<sg, BLOCK, 0, s>>>(psi_in, D, partials);
+    }
+    EMUSV_CHECK_LAUNCH();
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_init<<<1, BLOCK, 0, s>>>(ks, partials, sg, 0);
+    }
+    EMUSV_CHECK_LAUNCH();
+    return EMUSV_OK;
+}
+
+// out = s0 * sum_k c_k scale_k stored_k over ks->nvec vectors, and ks->outnorm2.
+int krylov_combine(int dtype, KState *ks, const void *psi_in, const unsigned char *basis, i64 D,
+                   void *out, double *partials, cudaStream_t s) {
+    const int sg = stream_grid(D);
+    {
+        ProfScope ps_(PROF_COMBINE, s);
+        if (dtype == EMUSV_C128) k_combine<double><<<sg, BLOCK, 0, s>>>(ks, psi_in, basis, D, out, partials);
+        else k_combine<float><<<sg, BLOCK, 0, s>>>(ks, psi_in, basis, D, out, partials);
+    }
+    EMUSV_CHECK_LAUNCH();
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_finish_combine<<<1, BLOCK, 0, s>>>(ks, partials, sg);
+    }
+    EMUSV_CHECK_LAUNCH();
+    return EMUSV_OK;
+}
+
+int krylov_stream_grid(i64 D) { return stream_grid(D); }
+size_t krylov_header_bytes() { return header_bytes(); }
+
 int read_status(KState *ks, cudaStream_t s, int *out) {
     if (!pinned_status) {
         if (cudaHostAlloc((void **)&pinned_status, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {

@@ -299,6 +299,7 @@ static __device__ void cheb_expm(const double2 (&d)[NE], const double2 (&l)[NE],
     };
     const int N = (int)ceil(1.1 * z) + 40;  // terms kept
     const int K = N + 30;                   // Miller's start
+    const double twoz = z > 0.0 ? 2.0 / z : 0.0;  // no division inside the recurrence
     double2 b1[NE], b2[NE];  // b_{k+1}, b_{k+2}
 #pragma unroll
     for (int e = 0; e < NE; ++e) b1[e] = b2[e] = make_double2(0.0, 0.0);
@@ -330,7 +331,7 @@ static __device__ void cheb_expm(const double2 (&d)[NE], const double2 (&l)[NE],
             }
         }
         // J~_{k-1} = (2k / z) J~_k - J~_{k+1}
-        const double jm = (z > 0.0 ? (2.0 * k / z) : 0.0) * jk - jk1;
+        const double jm = (twoz * k) * jk - jk1;
         jk1 = jk;
         jk = jm;
         ph = cm(ph, up_step);
@@ -492,7 +493,9 @@ static __device__ void krylov_decide(KState *ks, int j, double v, double vr, dou
     if (!poll) return;
     double err = krylov_eval(ks, j, dt);
     int jc = j;  // the stopping iteration
-    if (err < exp_tol && first_poll && j > 0) {
+    // NaN (both error terms zero: 0 * 0 / 0 fails the test, as in the reference) also
+    // sends the first test back over the untested iterations
+    if ((err < exp_tol || err != err) && first_poll && j > 0) {
         // the untested iterations, in order: the first that converges is where the
         // reference (testing every iteration) stops
         for (int jj = 0; jj < j; ++jj) {

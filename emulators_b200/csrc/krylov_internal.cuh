@@ -38,5 +38,13 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
                 double exp_tol, double norm_tol, int maxdim, int hint, bool energy_shift,
                 cudaStream_t s, int *status_out);
 int read_status(KState *ks, cudaStream_t s, int *out);
+// Input norm and KState reset (no energy shift): k_norm2 + k_init.
+int krylov_begin(int dtype, const void *psi_in, i64 D, KState *ks, double *partials, cudaStream_t s);
+// out = s0 sum_k c_k scale_k stored_k (ks->nvec vectors; stored_0 = psi_in, stored_k at
+// basis + k*D), and ks->outnorm2.
+int krylov_combine(int dtype, KState *ks, const void *psi_in, const unsigned char *basis, i64 D,
+                   void *out, double *partials, cudaStream_t s);
+int krylov_stream_grid(i64 D);   // grid of the streaming vector kernels for length D
+size_t krylov_header_bytes();    // KState + partial buffers at the head of a workspace
 
 }  // namespace emusv

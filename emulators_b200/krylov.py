@@ -10,6 +10,8 @@ Two routes behind the reference signature:
 * any other callable (Hermitian case): the reference's Lanczos loop driven from Python,
   with the vector arithmetic in this package's kernels (FP64-accumulated dots, axpy,
   multi-vector combination) and the small exponential on the GPU.
+* ``is_hermitian=False`` with a :class:`HamiltonianExpOperator` (the Monte Carlo stepper's
+  noisy Hamiltonian): the whole Arnoldi step runs in ``emusv_arnoldi_step``.
 """
 
 from __future__ import annotations
@@ -56,6 +58,7 @@ class _StepCache:
     buf: torch.Tensor | None = None
     capacity: int = 0
     last_iters: int = 0
+    last_dt: float = 0.0
 
 
 _caches: dict = {}
@@ -65,8 +68,8 @@ _caches: dict = {}
 use_iteration_hint: bool = True
 
 
-def _cache(device, n, code) -> _StepCache:
-    key = (device.index, n, code)
+def _cache(device, n, code, kind: str = "lanczos") -> _StepCache:
+    key = (device.index, n, code, kind)
     c = _caches.get(key)
     if c is None:
         c = _caches[key] = _StepCache()
@@ -113,6 +116,53 @@ def fused_step(op: HamiltonianExpOperator, v: torch.Tensor, exp_tolerance: float
     c.last_iters = info.iterations
     if st not in (_lib.OK, _lib.NOT_CONVERGED):
         _lib.check(st, "krylov step")
+    return out, info, st
+
+
+_MAX_ARNOLDI_DIM = 100
+
+
+def fused_arnoldi_step(op: HamiltonianExpOperator, v: torch.Tensor, exp_tolerance: float,
+                       norm_tolerance: float, max_krylov_dim: int, out: torch.Tensor | None = None):
+    """exp(-i dt H) v for the (noisy, non-Hermitian) Hamiltonian of ``op`` by Arnoldi in
+    one C-ABI call (krylov_exp.py:23-106 with is_hermitian=False)."""
+    v = _lib.require_cuda_vector(v, "state")
+    n = _lib.nqubits_of(v)
+    if n != op.ham.nqubits:
+        raise ValueError(f"state has {n} qubits, Hamiltonian {op.ham.nqubits}")
+    if not 1 <= max_krylov_dim <= _MAX_ARNOLDI_DIM:
+        raise ValueError(f"max_krylov_dim must be in 1..{_MAX_ARNOLDI_DIM} for Arnoldi")
+    code = _lib.dtype_code(v.dtype)
+    L = _lib.load()
+    c = _cache(v.device, n, code, "arnoldi")
+    out = torch.empty_like(v) if out is None else out
+    info = _lib.KrylovInfo()
+    # the device tests convergence from the hint on; the previous count predicts this
+    # one only for the same step length (the Monte Carlo stepper's bracketing steps vary)
+    same_dt = abs(op.dt) == c.last_dt
+    hint = max(0, c.last_iters - 3) if (use_iteration_hint and same_dt) else 0
+    if c.buf is None:
+        c.capacity = min(max_krylov_dim + 1, 32)
+    noise = op.ham._noise_ptr()
+    while True:
+        need = L.emusv_arnoldi_workspace_bytes(n, code, c.capacity)
+        if c.buf is None or c.buf.numel() < need:
+            c.buf = None
+            c.buf = torch.empty(need, dtype=torch.uint8, device=v.device)
+        st = L.emusv_arnoldi_step(n, code, op.dt, *op.ham._params(), noise, v.data_ptr(),
+                                  out.data_ptr(), float(exp_tolerance), float(norm_tolerance),
+                                  int(max_krylov_dim), hint, c.buf.data_ptr(), c.buf.numel(), info,
+                                  _lib.stream_of(v))
+        if st == _lib.WORKSPACE_TOO_SMALL:
+            if c.capacity >= max_krylov_dim + 1:
+                _lib.check(st, "arnoldi step")
+            c.capacity = min(2 * c.capacity, max_krylov_dim + 1)
+            continue
+        break
+    c.last_iters = info.iterations
+    c.last_dt = abs(op.dt)
+    if st not in (_lib.OK, _lib.NOT_CONVERGED):
+        _lib.check(st, "arnoldi step")
     return out, info, st
 
 
@@ -212,9 +262,14 @@ def krylov_exp_impl(op, v: torch.Tensor, is_hermitian: bool, exp_tolerance: floa
                     ) -> KrylovExpResult:
     """Same contract as krylov_exp.py:23-106 (the input ``v`` becomes invalid)."""
     if not is_hermitian:
-        raise NotImplementedError("emulators_b200: only the Hermitian (Lanczos) Krylov "
-                                  "exponential is implemented")
+        if not isinstance(op, HamiltonianExpOperator):
+            raise NotImplementedError("emulators_b200: the non-Hermitian (Arnoldi) Krylov "
+                                      "exponential takes a HamiltonianExpOperator")
+        out, info, st = fused_arnoldi_step(op, v, exp_tolerance, norm_tolerance, max_krylov_dim)
+        return KrylovExpResult(out, st == _lib.OK, bool(info.happy_breakdown), info.iterations)
     if isinstance(op, HamiltonianExpOperator):
+        if op.ham.noise is not None:
+            raise ValueError("a Hamiltonian with the noise term is not Hermitian")
         out, info, st = fused_step(op, v, exp_tolerance, norm_tolerance, max_krylov_dim)
         return KrylovExpResult(out, st == _lib.OK, bool(info.happy_breakdown), info.iterations)
     return _generic_lanczos(op, v, exp_tolerance, norm_tolerance, max_krylov_dim)

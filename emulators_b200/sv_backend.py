@@ -22,7 +22,7 @@ from .hamiltonian import RydbergHamiltonian
 from .observables import (correlation_matrix_sv_impl, energy_second_moment_sv_impl,
                           energy_sv_impl, energy_variance_sv_impl, qubit_occupation_sv_impl)
 from .state_vector import StateVector
-from .time_evolution import EvolveStateVector
+from .time_evolution import EvolveMonteCarlo, EvolveStateVector
 
 _TIME_CONVERSION_COEFF = 0.001  # Omega and delta in rad/us, dt in ns (sv_backend_impl.py:29)
 logger = logging.getLogger("emulators")
@@ -182,6 +182,7 @@ class SequenceData:
     interaction_matrix: Callable | torch.Tensor
     qubit_ids: tuple = ()
     lindblad_ops: list = dataclasses.field(default_factory=list)
+    has_stochastic_noise: bool = False
 
     def U(self, t: float) -> torch.Tensor:
         if callable(self.interaction_matrix):
@@ -197,17 +198,26 @@ class SequenceData:
 
 # ---------------------------------------------------------------- time loop
 class SVBackendImpl:
-    """sv_backend_impl.py:74-262 for the noiseless state-vector stepper."""
+    """sv_backend_impl.py:74-262 for the state-vector steppers: noiseless, and the Monte
+    Carlo stepper when the sequence has Lindblad operators (sv_backend_impl.py:82-95); the
+    density-matrix (Lindblad equation) stepper is not part of this package."""
 
     def __init__(self, config: SVConfig, data: SequenceData):
-        if data.lindblad_ops:
-            raise NotImplementedError("emulators_b200: Lindblad noise is not implemented")
         from . import krylov
 
         krylov.use_iteration_hint = bool(config.krylov_dim_hint)
         self._config = config
         self._data = data
-        self.stepper = EvolveStateVector(config.max_krylov_dim)
+        if data.lindblad_ops:
+            solver = str(getattr(config.solver, "value", config.solver))
+            if (solver == "default" and data.has_stochastic_noise) or solver == "montecarlo":
+                self.stepper = EvolveMonteCarlo(config.max_krylov_dim)
+            else:
+                raise NotImplementedError("emulators_b200: the density-matrix (Lindblad "
+                                          "equation) solver is not implemented; use "
+                                          "solver='montecarlo'")
+        else:
+            self.stepper = EvolveStateVector(config.max_krylov_dim)
         self.target_times = data.target_times
         self.omega, self.delta, self.phi = data.omega, data.delta, data.phi
         self.nsteps = data.omega.shape[0]
@@ -251,7 +261,7 @@ class SVBackendImpl:
             state = self.state
         if self._current_H is None:  # t = 0 (sv_backend_impl.py:224-234)
             self._current_H = self.stepper.get_hamiltonian(
-                self.omega[0], self.delta[0], self.phi[0], [], self._data.U(
+                self.omega[0], self.delta[0], self.phi[0], self._data.lindblad_ops, self._data.U(
                     0.5 * (self.target_times[step_idx] + self.target_times[step_idx + 1])),
                 state.data.device)
         for o in due:

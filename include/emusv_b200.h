@@ -166,6 +166,48 @@ size_t emusv_sample_scratch_bytes(int nqubits);
 int emusv_sample(int nqubits, int dtype, const void *psi, int num_shots, const double *uniforms,
                  long long *indices, void *scratch, size_t scratch_bytes, void *stream);
 
+/* ---- noisy (non-Hermitian) path of the Monte Carlo stepper ----
+ * `noise` (host, 8 doubles) is the 2x2 complex matrix -0.5i sum_j L_j^dag L_j of
+ * compute_noise_from_lindbladians (emu_base/jump_lindblad_operators.py:79-93), row-major
+ * with re/im interleaved: [00, 01, 10, 11]; it acts on every qubit. */
+
+/* out = H psi with the noise term.  Replaces RydbergHamiltonian.__mul__ with noise
+ * (emu_sv/hamiltonian.py:61-67 coefficients, 147-151 diagonal). out != psi. */
+int emusv_hpsi_noisy(int nqubits, int dtype, const double *omegas, const double *deltas,
+                     const double *phis, const double *interaction, const double *noise,
+                     const void *psi, void *out, void *stream);
+
+/* Bytes of device workspace emusv_arnoldi_step needs for `basis_capacity` stored vectors
+ * (plus one vector of H*psi partial sums, the Hessenberg matrix and partial sums). */
+size_t emusv_arnoldi_workspace_bytes(int nqubits, int dtype, int basis_capacity);
+
+/* One step psi_out = exp(-i dt H) psi_in with H non-Hermitian (noise may be NULL: the
+ * Hermitian H through the same Arnoldi path) by Arnoldi with the Expokit error estimate.
+ * Replaces EvolveMonteCarlo.evolve (emu_sv/time_evolution/implementations.py:148-166),
+ * i.e. krylov_exp with is_hermitian=False (emu_base/math/krylov_exp.py:23-131): full
+ * orthogonalisation (classical Gram-Schmidt twice, three streaming passes per iteration),
+ * happy-breakdown test every iteration, convergence tested on the device from iteration
+ * `krylov_dim_hint` on (0: every iteration); when the first test already converges the
+ * earlier iterations are tested in order, so the stopping iteration is the reference's.
+ * max_krylov_dim <= 100.  Same return codes as emusv_krylov_step.  Synchronises. */
+int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, const double *deltas,
+                       const double *phis, const double *interaction, const double *noise,
+                       const void *psi_in, void *psi_out, double exp_tolerance, double norm_tolerance,
+                       int max_krylov_dim, int krylov_dim_hint, void *workspace,
+                       size_t workspace_bytes, emusv_krylov_info *info, void *stream);
+
+/* Single-qubit reduced density matrices rho_i (i = qubit, device float64 [n][8]: 2x2
+ * complex row-major) of an unnormalised state: Tr(O rho_i) is expect_batch's entry for
+ * qubit i and operator O (emu_sv/algebra.py:4-25), the jump weights of
+ * EvolveMonteCarlo.do_quantum_jump (implementations.py:168-190). */
+size_t emusv_qubit_densities_scratch_bytes(int nqubits);
+int emusv_qubit_densities(int nqubits, int dtype, const void *psi, double *rho_dev, void *scratch,
+                          size_t scratch_bytes, void *stream);
+
+/* psi <- op (x) on qubit `qubit`, in place; op host 2x2 complex (8 doubles).  Replaces
+ * emu_sv/algebra.py:28-37 (apply). */
+int emusv_apply_1q(int nqubits, int dtype, void *psi, int qubit, const double *op, void *stream);
+
 /* ---- batched evolution: many registers in one persistent launch ----
  * Replaces running the reference's time loop (emu_sv/sv_backend_impl.py:197-209, one
  * krylov_exp per step, krylov_exp.py:23-131) once per register: every register of the

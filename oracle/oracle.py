@@ -128,17 +128,23 @@ class Hamiltonian:
         + sum_{i<j} U_ij n_i n_j
     """
 
-    def __init__(self, omegas, deltas, phis, U):
+    def __init__(self, omegas, deltas, phis, U, noise=None):
         self.n = len(omegas)
         self.omegas = _real(omegas) / 2.0  # hamiltonian.py:52
         self.deltas = _real(deltas)
         self.phis = _real(phis)
         self.U = _real(U).reshape(self.n, self.n)
-        self.complex = bool(np.any(self.phis != 0.0))  # hamiltonian.py:61
+        self.noise = None if noise is None else np.asarray(noise, dtype=np.complex128).reshape(2, 2)
+        self.complex = bool(np.any(self.phis != 0.0)) or noise is not None  # hamiltonian.py:61
         up = self.omegas * np.exp(1j * self.phis)  # hamiltonian.py:62-64
+        dn = np.conj(up)
+        if self.noise is not None:  # hamiltonian.py:65-67
+            up = up + self.noise[1, 0]
+            dn = dn + self.noise[0, 1]
         self.coef = np.ascontiguousarray(
-            np.stack([up.real, up.imag, up.real, -up.imag], axis=1), dtype=np.float64)
+            np.stack([up.real, up.imag, dn.real, dn.imag], axis=1), dtype=np.float64)
         self._diag = None
+        self._noise_diag = None
 
     @property
     def diag(self) -> np.ndarray:
@@ -149,17 +155,30 @@ class Hamiltonian:
             self._diag = d
         return self._diag
 
+    def noise_diag(self) -> np.ndarray:
+        """The noise part of the diagonal: noise[0,0] on every qubit in |g>, noise[1,1] on
+        every qubit in |r> (hamiltonian.py:147-151)."""
+        if self._noise_diag is None:
+            x = np.arange(1 << self.n)
+            pop = np.zeros(1 << self.n, dtype=np.int64)
+            for p in range(self.n):
+                pop += (x >> p) & 1
+            self._noise_diag = (self.n - pop) * self.noise[0, 0] + pop * self.noise[1, 1]
+        return self._noise_diag
+
     def apply(self, psi: np.ndarray) -> np.ndarray:
         """H * psi (hamiltonian.py:69-91)."""
         psi = _c128(psi)
         out = np.empty_like(psi)
         lib().or_hpsi(self.n, _p(self.coef), _p(self.diag), _p(psi), _p(out))
+        if self.noise is not None:
+            out += self.noise_diag() * psi
         return out
 
     __mul__ = apply
 
     def expect(self, psi: np.ndarray) -> float:
-        """Re <psi|H|psi> (hamiltonian.py:164-172)."""
+        """Re <psi|H|psi> (hamiltonian.py:164-172; the real part also with noise)."""
         return vdot(_c128(psi), self.apply(psi)).real
 
 
@@ -433,3 +452,117 @@ def neel_loss_and_grad(gw, set_index: int, nseg: int | None = None):
         g_om[seg] += go.sum()
         g_de[seg] += gd.sum()
     return loss, g_om, g_de, occ
+
+
+# ----------------------------------------------------------------------- Monte Carlo
+def noise_from_lindbladians(lindbladians) -> np.ndarray:
+    """-0.5i sum L^dag L (emu_base/jump_lindblad_operators.py:79-93)."""
+    acc = np.zeros((2, 2), dtype=np.complex128)
+    for L in lindbladians:
+        L = np.asarray(L, dtype=np.complex128)
+        acc += L.conj().T @ L
+    return -0.5j * acc
+
+
+def expect_batch(psi: np.ndarray, ops: np.ndarray, n: int) -> np.ndarray:
+    """T[q, i] = Tr(ops_i rho_q) with rho_q[a][b] = sum psi[.,a,.] conj(psi[.,b,.])
+    (emu_sv/algebra.py:4-25)."""
+    psi = _c128(psi)
+    out = np.empty((n, len(ops)), dtype=np.complex128)
+    for q in range(n):
+        v = psi.reshape(2 ** q, 2, -1)
+        rho = np.einsum("iaj,ibj->ab", v, v.conj())
+        for i, O in enumerate(ops):
+            out[q, i] = np.trace(np.asarray(O) @ rho)
+    return out
+
+
+def apply_1q(psi: np.ndarray, q: int, op) -> np.ndarray:
+    """op on qubit q (emu_sv/algebra.py:28-37)."""
+    psi = _c128(psi)
+    return np.einsum("ab,ibj->iaj", np.asarray(op, dtype=np.complex128),
+                     psi.reshape(2 ** q, 2, -1)).reshape(-1)
+
+
+class Brent:
+    """emu_base/math/brents_root_finding.py:4-94, one abscissa at a time."""
+
+    def __init__(self, start, end, f_start, f_end, epsilon):
+        self.eps = epsilon
+        self.a, self.b, self.fa, self.fb = start, end, f_start, f_end
+        assert self.fa * self.fb < 0
+        if abs(self.fa) < abs(self.fb):
+            self.a, self.b, self.fa, self.fb = self.b, self.a, self.fb, self.fa
+        self.c, self.fc, self.d = self.a, self.fa, self.a
+        self.bis = True
+        self.nxt = None
+
+    def next(self):
+        a, b, c, fa, fb, fc = self.a, self.b, self.c, self.fa, self.fb, self.fc
+        if abs(fc - fa) < self.eps or abs(fc - fb) < self.eps:
+            dx = fb * (b - a) / (fa - fb)
+        else:
+            s_, r_, t_ = fb / fa, fb / fc, fa / fc
+            dx = s_ * (t_ * (r_ - t_) * (c - b) + (r_ - 1) * (b - a)) / ((t_ - 1) * (s_ - 1) * (r_ - 1))
+        delta = abs(2 * self.eps * b)
+        ref = abs(b - c) if self.bis else abs(c - self.d)
+        if abs(dx) >= abs(3 * (a - b) / 4) or dx * (a - b) < 0 or abs(dx) >= ref / 2 or ref < delta:
+            dx, self.bis = (a - b) / 2, True
+        else:
+            self.bis = False
+        self.nxt = b + dx
+        self.d = c
+        self.c, self.fc = b, fb
+        return self.nxt
+
+    def provide(self, x, fx):
+        assert x == self.nxt
+        if self.fa * fx < 0:
+            self.b, self.fb = x, fx
+        else:
+            self.a, self.fa = x, fx
+        if abs(self.fa) < abs(self.fb):
+            self.a, self.b, self.fa, self.fb = self.b, self.a, self.fb, self.fa
+
+    def converged(self, tol):
+        return abs(self.b - self.a) < tol
+
+
+def monte_carlo_step(rnd, threshold, dt, omegas, deltas, phis, U, state, lindblads, tol,
+                     max_krylov_dim=100):
+    """One EvolveMonteCarlo.apply (emu_sv/time_evolution/implementations.py:192-250) with
+    the random draws taken from ``rnd`` (a ``random.Random`` or the module) in the
+    reference's order.  Returns (state, new threshold, number of jumps)."""
+    H = Hamiltonian(omegas, deltas, phis, U, noise_from_lindbladians(lindblads))
+    n = H.n
+
+    def evolve(t, psi):
+        return krylov_exp(lambda x: -1j * t * H.apply(x), psi, tol, tol, is_hermitian=False,
+                          max_krylov_dim=max_krylov_dim)
+
+    ops = [np.asarray(L, dtype=np.complex128) for L in lindblads]
+    agg = [L.conj().T @ L for L in ops]
+    cur, jtol, jumps = 0.0, dt * 0.1, 0
+    new = norm(state) ** 2 - threshold
+    while abs(dt - cur) > 1e-5:
+        old = new
+        state = evolve(dt - cur, state)
+        new = norm(state) ** 2 - threshold
+        if new > 0.0:
+            break
+        rf = Brent(cur, dt, old, new, jtol)
+        cur = dt
+        while not rf.converged(jtol):
+            t = rf.next()
+            state = evolve(t - cur, state)
+            cur = t
+            new = norm(state) ** 2 - threshold
+            rf.provide(cur, new)
+        w = expect_batch(state, agg, n).real  # do_quantum_jump, 168-190
+        q, L = rnd.choices([(q, L) for q in range(n) for L in ops], weights=w.reshape(-1).tolist())[0]
+        state = apply_1q(state, q, L)
+        state = state / norm(state)
+        threshold = rnd.uniform(0.0, norm(state) ** 2)
+        jumps += 1
+        new = norm(state) ** 2 - threshold
+    return state, threshold, jumps

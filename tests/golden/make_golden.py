@@ -13,6 +13,9 @@ so the four hot-path modules are loaded one by one behind package shells:
 * emu_sv/hamiltonian.py             (RydbergHamiltonian)
 * emu_sv/time_evolution/torch.py    (DifferentiableStateVectorEvolution)
 * emu_sv/custom_callback_implementations.py (occupation / correlation / energy moments)
+* emu_base/math/brents_root_finding.py, emu_base/jump_lindblad_operators.py,
+  emu_sv/algebra.py, emu_sv/time_evolution/interface.py and implementations.py
+  (the Monte Carlo stepper)
 
 ``pulser.*`` and ``pyparsing`` imports are served by a meta-path finder that fabricates
 empty placeholder classes; none of them is called on the paths exercised here.
@@ -33,6 +36,10 @@ Fixtures (inputs and reference outputs, all complex128/float64):
                        final-state probes (inner products with seeded vectors).
 * ring_n16_grad.npz    reference autograd gradient of the Neel loss for 2 parameter sets
                        of the N=16 ring over the first 2 segments (20 steps).
+* noisy.npz            the Monte Carlo path: H*psi with the noise term, Arnoldi
+                       krylov_exp (is_hermitian=False), expect_batch / apply, Brent's
+                       abscissae, and EvolveMonteCarlo steps (N=8, 40 steps, two seeds of
+                       Python's random module).
 
 Usage:  python tests/golden/make_golden.py [--reference PATH] [--only NAME ...]
 """
@@ -142,6 +149,13 @@ def load_reference(ref: str) -> dict:
         "ham": load("emu_sv.hamiltonian", "emu_sv/hamiltonian.py"),
     }
     mods["torch"] = load("emu_sv.time_evolution.torch", "emu_sv/time_evolution/torch.py")
+    mods["brent"] = load("emu_base.math.brents_root_finding", "emu_base/math/brents_root_finding.py")
+    mods["jump"] = load("emu_base.jump_lindblad_operators", "emu_base/jump_lindblad_operators.py")
+    mods["algebra"] = load("emu_sv.algebra", "emu_sv/algebra.py")
+    iface = load("emu_sv.time_evolution.interface", "emu_sv/time_evolution/interface.py")
+    sys.modules["emu_sv.time_evolution"].BaseStepper = iface.BaseStepper
+    mods["impl"] = load("emu_sv.time_evolution.implementations",
+                        "emu_sv/time_evolution/implementations.py")
     mods["cb"] = load("emu_sv.custom_callback_implementations",
                       "emu_sv/custom_callback_implementations.py")
     return mods
@@ -486,6 +500,129 @@ GENERATORS = {
     "lattice_n20": gen_lattice_n20,
     "ring_n16_grad": gen_ring_n16_grad,
 }
+
+
+def _lindblads(R, scale=1.0):
+    """relaxation, dephasing and depolarizing operators of the reference's own
+    get_lindblad_operators, plus one effective-noise style operator."""
+    class NM:
+        noise_types = ("relaxation", "dephasing", "depolarizing")
+        relaxation_rate = 0.9 * scale
+        dephasing_rate = 0.6 * scale
+        hyperfine_dephasing_rate = 0.0
+        depolarizing_rate = 0.3 * scale
+
+    ops = []
+    for t in NM.noise_types:
+        ops += R["jump"].get_lindblad_operators(noise_type=t, noise_model=NM)
+    ops.append(torch.tensor([[0.1, 0.2 + 0.1j], [0.0, -0.3j]], dtype=torch.complex128) * scale ** 0.5)
+    return ops
+
+
+def gen_noisy(R):
+    """Noisy (non-Hermitian) H*psi, Arnoldi krylov_exp, expect_batch / apply, Brent's root
+    finder and EvolveMonteCarlo steps with seeded random draws."""
+    import random
+
+    Ham = R["ham"].RydbergHamiltonian
+    kimpl = R["krylov"].krylov_exp_impl
+    out = {}
+    ops = _lindblads(R)
+    noise = R["jump"].compute_noise_from_lindbladians(ops)
+    out["noise"] = np_(noise)
+    for k, L in enumerate(ops):
+        out[f"L{k}"] = np_(L)
+    out["nops"] = np.array(len(ops))
+    # H*psi with noise
+    for k, (n, wp) in enumerate([(3, False), (5, True), (8, False), (11, True), (13, True)]):
+        torch.manual_seed(100 + k)
+        p = get_randn_ham_params(n, wp)
+        psi = torch.randn(2 ** n, dtype=torch.complex128)
+        H = Ham(*p, device="cpu", noise=noise)
+        pre = f"h{k}_"
+        for nm, v in zip(["omegas", "deltas", "phis", "U"], p):
+            out[pre + nm] = np_(v)
+        out[pre + "psi"] = np_(psi)
+        out[pre + "hpsi"] = np_(H * psi)
+        out[pre + "diag"] = np_(H.diag)
+    out["hcount"] = np.array(5)
+    # Arnoldi exponential (is_hermitian=False)
+    k = 0
+    for n in [5, 8, 10]:
+        for dt in [0.01, 0.05, 0.2]:
+            torch.manual_seed(200 + k)
+            p = get_randn_ham_params(n, k % 2 == 1)
+            s0 = torch.randn(2 ** n, dtype=torch.complex128)
+            s0 = s0 / s0.norm()
+            H = Ham(*p, device="cpu", noise=noise)
+            kr = kimpl(lambda x: -1j * dt * (H * x), s0.clone(), False, 1e-10, 1e-10, 100)
+            pre = f"a{k}_"
+            for nm, v in zip(["omegas", "deltas", "phis", "U"], p):
+                out[pre + nm] = np_(v)
+            out[pre + "n"] = np.array(n)
+            out[pre + "dt"] = np.array(dt)
+            out[pre + "state"] = np_(s0)
+            out[pre + "result"] = np_(kr.result)
+            out[pre + "iters"] = np.array(kr.iteration_count)
+            out[pre + "happy"] = np.array(kr.happy_breakdown)
+            k += 1
+    out["acount"] = np.array(k)
+    # algebra: the reference test vectors (test/emu_sv/test_algebra.py) and a random state
+    vec = torch.tensor([0.0, 0.0, 0.5j, 1.0], dtype=torch.complex128)
+    nops = torch.tensor([[[0.0, 0.0], [0.0, 1.0j]], [[1.0, 0.0], [0.0, 0.0]],
+                         [[0.0, 1.0j], [0.0, 0.0]]], dtype=torch.complex128)
+    out["alg_vec"] = np_(vec)
+    out["alg_ops"] = np_(nops)
+    out["alg_expect"] = np_(R["algebra"].expect_batch(vec, nops, 2))
+    torch.manual_seed(7)
+    v6 = torch.randn(64, dtype=torch.complex128)
+    agg = torch.stack([L.mH @ L for L in ops])
+    out["alg_v6"] = np_(v6)
+    out["alg_expect6"] = np_(R["algebra"].expect_batch(v6, agg, 6))
+    for q in range(6):
+        out[f"alg_apply6_{q}"] = np_(R["algebra"].apply(v6, q, ops[q % len(ops)]))
+    # Brent: abscissae asked for on (x+3)(x-1)^2 (test_brents_root_finding.py:44-53)
+    rf = R["brent"].BrentsRootFinder(start=-4.0, end=4 / 3.0, f_start=(-4 + 3) * 25.0,
+                                     f_end=(4 / 3 + 3) * (1 / 3) ** 2, epsilon=1e-6)
+    xs = []
+    while not rf.is_converged(1e-6):
+        x = rf.get_next_abscissa()
+        xs.append(x)
+        rf.provide_ordinate(x, (x + 3) * (x - 1) ** 2)
+    out["brent_x"] = np.array(xs)
+    out["brent_root"] = np.array(rf.current_guess)
+    # Monte Carlo steps: N=8 chain, strong noise so that jumps happen
+    w = wl.chain_n10()
+    n, dt, nsteps = 8, 0.05, 40
+    U = torch.as_tensor(w.U[:n, :n])
+    mc_ops = _lindblads(R, scale=3.0)
+    for seed in [11, 12]:
+        random.seed(seed)
+        stepper = R["impl"].EvolveMonteCarlo(100)
+        st = torch.zeros(2 ** n, dtype=torch.complex128)
+        st[0] = 1.0
+        thr, states = [stepper.jump_threshold], []
+        for k in range(nsteps):
+            om = torch.full((n,), 2 * np.pi * (0.5 + 0.5 * np.sin(0.3 * k)), dtype=torch.float64)
+            de = torch.full((n,), -4.0 + 0.2 * k, dtype=torch.float64)
+            ph = torch.zeros(n, dtype=torch.float64)
+            st, _ = stepper.apply(dt, om, de, ph, U, st, 1e-10, mc_ops)
+            thr.append(stepper.jump_threshold)
+            if (k + 1) % 10 == 0:
+                states.append(np_(st).copy())  # krylov_exp normalises its input in place
+        out[f"mc{seed}_thresholds"] = np.array(thr)
+        out[f"mc{seed}_states"] = np.stack(states)
+    out["mc_n"] = np.array(n)
+    out["mc_dt"] = np.array(dt)
+    out["mc_nsteps"] = np.array(nsteps)
+    out["mc_nops"] = np.array(len(mc_ops))
+    for k, L in enumerate(mc_ops):
+        out[f"mcL{k}"] = np_(L)
+    out["mc_U"] = np_(U)
+    return out
+
+
+GENERATORS["noisy"] = gen_noisy
 
 
 def main():

@@ -122,9 +122,14 @@ def test_product_refuses_cpu_tensors():
     H = RydbergHamiltonian(torch.ones(3), torch.zeros(3), torch.zeros(3), torch.zeros(3, 3), "cpu")
     with pytest.raises(RuntimeError, match="CUDA"):
         H * torch.zeros(8, dtype=torch.complex128)
-    with pytest.raises(NotImplementedError):
+    Hn = RydbergHamiltonian(torch.ones(3), torch.zeros(3), torch.zeros(3), torch.zeros(3, 3), "cpu",
+                            noise=torch.zeros(2, 2, dtype=torch.complex128))
+    assert Hn.complex
+    with pytest.raises(RuntimeError, match="CUDA"):
+        Hn * torch.zeros(8, dtype=torch.complex128)
+    with pytest.raises(ValueError):
         RydbergHamiltonian(torch.ones(3), torch.zeros(3), torch.zeros(3), torch.zeros(3, 3), "cpu",
-                           noise=torch.zeros(2, 2))
+                           noise=torch.zeros(3, 3))
 
 
 def test_workloads_match_their_specification():
