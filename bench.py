@@ -309,6 +309,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         log(f"batch: {result['secondary']['batch_256_c64']}")
         result["secondary"]["ring_n16_gradients_c128"] = grads_c5(dev)
         log(f"gradients: {result['secondary']['ring_n16_gradients_c128']}")
+    if not args.no_noisy and world == 1:
+        result["secondary"]["noisy_ladder_n22_c128"] = noisy_mc(dev)
+        log(f"noisy: {result['secondary']['noisy_ladder_n22_c128']}")
     if not args.no_precision and world == 1:
         result["secondary"]["precision"] = precision_check(w, dev)
         log(f"precision: {result['secondary']['precision']}")
@@ -614,6 +617,113 @@ def grads_c5(dev) -> dict:
             "speedup_vs_per_instance": round((b.nsets / el) * el1, 1)}
 
 
+def noisy_mc(dev, steps: int = 20, cpu_seconds: float = 10.0) -> dict:
+    """The Monte Carlo path on noisy_ladder_n22 (N=22, complex128, relaxation + dephasing):
+    (1) Arnoldi steps alone at the workload's dt, with the device time split by kernel kind
+    and the bandwidth of the orthogonalisation passes; (2) whole EvolveMonteCarlo steps
+    (Brent bracketing and quantum jumps included) from |g...g> with seeded draws; (3) the
+    oracle's Monte Carlo step on the host for a bounded sample."""
+    import random
+
+    import torch
+
+    from emulators_b200 import RydbergHamiltonian, _lib
+    from emulators_b200 import workloads as wl
+    from emulators_b200.krylov import HamiltonianExpOperator, fused_arnoldi_step
+    from emulators_b200.time_evolution import EvolveMonteCarlo
+    from oracle import oracle
+
+    w, ops = wl.noisy_ladder_n22()
+    n, D, es = w.nqubits, 1 << w.nqubits, 16
+    noise = -0.5j * sum(L.conj().T @ L for L in ops)
+    U = torch.as_tensor(w.U)
+
+    def ham(k):
+        return RydbergHamiltonian(torch.as_tensor(w.omega[k]), torch.as_tensor(w.delta[k]),
+                                  torch.as_tensor(w.phi[k]), U, dev, noise=torch.as_tensor(noise))
+
+    L = _lib.load()
+    s = torch.zeros(D, dtype=torch.complex128, device=dev)
+    s[0] = 1.0
+    for k in range(3):  # warm-up
+        s, info, _ = fused_arnoldi_step(HamiltonianExpOperator(ham(k), w.dt), s, 1e-10, 1e-10, 100)
+    torch.cuda.synchronize()
+    L.emusv_profile_begin(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    its, r2 = [], 0
+    for k in range(3, 3 + steps):
+        s, info, st = fused_arnoldi_step(HamiltonianExpOperator(ham(k), w.dt), s, 1e-10, 1e-10, 100)
+        _lib.check(st, "arnoldi")
+        its.append(info.iterations)
+        r2 += info.second_rounds
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    pms = np.zeros(8)
+    pl = np.zeros(8, dtype=np.int64)
+    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
+    # algorithmic bytes of the Gram-Schmidt passes of iteration j (every vector once per
+    # pass): dots (j+2) reads, update (j+2) reads + 1 write; a second round adds the
+    # re-read of v_0..v_j in the update pass (j+1) and the second update (j+2) reads + 1
+    # write, i.e. 2j+4 units, taken at the mean j of the steps
+    first = sum(sum(2 * (j + 2) + 1 for j in range(m)) for m in its)
+    jm = float(np.mean([(m - 1) / 2 for m in its]))
+    second = r2 * (2 * jm + 4)
+    ortho_bytes = (first + second) * D * es
+    hbm, which = peaks()
+    kinds = ["hpsi_pass_low", "orth", "small", "combine", "obs", "adjoint", "batch", "hpsi_pass_high"]
+    tot = pms.sum()
+    ortho_gbs = ortho_bytes / (pms[1] / 1e3) / 1e9
+    # whole Monte Carlo steps
+    random.seed(0)
+    mc = EvolveMonteCarlo(100)
+    st_ = torch.zeros(D, dtype=torch.complex128, device=dev)
+    st_[0] = 1.0
+    thr0 = mc.jump_threshold
+    jumps = 0
+    torch.cuda.synchronize()
+    e0.record()
+    for k in range(steps):
+        before = mc.jump_threshold
+        st_, _ = mc.apply(w.dt, torch.as_tensor(w.omega[k]), torch.as_tensor(w.delta[k]),
+                          torch.as_tensor(w.phi[k]), U, st_, 1e-10, [torch.as_tensor(o) for o in ops])
+        jumps += int(mc.jump_threshold != before)
+    e1.record()
+    torch.cuda.synchronize()
+    el_mc = e0.elapsed_time(e1) / 1e3
+    # the oracle's Monte Carlo step on the host, bounded sample
+    rnd = random.Random(0)
+    thr = rnd.uniform(0.0, 1.0)
+    cs = np.zeros(D, dtype=np.complex128)
+    cs[0] = 1.0
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps and (done == 0 or time.perf_counter() - t0 < cpu_seconds):
+        cs, thr, _ = oracle.monte_carlo_step(rnd, thr, w.dt, w.omega[done], w.delta[done], w.phi[done],
+                                             w.U, cs, ops, 1e-10)
+        done += 1
+    cpu_el = time.perf_counter() - t0
+    return {"workload": "noisy_ladder_n22: N=22 2x11 ladder 5.5um, relaxation 0.5/us + "
+                        "dephasing 1/us, dt=10ns, complex128",
+            "arnoldi_steps_per_s": round(steps / el, 2),
+            "arnoldi_iterations_mean": round(float(np.mean(its)), 2),
+            "kernel_time_shares": {kinds[i]: round(pms[i] / tot, 4) for i in range(8) if pl[i]},
+            "gram_schmidt": {"algorithmic_bytes_per_step": int(ortho_bytes / steps),
+                             "GB/s": round(ortho_gbs, 1), "frac": round(ortho_gbs / hbm, 4),
+                             "second_rounds_per_step": round(r2 / steps, 2),
+                             "note": "two streaming passes per iteration over w and v_0..v_j, "
+                                     "two more in iterations that take a second round"},
+            "monte_carlo_steps_per_s": round(steps / el_mc, 2),
+            "monte_carlo_jumps": jumps,
+            "monte_carlo_first_threshold": round(thr0, 6),
+            "cpu_baseline": {"value": round(done / cpu_el, 4), "unit": "steps/s",
+                             "cores": oracle.num_threads(), "kind": "port",
+                             "sample": f"first {done} Monte Carlo step(s) of the workload in "
+                                       f"complex128 on the host ({cpu_el:.1f} s)"},
+            "speedup_vs_cpu": round((steps / el_mc) / (done / cpu_el), 1)}
+
+
 # ------------------------------------------------------------------ CPU baseline (oracle)
 def cpu_baseline(w, budget_s: float) -> dict:
     """The oracle (C/OpenMP restatement of the reference path, FP64/complex128) timed on
@@ -677,6 +787,8 @@ def main():
                     help="skip the plain complex128 torch GPU path")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched evolution and batched gradient workloads")
+    ap.add_argument("--no-noisy", action="store_true",
+                    help="skip the Monte Carlo (noisy Hamiltonian, Arnoldi) workload")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the complex64-vs-complex128 run of the whole workload")
     args = ap.parse_args()

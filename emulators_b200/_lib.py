@@ -30,7 +30,7 @@ class KrylovInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("happy_breakdown", ctypes.c_int),
                 ("converged", ctypes.c_int), ("basis_vectors", ctypes.c_int),
                 ("error_estimate", ctypes.c_double), ("input_norm", ctypes.c_double),
-                ("output_norm", ctypes.c_double)]
+                ("output_norm", ctypes.c_double), ("second_rounds", ctypes.c_int)]
 
 
 SIGNATURES: dict[str, tuple] = {

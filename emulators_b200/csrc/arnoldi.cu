@@ -4,19 +4,24 @@
 // krylov_exp.py:23-106 with is_hermitian=False).
 //
 // Per iteration j (basis vectors stored unnormalised with FP64 scales, as in krylov.cu):
-//   1. w = H v_j by the streaming H*psi kernels (noise diagonal fused into pass L);
+//   1. w = (H - sigma) v_j by the streaming H*psi kernels (noise diagonal fused into pass
+//      L; sigma = the previous step's energy, as in the Lanczos step: same basis, T minus
+//      sigma on its diagonal, added back in every exponential);
 //   2. k_arn_ortho<DOTS>:    h_k = <v_k, w> for all k <= j and ||w|| in one pass;
-//   3. k_arn_ortho<UPDATE_DOTS>: w' = w - sum h_k v_k, g_k = <v_k, w'>, in one pass;
-//   4. k_arn_ortho<UPDATE>:  w'' = w' - sum g_k v_k and ||w''||.
-//   Classical Gram-Schmidt applied twice: the same Hessenberg column T[k][j] = h_k + g_k
-//   and vector as the reference's modified Gram-Schmidt (krylov_exp.py:54-58) in exact
-//   arithmetic, in three streaming passes instead of 2(j+1) dependent dot/axpy pairs.
+//   3. k_arn_ortho<UPDATE_DOTS>: w' = w - sum h_k v_k (and, for a second round, the dots
+//      g_k = <v_k, w'>) in one pass;
+//   4. k_arn_ortho<UPDATE>:  w'' = w' - sum g_k v_k and ||w''|| (second round only).
+//   Classical Gram-Schmidt, repeated when the first round removed more than half of
+//   ||w||^2 (the DGKS test): the same Hessenberg column T[k][j] = h_k (+ g_k) and vector as
+//   the reference's modified Gram-Schmidt (krylov_exp.py:54-58) in exact arithmetic, in two
+//   or three streaming passes instead of 2(j+1) dependent dot/axpy pairs.  The shift keeps
+//   ||(H - sigma) v_j|| near the spread of the spectrum, so the second round is rare.
 //   5. k_arn_decide (one CTA, FP64): ||w''||, the happy-breakdown test (krylov_exp.py:
 //   63-71) at every iteration, and from the host's hint on the exponential of the extended
 //   Hessenberg matrix and the Expokit error estimate (krylov_exp.py:76-86); when the first
 //   tested iteration already converges, the untested earlier ones are tested in order.
 // The small exponentials: exp(A) e_0 of the dense extended Hessenberg matrix by s
-// substeps of a 26-term Taylor series with ||A/s||_1 <= 2 (truncation below 1e-17 per
+// substeps of a 34-term Taylor series with ||A/s||_1 <= 4 (truncation below 1e-19 per
 // substep), matrix-vector products split over 2-8 threads per row.
 #include <string.h>
 
@@ -37,10 +42,14 @@ constexpr int ORTHO_THREADS = 256;
 constexpr int DECIDE_THREADS = 256;
 
 struct ArnState {
-    double2 T[ARN_M * ARN_M];  // Hessenberg matrix of H (row-major [r][c]) in the basis v_k
+    double2 T[ARN_M * ARN_M];  // Hessenberg matrix of H - sigma (row-major [r][c]), basis v_k
     double2 coef[ARN_M];       // coefficients of the next Gram-Schmidt update
+    int reorth;                // this iteration takes the second Gram-Schmidt round
+    int rounds2;               // second rounds taken in this run
 };
 
+// Pass A: dots.  Pass B: update with h; with reorth also the dots of the result.  Pass C:
+// update with the second round's coefficients (returns at once without reorth).
 enum ArnMode { ARN_DOTS = 0, ARN_UPDATE_DOTS = 1, ARN_UPDATE = 2 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -49,13 +58,17 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 
 // One streaming pass over w and v_0..v_j (see the header).  Partials per block:
 // [2k], [2k+1] = <v_k, w_out> (DOTS, UPDATE_DOTS), [ARN_NORM] = ||w_out||^2.
-template <typename R, int MODE>
+// E amplitudes per thread per chunk.  UPDATE_DOTS reads every v_k twice per chunk (the
+// update needs all of them before the dots of the result).
+template <typename R, int MODE, int E>
 __global__ void __launch_bounds__(ORTHO_THREADS)
 k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const unsigned char *basis,
             i64 D, void *w_, double *part) {
     typedef typename cvec<R>::T C;
     if (ks->status != KS_RUNNING) return;
-    constexpr int E = 8;  // amplitudes per thread per chunk
+    const bool reorth = as->reorth != 0;
+    if (MODE == ARN_UPDATE && !reorth) return;
+    const bool dots = MODE == ARN_DOTS || (MODE == ARN_UPDATE_DOTS && reorth);
     constexpr int NW = ORTHO_THREADS / 32;
     __shared__ double2 cf[ARN_M];
     __shared__ double sc[ARN_M];
@@ -116,7 +129,7 @@ k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const 
         }
 #pragma unroll
         for (int e = 0; e < E; ++e) nacc += wr[e] * wr[e] + wi[e] * wi[e];
-        if (MODE != ARN_UPDATE) {
+        if (dots) {
             for (int k = 0; k < nk; ++k) {
                 const C *v = vk(k);
                 double dr = 0.0, di = 0.0;  // sum conj(v) w
@@ -142,7 +155,7 @@ k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const 
     if (lane == 0) snorm[warp] = nacc;
     __syncthreads();
     double *row = part + (i64)blockIdx.x * ARN_PS;
-    if (MODE != ARN_UPDATE) {
+    if (dots) {
         for (int k = tid; k < nk; k += ORTHO_THREADS) {
             double2 t = make_double2(0.0, 0.0);
             for (int q = 0; q < NW; ++q) {
@@ -160,11 +173,12 @@ k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const 
     }
 }
 
-// Sums of the ortho partials over nb blocks (fixed order), value i of a row.
-__device__ __forceinline__ double arn_sum(const double *part, int nb, int i) {
+// Sum of value i of the ortho partial rows over nb blocks by one warp (lanes stride over
+// the blocks, then a fixed shuffle tree: deterministic).  Result in every lane.
+__device__ __forceinline__ double arn_sum_warp(const double *part, int nb, int i) {
     double t = 0.0;
-    for (int b = 0; b < nb; ++b) t += part[(i64)b * ARN_PS + i];
-    return t;
+    for (int b = threadIdx.x & 31; b < nb; b += 32) t += part[(i64)b * ARN_PS + i];
+    return warp_sum(t);
 }
 
 // After the DOTS (stage 0) or UPDATE_DOTS (stage 1) pass: column j of T and the next
@@ -172,20 +186,41 @@ __device__ __forceinline__ double arn_sum(const double *part, int nb, int i) {
 __global__ void __launch_bounds__(DECIDE_THREADS)
 k_arn_stage(KState *ks, ArnState *as, int j, const double *part, int nb, int stage) {
     if (ks->status != KS_RUNNING) return;
+    if (stage == 1 && !as->reorth) return;
     __shared__ int bad;
+    __shared__ double hsq[DECIDE_THREADS / 32];
     if (threadIdx.x == 0) bad = 0;
+    if (threadIdx.x < DECIDE_THREADS / 32) hsq[threadIdx.x] = 0.0;
     __syncthreads();
-    for (int k = threadIdx.x; k <= j; k += DECIDE_THREADS) {
-        const double2 h = make_double2(arn_sum(part, nb, 2 * k), arn_sum(part, nb, 2 * k + 1));
-        if (!isfinite(h.x) || !isfinite(h.y)) bad = 1;
-        double2 &t = as->T[k * ARN_M + j];
-        t = stage == 0 ? h : make_double2(t.x + h.x, t.y + h.y);
-        as->coef[k] = h;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NWD = DECIDE_THREADS / 32;
+    for (int k = warp; k <= j; k += NWD) {  // one warp per column entry
+        const double2 h = make_double2(arn_sum_warp(part, nb, 2 * k), arn_sum_warp(part, nb, 2 * k + 1));
+        if (lane == 0) {
+            if (!isfinite(h.x) || !isfinite(h.y)) bad = 1;
+            double2 &t = as->T[k * ARN_M + j];
+            t = stage == 0 ? h : make_double2(t.x + h.x, t.y + h.y);
+            as->coef[k] = h;
+            hsq[warp] += h.x * h.x + h.y * h.y;
+            if (stage == 0 && k == j) ks->a_re[j] = h.x;  // Re <v_j, (H - sigma) v_j>
+        }
     }
-    if (stage == 0 && threadIdx.x == 0) {
-        const double n2 = arn_sum(part, nb, ARN_NORM);
-        ks->hn[j] = sqrt(n2);
-        if (!isfinite(n2)) bad = 1;
+    __syncthreads();
+    if (stage == 0 && warp == 0) {
+        const double n2 = arn_sum_warp(part, nb, ARN_NORM);  // ||(H - sigma) v_j||^2
+        if (lane == 0) {
+            double hs = 0.0;
+            for (int q = 0; q < DECIDE_THREADS / 32; ++q) hs += hsq[q];
+            // ||H v_j|| (krylov_exp.py:52) from the shifted product
+            const double sg = ks->shift;
+            ks->hn[j] = sqrt(fmax(0.0, n2 + 2.0 * sg * ks->a_re[j] + sg * sg));
+            // second round unless the projection kept more than half of ||w||^2 (Daniel,
+            // Gragg, Kaufman and Stewart's test with eta = 1/sqrt(2)); ||w'||^2 is taken as
+            // ||w||^2 - sum |h_k|^2, the exact value for an orthonormal basis
+            as->reorth = !(n2 - hs > 0.5 * n2);
+            as->rounds2 = (j == 0 ? 0 : as->rounds2) + as->reorth;
+            if (!isfinite(n2)) bad = 1;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0 && bad) {
@@ -195,8 +230,10 @@ k_arn_stage(KState *ks, ArnState *as, int j, const double *part, int nb, int sta
 }
 
 // y = exp(A) e_0 for the M x M matrix A in shared memory (column-major A[c*M + r]).
-// s substeps of sum_{k<=26} (A/s)^k / k! with ||A/s||_1 <= 2.  Returns false when the
-// norm is not finite or would need more than 2^20 substeps.  All threads of the block.
+// s substeps of sum_{k<=34} (A/s)^k / k! with ||A/s||_1 <= 4: truncation below
+// 4^35/35! ~ 1e-19 relative per substep, terms at most 4^4/4! ~ 11 times the result (about
+// one digit of cancellation).  Returns false when the norm is not finite or would need
+// more than 2^20 substeps.  All threads of the block.
 __device__ bool arn_expm_col0(const double2 *A, int M, double2 *y, double2 *t, double2 *tn,
                               double *red) {
     const int tid = threadIdx.x;
@@ -212,8 +249,8 @@ __device__ bool arn_expm_col0(const double2 *A, int M, double2 *y, double2 *t, d
     }
     const double nrm = red[0];
     __syncthreads();
-    if (!isfinite(nrm) || nrm > 2.0 * 1048576.0) return false;
-    const int s = nrm > 2.0 ? (int)ceil(nrm / 2.0) : 1;
+    if (!isfinite(nrm) || nrm > 4.0 * 1048576.0) return false;
+    const int s = nrm > 4.0 ? (int)ceil(nrm / 4.0) : 1;
     const int TPR = M <= 32 ? 8 : (M <= 64 ? 4 : 2);
     const int r = tid / TPR, q = tid % TPR;
     if (tid < M) y[tid] = make_double2(tid == 0 ? 1.0 : 0.0, 0.0);
@@ -221,7 +258,7 @@ __device__ bool arn_expm_col0(const double2 *A, int M, double2 *y, double2 *t, d
     for (int step = 0; step < s; ++step) {
         if (tid < M) t[tid] = y[tid];
         __syncthreads();
-        for (int k = 1; k <= 26; ++k) {
+        for (int k = 1; k <= 34; ++k) {
             double2 acc = make_double2(0.0, 0.0);
             if (r < M) {
                 for (int c = q; c < M; c += TPR) {
@@ -250,13 +287,15 @@ __device__ bool arn_expm_col0(const double2 *A, int M, double2 *y, double2 *t, d
 
 // Extended matrix of iteration jj (krylov_exp.py:77-78) in my basis: A = -i dt T[:jj+2,
 // :jj+1] plus A[jj+2][jj+1] = 1 (M = jj + 3); happy: A = -i dt T[:jj+1, :jj+1] (M = jj + 1).
-__device__ void arn_build(const ArnState *as, int jj, double dt, bool happy, double2 *A, int *Mo) {
+__device__ void arn_build(const ArnState *as, int jj, double dt, double sigma, bool happy, double2 *A,
+                          int *Mo) {
     const int M = happy ? jj + 1 : jj + 3;
     for (int i = threadIdx.x; i < M * M; i += DECIDE_THREADS) {
         const int c = i / M, r = i % M;
         double2 v = make_double2(0.0, 0.0);
         if (c <= jj && r <= c + 1 && r <= (happy ? jj : jj + 1)) {  // Hessenberg entries
-            const double2 h = as->T[r * ARN_M + c];
+            double2 h = as->T[r * ARN_M + c];
+            if (r == c) h.x += sigma;  // T of H itself
             v = make_double2(dt * h.y, -dt * h.x);  // -i dt h
         }
         if (!happy && c == jj + 1 && r == jj + 2) v = make_double2(1.0, 0.0);
@@ -272,7 +311,7 @@ __device__ void arn_build(const ArnState *as, int jj, double dt, bool happy, dou
 __device__ double arn_eval(KState *ks, const ArnState *as, int jj, double dt, double2 *A, double2 *y,
                            double2 *t, double2 *tn, double *red, bool *fail) {
     int M;
-    arn_build(as, jj, dt, false, A, &M);
+    arn_build(as, jj, dt, ks->shift, false, A, &M);
     if (!arn_expm_col0(A, M, y, t, tn, red)) {
         *fail = true;
         return nan("");
@@ -306,8 +345,13 @@ k_arn_decide(KState *ks, ArnState *as, int j, const double *part, int nb, double
         }
         return;
     }
-    const double n2 = arn_sum(part, nb, ARN_NORM);
-    const double r = sqrt(n2);
+    __shared__ double n2s;
+    if (tid < 32) {
+        const double v = arn_sum_warp(part, nb, ARN_NORM);
+        if (tid == 0) n2s = v;
+    }
+    __syncthreads();
+    const double r = sqrt(n2s);
     if (!isfinite(r)) {
         if (tid == 0) {
             ks->status = KS_NONFINITE;
@@ -323,7 +367,7 @@ k_arn_decide(KState *ks, ArnState *as, int j, const double *part, int nb, double
     __syncthreads();
     if (fabs(dt) * r < norm_tol) {  // happy breakdown (krylov_exp.py:63-71)
         int M;
-        arn_build(as, j, dt, true, A, &M);
+        arn_build(as, j, dt, ks->shift, true, A, &M);
         const bool ok = arn_expm_col0(A, M, y, t, tn, red);
         for (int k = tid; k < M; k += DECIDE_THREADS) {
             ks->c_re[k] = y[k].x;
@@ -380,17 +424,29 @@ static size_t decide_smem(int maxdim) {
     return sizeof(double2) * (M * M + 3 * M) + sizeof(double) * DECIDE_THREADS;
 }
 
+// Grid of the ortho passes: the streaming grid of the vector kernels (up to four blocks per
+// SM), never more blocks than chunks; *grid_out receives it (the number of partial rows).
+// Measured on B200 (N=22, complex128, j ~ 35): one block per SM with chunks small enough
+// for the update-and-dots pass to find its second reads in L2 was 1.5x slower than the
+// wide grid that re-reads them from HBM.
 template <typename R>
 static int launch_ortho(int mode, const KState *ks, const ArnState *as, int j, const void *v0,
-                        const unsigned char *basis, i64 D, void *w, double *part, int grid,
-                        cudaStream_t s) {
+                        const unsigned char *basis, i64 D, void *w, double *part, cudaStream_t s,
+                        int *grid_out) {
+    constexpr int E = 8;
+    i64 grid = krylov_stream_grid(D);
+    const i64 chunks = (D + (i64)ORTHO_THREADS * E - 1) / ((i64)ORTHO_THREADS * E);
+    if (grid > chunks) grid = chunks;
+    *grid_out = (int)grid;
     ProfScope ps_(PROF_ORTH, s);
+#define ARN_LAUNCH(M) k_arn_ortho<R, M, E><<<(int)grid, ORTHO_THREADS, 0, s>>>(ks, as, j, v0, basis, D, w, part)
     if (mode == ARN_DOTS)
-        k_arn_ortho<R, ARN_DOTS><<<grid, ORTHO_THREADS, 0, s>>>(ks, as, j, v0, basis, D, w, part);
-    else if (mode == ARN_UPDATE_DOTS)
-        k_arn_ortho<R, ARN_UPDATE_DOTS><<<grid, ORTHO_THREADS, 0, s>>>(ks, as, j, v0, basis, D, w, part);
+        ARN_LAUNCH(ARN_DOTS);
+    else if (mode == ARN_UPDATE)
+        ARN_LAUNCH(ARN_UPDATE);
     else
-        k_arn_ortho<R, ARN_UPDATE><<<grid, ORTHO_THREADS, 0, s>>>(ks, as, j, v0, basis, D, w, part);
+        ARN_LAUNCH(ARN_UPDATE_DOTS);
+#undef ARN_LAUNCH
     EMUSV_CHECK_LAUNCH();
     return EMUSV_OK;
 }
@@ -441,10 +497,9 @@ int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, 
     auto stored = [&](int k) -> const void * {
         return k == 0 ? psi_in : (const void *)(basis + (size_t)k * D * es);
     };
-    const int sg = krylov_stream_grid(D);
     const size_t dsmem = decide_smem(max_krylov_dim);
     EMUSV_CHECK(cudaFuncSetAttribute(k_arn_decide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
-    int st = krylov_begin(dtype, psi_in, D, ks, part_n, s);
+    int st = krylov_begin(dtype, psi_in, D, ks, part_n, true, s);
     if (st) return st;
 
     int status = KS_RUNNING;
@@ -464,22 +519,24 @@ int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, 
         A.gate = &ks->status;
         A.err = &ks->kerr;
         A.part_buf = basis;
+        A.eshift = &ks->shift;
         if ((st = launch_hpsi(dtype, HP_STORE, P, A, 0, s, nullptr))) return st;
+        int og = 0;
         for (int mode = ARN_DOTS; mode <= ARN_UPDATE; ++mode) {
             st = dtype == EMUSV_C128
-                     ? launch_ortho<double>(mode, ks, as, j, psi_in, basis, D, w, part, sg, s)
-                     : launch_ortho<float>(mode, ks, as, j, psi_in, basis, D, w, part, sg, s);
+                     ? launch_ortho<double>(mode, ks, as, j, psi_in, basis, D, w, part, s, &og)
+                     : launch_ortho<float>(mode, ks, as, j, psi_in, basis, D, w, part, s, &og);
             if (st) return st;
             if (mode != ARN_UPDATE) {
                 ProfScope ps_(PROF_SMALL, s);
-                k_arn_stage<<<1, DECIDE_THREADS, 0, s>>>(ks, as, j, part, sg, mode);
+                k_arn_stage<<<1, DECIDE_THREADS, 0, s>>>(ks, as, j, part, og, mode);
                 EMUSV_CHECK_LAUNCH();
             }
         }
         const bool poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
         {
             ProfScope ps_(PROF_SMALL, s);
-            k_arn_decide<<<1, DECIDE_THREADS, dsmem, s>>>(ks, as, j, part, sg, dt, exp_tolerance,
+            k_arn_decide<<<1, DECIDE_THREADS, dsmem, s>>>(ks, as, j, part, og, dt, exp_tolerance,
                                                           norm_tolerance, poll ? 1 : 0,
                                                           (poll && !polled) ? 1 : 0, max_krylov_dim);
             EMUSV_CHECK_LAUNCH();
@@ -503,7 +560,9 @@ int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, 
     if ((st = krylov_combine(dtype, ks, psi_in, basis, D, psi_out, part_n, s))) return st;
     if (info) {
         KState h;
+        int r2 = 0;
         EMUSV_CHECK(cudaMemcpyAsync(&h, ks, offsetof(KState, a_re), cudaMemcpyDeviceToHost, s));
+        EMUSV_CHECK(cudaMemcpyAsync(&r2, &as->rounds2, sizeof(int), cudaMemcpyDeviceToHost, s));
         EMUSV_CHECK(cudaStreamSynchronize(s));
         info->iterations = h.iters;
         info->happy_breakdown = h.status == KS_HAPPY;
@@ -512,6 +571,7 @@ int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, 
         info->error_estimate = h.err;
         info->input_norm = h.s0;
         info->output_norm = sqrt(h.outnorm2);
+        info->second_rounds = r2;
     }
     return status == KS_MAXDIM ? EMUSV_NOT_CONVERGED : EMUSV_OK;
 }

@@ -38,7 +38,7 @@ struct HpsiArgs {
     const int *gate;   // if non-null and *gate != 0 the kernel returns at once
     void *part_buf;    // two-pass H*psi: buffer for the partial sums of pass L
     int *err;          // device word receiving EMUSV_TIMEOUT if a bounded wait gives up
-    const double *eshift;  // HP_LANCZOS: if non-null, the diagonal is taken minus *eshift
+    const double *eshift;  // HP_LANCZOS, HP_STORE: if non-null, the diagonal is taken minus *eshift
 };
 
 struct SmemLayout {
@@ -159,7 +159,7 @@ k_hpsi(const HamParams P, HpsiArgs A) {
             }
         }
         __syncthreads();
-        const double ehigh = gv[MAXQ] - (MODE == HP_LANCZOS && A.eshift ? *A.eshift : 0.0) +
+        const double ehigh = gv[MAXQ] - ((MODE == HP_LANCZOS || MODE == HP_STORE) && A.eshift ? *A.eshift : 0.0) +
                              (MODE == HP_DIAG ? 0.0 : P.dc_re);
 
         for (int k = tid; k < TILE; k += BLOCK) {

@@ -195,7 +195,7 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     A.partials = HA.partials;
     A.gate = HA.gate;
     A.err = HA.err;
-    A.eshift = EPI_F == EPI_LANCZOS ? HA.eshift : nullptr;
+    A.eshift = HA.eshift;  // null unless the caller shifts the diagonal
     int st;
     if (rem == 0) {
         A.out = HA.out;

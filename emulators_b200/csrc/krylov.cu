@@ -373,8 +373,9 @@ namespace {
 thread_local int *pinned_status = nullptr;
 }  // namespace
 
-// Input norm and KState reset (no energy shift), as the start of lanczos_run.
-int krylov_begin(int dtype, const void *psi_in, i64 D, KState *ks, double *partials, cudaStream_t s) {
+// Input norm and KState reset, as the start of lanczos_run (k_init).
+int krylov_begin(int dtype, const void *psi_in, i64 D, KState *ks, double *partials, bool energy_shift,
+                 cudaStream_t s) {
     const int sg = stream_grid(D);
     {
         ProfScope ps_(PROF_ORTH, s);
@@ -384,7 +385,7 @@ int krylov_begin(int dtype, const void *psi_in, i64 D, KState *ks, double *parti
     EMUSV_CHECK_LAUNCH();
     {
         ProfScope ps_(PROF_SMALL, s);
-        k_init<<<1, BLOCK, 0, s>>>(ks, partials, sg, 0);
+        k_init<<<1, BLOCK, 0, s>>>(ks, partials, sg, energy_shift ? 1 : 0);
     }
     EMUSV_CHECK_LAUNCH();
     return EMUSV_OK;
@@ -598,6 +599,7 @@ int emusv_krylov_step(int nqubits, int dtype, double dt, const double *omegas,
         info->error_estimate = h.err;
         info->input_norm = h.s0;
         info->output_norm = sqrt(h.outnorm2);
+        info->second_rounds = 0;
     }
     return status == KS_MAXDIM ? EMUSV_NOT_CONVERGED : EMUSV_OK;
 }

@@ -38,8 +38,10 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
                 double exp_tol, double norm_tol, int maxdim, int hint, bool energy_shift,
                 cudaStream_t s, int *status_out);
 int read_status(KState *ks, cudaStream_t s, int *out);
-// Input norm and KState reset (no energy shift): k_norm2 + k_init.
-int krylov_begin(int dtype, const void *psi_in, i64 D, KState *ks, double *partials, cudaStream_t s);
+// Input norm and KState reset (k_norm2 + k_init); with energy_shift, sigma = the previous
+// finished run's sigma + a_re[0] (the workspace must be zeroed before its first run).
+int krylov_begin(int dtype, const void *psi_in, i64 D, KState *ks, double *partials, bool energy_shift,
+                 cudaStream_t s);
 // out = s0 sum_k c_k scale_k stored_k (ks->nvec vectors; stored_0 = psi_in, stored_k at
 // basis + k*D), and ks->outnorm2.
 int krylov_combine(int dtype, KState *ks, const void *psi_in, const unsigned char *basis, i64 D,

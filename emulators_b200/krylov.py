@@ -148,7 +148,8 @@ def fused_arnoldi_step(op: HamiltonianExpOperator, v: torch.Tensor, exp_toleranc
         need = L.emusv_arnoldi_workspace_bytes(n, code, c.capacity)
         if c.buf is None or c.buf.numel() < need:
             c.buf = None
-            c.buf = torch.empty(need, dtype=torch.uint8, device=v.device)
+            # zeroed once: the state block carries the energy shift between steps
+            c.buf = torch.zeros(need, dtype=torch.uint8, device=v.device)
         st = L.emusv_arnoldi_step(n, code, op.dt, *op.ham._params(), noise, v.data_ptr(),
                                   out.data_ptr(), float(exp_tolerance), float(norm_tolerance),
                                   int(max_krylov_dim), hint, c.buf.data_ptr(), c.buf.numel(), info,

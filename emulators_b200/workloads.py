@@ -21,6 +21,10 @@ Workloads (all sizes are the ones the benchmarks and parity tests use):
                      rejection-sampled to a 5 um minimum distance, 10-segment
                      piecewise-linear Omega in [0, 2 pi] and delta in [-20, 20], phi=0,
                      1.5 us at dt=10 ns (150 steps).
+* ``noisy_ladder_n22`` N=22 2x11 ladder, 5.5 um spacing, the ladder_n26 pulse shapes over
+                     0.5 us at dt=10 ns (50 steps), Lindblad operators: relaxation
+                     (rate 0.5/us, sqrt(rate)|g><r|) and dephasing (rate 1/us,
+                     sqrt(rate/2) Z), complex128; the Monte Carlo stepper's workload.
 * ``ring_n16_grad``  N=16 ring of radius 10 um, 20-segment piecewise-constant Omega in
                      [0, 2 pi] and delta in [-20, 20], 64 parameter sets, 2 us at
                      dt=10 ns (200 steps, 10 steps per segment), loss = MSE between the
@@ -143,6 +147,22 @@ def ladder_n26(nsteps: int | None = None) -> Workload:
     return Workload("ladder_n26", pos, interaction_matrix(pos), dt,
                     _global(np.full_like(t, 4.0), n), _global(-10.0 + 20.0 * t / T, n),
                     np.zeros((len(t), n)), tolerance=1e-10, precision="c64", obs_every=100)
+
+
+def noisy_ladder_n22(nsteps: int | None = None):
+    """(Workload, Lindblad operators as 2x2 complex arrays)."""
+    n, T, dt = 22, 0.5, 0.01
+    pos = ladder(11, 5.5)
+    t = midpoints(T, dt)
+    if nsteps is not None:
+        t = t[:nsteps]
+    w = Workload("noisy_ladder_n22", pos, interaction_matrix(pos), dt,
+                 _global(np.full_like(t, 4.0), n), _global(-10.0 + 20.0 * t / T, n),
+                 np.zeros((len(t), n)), tolerance=1e-10, precision="c128")
+    relax = np.array([[0.0, np.sqrt(0.5)], [0.0, 0.0]], dtype=np.complex128)
+    c = np.sqrt(1.0 / 2)
+    deph = np.array([[c, 0.0], [0.0, -c]], dtype=np.complex128)
+    return w, [relax, deph]
 
 
 def piecewise_linear(knots_t: np.ndarray, knots_v: np.ndarray, t: np.ndarray) -> np.ndarray:
