@@ -312,6 +312,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     if not args.no_noisy and world == 1:
         result["secondary"]["noisy_ladder_n22_c128"] = noisy_mc(dev)
         log(f"noisy: {result['secondary']['noisy_ladder_n22_c128']}")
+    if not args.no_noisy and world == 1:
+        result["secondary"]["drive_preparation_pchip"] = drive_prep(dev)
+        log(f"drive preparation: {result['secondary']['drive_preparation_pchip']}")
     if not args.no_precision and world == 1:
         result["secondary"]["precision"] = precision_check(w, dev)
         log(f"precision: {result['secondary']['precision']}")
@@ -722,6 +725,70 @@ def noisy_mc(dev, steps: int = 20, cpu_seconds: float = 10.0) -> dict:
                              "sample": f"first {done} Monte Carlo step(s) of the workload in "
                                        f"complex128 on the host ({cpu_el:.1f} s)"},
             "speedup_vs_cpu": round((steps / el_mc) / (done / cpu_el), 1)}
+
+
+def drive_prep(dev, regs: int = 256, qubits: int = 16, T: int = 4000, dt_ns: int = 10,
+               cpu_seconds: float = 10.0) -> dict:
+    """Drive preparation for a long batched sequence set: amplitude, detuning and phase
+    samples of `regs` registers x `qubits` qubits on pulser's 1 ns grid (T knots each),
+    PCHIP-interpolated at the midpoints of a dt_ns grid in one launch; next to the oracle's
+    numpy PCHIP per signal (the reference loops over qubits and parameters) on the host."""
+    import torch
+
+    from emulators_b200.pchip import PCHIP1D
+    from oracle import oracle
+
+    rng = np.random.default_rng(11)
+    S = 3 * regs * qubits
+    t = np.arange(T, dtype=np.float64)
+    base = np.sin(np.outer(rng.uniform(0.5, 3.0, S), t) / T) * rng.uniform(0, 10, (S, 1))
+    y_host = torch.from_numpy(base).pin_memory()
+    tt = np.arange(0, T + 1, dt_ns, dtype=np.float64)
+    tm = 0.5 * (tt[:-1] + tt[1:])
+    xg = torch.as_tensor(t, device=dev)
+    xq = torch.as_tensor(tm, device=dev)
+    y = y_host.to(dev)
+    f = PCHIP1D(xg, y)
+    for _ in range(3):
+        f(xq)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reps = 20
+    for _ in range(reps):
+        out = f(xq)
+    e1.record()
+    torch.cuda.synchronize()
+    k_ms = e0.elapsed_time(e1) / reps
+    # end to end: host samples in, host midpoint samples out
+    out_host = torch.empty(S, len(tm), dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(5):
+        yd = y_host.to(dev, non_blocking=True)
+        o = PCHIP1D(xg, yd)(xq)
+        out_host.copy_(o, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / 5
+    # host: the oracle's PCHIP per signal, bounded sample
+    t0 = time.perf_counter()
+    done = 0
+    while done < S and (done == 0 or time.perf_counter() - t0 < cpu_seconds):
+        oracle.pchip(t, base[done], tm)
+        done += 1
+    cpu_s = (time.perf_counter() - t0) / done
+    ok = bool(np.array_equal(out[:64].cpu().numpy(),
+                             np.stack([oracle.pchip(t, base[i], tm) for i in range(64)])))
+    return {"workload": f"{regs} registers x {qubits} qubits x 3 parameters = {S} signals, "
+                        f"{T} knots (1 ns grid), {len(tm)} midpoints ({dt_ns} ns steps)",
+            "kernel_ms": round(k_ms, 4), "signals_per_s": round(S / (k_ms / 1e3), 1),
+            "e2e_ms": round(e2e_ms, 3), "e2e_h2d_bytes": int(S * T * 8),
+            "e2e_d2h_bytes": int(S * len(tm) * 8),
+            "cpu_baseline": {"signals_per_s": round(1.0 / cpu_s, 1), "cores": 1, "kind": "port",
+                             "sample": f"first {done} signals, oracle numpy PCHIP"},
+            "speedup_e2e_vs_cpu": round((S / (e2e_ms / 1e3)) * cpu_s, 1),
+            "first_64_signals_bit_identical_to_oracle": ok}
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)

@@ -57,6 +57,7 @@ SIGNATURES: dict[str, tuple] = {
     "emusv_qubit_densities_scratch_bytes": (_SZ, [_I]),
     "emusv_qubit_densities": (_I, [_I, _I, _P, _P, _P, _SZ, _P]),
     "emusv_apply_1q": (_I, [_I, _I, _P, _I, _P, _P]),
+    "emusv_pchip_eval": (_I, [_I, _P, _I, _P, _I64, _I, _P, _P, _I64, _P]),
     "emusv_sample_scratch_bytes": (_SZ, [_I]),
     "emusv_sample": (_I, [_I, _I, _P, _I, _P, _P, _P, _SZ, _P]),
     "emusv_batch_max_qubits": (_I, []),

@@ -213,6 +213,17 @@ int emusv_qubit_densities(int nqubits, int dtype, const void *psi, double *rho_d
  * emu_sv/algebra.py:28-37 (apply). */
 int emusv_apply_1q(int nqubits, int dtype, void *psi, int qubit, const double *op, void *stream);
 
+/* Drive preparation: out[s * out_stride + q] = PCHIP interpolant of the knots
+ * (x[k], y[s * y_stride + k]), k < nknots, at xq[q], for every signal s < nsignals and
+ * query q < nqueries (device float64 arrays; x strictly increasing -- the caller checks,
+ * as PCHIP1D._validate_xy does).  Replaces PCHIP1D (emu_base/math/pchip_torch.py:218-269)
+ * as used per qubit and laser parameter by _extract_omega_delta_phi
+ * (emu_base/pulser_adapter.py:155-231): monotone cubic Hermite interpolation, boundary
+ * cubics extended outside [x[0], x[n-1]], every operation rounded as the reference
+ * rounds it.  No synchronisation. */
+int emusv_pchip_eval(int nknots, const double *x, int nsignals, const double *y, int64_t y_stride,
+                     int nqueries, const double *xq, double *out, int64_t out_stride, void *stream);
+
 /* ---- batched evolution: many registers in one persistent launch ----
  * Replaces running the reference's time loop (emu_sv/sv_backend_impl.py:197-209, one
  * krylov_exp per step, krylov_exp.py:23-131) once per register: every register of the

@@ -566,3 +566,41 @@ def monte_carlo_step(rnd, threshold, dt, omegas, deltas, phis, U, state, lindbla
         jumps += 1
         new = norm(state) ** 2 - threshold
     return state, threshold, jumps
+
+
+# ----------------------------------------------------------------------- PCHIP
+def pchip(x, y, xq) -> np.ndarray:
+    """PCHIP1D(x, y)(xq), restating emu_base/math/pchip_torch.py:97-269 in numpy (the same
+    operation order: secants, weighted harmonic interior slopes, limited one-sided end
+    slopes, Hermite coefficients, Horner)."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    xq = np.asarray(xq, dtype=np.float64)
+    n = x.size
+    h = x[1:] - x[:-1]
+    delta = (y[1:] - y[:-1]) / h
+    d = np.zeros(n)
+    if n == 2:
+        d[:] = delta[0]
+    else:
+        dl, dr, hl, hr = delta[:-1], delta[1:], h[:-1], h[1:]
+        wl, wr = hl + 2.0 * hr, 2.0 * hl + hr
+        with np.errstate(divide="ignore", invalid="ignore"):
+            dh = (wl + wr) / (wl / dl + wr / dr)
+        d[1:-1] = np.where(dl * dr > 0, dh, 0.0)
+
+        def end(a, b, ha, hb):
+            e = ((2.0 * ha + hb) * a - ha * b) / (ha + hb)
+            if e * a < 0:
+                e = 0.0
+            if a * b < 0 and abs(e) > 3.0 * abs(a):
+                e = 3.0 * a
+            return e
+
+        d[0] = end(delta[0], delta[1], h[0], h[1])
+        d[-1] = end(delta[-1], delta[-2], h[-1], h[-2])
+    p2 = (3.0 * delta - 2.0 * d[:-1] - d[1:]) / h
+    p3 = (d[:-1] + d[1:] - 2.0 * delta) / (h * h)
+    i = np.clip(np.searchsorted(x, xq, side="right") - 1, 0, n - 2)
+    t = xq - x[i]
+    return y[:-1][i] + t * (d[:-1][i] + t * (p2[i] + t * p3[i]))

@@ -13,7 +13,8 @@ so the four hot-path modules are loaded one by one behind package shells:
 * emu_sv/hamiltonian.py             (RydbergHamiltonian)
 * emu_sv/time_evolution/torch.py    (DifferentiableStateVectorEvolution)
 * emu_sv/custom_callback_implementations.py (occupation / correlation / energy moments)
-* emu_base/math/brents_root_finding.py, emu_base/jump_lindblad_operators.py,
+* emu_base/math/pchip_torch.py, emu_base/math/brents_root_finding.py,
+  emu_base/jump_lindblad_operators.py,
   emu_sv/algebra.py, emu_sv/time_evolution/interface.py and implementations.py
   (the Monte Carlo stepper)
 
@@ -36,6 +37,8 @@ Fixtures (inputs and reference outputs, all complex128/float64):
                        final-state probes (inner products with seeded vectors).
 * ring_n16_grad.npz    reference autograd gradient of the Neel loss for 2 parameter sets
                        of the N=16 ring over the first 2 segments (20 steps).
+* pchip.npz            PCHIP1D (emu_base/math/pchip_torch.py): the reference's test data,
+                       random knots with extrapolated queries, drive-like 1 ns signals.
 * noisy.npz            the Monte Carlo path: H*psi with the noise term, Arnoldi
                        krylov_exp (is_hermitian=False), expect_batch / apply, Brent's
                        abscissae, and EvolveMonteCarlo steps (N=8, 40 steps, two seeds of
@@ -150,6 +153,7 @@ def load_reference(ref: str) -> dict:
     }
     mods["torch"] = load("emu_sv.time_evolution.torch", "emu_sv/time_evolution/torch.py")
     mods["brent"] = load("emu_base.math.brents_root_finding", "emu_base/math/brents_root_finding.py")
+    mods["pchip"] = load("emu_base.math.pchip_torch", "emu_base/math/pchip_torch.py")
     mods["jump"] = load("emu_base.jump_lindblad_operators", "emu_base/jump_lindblad_operators.py")
     mods["algebra"] = load("emu_sv.algebra", "emu_sv/algebra.py")
     iface = load("emu_sv.time_evolution.interface", "emu_sv/time_evolution/interface.py")
@@ -623,6 +627,50 @@ def gen_noisy(R):
 
 
 GENERATORS["noisy"] = gen_noisy
+
+
+def gen_pchip(R):
+    """PCHIP1D on the reference's own test data, random non-uniform knots (2, 3, 5 and 50
+    knots, queries inside and outside the knot range) and drive-like signals on a 1 ns grid
+    evaluated at 10 ns midpoints."""
+    P = R["pchip"].PCHIP1D
+    out, k = {}, 0
+    rng = np.random.default_rng(2024)
+
+    def add(x, y, xq):
+        nonlocal k
+        out[f"c{k}_x"] = np.asarray(x, dtype=np.float64)
+        out[f"c{k}_y"] = np.asarray(y, dtype=np.float64)
+        out[f"c{k}_xq"] = np.asarray(xq, dtype=np.float64)
+        out[f"c{k}_yq"] = np_(P(torch.as_tensor(x, dtype=torch.float64),
+                                torch.as_tensor(y, dtype=torch.float64))(
+            torch.as_tensor(xq, dtype=torch.float64)))
+        k += 1
+
+    add([0.0, 1.0, 2.5, 4.0], [0.0, 2.0, 1.0, 3.0], [0.0, 1.0, 2.5, 4.0, 0.3, 3.9])  # test_pchip.py
+    add([0.0, 1.0, 2.0, 3.0], [0.0, 1.0, 1.5, 2.0], np.linspace(0.0, 3.0, 301))
+    for n in [2, 3, 5, 50]:
+        x = np.cumsum(rng.uniform(0.1, 2.0, n))
+        y = rng.normal(size=n)
+        if n == 50:
+            y[10:20] = y[10]  # flat run (zero secants)
+        xq = rng.uniform(x[0] - 1.0, x[-1] + 1.0, 200)
+        add(x, y, xq)
+    # drive-like signals: 1 ns grid, smooth ramps with kinks, midpoints of a 10 ns grid
+    T = 800
+    t = np.arange(T, dtype=np.float64)
+    tt = np.arange(0, T + 1, 10, dtype=np.float64)
+    tmid = 0.5 * (tt[:-1] + tt[1:])
+    for j in range(4):
+        knots = np.sort(rng.uniform(0, T, 6))
+        vals = rng.uniform(-15, 15, 6)
+        y = np.interp(t, knots, vals) + 0.05 * np.sin(0.37 * t * (j + 1))
+        add(t, y, tmid)
+    out["count"] = np.array(k)
+    return out
+
+
+GENERATORS["pchip"] = gen_pchip
 
 
 def main():
