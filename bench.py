@@ -46,12 +46,13 @@ def peaks() -> tuple[float, str]:
 
 
 def ncu_traffic() -> int | None:
-    """DRAM bytes (read + write) of one H*psi at N=26 from the committed ncu summary
-    (profiles/hpsi_passes_ladder_n25_c64.md: a capture at N=25 scaled by 2)."""
-    p = os.path.join(REPO, "profiles", "hpsi_passes_ladder_n25_c64.md")
+    """DRAM bytes (read + write) of one Lanczos iteration at N=26 from the committed ncu
+    summary (profiles/lanczos_iteration_fused_pass_low_n25_c64.md: captures at N=25
+    scaled by 2)."""
+    p = os.path.join(REPO, "profiles", "lanczos_iteration_fused_pass_low_n25_c64.md")
     try:
         with open(p) as f:
-            m = re.search(r"traffic_bytes_per_hpsi_at_n26:\s*(\d+)", f.read())
+            m = re.search(r"traffic_bytes_per_lanczos_iteration_at_n26:\s*(\d+)", f.read())
         return int(m.group(1)) if m else None
     except OSError:
         return None
@@ -215,32 +216,35 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     pms = np.zeros(8)
     pl = np.zeros(8, dtype=np.int64)
     L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
-    # H*psi = one pass L (kind 0) + one or two strided passes (kind 7) per Lanczos iteration
-    nit = max(pl[0], 1)
-    passl_s = pms[0] / nit / 1e3
+    # One Lanczos iteration = the pass L with the previous iteration's recurrence fused in
+    # front (kind 0; plus one plain pass L of v_0 per step) + one or two strided passes
+    # (kind 7).  Algorithmic bytes per iteration (H*psi 2 D s + recurrence 4 D s).
+    m_total = max(int(sum(iters)), 1)
+    iter_s = (pms[0] + pms[7]) / m_total / 1e3
+    passl_s = pms[0] / max(pl[0], 1) / 1e3
     passh_s = pms[7] / max(pl[7], 1) / 1e3 if pl[7] else 0.0
-    hpsi_avg_s = (pms[0] + pms[7]) / nit / 1e3  # per H*psi application
     hbm, which = peaks()
-    alg_hpsi = 2 * D * es  # H*psi algorithmic bytes: read v, write H v (diagonal on chip)
-    achieved = alg_hpsi / hpsi_avg_s / 1e9
+    alg_iter = 6 * D * es
+    achieved = alg_iter / iter_s / 1e9
     total_ms = pms.sum()
     kinds = ["hpsi_pass_low", "orth", "small", "combine", "obs", "adjoint", "batch", "hpsi_pass_high"]
     shares = {kinds[i]: round(pms[i] / total_ms, 4) for i in range(8) if pl[i]}
-    orth_s = pms[1] / max(pl[1], 1) / 1e3
     per_pass = {
-        "pass_low": {"ms": round(passl_s * 1e3, 4), "bytes": 2 * D * es,
-                     "GB/s": round(2 * D * es / passl_s / 1e9, 1),
-                     "frac": round(2 * D * es / passl_s / 1e9 / hbm, 4)},
+        "pass_low_fused": {"ms": round(passl_s * 1e3, 4), "bytes": 5 * D * es,
+                           "note": "read H v_j, v_j, v_{j-1}; write w, partial sums; the mean "
+                                   "includes the step's one plain pass L (2 D s)",
+                           "GB/s": round(5 * D * es / passl_s / 1e9, 1),
+                           "frac": round(5 * D * es / passl_s / 1e9 / hbm, 4)},
         "pass_high": {"ms": round(passh_s * 1e3, 4), "bytes": 3 * D * es,
-                      "launches_per_hpsi": round(pl[7] / nit, 2),
+                      "launches_per_iteration": round(pl[7] / m_total, 2),
                       "GB/s": round(3 * D * es / passh_s / 1e9, 1) if passh_s else None,
                       "frac": round(3 * D * es / passh_s / 1e9 / hbm, 4) if passh_s else None},
-        "orth": {"ms": round(orth_s * 1e3, 4), "bytes": 4 * D * es,
-                 "GB/s": round(4 * D * es / orth_s / 1e9, 1),
-                 "frac": round(4 * D * es / orth_s / 1e9 / hbm, 4)},
+        "iteration": {"ms": round(iter_s * 1e3, 4), "streamed_units": 11,
+                      "streamed_GB/s": round(11 * D * es / iter_s / 1e9, 1),
+                      "streamed_frac": round(11 * D * es / iter_s / 1e9 / hbm, 4)},
     }
     log(f"profiled: ms by kind {pms.round(3).tolist()} launches {pl.tolist()}; "
-        f"H*psi {hpsi_avg_s * 1e3:.4f} ms = {achieved:.1f} GB/s algorithmic; {per_pass}")
+        f"Lanczos iteration {iter_s * 1e3:.4f} ms = {achieved:.1f} GB/s algorithmic; {per_pass}")
 
     # ---- H*psi alone (standalone launches, for the kernel roofline at both precisions)
     hstand = {}
@@ -282,16 +286,18 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                    "l2": "state and Krylov vectors (512 MiB each) exceed L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm",
-                     "kernel": "H*psi = k_pass_low + k_pass_high x2 (streaming passes, flips "
-                               "and diagonal on chip, Lanczos reductions fused), per Lanczos "
-                               "iteration; achieved = 2*D*8 algorithmic bytes / H*psi time",
+                     "kernel": "Lanczos iteration = k_pass_low with the three-term recurrence "
+                               "fused in front + k_pass_high x2 (flips and diagonal on chip, "
+                               "FP64 reductions fused); achieved = 6*D*8 algorithmic bytes "
+                               "(H*psi 2 D s + recurrence 4 D s) / iteration time",
                      "achieved": round(achieved, 1), "peak": hbm, "peak_source": which,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": ncu_traffic() if n == 26 and es == 8 else None,
-                     "traffic_source": "ncu --set full of the three passes at N=25, x2 "
-                                       "(profiles/hpsi_passes_ladder_n25_c64.md)",
-                     "algorithmic_bytes_per_launch": alg_hpsi,
-                     "avg_launch_ms": round(hpsi_avg_s * 1e3, 4),
+                     "traffic_source": "ncu --set full of the fused pass L and the pass H kernels "
+                                       "at N=25, x2 (profiles/lanczos_iteration_fused_pass_low_"
+                                       "n25_c64.md)",
+                     "algorithmic_bytes_per_launch": alg_iter,
+                     "avg_launch_ms": round(iter_s * 1e3, 4),
                      "per_kernel": per_pass,
                      "kernel_time_shares": shares},
         "gpu_launches": int(launches.sum()),

@@ -60,7 +60,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 // [2k], [2k+1] = <v_k, w_out> (DOTS, UPDATE_DOTS), [ARN_NORM] = ||w_out||^2.
 // E amplitudes per thread per chunk.  UPDATE_DOTS reads every v_k twice per chunk (the
 // update needs all of them before the dots of the result).
-template <typename R, int MODE, int E>
+template <typename R, int MODE, int E, int KB = 4>
 __global__ void __launch_bounds__(ORTHO_THREADS)
 k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const unsigned char *basis,
             i64 D, void *w_, double *part) {
@@ -103,7 +103,28 @@ k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const 
             }
         }
         if (MODE != ARN_DOTS) {
-            for (int k = 0; k < nk; ++k) {
+            // KB vectors per step: KB * E independent loads in flight per thread
+            int k = 0;
+            for (; k + KB <= nk; k += KB) {
+                C a[KB][E];
+#pragma unroll
+                for (int kb = 0; kb < KB; ++kb)
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
+                        a[kb][e] = x < D ? vk(k + kb)[x] : cmake<C>(0.0, 0.0);
+                    }
+#pragma unroll
+                for (int kb = 0; kb < KB; ++kb) {
+                    const double2 c = cf[k + kb];
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        wr[e] -= c.x * double(a[kb][e].x) - c.y * double(a[kb][e].y);
+                        wi[e] -= c.x * double(a[kb][e].y) + c.y * double(a[kb][e].x);
+                    }
+                }
+            }
+            for (; k < nk; ++k) {
                 const C *v = vk(k);
                 const double2 c = cf[k];
 #pragma unroll
@@ -130,7 +151,40 @@ k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const 
 #pragma unroll
         for (int e = 0; e < E; ++e) nacc += wr[e] * wr[e] + wi[e] * wi[e];
         if (dots) {
-            for (int k = 0; k < nk; ++k) {
+            int k = 0;
+            for (; k + KB <= nk; k += KB) {
+                C a[KB][E];
+#pragma unroll
+                for (int kb = 0; kb < KB; ++kb)
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
+                        a[kb][e] = x < D ? vk(k + kb)[x] : cmake<C>(0.0, 0.0);
+                    }
+                double dr[KB], di[KB];
+#pragma unroll
+                for (int kb = 0; kb < KB; ++kb) {
+                    dr[kb] = di[kb] = 0.0;
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        dr[kb] += double(a[kb][e].x) * wr[e] + double(a[kb][e].y) * wi[e];
+                        di[kb] += double(a[kb][e].x) * wi[e] - double(a[kb][e].y) * wr[e];
+                    }
+                }
+#pragma unroll
+                for (int kb = 0; kb < KB; ++kb) {
+                    dr[kb] = warp_sum(dr[kb]);
+                    di[kb] = warp_sum(di[kb]);
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int kb = 0; kb < KB; ++kb) {
+                        sacc[warp][k + kb].x += dr[kb];
+                        sacc[warp][k + kb].y += di[kb];
+                    }
+                }
+            }
+            for (; k < nk; ++k) {
                 const C *v = vk(k);
                 double dr = 0.0, di = 0.0;  // sum conj(v) w
 #pragma unroll
@@ -433,7 +487,7 @@ template <typename R>
 static int launch_ortho(int mode, const KState *ks, const ArnState *as, int j, const void *v0,
                         const unsigned char *basis, i64 D, void *w, double *part, cudaStream_t s,
                         int *grid_out) {
-    constexpr int E = 8;
+    constexpr int E = 4;
     i64 grid = krylov_stream_grid(D);
     const i64 chunks = (D + (i64)ORTHO_THREADS * E - 1) / ((i64)ORTHO_THREADS * E);
     if (grid > chunks) grid = chunks;

@@ -39,6 +39,11 @@ struct HpsiArgs {
     void *part_buf;    // two-pass H*psi: buffer for the partial sums of pass L
     int *err;          // device word receiving EMUSV_TIMEOUT if a bounded wait gives up
     const double *eshift;  // HP_LANCZOS, HP_STORE: if non-null, the diagonal is taken minus *eshift
+    // multi-pass Lanczos with the recurrence fused into pass L (launch_hpsi_stage)
+    const void *vj, *vp;    // stored v_j, v_{j-1}
+    const double *ocoef;    // device [3]: recurrence coefficients on the stored vectors
+    const double *oscale;   // device scale of v_j
+    double *part_o;         // partials of ||w||^2, <v_j, w>
 };
 
 struct SmemLayout {

@@ -112,11 +112,11 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
     }
 }
 
-template <typename R, bool REALC, int EPI, bool NOISY>
+template <typename R, bool REALC, int EPI, bool NOISY, bool ORTH = false>
 static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
-    auto kern = k_pass_low<R, REALC, TB, RB, EPI, 0, NOISY>;
+    auto kern = k_pass_low<R, REALC, TB, RB, EPI, 0, NOISY, ORTH>;
     const size_t smem = pass_low_smem<C, TB>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -177,8 +177,11 @@ static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *pa
 // pass L) are skipped, so every H pass keeps the compile-time chunk of CMIN bits.  The
 // partial sums live in HA.part_buf (which may be HA.out: every pass reads a tile before
 // writing it).
+// stages: bit 0 = pass L, bit 1 = the H passes, bit 2 = pass L with the Lanczos recurrence
+// fused in front (ORTH; the H passes of the same H*psi follow in a later call)
 template <typename R, bool REALC, int EPI_F, int CMIN, bool NOISY>
-static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
+static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out,
+                      int stages = 3) {
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB;
     const int n = H.n;
     PassParams P;
@@ -198,11 +201,25 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     A.eshift = HA.eshift;  // null unless the caller shifts the diagonal
     int st;
     if (rem == 0) {
+        if (stages != 3) return EMUSV_BAD_ARGUMENT;
         A.out = HA.out;
         return launch_low<R, REALC, EPI_F, NOISY>(P, A, s, grid_out);
     }
     A.out = HA.part_buf;
-    if ((st = launch_low<R, REALC, EPI_PARTIAL, NOISY>(P, A, s, nullptr))) return st;
+    if (stages & 4) {
+        if constexpr (!NOISY) {
+            A.vj = HA.vj;
+            A.vp = HA.vp;
+            A.ocoef = HA.ocoef;
+            A.oscale = HA.oscale;
+            A.part_o = HA.part_o;
+            return launch_low<R, REALC, EPI_PARTIAL, false, true>(P, A, s, grid_out);
+        }
+        return EMUSV_BAD_ARGUMENT;
+    }
+    if (stages & 1)
+        if ((st = launch_low<R, REALC, EPI_PARTIAL, NOISY>(P, A, s, nullptr))) return st;
+    if (!(stages & 2)) return EMUSV_OK;
     if (rem > G) {
         if ((st = launch_high<R, REALC, EPI_PARTIAL, CMIN>(P, n - 2 * G, A, HA.part_buf, s, nullptr)))
             return st;
@@ -214,11 +231,33 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
 // 64-byte rows (PassShape CMIN) where two H passes cover the bits above pass L, else
 // 32-byte rows
 template <typename R, bool REALC, int EPI_F, bool NOISY = false>
-static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
+static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out,
+                      int stages = 3) {
     constexpr int TB = PassShape<R>::TB, CMIN = PassShape<R>::CMIN;
     if (H.n - TB <= 2 * (TB - CMIN))
-        return run_passes<R, REALC, EPI_F, CMIN, NOISY>(H, HA, s, grid_out);
-    return run_passes<R, REALC, EPI_F, CMIN - 1, NOISY>(H, HA, s, grid_out);
+        return run_passes<R, REALC, EPI_F, CMIN, NOISY>(H, HA, s, grid_out, stages);
+    return run_passes<R, REALC, EPI_F, CMIN - 1, NOISY>(H, HA, s, grid_out, stages);
+}
+
+// The stages of a multi-pass Lanczos H*psi launched separately (stages as run_passes):
+// 1 = pass L of v_0, 2 = the H passes (their partial sums from a previous pass L),
+// 4 = the recurrence of the previous iteration fused into this iteration's pass L.
+int launch_hpsi_stage(int dtype, int stages, const HamParams &H, const HpsiArgs &A, cudaStream_t s,
+                      int *grid_out) {
+    if (H.noisy) return EMUSV_BAD_ARGUMENT;
+    if (dtype == EMUSV_C64)
+        return H.real_coef ? run_passes<float, true, EPI_LANCZOS>(H, A, s, grid_out, stages)
+                           : run_passes<float, false, EPI_LANCZOS>(H, A, s, grid_out, stages);
+    if (dtype == EMUSV_C128)
+        return H.real_coef ? run_passes<double, true, EPI_LANCZOS>(H, A, s, grid_out, stages)
+                           : run_passes<double, false, EPI_LANCZOS>(H, A, s, grid_out, stages);
+    return EMUSV_BAD_ARGUMENT;
+}
+
+// Registers whose H*psi takes more than one pass (the fused recurrence needs pass L to
+// produce partial sums for later passes).
+bool hpsi_multipass(int dtype, int n) {
+    return n > (dtype == EMUSV_C64 ? PassShape<float>::TB : PassShape<double>::TB);
 }
 
 // mode: HP_STORE or HP_LANCZOS (values of HpsiMode)

@@ -72,6 +72,12 @@ struct PassArgs {
     const int *gate;        // kernel returns at once when *gate != 0
     int *err;               // receives EMUSV_TIMEOUT when a bounded wait gives up
     const double *eshift;   // pass L: if non-null, the diagonal is taken minus *eshift
+    // pass L with the Lanczos recurrence fused in front (ORTH): u holds H v_j and receives
+    // w = H v_j - a v_j - b v_{j-1} (in place, stored form), the pass works on w
+    const void *vj, *vp;    // stored v_j, v_{j-1} (vp may be null)
+    const double *ocoef;    // device [3]: a_re scale_j, a_im scale_j, b scale_{j-1}
+    const double *oscale;   // device scale_j (for <v_j, w>)
+    double *part_o;         // [gridDim.x * NRED]: ||w||^2, <v_j, w>
 };
 
 // ------------------------------------------------------------------ PTX helpers
@@ -251,10 +257,15 @@ __host__ __device__ constexpr size_t pass_low_smem() {
     return SL * (sizeof(C) << TB) + 8 * SL + sizeof(double) * (MAXQ * UPAD + MAXQ + SL * 64 + 8 * NRED);
 }
 
-// NOISY: the diagonal has the imaginary part dc_im + dg_im * popcount(x) (noise term)
-template <typename R, bool REALC, int TB, int RB, int EPI, int PB, bool NOISY = false>
+// NOISY: the diagonal has the imaginary part dc_im + dg_im * popcount(x) (noise term).
+// ORTH: each tile is first turned from H v_j into w = H v_j - a v_j - b v_{j-1} (the Lanczos
+// recurrence, written back in place and kept in shared memory for the pass), one tile
+// ahead of the flips so that the pass keeps one block barrier per tile; FP64 partials of
+// ||w||^2 and <v_j, w> go to A.part_o.  PB = 0, EPI_PARTIAL.
+template <typename R, bool REALC, int TB, int RB, int EPI, int PB, bool NOISY = false, bool ORTH = false>
 __global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_low(const PassParams P, PassArgs A) {
+    static_assert(!ORTH || (PB == 0 && EPI == EPI_PARTIAL && !NOISY), "ORTH: plain pass L only");
     const double eshift = A.eshift ? *A.eshift : 0.0;
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
@@ -295,6 +306,56 @@ k_pass_low(const PassParams P, PassArgs A) {
         }
     }
 
+    // ORTH: the recurrence's coefficients on the stored vectors, and the tile conversion
+    double ocr = 0.0, oci = 0.0, ocb = 0.0, osj = 0.0;
+    double ored[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) ored[k] = 0.0;
+    if (ORTH) {
+        ocr = A.ocoef[0];
+        oci = A.ocoef[1];
+        ocb = A.ocoef[2];
+        osj = *A.oscale;
+    }
+    auto convert = [&](int b, int64_t tbase) {
+        C *tl = tiles + ((int64_t)b << TB);
+        C *wout = const_cast<C *>(u);
+        const C *vj = reinterpret_cast<const C *>(A.vj);
+        const C *vp = reinterpret_cast<const C *>(A.vp);
+        C pj[NA], pp[NA];
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+            const int64_t x = tbase + tid + a * NT;
+            pj[a] = vj[x];
+            pp[a] = vp ? vp[x] : cmake<C>(0.0, 0.0);
+        }
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+            const int l = tid + a * NT;
+            const C h = tl[l];
+            const double jr = double(pj[a].x), ji = double(pj[a].y);
+            const double wr = double(h.x) - (ocr * jr - oci * ji) - ocb * double(pp[a].x);
+            const double wi = double(h.y) - (ocr * ji + oci * jr) - ocb * double(pp[a].y);
+            const C o = cmake<C>(wr, wi);
+            tl[l] = o;
+            wout[tbase + l] = o;
+            const double orr = double(o.x), oi = double(o.y);
+            const double vr = osj * jr, vi = osj * ji;
+            ored[0] += orr * orr + oi * oi;
+            ored[1] += vr * orr + vi * oi;  // <v_j, w>
+            ored[2] += vr * oi - vi * orr;
+        }
+    };
+    bool ok = true;
+    if (ORTH && cid < nsuper) {  // the first tile, converted before the loop
+        if (!mbar_wait(&bars[0], 0)) {
+            ok = false;
+            report_timeout(A);
+        } else {
+            convert(0, ((((int64_t)cid) << PB) | rank) << TB);
+        }
+    }
+
     // per-thread constants: energy of the thread bits and thread x register crosses
     double ET = 0.0;
 #pragma unroll
@@ -330,7 +391,6 @@ k_pass_low(const PassParams P, PassArgs A) {
     double red[NRED];
 #pragma unroll
     for (int k = 0; k < NRED; ++k) red[k] = 0.0;
-    bool ok = true;
 
     int it = 0, buf = 0;
     uint32_t phase = 0;
@@ -356,7 +416,7 @@ k_pass_low(const PassParams P, PassArgs A) {
                 sc[lane] = cx;  // crossT[0..SB) then crossR[0..RB)
             }
         }
-        if (ok && !mbar_wait(&bars[buf], phase)) {
+        if (!ORTH && ok && !mbar_wait(&bars[buf], phase)) {  // ORTH: waited when converted
             ok = false;
             report_timeout(A);
         }
@@ -467,6 +527,19 @@ k_pass_low(const PassParams P, PassArgs A) {
                 }
             }
         }
+        if (ORTH && ok) {  // convert the next tile (its buffer is not read before the barrier)
+            const int64_t s1 = s + nclusters;
+            if (s1 < nsuper) {
+                const int b1 = buf + 1 == SL ? 0 : buf + 1;
+                const uint32_t ph1 = buf + 1 == SL ? (phase ^ 1u) : phase;
+                if (!mbar_wait(&bars[b1], ph1)) {
+                    ok = false;
+                    report_timeout(A);
+                } else {
+                    convert(b1, s1 << TB);
+                }
+            }
+        }
         if (++buf == SL) {
             buf = 0;
             phase ^= 1u;
@@ -475,6 +548,13 @@ k_pass_low(const PassParams P, PassArgs A) {
     // no CTA may leave while a sibling can still read its shared memory
     if (PB) cluster_sync_all();
     write_partials<EPI>(A, red, red_scr);
+    if (ORTH) {
+        block_sum<NRED>(ored, red_scr);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < NRED; ++k) A.part_o[(int64_t)blockIdx.x * NRED + k] = ored[k];
+        }
+    }
 }
 
 // ------------------------------------------------------------------------- pass H

@@ -24,6 +24,9 @@ namespace emusv {
 int hpsi_tile_bits(int n);
 int launch_hpsi(int dtype, int mode, const HamParams &P, HpsiArgs A, int max_grid,
                 cudaStream_t s, int *grid_out);
+int launch_hpsi_stage(int dtype, int stages, const HamParams &H, const HpsiArgs &A, cudaStream_t s,
+                      int *grid_out);
+bool hpsi_uses_passes(int dtype, int n);
 int max_grid_blocks();
 
 struct Workspace {
@@ -169,6 +172,31 @@ k_orth(KState *ks, int j, const double *part_h, int nb_h, const void *vj_, const
     block_sum<NRED>(acc, red);
     if (threadIdx.x == 0)
         for (int k = 0; k < NRED; ++k) part_o[(i64)blockIdx.x * NRED + k] = acc[k];
+}
+
+// The recurrence coefficients of iteration j from the H*psi partials (as k_orth's
+// preamble), for the recurrence fused into the next iteration's pass L: on the stored
+// vectors, w = H v_j - ocoef[0..1] u_j - ocoef[2] u_{j-1}.
+__global__ void k_orth_coef(KState *ks, int j, const double *part_h, int nb_h) {
+    if (ks->status != KS_RUNNING) return;
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double s[NRED];
+    sum_partials<NRED>(part_h, nb_h, NRED, s, red);
+    if (threadIdx.x == 0) {
+        const double b = j > 0 ? ks->r[j - 1] : 0.0;
+        const double cr = j > 0 ? ks->vv_re[j] : 0.0, ci = j > 0 ? ks->vv_im[j] : 0.0;
+        const double ar = s[1] - b * cr, ai = s[2] - b * ci;
+        ks->a_re[j] = ar;
+        ks->a_im[j] = ai;
+        ks->b_re[j] = b;
+        ks->b_im[j] = 0.0;
+        const double sg = ks->shift;
+        ks->hn[j] = sqrt(fmax(0.0, s[0] + 2.0 * sg * s[1] + sg * sg));
+        const double sj = ks->scale[j], sp = j > 0 ? ks->scale[j - 1] : 0.0;
+        ks->ocoef[0] = ar * sj;
+        ks->ocoef[1] = ai * sj;
+        ks->ocoef[2] = b * sp;
+    }
 }
 
 // Decide iteration j (krylov_decide) from the orthogonalisation's partial sums.  Later
@@ -463,7 +491,71 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
     EMUSV_CHECK_LAUNCH();
 
     int status = KS_RUNNING;
-    for (int j = 0; j < max_krylov_dim; ++j) {
+    // Registers whose H*psi takes several passes run the recurrence of iteration j inside
+    // the pass L of iteration j+1 (one streaming pass fewer per iteration): pass L of v_0
+    // first, then per iteration the H passes, the coefficients, the fused pass L, k_small.
+    const bool fused = hpsi_uses_passes(dtype, nqubits);
+    if (fused) {
+        HpsiArgs A0 = {};
+        A0.u = stored(0);
+        A0.su_dev = &W.ks->scale[0];
+        A0.part_buf = part_vec;
+        A0.gate = &W.ks->status;
+        A0.err = &W.ks->kerr;
+        A0.eshift = &W.ks->shift;
+        A0.tile_bits = hpsi_tile_bits(nqubits);
+        int st = launch_hpsi_stage(dtype, 1, P, A0, s, nullptr);
+        if (st) return st;
+    }
+    for (int j = 0; fused && j < max_krylov_dim; ++j) {
+        if (j + 1 > capacity) {
+            int st = read_status(W.ks, s, &status);
+            if (st) return st;
+            if (status == KS_RUNNING) return EMUSV_WORKSPACE_TOO_SMALL;
+            break;
+        }
+        HpsiArgs A = {};
+        A.u = stored(j);
+        A.su_dev = &W.ks->scale[j];
+        A.out = const_cast<void *>(stored(j + 1));
+        A.partials = W.part_h;
+        A.tile_bits = hpsi_tile_bits(nqubits);
+        A.gate = &W.ks->status;
+        A.err = &W.ks->kerr;
+        A.part_buf = part_vec;
+        A.eshift = &W.ks->shift;
+        int gh = 0, go = 0;
+        int st = launch_hpsi_stage(dtype, 2, P, A, s, &gh);
+        if (st) return st;
+        {
+            ProfScope ps_(PROF_SMALL, s);
+            k_orth_coef<<<1, BLOCK, 0, s>>>(W.ks, j, W.part_h, gh);
+        }
+        EMUSV_CHECK_LAUNCH();
+        HpsiArgs B = A;
+        B.u = stored(j + 1);  // H v_j in, w out (in place)
+        B.su_dev = nullptr;
+        B.su = 1.0;
+        B.vj = stored(j);
+        B.vp = j > 0 ? stored(j - 1) : nullptr;
+        B.ocoef = W.ks->ocoef;
+        B.oscale = &W.ks->scale[j];
+        B.part_o = W.part_o;
+        if ((st = launch_hpsi_stage(dtype, 4, P, B, s, &go))) return st;
+        const int poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
+        {
+            ProfScope ps_(PROF_SMALL, s);
+            k_small<<<1, 32, 0, s>>>(W.ks, j, W.part_o, go, dt, exp_tolerance, norm_tolerance, 1,
+                                     j == 0, max_krylov_dim);
+        }
+        EMUSV_CHECK_LAUNCH();
+        if (poll) {
+            st = read_status(W.ks, s, &status);
+            if (st) return st;
+            if (status != KS_RUNNING) break;
+        }
+    }
+    for (int j = 0; !fused && j < max_krylov_dim; ++j) {
         if (j + 1 > capacity) {
             int st = read_status(W.ks, s, &status);
             if (st) return st;

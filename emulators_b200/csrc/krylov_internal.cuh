@@ -25,6 +25,7 @@ struct KState {
     double hn[KMAX];                 // ||H v_k||
     double scale[KMAX + 2];          // v_k = scale[k] * stored_k
     double c_re[KMAX + 2], c_im[KMAX + 2];  // result coefficients
+    double ocoef[4];  // recurrence coefficients on the stored vectors (fused pass L)
 };
 
 

@@ -4,6 +4,7 @@
                                           [--max-krylov-dim 100]
     python -m emulators_b200.profile_case --batch 64 --steps 3        # batched engine
     python -m emulators_b200.profile_case --adjoint 8 --dtype c128    # batched adjoint
+    python -m emulators_b200.profile_case --arnoldi 2 --n 20 --dtype c128  # noisy Arnoldi
 
 Builds the 2 x n/2 ladder at 5.5 um with the ladder_n26 drive, runs `--hpsi` standalone
 H*psi launches and `--steps` Krylov time steps from |g...g>, prints device times.  Sized
@@ -34,6 +35,9 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: the first BATCH registers of the 256-register batch "
                          "workload for --steps steps in one persistent launch")
+    ap.add_argument("--arnoldi", type=int, default=0,
+                    help="instead: ARNOLDI Arnoldi steps of the noisy ladder workload cut to "
+                         "--n qubits (complex128 unless --dtype c64)")
     ap.add_argument("--adjoint", type=int, default=0,
                     help="instead: ADJOINT parameter sets of the N=16 ring gradient "
                          "workload, 4 segments: forward, one checkpoint-segment "
@@ -43,6 +47,8 @@ def main(argv=None) -> int:
         return _batch_case(a)
     if a.adjoint:
         return _adjoint_case(a)
+    if a.arnoldi:
+        return _arnoldi_case(a)
     dev = torch.device("cuda", 0)
     dt_ = torch.complex64 if a.dtype == "c64" else torch.complex128
     n = a.n
@@ -102,6 +108,33 @@ def _batch_case(a) -> int:
     print(json.dumps({"registers": a.batch, "steps": k, "ms": e0.elapsed_time(e1),
                       "iterations_mean": float(iters[iters > 0].mean()),
                       "failed": int((status != 0).sum())}))
+    return 0
+
+
+def _arnoldi_case(a) -> int:
+    from .krylov import fused_arnoldi_step
+
+    w, ops = wl.noisy_ladder_n22()
+    n = a.n - (a.n % 2)
+    dev = torch.device("cuda", 0)
+    dt_ = torch.complex64 if a.dtype == "c64" else torch.complex128
+    noise = -0.5j * sum(L.conj().T @ L for L in ops)
+    U = torch.as_tensor(wl.interaction_matrix(wl.ladder(n // 2, 5.5)))
+    H = RydbergHamiltonian(torch.full((n,), 4.0), torch.full((n,), -9.0), torch.zeros(n), U, dev,
+                           noise=torch.as_tensor(noise))
+    v = torch.zeros(1 << n, dtype=dt_, device=dev)
+    v[0] = 1.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    its = []
+    e0.record()
+    for _ in range(a.arnoldi):
+        v, info, st = fused_arnoldi_step(HamiltonianExpOperator(H, w.dt), v, 1e-10, 1e-10, 100)
+        _lib.check(st, "arnoldi")
+        its.append((info.iterations, info.second_rounds))
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"n": n, "dtype": a.dtype, "step_ms": e0.elapsed_time(e1) / a.arnoldi,
+                      "iterations_second_rounds": its}))
     return 0
 
 
