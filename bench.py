@@ -319,6 +319,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         result["secondary"]["noisy_ladder_n22_c128"] = noisy_mc(dev)
         log(f"noisy: {result['secondary']['noisy_ladder_n22_c128']}")
     if not args.no_noisy and world == 1:
+        result["secondary"]["lindblad_ladder_n12_c128"] = lindblad_dm(dev)
+        log(f"lindblad: {result['secondary']['lindblad_ladder_n12_c128']}")
         result["secondary"]["drive_preparation_pchip"] = drive_prep(dev)
         log(f"drive preparation: {result['secondary']['drive_preparation_pchip']}")
     if not args.no_precision and world == 1:
@@ -795,6 +797,72 @@ def drive_prep(dev, regs: int = 256, qubits: int = 16, T: int = 4000, dt_ns: int
                              "sample": f"first {done} signals, oracle numpy PCHIP"},
             "speedup_e2e_vs_cpu": round((S / (e2e_ms / 1e3)) * cpu_s, 1),
             "first_64_signals_bit_identical_to_oracle": ok}
+
+
+def lindblad_dm(dev, steps: int = 8) -> dict:
+    """The density-matrix path on lindblad_ladder_n12 (a 4^12 density matrix, complex128):
+    EvolveDensityMatrix steps through the fused Arnoldi step over the 24-bit vector, next to
+    the oracle's dense Lindbladian on the host (one application, timed, times the GPU run's
+    Arnoldi iterations per step)."""
+    import torch
+
+    from emulators_b200 import _lib
+    from emulators_b200.density_matrix import DensityMatrix
+    from emulators_b200.time_evolution import EvolveDensityMatrix
+    from emulators_b200 import workloads as wl
+    from oracle import oracle
+
+    w, ops = wl.lindblad_ladder_n12()
+    n = w.nqubits
+    U = torch.as_tensor(w.U)
+    tops = [torch.as_tensor(L) for L in ops]
+    stepper = EvolveDensityMatrix(100)
+    rho = DensityMatrix.make(n).data
+    its = []
+
+    def step(k, r):
+        r, ham = stepper.apply(w.dt, torch.as_tensor(w.omega[k]), torch.as_tensor(w.delta[k]),
+                               torch.as_tensor(w.phi[k]), U, r, w.tolerance, tops)
+        return r
+
+    for k in range(2):
+        rho = step(k, rho)
+    torch.cuda.synchronize()
+    L = _lib.load()
+    L.emusv_profile_begin(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(2, 2 + steps):
+        rho = step(k, rho)
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    pms = np.zeros(8)
+    pl = np.zeros(8, dtype=np.int64)
+    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
+    from emulators_b200 import krylov
+    iters = krylov._cache(rho.device, n, _lib.dtype_code(rho.dtype), "lindblad").last_iters
+    kinds = ["hpsi_pass_low+jumps", "orth", "small", "combine", "obs", "adjoint", "batch",
+             "hpsi_pass_high"]
+    tot = pms.sum()
+    trace = float(DensityMatrix(rho).norm())
+    # host: one dense Lindbladian application of the oracle at the same size
+    r0 = np.zeros((1 << n, 1 << n), dtype=np.complex128)
+    r0[0, 0] = 1.0
+    t0 = time.perf_counter()
+    oracle.lindbladian_apply(w.omega[0], w.delta[0], w.phi[0], w.U, ops, r0)
+    t_apply = time.perf_counter() - t0
+    cpu_step_s = t_apply * max(iters, 1)
+    return {"workload": "lindblad_ladder_n12: 4^12 density matrix (N=12 2x6 ladder 5.5um), "
+                        "relaxation 0.5/us + dephasing 1/us, dt=10ns, complex128",
+            "steps_per_s": round(steps / el, 3), "arnoldi_iterations_last_step": iters,
+            "trace_after": round(trace, 12),
+            "kernel_time_shares": {kinds[i]: round(pms[i] / tot, 4) for i in range(8) if pl[i]},
+            "cpu_baseline": {"steps_per_s": round(1.0 / cpu_step_s, 5), "cores": oracle.num_threads(),
+                             "kind": "port",
+                             "sample": f"one dense Lindbladian application of the oracle at N=12 "
+                                       f"({t_apply:.2f} s) x {iters} Arnoldi iterations per step"},
+            "speedup_vs_cpu": round((steps / el) * cpu_step_s, 1)}
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)

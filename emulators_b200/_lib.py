@@ -58,6 +58,13 @@ SIGNATURES: dict[str, tuple] = {
     "emusv_qubit_densities": (_I, [_I, _I, _P, _P, _P, _SZ, _P]),
     "emusv_apply_1q": (_I, [_I, _I, _P, _I, _P, _P]),
     "emusv_pchip_eval": (_I, [_I, _P, _I, _P, _I64, _I, _P, _P, _I64, _P]),
+    "emusv_lindblad_apply": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P]),
+    "emusv_lindblad_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "emusv_lindblad_arnoldi_step": (_I, [_I, _I, _D, _P, _P, _P, _P, _I, _P, _P, _P, _D, _D, _I, _I,
+                                         _P, _SZ, ctypes.POINTER(KrylovInfo), _P]),
+    "emusv_dm_scratch_bytes": (_SZ, [_I, _I]),
+    "emusv_dm_energy": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
+    "emusv_dm_diagonal_amplitudes": (_I, [_I, _I, _P, _P, _P]),
     "emusv_sample_scratch_bytes": (_SZ, [_I]),
     "emusv_sample": (_I, [_I, _I, _P, _I, _P, _P, _P, _SZ, _P]),
     "emusv_batch_max_qubits": (_I, []),

@@ -33,6 +33,10 @@ namespace emusv {
 int launch_hpsi(int dtype, int mode, const HamParams &P, HpsiArgs A, int max_grid,
                 cudaStream_t s, int *grid_out);
 int hpsi_tile_bits(int n);
+int arnoldi_run(const HamParams &P, const LindbladJumps *J, int dtype, double dt, const void *psi_in,
+                void *psi_out, double exp_tolerance, double norm_tolerance, int max_krylov_dim,
+                int krylov_dim_hint, void *workspace, size_t workspace_bytes,
+                emusv_krylov_info *info, void *stream);
 
 constexpr int ARN_KMAX = 100;                  // largest Arnoldi max_krylov_dim
 constexpr int ARN_M = ARN_KMAX + 2;            // largest extended matrix
@@ -525,9 +529,25 @@ int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, 
                        int max_krylov_dim, int krylov_dim_hint, void *workspace,
                        size_t workspace_bytes, emusv_krylov_info *info, void *stream) {
     HamParams P;
+    if (!make_params(nqubits, omegas, deltas, phis, interaction, &P) || !add_noise(noise, &P))
+        return EMUSV_BAD_ARGUMENT;
+    return arnoldi_run(P, nullptr, dtype, dt, psi_in, psi_out, exp_tolerance, norm_tolerance,
+                       max_krylov_dim, krylov_dim_hint, workspace, workspace_bytes, info, stream);
+}
+
+}  // extern "C"
+
+namespace emusv {
+
+// The Arnoldi step for the operator of P (nqubits = P.n bits), plus, when J is given, the
+// Lindblad jump term i sum_q K_q added to every product (lindblad.cu).
+int arnoldi_run(const HamParams &P, const LindbladJumps *J, int dtype, double dt, const void *psi_in,
+                void *psi_out, double exp_tolerance, double norm_tolerance, int max_krylov_dim,
+                int krylov_dim_hint, void *workspace, size_t workspace_bytes,
+                emusv_krylov_info *info, void *stream) {
+    const int nqubits = P.n;
     if (!psi_in || !psi_out || !workspace || (dtype != EMUSV_C128 && dtype != EMUSV_C64) ||
-        max_krylov_dim < 1 || max_krylov_dim > ARN_KMAX || !isfinite(dt) ||
-        !make_params(nqubits, omegas, deltas, phis, interaction, &P) || !add_noise(noise, &P))
+        max_krylov_dim < 1 || max_krylov_dim > ARN_KMAX || !isfinite(dt))
         return EMUSV_BAD_ARGUMENT;
     if ((reinterpret_cast<uintptr_t>(workspace) & 255) || (reinterpret_cast<uintptr_t>(psi_in) & 15) ||
         (reinterpret_cast<uintptr_t>(psi_out) & 15))
@@ -575,6 +595,8 @@ int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, 
         A.part_buf = basis;
         A.eshift = &ks->shift;
         if ((st = launch_hpsi(dtype, HP_STORE, P, A, 0, s, nullptr))) return st;
+        if (J && (st = launch_lindblad_jumps(dtype, *J, stored(j), &ks->scale[j], w, &ks->status, s)))
+            return st;
         int og = 0;
         for (int mode = ARN_DOTS; mode <= ARN_UPDATE; ++mode) {
             st = dtype == EMUSV_C128
@@ -630,4 +652,4 @@ int emusv_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas, 
     return status == KS_MAXDIM ? EMUSV_NOT_CONVERGED : EMUSV_OK;
 }
 
-}  // extern "C"
+}  // namespace emusv

@@ -58,6 +58,19 @@ bool make_params(int n, const double *omegas, const double *deltas, const double
 // P.  Returns false on a non-finite entry.
 bool add_noise(const double *noise, HamParams *P);
 
+// The jump term of a Lindbladian on a density matrix stored as a vector of 2N bits (row
+// index in the high N bits): i sum_q K_q, K = sum_k L_k (x) conj(L_k) acting on the row
+// bit and the column bit of qubit q; K[(i*2 + j)*4 + (i'*2 + j')] (re, im interleaved).
+struct LindbladJumps {
+    int nq;          // N
+    unsigned mask;   // nonzero entries of K
+    double K[32];
+};
+// out += i * (*su) * sum_q K_q u  (device vectors of 4^N amplitudes); returns at once when
+// *gate != 0.
+int launch_lindblad_jumps(int dtype, const LindbladJumps &J, const void *u, const double *su,
+                          void *out, const int *gate, cudaStream_t s);
+
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

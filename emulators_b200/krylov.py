@@ -167,6 +167,46 @@ def fused_arnoldi_step(op: HamiltonianExpOperator, v: torch.Tensor, exp_toleranc
     return out, info, st
 
 
+def fused_lindblad_step(ham, dt: float, rho: torch.Tensor, exp_tolerance: float,
+                        norm_tolerance: float, max_krylov_dim: int):
+    """exp(-i dt L) rho for a RydbergLindbladian by Arnoldi over the 4^N vector in one
+    C-ABI call (EvolveDensityMatrix: implementations.py:87-120)."""
+    rho = ham._check(rho)
+    n = ham.nqubits
+    if not 1 <= max_krylov_dim <= _MAX_ARNOLDI_DIM:
+        raise ValueError(f"max_krylov_dim must be in 1..{_MAX_ARNOLDI_DIM} for Arnoldi")
+    code = _lib.dtype_code(rho.dtype)
+    L = _lib.load()
+    c = _cache(rho.device, n, code, "lindblad")
+    out = torch.empty_like(rho)
+    info = _lib.KrylovInfo()
+    same_dt = abs(dt) == c.last_dt
+    hint = max(0, c.last_iters - 3) if (use_iteration_hint and same_dt) else 0
+    if c.buf is None:
+        c.capacity = min(max_krylov_dim + 1, 32)
+    while True:
+        need = L.emusv_lindblad_workspace_bytes(n, code, c.capacity)
+        if c.buf is None or c.buf.numel() < need:
+            c.buf = None
+            c.buf = torch.zeros(need, dtype=torch.uint8, device=rho.device)
+        st = L.emusv_lindblad_arnoldi_step(n, code, float(dt), *ham._params(),
+                                           len(ham.pulser_lindblads), _lib.ptr(ham._ops),
+                                           rho.data_ptr(), out.data_ptr(), float(exp_tolerance),
+                                           float(norm_tolerance), int(max_krylov_dim), hint,
+                                           c.buf.data_ptr(), c.buf.numel(), info, _lib.stream_of(rho))
+        if st == _lib.WORKSPACE_TOO_SMALL:
+            if c.capacity >= max_krylov_dim + 1:
+                _lib.check(st, "lindblad step")
+            c.capacity = min(2 * c.capacity, max_krylov_dim + 1)
+            continue
+        break
+    c.last_iters = info.iterations
+    c.last_dt = abs(dt)
+    if st not in (_lib.OK, _lib.NOT_CONVERGED):
+        _lib.check(st, "lindblad step")
+    return out, info, st
+
+
 # ------------------------------------------------------------------ generic Lanczos
 def _dot(a: torch.Tensor, b: torch.Tensor, res: torch.Tensor, sc: torch.Tensor) -> None:
     _lib.check(_lib.load().emusv_vec_dot(a.numel(), _lib.dtype_code(a.dtype), a.data_ptr(),

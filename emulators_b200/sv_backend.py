@@ -22,7 +22,10 @@ from .hamiltonian import RydbergHamiltonian
 from .observables import (correlation_matrix_sv_impl, energy_second_moment_sv_impl,
                           energy_sv_impl, energy_variance_sv_impl, qubit_occupation_sv_impl)
 from .state_vector import StateVector
-from .time_evolution import EvolveMonteCarlo, EvolveStateVector
+from .density_matrix import (DensityMatrix, correlation_matrix_sv_den_mat_impl,
+                             energy_second_moment_den_mat_impl, energy_variance_sv_den_mat_impl,
+                             qubit_occupation_sv_den_mat_impl)
+from .time_evolution import EvolveDensityMatrix, EvolveMonteCarlo, EvolveStateVector
 
 _TIME_CONVERSION_COEFF = 0.001  # Omega and delta in rad/us, dt in ns (sv_backend_impl.py:29)
 logger = logging.getLogger("emulators")
@@ -49,24 +52,32 @@ class Observable:
         raise NotImplementedError
 
 
+def _dm(state) -> bool:
+    return isinstance(state, DensityMatrix)
+
+
 class Occupation(Observable):
     tag = "occupation"
 
     def apply(self, *, config, state, hamiltonian):
-        return qubit_occupation_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+        f = qubit_occupation_sv_den_mat_impl if _dm(state) else qubit_occupation_sv_impl
+        return f(config=config, state=state, hamiltonian=hamiltonian)
 
 
 class CorrelationMatrix(Observable):
     tag = "correlation_matrix"
 
     def apply(self, *, config, state, hamiltonian):
-        return correlation_matrix_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+        f = correlation_matrix_sv_den_mat_impl if _dm(state) else correlation_matrix_sv_impl
+        return f(config=config, state=state, hamiltonian=hamiltonian)
 
 
 class Energy(Observable):
     tag = "energy"
 
     def apply(self, *, config, state, hamiltonian):
+        if _dm(state):
+            return hamiltonian.expect(state).cpu()
         return energy_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
 
 
@@ -74,20 +85,24 @@ class EnergyVariance(Observable):
     tag = "energy_variance"
 
     def apply(self, *, config, state, hamiltonian):
-        return energy_variance_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+        f = energy_variance_sv_den_mat_impl if _dm(state) else energy_variance_sv_impl
+        return f(config=config, state=state, hamiltonian=hamiltonian)
 
 
 class EnergySecondMoment(Observable):
     tag = "energy_second_moment"
 
     def apply(self, *, config, state, hamiltonian):
-        return energy_second_moment_sv_impl(config=config, state=state, hamiltonian=hamiltonian)
+        f = energy_second_moment_den_mat_impl if _dm(state) else energy_second_moment_sv_impl
+        return f(config=config, state=state, hamiltonian=hamiltonian)
 
 
 class StateResult(Observable):
     tag = "state"
 
     def apply(self, *, config, state, hamiltonian):
+        if _dm(state):
+            return DensityMatrix(state.data.clone())
         return StateVector(state.data.clone())
 
 
@@ -198,9 +213,9 @@ class SequenceData:
 
 # ---------------------------------------------------------------- time loop
 class SVBackendImpl:
-    """sv_backend_impl.py:74-262 for the state-vector steppers: noiseless, and the Monte
-    Carlo stepper when the sequence has Lindblad operators (sv_backend_impl.py:82-95); the
-    density-matrix (Lindblad equation) stepper is not part of this package."""
+    """sv_backend_impl.py:74-262: the noiseless state-vector stepper, and with Lindblad
+    operators the Monte Carlo stepper or the density-matrix stepper, chosen as the
+    reference chooses (sv_backend_impl.py:82-95)."""
 
     def __init__(self, config: SVConfig, data: SequenceData):
         from . import krylov
@@ -208,14 +223,14 @@ class SVBackendImpl:
         krylov.use_iteration_hint = bool(config.krylov_dim_hint)
         self._config = config
         self._data = data
+        state_type = StateVector
         if data.lindblad_ops:
             solver = str(getattr(config.solver, "value", config.solver))
             if (solver == "default" and data.has_stochastic_noise) or solver == "montecarlo":
                 self.stepper = EvolveMonteCarlo(config.max_krylov_dim)
             else:
-                raise NotImplementedError("emulators_b200: the density-matrix (Lindblad "
-                                          "equation) solver is not implemented; use "
-                                          "solver='montecarlo'")
+                self.stepper = EvolveDensityMatrix(config.max_krylov_dim)
+                state_type = DensityMatrix
         else:
             self.stepper = EvolveStateVector(config.max_krylov_dim)
         self.target_times = data.target_times
@@ -227,7 +242,12 @@ class SVBackendImpl:
                 raise ValueError(
                     "Mismatch in number of atoms: initial state has "
                     f"{config.initial_state.n_qudits} and the sequence has {self.nqubits}")
-            self.state = StateVector(config.initial_state.data.clone().to(config.vector_dtype))
+            init = config.initial_state
+            if state_type is DensityMatrix and not isinstance(init, DensityMatrix):
+                init = DensityMatrix.from_state_vector(init)  # sv_backend_impl.py:143-160
+            self.state = state_type(init.data.clone().to(config.vector_dtype))
+        elif state_type is DensityMatrix:
+            self.state = DensityMatrix(DensityMatrix.make(self.nqubits).data.to(config.vector_dtype))
         else:
             self.state = StateVector.make(self.nqubits, dtype=config.vector_dtype)
         self.results = Results(data.qubit_ids, int(self.target_times[-1]))
@@ -256,7 +276,7 @@ class SVBackendImpl:
             return
         norm = self.state.norm()
         if not torch.allclose(norm, torch.tensor(1.0, dtype=torch.float64)):
-            state = StateVector((1.0 / norm.item()) * self.state.data)
+            state = type(self.state)((1.0 / norm.item()) * self.state.data)
         else:
             state = self.state
         if self._current_H is None:  # t = 0 (sv_backend_impl.py:224-234)

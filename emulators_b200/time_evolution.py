@@ -181,3 +181,32 @@ class EvolveMonteCarlo(BaseStepper):
             state = self.do_quantum_jump(state, pulser_lindblads, aggregated, len(omegas))
             new_gap = _norm2(state) - self.jump_threshold
         return state, ham
+
+
+class EvolveDensityMatrix(BaseStepper):
+    """Evolution of a density matrix under the Lindbladian (implementations.py:63-120):
+    exp(-i dt L) rho by the fused Arnoldi step over the 4^N vector."""
+
+    def __init__(self, max_krylov_dim: int = DEFAULT_MAX_KRYLOV_DIM) -> None:
+        super().__init__(max_krylov_dim)
+
+    @staticmethod
+    def get_hamiltonian(omegas, deltas, phis, pulser_lindblads, interaction_matrix, device):
+        from .density_matrix import RydbergLindbladian
+
+        return RydbergLindbladian(omegas=omegas, deltas=deltas, phis=phis,
+                                  pulser_lindblads=pulser_lindblads,
+                                  interaction_matrix=interaction_matrix, device=device)
+
+    def apply(self, dt, omegas, deltas, phis, full_interaction_matrix, state, krylov_tolerance,
+              pulser_lindblads):
+        from .krylov import fused_lindblad_step
+
+        ham = self.get_hamiltonian(omegas, deltas, phis, pulser_lindblads, full_interaction_matrix,
+                                   state.device)
+        out, info, st = fused_lindblad_step(ham, dt, state, krylov_tolerance, krylov_tolerance,
+                                            self.max_krylov_dim)
+        if st != _lib.OK:
+            raise RecursionError("exponentiation algorithm did not converge to precision in "
+                                 "allotted number of steps.")
+        return out, ham

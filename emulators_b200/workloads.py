@@ -25,6 +25,10 @@ Workloads (all sizes are the ones the benchmarks and parity tests use):
                      0.5 us at dt=10 ns (50 steps), Lindblad operators: relaxation
                      (rate 0.5/us, sqrt(rate)|g><r|) and dephasing (rate 1/us,
                      sqrt(rate/2) Z), complex128; the Monte Carlo stepper's workload.
+* ``lindblad_ladder_n12`` N=12 2x6 ladder, 5.5 um spacing, Omega 4, delta -10 -> 10 over
+                     0.2 us at dt=10 ns (20 steps), the noisy ladder's Lindblad operators;
+                     a 4^12 density matrix (complex128), the density-matrix stepper's
+                     workload.
 * ``ring_n16_grad``  N=16 ring of radius 10 um, 20-segment piecewise-constant Omega in
                      [0, 2 pi] and delta in [-20, 20], 64 parameter sets, 2 us at
                      dt=10 ns (200 steps, 10 steps per segment), loss = MSE between the
@@ -163,6 +167,17 @@ def noisy_ladder_n22(nsteps: int | None = None):
     c = np.sqrt(1.0 / 2)
     deph = np.array([[c, 0.0], [0.0, -c]], dtype=np.complex128)
     return w, [relax, deph]
+
+
+def lindblad_ladder_n12():
+    """(Workload, Lindblad operators as 2x2 complex arrays)."""
+    n, T, dt = 12, 0.2, 0.01
+    pos = ladder(6, 5.5)
+    t = midpoints(T, dt)
+    w = Workload("lindblad_ladder_n12", pos, interaction_matrix(pos), dt,
+                 _global(np.full_like(t, 4.0), n), _global(-10.0 + 20.0 * t / T, n),
+                 np.zeros((len(t), n)), tolerance=1e-10, precision="c128")
+    return w, noisy_ladder_n22()[1]
 
 
 def piecewise_linear(knots_t: np.ndarray, knots_v: np.ndarray, t: np.ndarray) -> np.ndarray:

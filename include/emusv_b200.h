@@ -213,6 +213,47 @@ int emusv_qubit_densities(int nqubits, int dtype, const void *psi, double *rho_d
  * emu_sv/algebra.py:28-37 (apply). */
 int emusv_apply_1q(int nqubits, int dtype, void *psi, int qubit, const double *op, void *stream);
 
+/* ---- Lindblad density-matrix path (registers up to EMUSV_MAX_QUBITS / 2 qubits) ----
+ * A density matrix is a device array of 2^N x 2^N complex amplitudes, row-major (the
+ * reference's tensor layout).  `ops` (host, nops x 8 doubles) are the 2x2 jump operators
+ * L_k, row-major with re/im interleaved; every L_k acts on every qubit. */
+
+/* out = L(rho) = Heff rho - rho Heff^dag + i sum_kq L_kq rho L_kq^dag (Heff = H -
+ * 0.5i sum L^dag L), the reference's RydbergLindbladian.__matmul__
+ * (emu_sv/lindblad_operator.py:184-211) for Hermitian rho.  out != rho. */
+int emusv_lindblad_apply(int nqubits, int dtype, const double *omegas, const double *deltas,
+                         const double *phis, const double *interaction, int nops, const double *ops,
+                         const void *rho, void *out, void *stream);
+
+/* Workspace of emusv_lindblad_arnoldi_step for `basis_capacity` stored 4^N vectors. */
+size_t emusv_lindblad_workspace_bytes(int nqubits, int dtype, int basis_capacity);
+
+/* rho_out = exp(-i dt L) rho_in by the Arnoldi step of emusv_arnoldi_step on the 4^N
+ * vector: EvolveDensityMatrix.apply (emu_sv/time_evolution/implementations.py:87-120,
+ * krylov_exp with is_hermitian=False).  Same contract and return codes as
+ * emusv_arnoldi_step (zero the workspace once; max_krylov_dim <= 100). */
+int emusv_lindblad_arnoldi_step(int nqubits, int dtype, double dt, const double *omegas,
+                                const double *deltas, const double *phis, const double *interaction,
+                                int nops, const double *ops, const void *rho_in, void *rho_out,
+                                double exp_tolerance, double norm_tolerance, int max_krylov_dim,
+                                int krylov_dim_hint, void *workspace, size_t workspace_bytes,
+                                emusv_krylov_info *info, void *stream);
+
+/* Scratch of emusv_dm_energy (two 4^N vectors and partial sums). */
+size_t emusv_dm_scratch_bytes(int nqubits, int dtype);
+
+/* result_dev[0..1] = Tr(H rho), [2..3] = Tr(H^2 rho) (device float64 [4]; H without the
+ * noise term): RydbergLindbladian.expect and the density-matrix energy moments
+ * (lindblad_operator.py:213-218, custom_callback_implementations.py:150-200). */
+int emusv_dm_energy(int nqubits, int dtype, const double *omegas, const double *deltas,
+                    const double *phis, const double *interaction, const void *rho, double *result_dev,
+                    void *scratch, size_t scratch_bytes, void *stream);
+
+/* amps[r] = sqrt(max(Re rho[r][r], 0)) (device, 2^N amplitudes of rho's dtype): the
+ * state-vector occupation / correlation reductions applied to it give Tr(rho n_i) and
+ * Tr(rho n_i n_j) (custom_callback_implementations.py:50-135, the density-matrix forms). */
+int emusv_dm_diagonal_amplitudes(int nqubits, int dtype, const void *rho, void *amps, void *stream);
+
 /* Drive preparation: out[s * out_stride + q] = PCHIP interpolant of the knots
  * (x[k], y[s * y_stride + k]), k < nknots, at xq[q], for every signal s < nsignals and
  * query q < nqueries (device float64 arrays; x strictly increasing -- the caller checks,

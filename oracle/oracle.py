@@ -604,3 +604,51 @@ def pchip(x, y, xq) -> np.ndarray:
     i = np.clip(np.searchsorted(x, xq, side="right") - 1, 0, n - 2)
     t = xq - x[i]
     return y[:-1][i] + t * (d[:-1][i] + t * (p2[i] + t * p3[i]))
+
+
+# ----------------------------------------------------------------------- Lindblad
+def _row_op(op, rho, q, n):
+    """op on the row index of qubit q (qubit 0 = most significant bit): op @ rho there."""
+    A = rho.reshape(2 ** q, 2, 2 ** (n - q - 1), 2 ** n)
+    return np.einsum("ab,ibjc->iajc", np.asarray(op, dtype=np.complex128), A).reshape(rho.shape)
+
+
+def _col_op_conj(op, rho, q, n):
+    """rho @ op^dag on the column index of qubit q."""
+    B = rho.reshape(2 ** n, 2 ** q, 2, 2 ** (n - q - 1))
+    return np.einsum("ab,kibj->kiaj", np.conj(np.asarray(op, dtype=np.complex128)), B).reshape(rho.shape)
+
+
+def lindbladian_apply(omegas, deltas, phis, U, lindblads, rho) -> np.ndarray:
+    """RydbergLindbladian @ rho, restating emu_sv/lindblad_operator.py:96-211 with the same
+    per-qubit views: Heff = H - 0.5i sum L^dag L on every qubit (H on the row index column
+    by column); res = Heff rho - (Heff rho)^dag + i sum_kq L_kq rho L_kq^dag; returns
+    0.5 (res - res^dag)."""
+    n = len(omegas)
+    rho = np.asarray(rho, dtype=np.complex128)
+    H = Hamiltonian(omegas, deltas, phis, U)
+    hr = np.stack([H.apply(np.ascontiguousarray(rho[:, c])) for c in range(rho.shape[1])], axis=1)
+    noise = noise_from_lindbladians(lindblads)
+    for q in range(n):
+        hr = hr + _row_op(noise, rho, q, n)
+    res = hr - hr.conj().T
+    for q in range(n):
+        for L in lindblads:
+            res = res + 1j * _col_op_conj(L, _row_op(L, rho, q, n), q, n)
+    return 0.5 * (res - res.conj().T)
+
+
+def lindblad_step(dt, omegas, deltas, phis, U, lindblads, rho, tol, max_krylov_dim=100):
+    """EvolveDensityMatrix.apply (emu_sv/time_evolution/implementations.py:87-120):
+    krylov_exp(-1j dt (L @ rho), is_hermitian=False) on the flattened matrix."""
+    D = np.asarray(rho).shape[0]
+
+    def op(x):
+        return -1j * dt * lindbladian_apply(omegas, deltas, phis, U, lindblads,
+                                            x.reshape(D, D)).reshape(-1)
+
+    r = krylov_exp_impl(op, np.asarray(rho).reshape(-1), False, tol, tol, max_krylov_dim)
+    if not r.converged:
+        raise RecursionError("exponentiation algorithm did not converge to precision in "
+                             "allotted number of steps.")
+    return r.result.reshape(D, D), r

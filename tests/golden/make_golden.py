@@ -15,8 +15,8 @@ so the four hot-path modules are loaded one by one behind package shells:
 * emu_sv/custom_callback_implementations.py (occupation / correlation / energy moments)
 * emu_base/math/pchip_torch.py, emu_base/math/brents_root_finding.py,
   emu_base/jump_lindblad_operators.py,
-  emu_sv/algebra.py, emu_sv/time_evolution/interface.py and implementations.py
-  (the Monte Carlo stepper)
+  emu_sv/algebra.py, emu_sv/lindblad_operator.py, emu_sv/time_evolution/interface.py and
+  implementations.py (the Monte Carlo and density-matrix steppers)
 
 ``pulser.*`` and ``pyparsing`` imports are served by a meta-path finder that fabricates
 empty placeholder classes; none of them is called on the paths exercised here.
@@ -37,6 +37,8 @@ Fixtures (inputs and reference outputs, all complex128/float64):
                        final-state probes (inner products with seeded vectors).
 * ring_n16_grad.npz    reference autograd gradient of the Neel loss for 2 parameter sets
                        of the N=16 ring over the first 2 segments (20 steps).
+* lindblad.npz         RydbergLindbladian @ rho, EvolveDensityMatrix steps and the
+                       density-matrix observables (emu_sv/lindblad_operator.py).
 * pchip.npz            PCHIP1D (emu_base/math/pchip_torch.py): the reference's test data,
                        random knots with extrapolated queries, drive-like 1 ns signals.
 * noisy.npz            the Monte Carlo path: H*psi with the noise term, Arnoldi
@@ -156,12 +158,19 @@ def load_reference(ref: str) -> dict:
     mods["pchip"] = load("emu_base.math.pchip_torch", "emu_base/math/pchip_torch.py")
     mods["jump"] = load("emu_base.jump_lindblad_operators", "emu_base/jump_lindblad_operators.py")
     mods["algebra"] = load("emu_sv.algebra", "emu_sv/algebra.py")
+    # the real Lindbladian (its package-level imports served from the loaded modules)
+    sys.modules["emu_base"].compute_noise_from_lindbladians = mods["jump"].compute_noise_from_lindbladians
+    sys.modules["emu_base"].matmul_2x2_with_batched = None  # GPU-only branch, not taken on CPU
+    mods["lindblad"] = load("emu_sv.lindblad_operator", "emu_sv/lindblad_operator.py")
+    # density matrices: the same minimal holder of ``data`` as the state vectors
+    mods["lindblad"].DensityMatrix = StateVector
     iface = load("emu_sv.time_evolution.interface", "emu_sv/time_evolution/interface.py")
     sys.modules["emu_sv.time_evolution"].BaseStepper = iface.BaseStepper
     mods["impl"] = load("emu_sv.time_evolution.implementations",
                         "emu_sv/time_evolution/implementations.py")
     mods["cb"] = load("emu_sv.custom_callback_implementations",
                       "emu_sv/custom_callback_implementations.py")
+    mods["cb"].DensityMatrix = StateVector
     return mods
 
 
@@ -671,6 +680,69 @@ def gen_pchip(R):
 
 
 GENERATORS["pchip"] = gen_pchip
+
+
+def gen_lindblad(R):
+    """RydbergLindbladian @ rho (n = 3, 4, 5; real and complex drives), EvolveDensityMatrix
+    steps (n = 4, 12 steps of 50 ns) and the density-matrix observables of the final state."""
+    Lop = R["lindblad"].RydbergLindbladian
+    cb = R["cb"]
+    ops = _lindblads(R, scale=2.0)
+    out = {"nops": np.array(len(ops))}
+    for k, L in enumerate(ops):
+        out[f"L{k}"] = np_(L)
+
+    def rand_rho(n, seed):
+        g = torch.Generator().manual_seed(seed)
+        a = torch.randn(2 ** n, 3, dtype=torch.complex128, generator=g)
+        r = a @ a.mH
+        return r / torch.trace(r).real
+
+    for k, (n, wp) in enumerate([(3, False), (4, True), (5, False)]):
+        torch.manual_seed(300 + k)
+        p = get_randn_ham_params(n, wp)
+        rho = rand_rho(n, 400 + k)
+        L = Lop(*p[:3], ops, p[3], device="cpu")
+        pre = f"c{k}_"
+        for nm, v in zip(["omegas", "deltas", "phis", "U"], p):
+            out[pre + nm] = np_(v)
+        out[pre + "rho"] = np_(rho)
+        out[pre + "Lrho"] = np_(L @ rho.clone())
+        out[pre + "energy"] = np_(L.expect(StateVector(rho.clone())))
+    out["count"] = np.array(3)
+    # EvolveDensityMatrix: N=4 chain, time-dependent drive
+    n, dt, nsteps = 4, 0.05, 12
+    U = torch.as_tensor(wl.interaction_matrix(wl.chain(n, 6.0)))
+    stepper = R["impl"].EvolveDensityMatrix(100)
+    rho = torch.zeros(2 ** n, 2 ** n, dtype=torch.complex128)
+    rho[0, 0] = 1.0
+    snaps = []
+    for k in range(nsteps):
+        om = torch.full((n,), 2 * np.pi * (0.6 + 0.4 * np.sin(0.5 * k)), dtype=torch.float64)
+        de = torch.full((n,), -3.0 + 0.5 * k, dtype=torch.float64)
+        ph = torch.full((n,), 0.1 * k, dtype=torch.float64)
+        rho, ham = stepper.apply(dt, om, de, ph, U, rho, 1e-10, ops)
+        if (k + 1) % 4 == 0:
+            snaps.append(np_(rho).copy())
+    out["ev_states"] = np.stack(snaps)
+    out["ev_n"] = np.array(n)
+    out["ev_dt"] = np.array(dt)
+    out["ev_nsteps"] = np.array(nsteps)
+    out["ev_U"] = np_(U)
+    st = StateVector(rho.clone())
+    out["ev_occupation"] = np_(cb.qubit_occupation_sv_den_mat_impl(None, config=None, state=st,
+                                                                    hamiltonian=None))
+    out["ev_correlation"] = np_(cb.correlation_matrix_sv_den_mat_impl(None, config=None, state=st,
+                                                                       hamiltonian=None))
+    out["ev_energy"] = np_(ham.expect(st))
+    out["ev_variance"] = np_(cb.energy_variance_sv_den_mat_impl(None, config=None, state=st,
+                                                                 hamiltonian=ham))
+    out["ev_second_moment"] = np_(cb.energy_second_moment_den_mat_impl(None, config=None, state=st,
+                                                                        hamiltonian=ham))
+    return out
+
+
+GENERATORS["lindblad"] = gen_lindblad
 
 
 def main():

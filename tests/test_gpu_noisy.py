@@ -172,7 +172,8 @@ def test_monte_carlo_steps_match_reference():
 
 def test_backend_runs_monte_carlo_solver():
     """SVBackendImpl picks the Monte Carlo stepper for Lindblad operators with
-    solver='montecarlo' (sv_backend_impl.py:82-95) and keeps the state's norm <= 1."""
+    solver='montecarlo' and the density-matrix stepper with solver='lindblad'
+    (sv_backend_impl.py:82-95); the Monte Carlo state's norm stays <= 1."""
     from emulators_b200 import workloads as wl
     from emulators_b200.sv_backend import SequenceData, SVBackendImpl, SVConfig
     from emulators_b200.time_evolution import EvolveMonteCarlo
@@ -188,5 +189,6 @@ def test_backend_runs_monte_carlo_solver():
         impl.step(k)
     nrm = float(torch.linalg.vector_norm(impl.state.data))
     assert 0.0 < nrm <= 1.0 + 1e-12
-    with pytest.raises(NotImplementedError):
-        SVBackendImpl(SVConfig(solver="lindblad"), data)
+    from emulators_b200.time_evolution import EvolveDensityMatrix
+
+    assert isinstance(SVBackendImpl(SVConfig(solver="lindblad"), data).stepper, EvolveDensityMatrix)
