@@ -77,6 +77,26 @@ static bool make_lindblad_params(int n, const double *omegas, const double *delt
     return true;
 }
 
+// noise = -0.5i sum_k L_k^dag L_k (emu_base/jump_lindblad_operators.py:79-93), 8 doubles
+static void noise_term(int nops, const double *ops, double *noise) {
+    for (int e = 0; e < 8; ++e) noise[e] = 0.0;
+    for (int k = 0; k < nops; ++k) {
+        const double *L = ops + 8 * k;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                double re = 0.0, im = 0.0;  // (L^dag L)[a][b] = sum_c conj(L[c][a]) L[c][b]
+                for (int c = 0; c < 2; ++c) {
+                    const double xr = L[(2 * c + a) * 2], xi = -L[(2 * c + a) * 2 + 1];
+                    const double yr = L[(2 * c + b) * 2], yi = L[(2 * c + b) * 2 + 1];
+                    re += xr * yr - xi * yi;
+                    im += xr * yi + xi * yr;
+                }
+                noise[(2 * a + b) * 2] += 0.5 * im;  // -0.5i (re + i im)
+                noise[(2 * a + b) * 2 + 1] += -0.5 * re;
+            }
+    }
+}
+
 static bool make_jumps(int n, int nops, const double *ops, LindbladJumps *J) {
     memset(J, 0, sizeof(*J));
     J->nq = n;
@@ -215,23 +235,9 @@ int emusv_lindblad_apply(int nqubits, int dtype, const double *omegas, const dou
                          const void *rho, void *out, void *stream) {
     HamParams P;
     LindbladJumps J;
-    double noise[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double noise[8];
     if (!rho || !out || rho == out || nops < 0 || (nops > 0 && !ops)) return EMUSV_BAD_ARGUMENT;
-    for (int k = 0; k < nops; ++k) {  // -0.5i sum L^dag L
-        const double *L = ops + 8 * k;
-        for (int a = 0; a < 2; ++a)
-            for (int b = 0; b < 2; ++b) {
-                double re = 0.0, im = 0.0;  // (L^dag L)[a][b] = sum_c conj(L[c][a]) L[c][b]
-                for (int c = 0; c < 2; ++c) {
-                    const double xr = L[(2 * c + a) * 2], xi = -L[(2 * c + a) * 2 + 1];
-                    const double yr = L[(2 * c + b) * 2], yi = L[(2 * c + b) * 2 + 1];
-                    re += xr * yr - xi * yi;
-                    im += xr * yi + xi * yr;
-                }
-                noise[(2 * a + b) * 2] += 0.5 * im;  // -0.5i (re + i im)
-                noise[(2 * a + b) * 2 + 1] += -0.5 * re;
-            }
-    }
+    noise_term(nops, ops, noise);
     if (!make_lindblad_params(nqubits, omegas, deltas, phis, interaction, nops ? noise : nullptr, false, &P) ||
         !make_jumps(nqubits, nops, ops, &J))
         return EMUSV_BAD_ARGUMENT;
@@ -261,23 +267,9 @@ int emusv_lindblad_arnoldi_step(int nqubits, int dtype, double dt, const double 
                                 emusv_krylov_info *info, void *stream) {
     HamParams P;
     LindbladJumps J;
-    double noise[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double noise[8];
     if (nops < 0 || (nops > 0 && !ops)) return EMUSV_BAD_ARGUMENT;
-    for (int k = 0; k < nops; ++k) {
-        const double *L = ops + 8 * k;
-        for (int a = 0; a < 2; ++a)
-            for (int b = 0; b < 2; ++b) {
-                double re = 0.0, im = 0.0;
-                for (int c = 0; c < 2; ++c) {
-                    const double xr = L[(2 * c + a) * 2], xi = -L[(2 * c + a) * 2 + 1];
-                    const double yr = L[(2 * c + b) * 2], yi = L[(2 * c + b) * 2 + 1];
-                    re += xr * yr - xi * yi;
-                    im += xr * yi + xi * yr;
-                }
-                noise[(2 * a + b) * 2] += 0.5 * im;
-                noise[(2 * a + b) * 2 + 1] += -0.5 * re;
-            }
-    }
+    noise_term(nops, ops, noise);
     if (!make_lindblad_params(nqubits, omegas, deltas, phis, interaction, nops ? noise : nullptr, false, &P) ||
         !make_jumps(nqubits, nops, ops, &J))
         return EMUSV_BAD_ARGUMENT;
