@@ -662,26 +662,21 @@ def noisy_mc(dev, steps: int = 20, cpu_seconds: float = 10.0) -> dict:
     L.emusv_profile_begin(1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    its, r2 = [], 0
+    its = []
     for k in range(3, 3 + steps):
         s, info, st = fused_arnoldi_step(HamiltonianExpOperator(ham(k), w.dt), s, 1e-10, 1e-10, 100)
         _lib.check(st, "arnoldi")
         its.append(info.iterations)
-        r2 += info.second_rounds
     e1.record()
     torch.cuda.synchronize()
     el = e0.elapsed_time(e1) / 1e3
     pms = np.zeros(8)
     pl = np.zeros(8, dtype=np.int64)
     L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
-    # algorithmic bytes of the Gram-Schmidt passes of iteration j (every vector once per
-    # pass): dots (j+2) reads, update (j+2) reads + 1 write; a second round adds the
-    # re-read of v_0..v_j in the update pass (j+1) and the second update (j+2) reads + 1
-    # write, i.e. 2j+4 units, taken at the mean j of the steps
-    first = sum(sum(2 * (j + 2) + 1 for j in range(m)) for m in its)
-    jm = float(np.mean([(m - 1) / 2 for m in its]))
-    second = r2 * (2 * jm + 4)
-    ortho_bytes = (first + second) * D * es
+    # algorithmic bytes of the two Gram-Schmidt passes of iteration j (every vector once
+    # per pass): dots over w, v~_j and v_0..v_{j-1} (j+2 reads), update (j+2 reads, w' and
+    # the corrected v_j written)
+    ortho_bytes = sum(sum(2 * (max(j, 1) + 2) + 2 for j in range(m)) for m in its) * D * es
     hbm, which = peaks()
     kinds = ["hpsi_pass_low", "orth", "small", "combine", "obs", "adjoint", "batch", "hpsi_pass_high"]
     tot = pms.sum()
@@ -722,9 +717,8 @@ def noisy_mc(dev, steps: int = 20, cpu_seconds: float = 10.0) -> dict:
             "kernel_time_shares": {kinds[i]: round(pms[i] / tot, 4) for i in range(8) if pl[i]},
             "gram_schmidt": {"algorithmic_bytes_per_step": int(ortho_bytes / steps),
                              "GB/s": round(ortho_gbs, 1), "frac": round(ortho_gbs / hbm, 4),
-                             "second_rounds_per_step": round(r2 / steps, 2),
-                             "note": "two streaming passes per iteration over w and v_0..v_j, "
-                                     "two more in iterations that take a second round"},
+                             "note": "two streaming passes per iteration over w and the "
+                                     "basis, the second Gram-Schmidt round lagged into them"},
             "monte_carlo_steps_per_s": round(steps / el_mc, 2),
             "monte_carlo_jumps": jumps,
             "monte_carlo_first_threshold": round(thr0, 6),

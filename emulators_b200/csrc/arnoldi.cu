@@ -4,19 +4,15 @@
 // krylov_exp.py:23-106 with is_hermitian=False).
 //
 // Per iteration j (basis vectors stored unnormalised with FP64 scales, as in krylov.cu):
-//   1. w = (H - sigma) v_j by the streaming H*psi kernels (noise diagonal fused into pass
+//   1. w = (H - sigma) v~_j by the streaming H*psi kernels (noise diagonal fused into pass
 //      L; sigma = the previous step's energy, as in the Lanczos step: same basis, T minus
 //      sigma on its diagonal, added back in every exponential);
-//   2. k_arn_ortho<DOTS>:    h_k = <v_k, w> for all k <= j and ||w|| in one pass;
-//   3. k_arn_ortho<UPDATE_DOTS>: w' = w - sum h_k v_k (and, for a second round, the dots
-//      g_k = <v_k, w'>) in one pass;
-//   4. k_arn_ortho<UPDATE>:  w'' = w' - sum g_k v_k and ||w''|| (second round only).
-//   Classical Gram-Schmidt, repeated when the first round removed more than half of
-//   ||w||^2 (the DGKS test): the same Hessenberg column T[k][j] = h_k (+ g_k) and vector as
-//   the reference's modified Gram-Schmidt (krylov_exp.py:54-58) in exact arithmetic, in two
-//   or three streaming passes instead of 2(j+1) dependent dot/axpy pairs.  The shift keeps
-//   ||(H - sigma) v_j|| near the spread of the spectrum, so the second round is rare.
-//   5. k_arn_decide (one CTA, FP64): ||w''||, the happy-breakdown test (krylov_exp.py:
+//   2. two Gram-Schmidt passes with the second round of v~_j lagged into them (see
+//      k_arn_lagdots below): the same Hessenberg matrix and basis as the reference's
+//      modified Gram-Schmidt (krylov_exp.py:54-58) in exact arithmetic, every vector
+//      orthogonalised twice, in two streaming passes instead of 2(j+1) dependent dot/axpy
+//      pairs;
+//   3. k_arn_decide (one CTA, FP64): ||w'||, the happy-breakdown test (krylov_exp.py:
 //   63-71) at every iteration, and from the host's hint on the exponential of the extended
 //   Hessenberg matrix and the Expokit error estimate (krylov_exp.py:76-86); when the first
 //   tested iteration already converges, the untested earlier ones are tested in order.
@@ -40,198 +36,254 @@ int arnoldi_run(const HamParams &P, const LindbladJumps *J, int dtype, double dt
 
 constexpr int ARN_KMAX = 100;                  // largest Arnoldi max_krylov_dim
 constexpr int ARN_M = ARN_KMAX + 2;            // largest extended matrix
-constexpr int ARN_PS = 2 * (ARN_KMAX + 1) + 2;  // partial-row stride: dots re/im, norm
-constexpr int ARN_NORM = 2 * (ARN_KMAX + 1);   // norm slot of a partial row
+constexpr int ARN_KA = ARN_KMAX + 1;           // finalised basis vectors at most
+// partial row of a pass: z_k = <v_k, w> (re, im), s_k = <v_k, vt>, a = <vt, w>, ||w||^2,
+// ||vt||^2 (pass A); pass B writes its norm at ARN_NORM
+constexpr int ARN_S0 = 2 * ARN_KA, ARN_A0 = 4 * ARN_KA, ARN_NORM = ARN_A0 + 2;
+constexpr int ARN_PS = ARN_A0 + 4;
 constexpr int ORTHO_THREADS = 256;
 constexpr int DECIDE_THREADS = 256;
 
 struct ArnState {
     double2 T[ARN_M * ARN_M];  // Hessenberg matrix of H - sigma (row-major [r][c]), basis v_k
-    double2 coef[ARN_M];       // coefficients of the next Gram-Schmidt update
-    int reorth;                // this iteration takes the second Gram-Schmidt round
-    int rounds2;               // second rounds taken in this run
+    double2 cw1[ARN_M];        // pass B: w' = cw w - ct vt - sum cw1_l v_l
+    double2 cvj[ARN_M];        //         v_j = cv vt - sum cvj_l v_l
+    double2 ct;
+    double cw, cv;
 };
 
-// Pass A: dots.  Pass B: update with h; with reorth also the dots of the result.  Pass C:
-// update with the second round's coefficients (returns at once without reorth).
-enum ArnMode { ARN_DOTS = 0, ARN_UPDATE_DOTS = 1, ARN_UPDATE = 2 };
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-// One streaming pass over w and v_0..v_j (see the header).  Partials per block:
-// [2k], [2k+1] = <v_k, w_out> (DOTS, UPDATE_DOTS), [ARN_NORM] = ||w_out||^2.
-// E amplitudes per thread per chunk.  UPDATE_DOTS reads every v_k twice per chunk (the
-// update needs all of them before the dots of the result).
-template <typename R, int MODE, int E, int KB = 4>
+// The orthogonalisation is classical Gram-Schmidt with its second round lagged by one
+// iteration (the low-synchronisation "DCGS2" form): iteration j receives w = (H - sigma) vt
+// for the not yet reorthogonalised vt = v~_j, and
+//   pass A (k_arn_lagdots): one pass over w, vt and the final v_0..v_{j-1}: z = V^H w,
+//     s = V^H vt, <vt, w>, ||w||^2, ||vt||^2;
+//   k_arn_lagstage: v_j = (vt - V s) / alpha (alpha^2 = ||vt||^2 - |s|^2) corrects the
+//     previous Hessenberg column (T[:, j-1] += beta s, T[j][j-1] = beta alpha), H v_j =
+//     (w - V_j T s) / alpha by the Arnoldi relation, h = V_j^H H v_j from z, s and T;
+//   pass B (k_arn_lagupdate): w' = H v_j - V_j h and the corrected v_j in one pass (both
+//     combinations of w, vt and V), ||w'||^2.
+// Two streaming passes per iteration; every basis vector but the newest is orthogonalised
+// twice, as in classical Gram-Schmidt with reorthogonalisation.
+template <typename R, int E = 4, int KB = 4>
 __global__ void __launch_bounds__(ORTHO_THREADS)
-k_arn_ortho(const KState *ks, const ArnState *as, int j, const void *v0_, const unsigned char *basis,
-            i64 D, void *w_, double *part) {
+k_arn_lagdots(const KState *ks, int j, const void *v0_, const unsigned char *basis, i64 D,
+              const void *w_, double *part) {
     typedef typename cvec<R>::T C;
     if (ks->status != KS_RUNNING) return;
-    const bool reorth = as->reorth != 0;
-    if (MODE == ARN_UPDATE && !reorth) return;
-    const bool dots = MODE == ARN_DOTS || (MODE == ARN_UPDATE_DOTS && reorth);
     constexpr int NW = ORTHO_THREADS / 32;
-    __shared__ double2 cf[ARN_M];
     __shared__ double sc[ARN_M];
-    __shared__ double2 sacc[NW][ARN_KMAX + 1];
-    __shared__ double snorm[NW];
-    const int nk = j + 1;
+    __shared__ double2 accz[NW][ARN_KA], accs[NW][ARN_KA];
+    __shared__ double sa[NW][4];
+    const bool has_vt = j >= 1;
+    const int nk = has_vt ? j : 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < nk; k += ORTHO_THREADS) {
-        sc[k] = ks->scale[k];
-        const double2 c = as->coef[k];
-        cf[k] = make_double2(c.x * ks->scale[k], c.y * ks->scale[k]);
+    for (int k = tid; k < nk; k += ORTHO_THREADS) sc[k] = ks->scale[k];
+    for (int k = tid; k < NW * ARN_KA; k += ORTHO_THREADS) {
+        (&accz[0][0])[k] = make_double2(0.0, 0.0);
+        (&accs[0][0])[k] = make_double2(0.0, 0.0);
     }
-    for (int k = tid; k < NW * (ARN_KMAX + 1); k += ORTHO_THREADS)
-        (&sacc[0][0])[k] = make_double2(0.0, 0.0);
+    const double st = has_vt ? ks->scale[j] : 0.0;
     __syncthreads();
     const C *v0 = reinterpret_cast<const C *>(v0_);
     const C *bs = reinterpret_cast<const C *>(basis);
-    C *w = reinterpret_cast<C *>(w_);
+    const C *w = reinterpret_cast<const C *>(w_);
+    const C *vt = has_vt ? bs + (i64)j * D : nullptr;
     auto vk = [&](int k) -> const C * { return k == 0 ? v0 : bs + (i64)k * D; };
-    double nacc = 0.0;
+    double nw = 0.0, nv = 0.0, ar = 0.0, ai = 0.0;
     const i64 CH = (i64)ORTHO_THREADS * E;
     for (i64 c0 = (i64)blockIdx.x * CH; c0 < D; c0 += (i64)gridDim.x * CH) {
-        double wr[E], wi[E];
+        double wr[E], wi[E], tr[E], ti[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
-            wr[e] = wi[e] = 0.0;
+            wr[e] = wi[e] = tr[e] = ti[e] = 0.0;
             if (x < D) {
                 const C a = w[x];
                 wr[e] = double(a.x);
                 wi[e] = double(a.y);
-            }
-        }
-        if (MODE != ARN_DOTS) {
-            // KB vectors per step: KB * E independent loads in flight per thread
-            int k = 0;
-            for (; k + KB <= nk; k += KB) {
-                C a[KB][E];
-#pragma unroll
-                for (int kb = 0; kb < KB; ++kb)
-#pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
-                        a[kb][e] = x < D ? vk(k + kb)[x] : cmake<C>(0.0, 0.0);
-                    }
-#pragma unroll
-                for (int kb = 0; kb < KB; ++kb) {
-                    const double2 c = cf[k + kb];
-#pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        wr[e] -= c.x * double(a[kb][e].x) - c.y * double(a[kb][e].y);
-                        wi[e] -= c.x * double(a[kb][e].y) + c.y * double(a[kb][e].x);
-                    }
+                if (has_vt) {
+                    const C b = vt[x];
+                    tr[e] = st * double(b.x);
+                    ti[e] = st * double(b.y);
                 }
             }
-            for (; k < nk; ++k) {
-                const C *v = vk(k);
-                const double2 c = cf[k];
+            nw += wr[e] * wr[e] + wi[e] * wi[e];
+            nv += tr[e] * tr[e] + ti[e] * ti[e];
+            ar += tr[e] * wr[e] + ti[e] * wi[e];
+            ai += tr[e] * wi[e] - ti[e] * wr[e];
+        }
+        int k = 0;
+        for (; k < nk; k += KB) {
+            C a[KB][E];
+#pragma unroll
+            for (int kb = 0; kb < KB; ++kb)
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
                     const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
-                    if (x < D) {
-                        const C a = v[x];
-                        wr[e] -= c.x * double(a.x) - c.y * double(a.y);
-                        wi[e] -= c.x * double(a.y) + c.y * double(a.x);
-                    }
+                    a[kb][e] = (k + kb < nk && x < D) ? vk(k + kb)[x] : cmake<C>(0.0, 0.0);
+                }
+            double zr[KB], zi[KB], sr[KB], si[KB];
+#pragma unroll
+            for (int kb = 0; kb < KB; ++kb) {
+                zr[kb] = zi[kb] = sr[kb] = si[kb] = 0.0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const double px = double(a[kb][e].x), py = double(a[kb][e].y);
+                    zr[kb] += px * wr[e] + py * wi[e];
+                    zi[kb] += px * wi[e] - py * wr[e];
+                    sr[kb] += px * tr[e] + py * ti[e];
+                    si[kb] += px * ti[e] - py * tr[e];
                 }
             }
 #pragma unroll
-            for (int e = 0; e < E; ++e) {  // store, and continue with the stored (rounded) values
-                const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
-                if (x < D) {
-                    const C o = cmake<C>(wr[e], wi[e]);
-                    w[x] = o;
-                    wr[e] = double(o.x);
-                    wi[e] = double(o.y);
+            for (int kb = 0; kb < KB; ++kb) {
+                zr[kb] = warp_sum(zr[kb]);
+                zi[kb] = warp_sum(zi[kb]);
+                if (has_vt) {
+                    sr[kb] = warp_sum(sr[kb]);
+                    si[kb] = warp_sum(si[kb]);
+                }
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int kb = 0; kb < KB; ++kb) {
+                    if (k + kb >= nk) break;
+                    accz[warp][k + kb].x += zr[kb];
+                    accz[warp][k + kb].y += zi[kb];
+                    accs[warp][k + kb].x += sr[kb];
+                    accs[warp][k + kb].y += si[kb];
+                }
+            }
+        }
+    }
+    nw = warp_sum(nw);
+    nv = warp_sum(nv);
+    ar = warp_sum(ar);
+    ai = warp_sum(ai);
+    if (lane == 0) {
+        sa[warp][0] = ar;
+        sa[warp][1] = ai;
+        sa[warp][2] = nw;
+        sa[warp][3] = nv;
+    }
+    __syncthreads();
+    double *row = part + (i64)blockIdx.x * ARN_PS;
+    for (int k = tid; k < nk; k += ORTHO_THREADS) {
+        double2 z = make_double2(0.0, 0.0), q = make_double2(0.0, 0.0);
+        for (int u = 0; u < NW; ++u) {
+            z.x += accz[u][k].x;
+            z.y += accz[u][k].y;
+            q.x += accs[u][k].x;
+            q.y += accs[u][k].y;
+        }
+        row[2 * k] = sc[k] * z.x;
+        row[2 * k + 1] = sc[k] * z.y;
+        row[ARN_S0 + 2 * k] = sc[k] * q.x;
+        row[ARN_S0 + 2 * k + 1] = sc[k] * q.y;
+    }
+    if (tid < 4) {
+        double t = 0.0;
+        for (int u = 0; u < NW; ++u) t += sa[u][tid];
+        row[ARN_A0 + tid] = t;
+    }
+}
+
+// Pass B: w' = cw w - ct vt - sum cw1_l v_l (in place over w) and, for j >= 1, the
+// corrected v_j = cv vt - sum cvj_l v_l (in place over vt, stored with scale 1); ||w'||^2.
+template <typename R, int E = 4, int KB = 4>
+__global__ void __launch_bounds__(ORTHO_THREADS)
+k_arn_lagupdate(const KState *ks, const ArnState *as, int j, const void *v0_, unsigned char *basis,
+                i64 D, void *w_, double *part) {
+    typedef typename cvec<R>::T C;
+    if (ks->status != KS_RUNNING) return;
+    constexpr int NW = ORTHO_THREADS / 32;
+    __shared__ double2 c1[ARN_M], c2[ARN_M];
+    __shared__ double snorm[NW];
+    const bool has_vt = j >= 1;
+    const int nk = has_vt ? j : 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k = tid; k < nk; k += ORTHO_THREADS) {
+        const double sk = ks->scale[k];
+        c1[k] = make_double2(as->cw1[k].x * sk, as->cw1[k].y * sk);
+        c2[k] = make_double2(as->cvj[k].x * sk, as->cvj[k].y * sk);
+    }
+    const double st = has_vt ? ks->scale[j] : 0.0;
+    const double cw = as->cw, cv = as->cv * st;
+    const double2 ct = make_double2(as->ct.x * st, as->ct.y * st);
+    __syncthreads();
+    const C *v0 = reinterpret_cast<const C *>(v0_);
+    C *bs = reinterpret_cast<C *>(basis);
+    C *w = reinterpret_cast<C *>(w_);
+    C *vt = has_vt ? bs + (i64)j * D : nullptr;
+    auto vk = [&](int k) -> const C * { return k == 0 ? v0 : bs + (i64)k * D; };
+    double nacc = 0.0;
+    const i64 CH = (i64)ORTHO_THREADS * E;
+    for (i64 c0 = (i64)blockIdx.x * CH; c0 < D; c0 += (i64)gridDim.x * CH) {
+        double ur[E], ui[E], qr[E], qi[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
+            ur[e] = ui[e] = qr[e] = qi[e] = 0.0;
+            if (x < D) {
+                const C a = w[x];
+                ur[e] = cw * double(a.x);
+                ui[e] = cw * double(a.y);
+                if (has_vt) {
+                    const C b = vt[x];
+                    const double bx = double(b.x), by = double(b.y);
+                    ur[e] -= ct.x * bx - ct.y * by;
+                    ui[e] -= ct.x * by + ct.y * bx;
+                    qr[e] = cv * bx;
+                    qi[e] = cv * by;
+                }
+            }
+        }
+        int k = 0;
+        for (; k < nk; k += KB) {
+            C a[KB][E];
+#pragma unroll
+            for (int kb = 0; kb < KB; ++kb)
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
+                    a[kb][e] = (k + kb < nk && x < D) ? vk(k + kb)[x] : cmake<C>(0.0, 0.0);
+                }
+#pragma unroll
+            for (int kb = 0; kb < KB; ++kb) {
+                if (k + kb >= nk) break;
+                const double2 p1 = c1[k + kb], p2 = c2[k + kb];
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const double px = double(a[kb][e].x), py = double(a[kb][e].y);
+                    ur[e] -= p1.x * px - p1.y * py;
+                    ui[e] -= p1.x * py + p1.y * px;
+                    qr[e] -= p2.x * px - p2.y * py;
+                    qi[e] -= p2.x * py + p2.y * px;
                 }
             }
         }
 #pragma unroll
-        for (int e = 0; e < E; ++e) nacc += wr[e] * wr[e] + wi[e] * wi[e];
-        if (dots) {
-            int k = 0;
-            for (; k + KB <= nk; k += KB) {
-                C a[KB][E];
-#pragma unroll
-                for (int kb = 0; kb < KB; ++kb)
-#pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
-                        a[kb][e] = x < D ? vk(k + kb)[x] : cmake<C>(0.0, 0.0);
-                    }
-                double dr[KB], di[KB];
-#pragma unroll
-                for (int kb = 0; kb < KB; ++kb) {
-                    dr[kb] = di[kb] = 0.0;
-#pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        dr[kb] += double(a[kb][e].x) * wr[e] + double(a[kb][e].y) * wi[e];
-                        di[kb] += double(a[kb][e].x) * wi[e] - double(a[kb][e].y) * wr[e];
-                    }
-                }
-#pragma unroll
-                for (int kb = 0; kb < KB; ++kb) {
-                    dr[kb] = warp_sum(dr[kb]);
-                    di[kb] = warp_sum(di[kb]);
-                }
-                if (lane == 0) {
-#pragma unroll
-                    for (int kb = 0; kb < KB; ++kb) {
-                        sacc[warp][k + kb].x += dr[kb];
-                        sacc[warp][k + kb].y += di[kb];
-                    }
-                }
-            }
-            for (; k < nk; ++k) {
-                const C *v = vk(k);
-                double dr = 0.0, di = 0.0;  // sum conj(v) w
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
-                    if (x < D) {
-                        const C a = v[x];
-                        dr += double(a.x) * wr[e] + double(a.y) * wi[e];
-                        di += double(a.x) * wi[e] - double(a.y) * wr[e];
-                    }
-                }
-                dr = warp_sum(dr);
-                di = warp_sum(di);
-                if (lane == 0) {
-                    sacc[warp][k].x += dr;
-                    sacc[warp][k].y += di;
-                }
+        for (int e = 0; e < E; ++e) {
+            const i64 x = c0 + tid + (i64)e * ORTHO_THREADS;
+            if (x < D) {
+                const C o = cmake<C>(ur[e], ui[e]);
+                w[x] = o;
+                nacc += double(o.x) * double(o.x) + double(o.y) * double(o.y);
+                if (has_vt) vt[x] = cmake<C>(qr[e], qi[e]);
             }
         }
     }
     nacc = warp_sum(nacc);
     if (lane == 0) snorm[warp] = nacc;
     __syncthreads();
-    double *row = part + (i64)blockIdx.x * ARN_PS;
-    if (dots) {
-        for (int k = tid; k < nk; k += ORTHO_THREADS) {
-            double2 t = make_double2(0.0, 0.0);
-            for (int q = 0; q < NW; ++q) {
-                t.x += sacc[q][k].x;
-                t.y += sacc[q][k].y;
-            }
-            row[2 * k] = sc[k] * t.x;
-            row[2 * k + 1] = sc[k] * t.y;
-        }
-    }
     if (tid == 0) {
         double t = 0.0;
-        for (int q = 0; q < NW; ++q) t += snorm[q];
-        row[ARN_NORM] = t;
+        for (int u = 0; u < NW; ++u) t += snorm[u];
+        part[(i64)blockIdx.x * ARN_PS + ARN_NORM] = t;
     }
 }
 
-// Sum of value i of the ortho partial rows over nb blocks by one warp (lanes stride over
+// Sum of value i of the pass partial rows over nb blocks by one warp (lanes stride over
 // the blocks, then a fixed shuffle tree: deterministic).  Result in every lane.
 __device__ __forceinline__ double arn_sum_warp(const double *part, int nb, int i) {
     double t = 0.0;
@@ -239,51 +291,120 @@ __device__ __forceinline__ double arn_sum_warp(const double *part, int nb, int i
     return warp_sum(t);
 }
 
-// After the DOTS (stage 0) or UPDATE_DOTS (stage 1) pass: column j of T and the next
-// update's coefficients; stage 0 also records ||H v_j|| (krylov_exp.py:52).
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // conj(a) b
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
+// After pass A of iteration j: the lagged correction of v_j and of column j-1, column j of
+// T, ||H v_j|| (krylov_exp.py:52), and pass B's coefficients (see the pass comments).
 __global__ void __launch_bounds__(DECIDE_THREADS)
-k_arn_stage(KState *ks, ArnState *as, int j, const double *part, int nb, int stage) {
+k_arn_lagstage(KState *ks, ArnState *as, int j, const double *part, int nb) {
     if (ks->status != KS_RUNNING) return;
-    if (stage == 1 && !as->reorth) return;
+    __shared__ double2 zs[ARN_M], ss[ARN_M], hs[ARN_M], cc[ARN_M];
+    __shared__ double sa[4];
+    __shared__ double salpha;
     __shared__ int bad;
-    __shared__ double hsq[DECIDE_THREADS / 32];
-    if (threadIdx.x == 0) bad = 0;
-    if (threadIdx.x < DECIDE_THREADS / 32) hsq[threadIdx.x] = 0.0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NWD = DECIDE_THREADS / 32;
-    for (int k = warp; k <= j; k += NWD) {  // one warp per column entry
-        const double2 h = make_double2(arn_sum_warp(part, nb, 2 * k), arn_sum_warp(part, nb, 2 * k + 1));
+    const bool has_vt = j >= 1;
+    const int nk = has_vt ? j : 1;
+    if (tid == 0) bad = 0;
+    for (int k = warp; k < nk; k += NWD) {  // one warp per value
+        const double2 z = make_double2(arn_sum_warp(part, nb, 2 * k), arn_sum_warp(part, nb, 2 * k + 1));
+        const double2 q = make_double2(arn_sum_warp(part, nb, ARN_S0 + 2 * k),
+                                       arn_sum_warp(part, nb, ARN_S0 + 2 * k + 1));
         if (lane == 0) {
-            if (!isfinite(h.x) || !isfinite(h.y)) bad = 1;
-            double2 &t = as->T[k * ARN_M + j];
-            t = stage == 0 ? h : make_double2(t.x + h.x, t.y + h.y);
-            as->coef[k] = h;
-            hsq[warp] += h.x * h.x + h.y * h.y;
-            if (stage == 0 && k == j) ks->a_re[j] = h.x;  // Re <v_j, (H - sigma) v_j>
+            zs[k] = z;
+            ss[k] = has_vt ? q : make_double2(0.0, 0.0);
+        }
+    }
+    if (warp == NWD - 1) {
+        for (int i = 0; i < 4; ++i) {
+            const double v = arn_sum_warp(part, nb, ARN_A0 + i);
+            if (lane == 0) sa[i] = v;
         }
     }
     __syncthreads();
-    if (stage == 0 && warp == 0) {
-        const double n2 = arn_sum_warp(part, nb, ARN_NORM);  // ||(H - sigma) v_j||^2
-        if (lane == 0) {
-            double hs = 0.0;
-            for (int q = 0; q < DECIDE_THREADS / 32; ++q) hs += hsq[q];
-            // ||H v_j|| (krylov_exp.py:52) from the shifted product
-            const double sg = ks->shift;
-            ks->hn[j] = sqrt(fmax(0.0, n2 + 2.0 * sg * ks->a_re[j] + sg * sg));
-            // second round unless the projection kept more than half of ||w||^2 (Daniel,
-            // Gragg, Kaufman and Stewart's test with eta = 1/sqrt(2)); ||w'||^2 is taken as
-            // ||w||^2 - sum |h_k|^2, the exact value for an orthonormal basis
-            as->reorth = !(n2 - hs > 0.5 * n2);
-            as->rounds2 = (j == 0 ? 0 : as->rounds2) + as->reorth;
-            if (!isfinite(n2)) bad = 1;
+    if (tid == 0) {
+        double alpha = 1.0;
+        if (has_vt) {
+            double s2 = 0.0;
+            for (int k = 0; k < nk; ++k) s2 += ss[k].x * ss[k].x + ss[k].y * ss[k].y;
+            const double a2 = sa[3] - s2;  // ||vt||^2 - |V^H vt|^2
+            alpha = a2 > 0.0 ? sqrt(a2) : 0.0;
+            if (!(alpha > 0.0) || !isfinite(alpha)) bad = 1;
+            const double beta = ks->r[j - 1];
+            for (int l = 0; l < j; ++l) {  // column j-1: w'_{j-1} = beta (alpha v_j + V s)
+                double2 &t = as->T[l * ARN_M + (j - 1)];
+                t.x += beta * ss[l].x;
+                t.y += beta * ss[l].y;
+            }
+            as->T[j * ARN_M + (j - 1)] = make_double2(beta * alpha, 0.0);
+            ks->r[j - 1] = beta * alpha;
+        }
+        salpha = alpha;
+    }
+    __syncthreads();
+    const double alpha = salpha;
+    // (T s)_l for l <= j over the columns k < j (Hessenberg rows: k >= l - 1)
+    for (int l = tid; l <= j; l += DECIDE_THREADS) {
+        double2 acc = make_double2(0.0, 0.0);
+        if (has_vt)
+            for (int k = l > 0 ? l - 1 : 0; k < j; ++k) {
+                const double2 t = as->T[l * ARN_M + k], q = ss[k];
+                acc.x += t.x * q.x - t.y * q.y;
+                acc.y += t.x * q.y + t.y * q.x;
+            }
+        hs[l] = acc;
+    }
+    __syncthreads();
+    if (tid == 0) {  // <v_j, w> = (<vt, w> - s^H z) / alpha
+        if (has_vt) {
+            double2 t = make_double2(sa[0], sa[1]);
+            for (int k = 0; k < nk; ++k) {
+                const double2 p = cmulc(ss[k], zs[k]);
+                t.x -= p.x;
+                t.y -= p.y;
+            }
+            zs[j] = make_double2(t.x / alpha, t.y / alpha);
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && bad) {
-        ks->status = KS_NONFINITE;
-        ks->iters = j + 1;
+    for (int l = tid; l <= j; l += DECIDE_THREADS) {  // h_l = (z_l - (T s)_l) / alpha
+        const double2 h = make_double2((zs[l].x - hs[l].x) / alpha, (zs[l].y - hs[l].y) / alpha);
+        if (!isfinite(h.x) || !isfinite(h.y)) bad = 1;
+        as->T[l * ARN_M + j] = h;
+        cc[l] = make_double2(hs[l].x + alpha * h.x, hs[l].y + alpha * h.y);
+        if (l == j) ks->a_re[j] = h.x;  // Re <v_j, (H - sigma) v_j>
+    }
+    __syncthreads();
+    // pass B: w' = (w - V_j c) / alpha with v_j = (vt - V s) / alpha substituted
+    for (int l = tid; l < nk; l += DECIDE_THREADS) {
+        const double2 sl = ss[l], cj = has_vt ? cc[j] : make_double2(0.0, 0.0);
+        const double2 p = make_double2((cj.x * sl.x - cj.y * sl.y) / alpha, (cj.x * sl.y + cj.y * sl.x) / alpha);
+        as->cw1[l] = has_vt ? make_double2((cc[l].x - p.x) / alpha, (cc[l].y - p.y) / alpha) : cc[l];
+        as->cvj[l] = make_double2(sl.x / alpha, sl.y / alpha);
+    }
+    if (tid == 0) {
+        as->cw = 1.0 / alpha;
+        as->cv = 1.0 / alpha;
+        as->ct = has_vt ? make_double2(cc[j].x / (alpha * alpha), cc[j].y / (alpha * alpha))
+                        : make_double2(0.0, 0.0);
+        // ||(H - sigma) v_j||^2 = ||w - V_j (T s)||^2 / alpha^2, then ||H v_j||
+        double n2 = sa[2];
+        for (int l = 0; l <= j; ++l) {
+            if (!has_vt && l > 0) break;
+            const double2 p = cmulc(hs[l], zs[l]);
+            n2 += -2.0 * p.x + hs[l].x * hs[l].x + hs[l].y * hs[l].y;
+        }
+        n2 /= alpha * alpha;
+        const double sg = ks->shift;
+        ks->hn[j] = sqrt(fmax(0.0, n2 + 2.0 * sg * ks->a_re[j] + sg * sg));
+        if (!isfinite(n2)) bad = 1;
+        if (bad) {
+            ks->status = KS_NONFINITE;
+            ks->iters = j + 1;
+        }
     }
 }
 
@@ -418,9 +539,10 @@ k_arn_decide(KState *ks, ArnState *as, int j, const double *part, int nb, double
         return;
     }
     if (tid == 0) {
-        as->T[(j + 1) * ARN_M + j] = make_double2(r, 0.0);  // krylov_exp.py:61
+        as->T[(j + 1) * ARN_M + j] = make_double2(r, 0.0);  // krylov_exp.py:61 (until corrected)
         ks->r[j] = r;
         ks->scale[j + 1] = 1.0 / r;
+        if (j >= 1) ks->scale[j] = 1.0;  // pass B stored the corrected v_j normalised
     }
     __syncthreads();
     if (fabs(dt) * r < norm_tol) {  // happy breakdown (krylov_exp.py:63-71)
@@ -482,29 +604,23 @@ static size_t decide_smem(int maxdim) {
     return sizeof(double2) * (M * M + 3 * M) + sizeof(double) * DECIDE_THREADS;
 }
 
-// Grid of the ortho passes: the streaming grid of the vector kernels (up to four blocks per
-// SM), never more blocks than chunks; *grid_out receives it (the number of partial rows).
-// Measured on B200 (N=22, complex128, j ~ 35): one block per SM with chunks small enough
-// for the update-and-dots pass to find its second reads in L2 was 1.5x slower than the
-// wide grid that re-reads them from HBM.
+// Grid of the Gram-Schmidt passes: the streaming grid of the vector kernels (up to four
+// blocks per SM), never more blocks than chunks; *grid_out receives it (the number of
+// partial rows).
 template <typename R>
-static int launch_ortho(int mode, const KState *ks, const ArnState *as, int j, const void *v0,
-                        const unsigned char *basis, i64 D, void *w, double *part, cudaStream_t s,
-                        int *grid_out) {
+static int launch_lagged(int pass, const KState *ks, const ArnState *as, int j, const void *v0,
+                         unsigned char *basis, i64 D, void *w, double *part, cudaStream_t s,
+                         int *grid_out) {
     constexpr int E = 4;
     i64 grid = krylov_stream_grid(D);
     const i64 chunks = (D + (i64)ORTHO_THREADS * E - 1) / ((i64)ORTHO_THREADS * E);
     if (grid > chunks) grid = chunks;
     *grid_out = (int)grid;
     ProfScope ps_(PROF_ORTH, s);
-#define ARN_LAUNCH(M) k_arn_ortho<R, M, E><<<(int)grid, ORTHO_THREADS, 0, s>>>(ks, as, j, v0, basis, D, w, part)
-    if (mode == ARN_DOTS)
-        ARN_LAUNCH(ARN_DOTS);
-    else if (mode == ARN_UPDATE)
-        ARN_LAUNCH(ARN_UPDATE);
+    if (pass == 0)
+        k_arn_lagdots<R, E><<<(int)grid, ORTHO_THREADS, 0, s>>>(ks, j, v0, basis, D, w, part);
     else
-        ARN_LAUNCH(ARN_UPDATE_DOTS);
-#undef ARN_LAUNCH
+        k_arn_lagupdate<R, E><<<(int)grid, ORTHO_THREADS, 0, s>>>(ks, as, j, v0, basis, D, w, part);
     EMUSV_CHECK_LAUNCH();
     return EMUSV_OK;
 }
@@ -598,14 +714,14 @@ int arnoldi_run(const HamParams &P, const LindbladJumps *J, int dtype, double dt
         if (J && (st = launch_lindblad_jumps(dtype, *J, stored(j), &ks->scale[j], w, &ks->status, s)))
             return st;
         int og = 0;
-        for (int mode = ARN_DOTS; mode <= ARN_UPDATE; ++mode) {
+        for (int pass = 0; pass < 2; ++pass) {
             st = dtype == EMUSV_C128
-                     ? launch_ortho<double>(mode, ks, as, j, psi_in, basis, D, w, part, s, &og)
-                     : launch_ortho<float>(mode, ks, as, j, psi_in, basis, D, w, part, s, &og);
+                     ? launch_lagged<double>(pass, ks, as, j, psi_in, basis, D, w, part, s, &og)
+                     : launch_lagged<float>(pass, ks, as, j, psi_in, basis, D, w, part, s, &og);
             if (st) return st;
-            if (mode != ARN_UPDATE) {
+            if (pass == 0) {
                 ProfScope ps_(PROF_SMALL, s);
-                k_arn_stage<<<1, DECIDE_THREADS, 0, s>>>(ks, as, j, part, og, mode);
+                k_arn_lagstage<<<1, DECIDE_THREADS, 0, s>>>(ks, as, j, part, og);
                 EMUSV_CHECK_LAUNCH();
             }
         }
@@ -636,9 +752,7 @@ int arnoldi_run(const HamParams &P, const LindbladJumps *J, int dtype, double dt
     if ((st = krylov_combine(dtype, ks, psi_in, basis, D, psi_out, part_n, s))) return st;
     if (info) {
         KState h;
-        int r2 = 0;
         EMUSV_CHECK(cudaMemcpyAsync(&h, ks, offsetof(KState, a_re), cudaMemcpyDeviceToHost, s));
-        EMUSV_CHECK(cudaMemcpyAsync(&r2, &as->rounds2, sizeof(int), cudaMemcpyDeviceToHost, s));
         EMUSV_CHECK(cudaStreamSynchronize(s));
         info->iterations = h.iters;
         info->happy_breakdown = h.status == KS_HAPPY;
@@ -647,7 +761,7 @@ int arnoldi_run(const HamParams &P, const LindbladJumps *J, int dtype, double dt
         info->error_estimate = h.err;
         info->input_norm = h.s0;
         info->output_norm = sqrt(h.outnorm2);
-        info->second_rounds = r2;
+        info->second_rounds = h.iters > 0 ? h.iters - 1 : 0;  // every vector but the first
     }
     return status == KS_MAXDIM ? EMUSV_NOT_CONVERGED : EMUSV_OK;
 }

@@ -52,8 +52,8 @@ typedef struct {
     double error_estimate; /* last Expokit estimate (krylov_exp.py:81-84) */
     double input_norm;    /* ||psi_in|| */
     double output_norm;   /* ||psi_out|| (FP64 reduction fused into the combination) */
-    int second_rounds;    /* emusv_arnoldi_step: iterations that took a second Gram-Schmidt
-                             round (0 for the Lanczos steps) */
+    int second_rounds;    /* emusv_arnoldi_step: basis vectors orthogonalised a second time
+                             (lagged into the next iteration; 0 for the Lanczos steps) */
 } emusv_krylov_info;
 
 /* Library identification: returns the sm architecture compiled in (e.g. 100). */
@@ -189,8 +189,8 @@ size_t emusv_arnoldi_workspace_bytes(int nqubits, int dtype, int basis_capacity)
  * from H inside H*psi (same basis and coefficients): zero it once before its first call. 
  * Replaces EvolveMonteCarlo.evolve (emu_sv/time_evolution/implementations.py:148-166),
  * i.e. krylov_exp with is_hermitian=False (emu_base/math/krylov_exp.py:23-131): full
- * orthogonalisation (classical Gram-Schmidt, a second round when the first removed more
- * than half of ||H v_j||^2; two or three streaming passes per iteration),
+ * orthogonalisation (classical Gram-Schmidt with the second round lagged by one iteration:
+ * two streaming passes per iteration),
  * happy-breakdown test every iteration, convergence tested on the device from iteration
  * `krylov_dim_hint` on (0: every iteration); when the first test already converges the
  * earlier iterations are tested in order, so the stopping iteration is the reference's.
