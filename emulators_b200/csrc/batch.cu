@@ -863,31 +863,10 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_post(const BArg
                     rr[a] += gr[a] * double(e[a].x) - gi[a] * double(e[a].y);
                     ri[a] += gr[a] * double(e[a].y) + gi[a] * double(e[a].x);
                 }
-                for (int p = 0; p < n; ++p) {
-                    double tr = 0, ti = 0, ur = 0, ui = 0;
-#pragma unroll
-                    for (int a = 0; a < AMP; ++a) {
-                        C w;
-                        int bit;
-                        if (p < 5) {
-                            w = shfl_c(e[a], 1 << p);
-                            bit = (lane >> p) & 1;
-                        } else if (p < T) {
-                            w = e[a ^ (1 << (p - 5))];
-                            bit = (a >> (p - 5)) & 1;
-                        } else {
-                            w = ldcg(Ek + (base ^ (1LL << p)) + lane + 32 * a);
-                            bit = (int)((base >> p) & 1);
-                        }
-                        const double pr = gr[a] * double(w.x) - gi[a] * double(w.y);
-                        const double pi = gr[a] * double(w.y) + gi[a] * double(w.x);
-                        tr += pr;
-                        ti += pi;
-                        if (bit) {
-                            ur += pr;
-                            ui += pi;
-                        }
-                    }
+                // per bit p: sum conj(G) E(x^p) and its part with x_p = 1; the partner is
+                // in another lane (p < 5), another register (p < T, compile-time index so
+                // e[] stays in registers) or another tile (p >= T)
+                auto bit_sums = [&](int p, double tr, double ti, double ur, double ui) {
                     tr = warp_sum(tr);
                     ti = warp_sum(ti);
                     ur = warp_sum(ur);
@@ -898,6 +877,53 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_post(const BArg
                         acc[2] += ur;
                         acc[3] += ui;
                     }
+                };
+                auto term = [&](int a, const C &w, bool bit, double &tr, double &ti, double &ur,
+                                double &ui) {
+                    const double pr = gr[a] * double(w.x) - gi[a] * double(w.y);
+                    const double pi = gr[a] * double(w.y) + gi[a] * double(w.x);
+                    tr += pr;
+                    ti += pi;
+                    if (bit) {
+                        ur += pr;
+                        ui += pi;
+                    }
+                };
+                if constexpr (AMP <= 16 && MINB == 1) {  // unrolled: e[] stays in registers
+#pragma unroll
+                    for (int p = 0; p < 5; ++p) {
+                        double tr = 0, ti = 0, ur = 0, ui = 0;
+#pragma unroll
+                        for (int a = 0; a < AMP; ++a)
+                            term(a, shfl_c(e[a], 1 << p), (lane >> p) & 1, tr, ti, ur, ui);
+                        bit_sums(p, tr, ti, ur, ui);
+                    }
+#pragma unroll
+                    for (int p = 5; p < T; ++p) {
+                        double tr = 0, ti = 0, ur = 0, ui = 0;
+#pragma unroll
+                        for (int a = 0; a < AMP; ++a)
+                            term(a, e[a ^ (1 << (p - 5))], (a >> (p - 5)) & 1, tr, ti, ur, ui);
+                        bit_sums(p, tr, ti, ur, ui);
+                    }
+                } else {  // the unrolled form would not fit the register budget
+                    for (int p = 0; p < T; ++p) {
+                        double tr = 0, ti = 0, ur = 0, ui = 0;
+#pragma unroll
+                        for (int a = 0; a < AMP; ++a) {
+                            if (p < 5) term(a, shfl_c(e[a], 1 << p), (lane >> p) & 1, tr, ti, ur, ui);
+                            else term(a, e[a ^ (1 << (p - 5))], (a >> (p - 5)) & 1, tr, ti, ur, ui);
+                        }
+                        bit_sums(p, tr, ti, ur, ui);
+                    }
+                }
+                for (int p = T; p < n; ++p) {
+                    double tr = 0, ti = 0, ur = 0, ui = 0;
+                    const bool bit = (base >> p) & 1;
+#pragma unroll
+                    for (int a = 0; a < AMP; ++a)
+                        term(a, ldcg(Ek + (base ^ (1LL << p)) + lane + 32 * a), bit, tr, ti, ur, ui);
+                    bit_sums(p, tr, ti, ur, ui);
                 }
             }
             for (int p = 0; p < n; ++p) {  // S_pp = sum over x with bit p of rho(x)
