@@ -504,6 +504,125 @@ def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1) -> dict:
                       f"{warm} warm-up step(s); CUDA events"}
 
 
+# ------------------------------------------------------------------ plain complex128 GPU gradients
+def _plain_lanczos(op, v, tol: float, mk: int):
+    """Lanczos basis and tridiagonal matrix of `op` from `v` with the reference's stopping
+    rule (emu_base/math/double_krylov.py:59-113): host tridiagonal matrix, Expokit error
+    estimate from the extended matrix's exponential, RecursionError past `mk`."""
+    import scipy.linalg
+    import torch
+
+    V = [v / torch.linalg.vector_norm(v)]
+    T = np.zeros((mk + 2, mk + 2), dtype=np.complex128)
+    for j in range(mk):
+        w = op(V[-1])
+        nn = torch.linalg.vector_norm(w).item()
+        for k in range(max(0, j - 1), j + 1):
+            ov = torch.vdot(V[k], w).item()
+            T[k, j] = ov
+            w -= ov * V[k]
+        n2 = torch.linalg.vector_norm(w).item()
+        T[j + 1, j] = n2
+        if n2 < tol:
+            return V, T[:len(V), :len(V)].copy()
+        V.append(w / n2)
+        T[j + 2, j + 1] = 1.0
+        e = scipy.linalg.expm(T[:j + 3, :j + 3])[:, 0]
+        err1, err2 = abs(e[j + 1]), abs(e[j + 2] * nn)
+        err = err1 if err1 < err2 else err1 * err2 / (err1 - err2)
+        if err < tol:
+            return V, T[:len(V), :len(V)].copy()
+    raise RecursionError("plain Lanczos did not converge")
+
+
+def plain_torch_grads_c128(gw, dev, p: int = 0, steps: int = 20) -> dict:
+    """Neel-loss gradients of parameter set `p` over its first `steps` steps, the reference's
+    way with plain torch tensor ops in complex128 (the reference modules are not on the
+    GPU machine): per step the Lanczos exponential forward (states kept); then per step
+    backwards the double Krylov decomposition (two Lanczos bases, the block exponential of
+    the two tridiagonal matrices joined at one corner, emu_base/math/double_krylov.py:5-56),
+    E = dS^T V_s, the per-qubit derivative operators dH/dOmega = 0.5 sigma^x and
+    dH/dDelta = -n (emu_sv/time_evolution/torch.py:36-119,327-351) and exp(+i dt H) on the
+    incoming gradient (torch.py:362-371).  Drives are real (phi = 0), as in the workload."""
+    import scipy.linalg
+    import torch
+
+    n, D = gw.nqubits, 1 << gw.nqubits
+    U = np.asarray(gw.U)
+    dt, tol, mk = gw.dt, gw.tolerance, 120
+    ctype = torch.complex128
+
+    def diagonal(de):
+        d = torch.zeros(D, dtype=ctype, device=dev)
+        for i in range(n):
+            d.view(2 ** i, 2, -1)[:, 1] -= float(de)
+            for j in range(i + 1, n):
+                if U[i, j] != 0.0:
+                    d.view(2 ** i, 2, 2 ** (j - i - 1), 2, -1)[:, 1, :, 1] += float(U[i, j])
+        return d
+
+    def hpsi(v, d, half_om):
+        out = d * v
+        for i in range(n):
+            vv, oo = v.view(2 ** i, 2, -1), out.view(2 ** i, 2, -1)
+            oo[:, 1] += half_om * vv[:, 0]
+            oo[:, 0] += half_om * vv[:, 1]
+        return out
+
+    def expm_apply(op, v):  # krylov_exp (emu_base/math/krylov_exp.py:23-131)
+        nrm = torch.linalg.vector_norm(v).item()
+        V, T = _plain_lanczos(op, v, tol, mk)
+        e = scipy.linalg.expm(T)[:, 0]
+        return nrm * sum(complex(e[i]) * V[i] for i in range(len(V)))
+
+    seg_of = [k // gw.steps_per_segment for k in range(steps)]
+    om, de = gw.omega_seg[p], gw.delta_seg[p]
+    if dev.type == "cuda":
+        torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    states = []
+    s = torch.zeros(D, dtype=ctype, device=dev)
+    s[0] = 1.0
+    for k in range(steps):
+        states.append(s)
+        d = diagonal(de[seg_of[k]])
+        half = 0.5 * float(om[seg_of[k]])
+        s = expm_apply(lambda x: (-1j * dt) * hpsi(x, d, half), s)
+    sf = s.detach().clone().requires_grad_(True)
+    occ = torch.stack([torch.linalg.vector_norm(sf.view(2 ** i, 2, -1)[:, 1]) ** 2 for i in range(n)])
+    loss = torch.mean((occ - torch.as_tensor(gw.target, device=dev)) ** 2)
+    (g,) = torch.autograd.grad(loss, sf)
+    g_om = torch.zeros(gw.nsegments, dtype=torch.float64, device=dev)
+    g_de = torch.zeros_like(g_om)
+    for k in reversed(range(steps)):
+        d = diagonal(de[seg_of[k]])
+        half = 0.5 * float(om[seg_of[k]])
+        fwd = lambda x: (-1j * dt) * hpsi(x, d, half)
+        Vs, Ts = _plain_lanczos(fwd, states[k], tol, mk)
+        Vg, Tg = _plain_lanczos(fwd, g, tol, mk)
+        ms = len(Vs)
+        big = scipy.linalg.block_diag(Ts, Tg)
+        big[0, ms] = torch.linalg.vector_norm(states[k]).item() * torch.linalg.vector_norm(g).item()
+        dS = torch.as_tensor(scipy.linalg.expm(big)[:ms, ms:], device=dev)
+        E = dS.mT @ torch.stack(Vs)
+        G = torch.stack(Vg).conj()
+        mg = E.shape[0]
+        for i in range(n):
+            Ev = E.view(mg, 2 ** i, 2, -1)
+            r = torch.zeros_like(Ev)  # dH/dOmega_i E
+            r[:, :, 1] = 0.5 * Ev[:, :, 0]
+            r[:, :, 0] = 0.5 * Ev[:, :, 1]
+            g_om[seg_of[k]] += (-1j * dt * torch.tensordot(G, r.view(mg, D))).real
+            r = -Ev.clone()  # dH/dDelta_i E
+            r[:, :, 0] = 0.0
+            g_de[seg_of[k]] += (-1j * dt * torch.tensordot(G, r.view(mg, D))).real
+        g = expm_apply(lambda x: (1j * dt) * hpsi(x, d, half), g)
+    go, gd = g_om.cpu().numpy(), g_de.cpu().numpy()
+    el = time.perf_counter() - t0
+    return {"loss": float(loss.detach()), "g_omega": go, "g_delta": gd, "s": el,
+            "occupation": occ.detach().cpu().numpy()}
+
+
 # ------------------------------------------------------------------ batched workloads
 def batch_c4(dev, per_instance_sample: int = 8) -> dict:
     """The 256-register batch (N in 12..18, 150 steps each, complex64/FP64) in one
@@ -576,7 +695,8 @@ def batch_c4(dev, per_instance_sample: int = 8) -> dict:
 def grads_c5(dev) -> dict:
     """Neel-loss gradients of the 64 parameter sets of the N=16 ring (20 segments x 10
     steps, complex128, checkpoints every 16 steps) through the batched forward and adjoint,
-    next to one set through the per-step autograd.Function chain (the reference's way)."""
+    next to one set through the per-step autograd.Function chain and to the plain
+    complex128 torch path of the reference's per-step backward (`plain_torch_grads_c128`)."""
     import torch
 
     from emulators_b200 import DifferentiableStateVectorEvolution as DSE
@@ -618,8 +738,20 @@ def grads_c5(dev) -> dict:
     el1 = e0.elapsed_time(e1) / 1e3
     rel = max(float(np.abs(g_om.cpu().numpy() - go[p]).max() / np.abs(go[p]).max()),
               float(np.abs(g_de.cpu().numpy() - gd[p]).max() / np.abs(gd[p]).max()))
+    # the plain complex128 torch path (the reference's per-step backward), set 0, first
+    # two segments; its rate scaled to all steps of a set
+    ps = 2 * gw.steps_per_segment
+    plain = plain_torch_grads_c128(gw, dev, p=0, steps=ps)
+    plain_gps = 1.0 / (plain["s"] * b.nsteps / ps)
     return {"sets": b.nsets, "steps": b.nsteps, "s": round(el, 3),
             "grads_per_s": round(b.nsets / el, 3), "max_krylov_dim": kd,
+            "plain_torch_c128_gpu": {
+                "sample": f"set 0, steps 0..{ps - 1} forward and backward (loss after step "
+                          f"{ps - 1}), the reference's per-step backward in plain torch ops, "
+                          f"complex128; wall time with a synchronize on both sides, rate "
+                          f"scaled to {b.nsteps} steps",
+                "s": round(plain["s"], 3), "grads_per_s": round(plain_gps, 5)},
+            "batched_over_plain": round((b.nsets / el) / plain_gps, 1),
             "per_instance_autograd": {"sample": "set 0, all steps, the per-step autograd "
                                                 "Function (fused step forward, adjoint step "
                                                 "backward), every step's state kept",

@@ -76,3 +76,21 @@ def test_batched_gradients_central_differences():
                 vals.append(float(((occ - bb.target.to(occ.device)) ** 2).mean()))
             fd = (vals[0] - vals[1]) / (2 * h)
             assert abs(fd - grad[k]) <= 1e-5 * max(abs(grad[k]), 1e-3), (which, k, fd, grad[k])
+
+
+def test_plain_torch_gradient_arm_matches_reference_autograd():
+    """The bench's plain complex128 torch gradient path (the baseline the batched gradients
+    are compared with) reproduces the reference's autograd gradients for the first 20 steps
+    of parameter set 0."""
+    import bench
+    from emulators_b200 import workloads as wl
+
+    g = golden("ring_n16_grad")
+    gw = wl.ring_n16_grad()
+    r = bench.plain_torch_grads_c128(gw, torch.device("cuda", 0), p=0,
+                                     steps=int(g["nseg"]) * gw.steps_per_segment)
+    nseg = int(g["nseg"])
+    assert abs(r["loss"] - float(g["p0_loss"])) < 1e-11
+    np.testing.assert_allclose(r["g_omega"][:nseg], g["p0_g_omega"], rtol=1e-7, atol=1e-11)
+    np.testing.assert_allclose(r["g_delta"][:nseg], g["p0_g_delta"], rtol=1e-7, atol=1e-11)
+    assert not np.any(r["g_omega"][nseg:]) and not np.any(r["g_delta"][nseg:])
