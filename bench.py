@@ -257,16 +257,26 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         torch.cuda.synchronize()
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         reps = 10
+        L.emusv_profile_begin(0)  # launch counts only
         s0.record()
         for _ in range(reps):
             L.emusv_hpsi(n, _lib.dtype_code(dt_), *H._params(), v.data_ptr(), o.data_ptr(),
                          torch.cuda.current_stream().cuda_stream)
         s1.record()
         torch.cuda.synchronize()
+        hl = np.zeros(8, dtype=np.int64)
+        L.emusv_profile_end(None, hl.ctypes.data, 8)
         t1 = s0.elapsed_time(s1) / 1e3 / reps
-        byts = 2 * D * (8 if name == "c64" else 16)
+        es_ = 8 if name == "c64" else 16
+        byts = 2 * D * es_
+        # vector units streamed per H*psi: pass L 2 (read, write), each H pass 3 (read the
+        # vector and the partial sums, write)
+        units = (2 * hl[0] + 3 * hl[7]) / reps
         hstand[name] = {"ms": round(t1 * 1e3, 4), "GB/s": round(byts / t1 / 1e9, 1),
-                        "frac": round(byts / t1 / 1e9 / hbm, 4)}
+                        "frac": round(byts / t1 / 1e9 / hbm, 4),
+                        "passes": int((hl[0] + hl[7]) // reps), "streamed_units": float(units),
+                        "streamed_GB/s": round(units * D * es_ / t1 / 1e9, 1),
+                        "streamed_frac": round(units * D * es_ / t1 / 1e9 / hbm, 4)}
         del v, o
 
     # ---- end-to-end through the public backend API, host buffers

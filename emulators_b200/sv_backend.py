@@ -10,8 +10,10 @@ observables are small local classes with pulser's names and evaluation-time sema
 
 from __future__ import annotations
 
+import bisect
 import dataclasses
 import logging
+import math
 import time
 from typing import Callable, Sequence
 
@@ -30,6 +32,40 @@ from .time_evolution import EvolveDensityMatrix, EvolveMonteCarlo, EvolveStateVe
 _TIME_CONVERSION_COEFF = 0.001  # Omega and delta in rad/us, dt in ns (sv_backend_impl.py:29)
 logger = logging.getLogger("emulators")
 
+# Relative times closer than this are one time (pulser.backend.observable.TIME_TOLERANCE, a
+# third-party constant; 1e-6 is the value the target-time fixtures were generated with).
+TIME_TOLERANCE = 1e-6
+
+
+# ---------------------------------------------------------------- target-time grid
+def fuzzy_union(base: Sequence[float], extra, tol: float = TIME_TOLERANCE) -> list[float]:
+    """Sorted ``base`` with the sorted ``extra`` times merged in; a time of ``extra`` within
+    ``tol`` of one already present is dropped, so ``base`` wins (pulser_adapter.py:80-95)."""
+    merged = list(base)
+    for t in extra:
+        i = bisect.bisect_left(merged, t)
+        if i > 0 and t - merged[i - 1] <= tol:
+            continue
+        if i < len(merged) and merged[i] - t <= tol:
+            continue
+        merged.insert(i, t)
+    return merged
+
+
+def get_target_times(duration: float, dt: float, observable_times=(),
+                     tol: float = TIME_TOLERANCE) -> list[float]:
+    """Absolute times (ns) at which a sequence of ``duration`` ns is sampled
+    (pulser_adapter.py:130-151): the relative grid i dt / duration for i = 0..floor(duration
+    / dt), 1.0 appended unless the grid already ends within ``tol`` of it, the observables'
+    relative evaluation times merged in by :func:`fuzzy_union`, all scaled by duration."""
+    duration = float(duration)
+    n_steps = math.floor(duration / dt)
+    rel = [i * float(dt) / duration for i in range(n_steps + 1)]
+    if rel[-1] < 1.0 - tol:
+        rel.append(1.0)
+    rel = fuzzy_union(rel, sorted(set(float(t) for t in observable_times)), tol)
+    return [t * duration for t in rel]
+
 
 # ---------------------------------------------------------------- observables
 class Observable:
@@ -43,10 +79,12 @@ class Observable:
     def name(self) -> str:
         return self.tag + (f"_{self.tag_suffix}" if self.tag_suffix else "")
 
-    def due(self, t: float, dt_frac: float) -> bool:
+    def due(self, t: float) -> bool:
+        """Whether relative time ``t`` is one of this observable's evaluation times, to
+        TIME_TOLERANCE (pulser_adapter.py:98-127); without evaluation times, every step."""
         if self.evaluation_times is None:
             return True
-        return any(abs(t - e) <= 0.5 * dt_frac + 1e-12 for e in self.evaluation_times)
+        return any(abs(t - e) <= TIME_TOLERANCE for e in self.evaluation_times)
 
     def apply(self, *, config, state, hamiltonian):  # pragma: no cover - overridden
         raise NotImplementedError
@@ -205,6 +243,20 @@ class SequenceData:
         return self.interaction_matrix
 
     @classmethod
+    def from_samples(cls, amp, det, phase, duration: float, dt: float, interaction_matrix,
+                     observable_times=(), qubit_ids: tuple = (), device=None) -> "SequenceData":
+        """From per-qubit drive samples ``[qubits, T]`` on pulser's 1 ns grid: the target-time
+        grid of ``duration`` ns with step ``dt`` ns and the observables' relative times
+        (:func:`get_target_times`), then the PCHIP midpoint samples of every signal on the
+        GPU (:func:`emulators_b200.pchip.midpoint_samples`), as the reference's adapter
+        builds its data (pulser_adapter.py:130-231)."""
+        from .pchip import midpoint_samples
+
+        times = get_target_times(duration, dt, observable_times)
+        om, de, ph = (a.cpu() for a in midpoint_samples(amp, det, phase, times, device))
+        return cls(om, de, ph, times, torch.as_tensor(interaction_matrix), tuple(qubit_ids))
+
+    @classmethod
     def from_workload(cls, w) -> "SequenceData":
         times = list(np.round(np.arange(w.nsteps + 1) * w.dt * 1000.0, 9))
         return cls(torch.as_tensor(w.omega), torch.as_tensor(w.delta), torch.as_tensor(w.phi),
@@ -254,9 +306,6 @@ class SVBackendImpl:
         self._current_H: RydbergHamiltonian | None = None
         self.time = time.time()
 
-    def _dt_frac(self) -> float:
-        return (self.target_times[1] - self.target_times[0]) / self.target_times[-1]
-
     def step(self, step_idx: int) -> None:
         dt = self.target_times[step_idx + 1] - self.target_times[step_idx]
         self._current_H = None
@@ -271,7 +320,7 @@ class SVBackendImpl:
     def _apply_observables(self, step_idx: int) -> None:
         """sv_backend_impl.py:211-242: renormalised state, H of the step just done."""
         t = self.target_times[step_idx] / self.target_times[-1]
-        due = [o for o in self._config.observables if o.due(t, self._dt_frac())]
+        due = [o for o in self._config.observables if o.due(t)]
         if not due:
             return
         norm = self.state.norm()

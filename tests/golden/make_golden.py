@@ -171,6 +171,7 @@ def load_reference(ref: str) -> dict:
     mods["cb"] = load("emu_sv.custom_callback_implementations",
                       "emu_sv/custom_callback_implementations.py")
     mods["cb"].DensityMatrix = StateVector
+    mods["adapter"] = load("emu_base.pulser_adapter", "emu_base/pulser_adapter.py")
     return mods
 
 
@@ -743,6 +744,50 @@ def gen_lindblad(R):
 
 
 GENERATORS["lindblad"] = gen_lindblad
+
+
+def gen_target_times(R):
+    """The reference's target-time grid (emu_base/pulser_adapter.py:130-151): a uniform
+    dt grid over the sequence duration merged with the observables' evaluation times,
+    near-duplicates (TIME_TOLERANCE, 1e-6 under the pulser stand-in above) dropped.  Cases:
+    the two of test/emu_base/test_adapter.py:905-966 plus seeded ones (durations that dt
+    does not divide, times within and just outside the tolerance of grid points)."""
+    from types import SimpleNamespace
+
+    ad = R["adapter"]
+    rng = np.random.default_rng(2024)
+    cases = [
+        (20.0, 5.5, [[0.0, 0.9 / 20, 11.9 / 20, 18.1 / 20]], None),
+        (20.0, 5.5, [None], [0.5]),
+        (2000.0, 10.0, [[0.05 * k for k in range(1, 21)]], None),
+        (100.0, 30.0, [[0.5]], None),
+        (100.0, 33.3333333, [[0.25, 0.75]], None),
+        (100.0, 100.0, [[0.5], [0.5, 0.25]], None),
+    ]
+    g = 7.0 / 1237.0  # grid of case 6: near-duplicates of grid points and of each other
+    near = [3 * g + 4e-7, 5 * g - 9e-7, 8 * g + 2e-6, 0.5, 0.5 + 5e-7, 0.5 + 3e-6, 1.0 - 4e-7]
+    cases.append((1237.0, 7.0, [list(rng.uniform(0, 1, 6)) + near], None))
+    cases.append((3000.0, 5.0, [[1 / 3, 2 / 3, 0.9999999, 1.0], [0.0, 1 / 3]], None))
+    cases.append((1500.0, 4.9, [list(rng.uniform(0, 1, 25))], [0.1, 0.2]))
+    out = {}
+    for k, (dur, dt, obs_times, default) in enumerate(cases):
+        seq = SimpleNamespace(get_duration=lambda include_fall_time=False, d=dur: d)
+        cfg = SimpleNamespace(
+            observables=[SimpleNamespace(evaluation_times=t) for t in obs_times],
+            default_evaluation_times=np.asarray(default if default is not None else [1.0]),
+            with_modulation=False)
+        tt = ad._get_target_times(seq, cfg, dt)
+        union = sorted(ad._unique_observable_times(cfg))
+        out[f"c{k}_duration"] = np.array(dur)
+        out[f"c{k}_dt"] = np.array(dt)
+        out[f"c{k}_obs"] = np.array(union, dtype=np.float64)
+        out[f"c{k}_expected"] = np.array(tt, dtype=np.float64)
+    out["count"] = np.array(len(cases))
+    out["tolerance"] = np.array(float(ad.TIME_TOLERANCE))
+    return out
+
+
+GENERATORS["target_times"] = gen_target_times
 
 
 def main():
