@@ -79,12 +79,14 @@ class Observable:
     def name(self) -> str:
         return self.tag + (f"_{self.tag_suffix}" if self.tag_suffix else "")
 
-    def due(self, t: float) -> bool:
+    def due(self, t: float, default_times: Sequence[float] | None = None) -> bool:
         """Whether relative time ``t`` is one of this observable's evaluation times, to
-        TIME_TOLERANCE (pulser_adapter.py:98-127); without evaluation times, every step."""
-        if self.evaluation_times is None:
+        TIME_TOLERANCE (pulser_adapter.py:98-127).  An observable without its own times
+        takes the config's ``default_times``; with neither, it is due at every step."""
+        times = self.evaluation_times if self.evaluation_times is not None else default_times
+        if times is None:
             return True
-        return any(abs(t - e) <= TIME_TOLERANCE for e in self.evaluation_times)
+        return any(abs(t - e) <= TIME_TOLERANCE for e in times)
 
     def apply(self, *, config, state, hamiltonian):  # pragma: no cover - overridden
         raise NotImplementedError
@@ -215,6 +217,11 @@ class SVConfig:
         self.initial_state = initial_state
         self.precision = precision
         self.krylov_dim_hint = krylov_dim_hint
+        # relative times of the observables that have none of their own; "Full" (or none
+        # given) evaluates them at every step
+        d = kwargs.pop("default_evaluation_times", None)
+        self.default_evaluation_times = None if d is None or isinstance(d, str) else \
+            tuple(float(t) for t in d)
         self._backend_options = dict(kwargs)
 
     @property
@@ -320,7 +327,8 @@ class SVBackendImpl:
     def _apply_observables(self, step_idx: int) -> None:
         """sv_backend_impl.py:211-242: renormalised state, H of the step just done."""
         t = self.target_times[step_idx] / self.target_times[-1]
-        due = [o for o in self._config.observables if o.due(t)]
+        due = [o for o in self._config.observables
+               if o.due(t, self._config.default_evaluation_times)]
         if not due:
             return
         norm = self.state.norm()

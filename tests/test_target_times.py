@@ -46,6 +46,18 @@ def test_observable_due_to_time_tolerance():
     assert Occupation().due(0.123)
 
 
+def test_config_default_evaluation_times():
+    """Observables without their own times take the config's default times."""
+    from emulators_b200.sv_backend import Energy, Occupation, SVConfig
+
+    cfg = SVConfig(observables=[Occupation(), Energy([0.5])], default_evaluation_times=[1.0])
+    occ, en = cfg.observables
+    d = cfg.default_evaluation_times
+    assert d == (1.0,)
+    assert not occ.due(0.5, d) and occ.due(1.0, d) and en.due(0.5, d) and not en.due(1.0, d)
+    assert SVConfig(default_evaluation_times="Full").default_evaluation_times is None
+
+
 @pytest.mark.gpu
 def test_sequence_data_from_samples():
     """The adapter path on the GPU: grid with an off-grid observation time, then the PCHIP
