@@ -216,10 +216,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     pms = np.zeros(8)
     pl = np.zeros(8, dtype=np.int64)
     L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
-    # One Lanczos iteration = the pass L with the previous iteration's recurrence fused in
-    # front (kind 0; plus one plain pass L of v_0 per step) + one or two strided passes
-    # (kind 7).  Algorithmic bytes per iteration (H*psi 2 D s + recurrence 4 D s).
+    # One Lanczos iteration (H-first order) = one or two strided pass H kernels (kind 7: the
+    # flips of the bits above the pass-L tile; 2 vector units for the first, 3 for a second
+    # that adds to the first's sums) + the recurrence pass L (kind 0: read v_j, the pass H
+    # sums and v_{j-1}, write w; 4 units), plus per step one read-only energy pass over v_0
+    # (kind 0, 1 unit).  Algorithmic bytes per iteration: H*psi 2 D s + recurrence 4 D s.
     m_total = max(int(sum(iters)), 1)
+    nsteps_p = max(len(iters), 1)
     iter_s = (pms[0] + pms[7]) / m_total / 1e3
     passl_s = pms[0] / max(pl[0], 1) / 1e3
     passh_s = pms[7] / max(pl[7], 1) / 1e3 if pl[7] else 0.0
@@ -229,19 +232,24 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     total_ms = pms.sum()
     kinds = ["hpsi_pass_low", "orth", "small", "combine", "obs", "adjoint", "batch", "hpsi_pass_high"]
     shares = {kinds[i]: round(pms[i] / total_ms, 4) for i in range(8) if pl[i]}
+    h_per_iter = pl[7] / m_total
+    h_units = 2.0 if h_per_iter < 1.5 else 5.0  # one H pass: 2 units; two: 2 + 3
+    low_units_mean = (4 * m_total + nsteps_p) / max(pl[0], 1)
+    iter_units = h_units + 4 + nsteps_p / m_total
     per_pass = {
-        "pass_low_fused": {"ms": round(passl_s * 1e3, 4), "bytes": 5 * D * es,
-                           "note": "read H v_j, v_j, v_{j-1}; write w, partial sums; the mean "
-                                   "includes the step's one plain pass L (2 D s)",
-                           "GB/s": round(5 * D * es / passl_s / 1e9, 1),
-                           "frac": round(5 * D * es / passl_s / 1e9 / hbm, 4)},
-        "pass_high": {"ms": round(passh_s * 1e3, 4), "bytes": 3 * D * es,
-                      "launches_per_iteration": round(pl[7] / m_total, 2),
-                      "GB/s": round(3 * D * es / passh_s / 1e9, 1) if passh_s else None,
-                      "frac": round(3 * D * es / passh_s / 1e9 / hbm, 4) if passh_s else None},
-        "iteration": {"ms": round(iter_s * 1e3, 4), "streamed_units": 11,
-                      "streamed_GB/s": round(11 * D * es / iter_s / 1e9, 1),
-                      "streamed_frac": round(11 * D * es / iter_s / 1e9 / hbm, 4)},
+        "pass_low": {"ms": round(passl_s * 1e3, 4), "units_mean": round(low_units_mean, 3),
+                     "note": "recurrence pass L: read v_j, the pass H sums, v_{j-1}; write w "
+                             "(4 D s); the mean includes the step's energy pass over v_0 (1 D s)",
+                     "GB/s": round(low_units_mean * D * es / passl_s / 1e9, 1),
+                     "frac": round(low_units_mean * D * es / passl_s / 1e9 / hbm, 4)},
+        "pass_high": {"ms": round(passh_s * 1e3, 4),
+                      "units_mean": round(h_units / max(h_per_iter, 1e-9), 3),
+                      "launches_per_iteration": round(h_per_iter, 2),
+                      "GB/s": round(h_units / h_per_iter * D * es / passh_s / 1e9, 1) if passh_s else None,
+                      "frac": round(h_units / h_per_iter * D * es / passh_s / 1e9 / hbm, 4) if passh_s else None},
+        "iteration": {"ms": round(iter_s * 1e3, 4), "streamed_units": round(iter_units, 3),
+                      "streamed_GB/s": round(iter_units * D * es / iter_s / 1e9, 1),
+                      "streamed_frac": round(iter_units * D * es / iter_s / 1e9 / hbm, 4)},
     }
     log(f"profiled: ms by kind {pms.round(3).tolist()} launches {pl.tolist()}; "
         f"Lanczos iteration {iter_s * 1e3:.4f} ms = {achieved:.1f} GB/s algorithmic; {per_pass}")
@@ -296,10 +304,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                    "l2": "state and Krylov vectors (512 MiB each) exceed L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm",
-                     "kernel": "Lanczos iteration = k_pass_low with the three-term recurrence "
-                               "fused in front + k_pass_high x2 (flips and diagonal on chip, "
-                               "FP64 reductions fused); achieved = 6*D*8 algorithmic bytes "
-                               "(H*psi 2 D s + recurrence 4 D s) / iteration time",
+                     "kernel": "Lanczos iteration = k_pass_high x2 (flips of the bits above "
+                               "the pass-L tile) + k_pass_lz (H v formed on chip, three-term "
+                               "recurrence, FP64 reductions); achieved = 6*D*8 algorithmic "
+                               "bytes (H*psi 2 D s + recurrence 4 D s) / iteration time",
                      "achieved": round(achieved, 1), "peak": hbm, "peak_source": which,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": ncu_traffic() if n == 26 and es == 8 else None,

@@ -11,6 +11,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(PKG)
@@ -45,15 +46,24 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     if not force and up_to_date():
         return LIB
     os.makedirs(OBJDIR, exist_ok=True)
-    objs = []
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+    jobs = []
     for src in sources():
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
-        if verbose:
+        jobs.append(([NVCC, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj], obj))
+    if verbose:
+        for cmd, _ in jobs:
             print(" ".join(cmd), flush=True)
-        subprocess.check_call(cmd)
-        objs.append(obj)
+    # one nvcc per translation unit, run side by side (ptxas output stays per file)
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        results = list(ex.map(lambda j: subprocess.run(j[0], capture_output=True, text=True), jobs))
+    for (cmd, _), r in zip(jobs, results):
+        if r.stdout or r.stderr:
+            sys.stdout.write(r.stdout + r.stderr)
+        if r.returncode:
+            raise subprocess.CalledProcessError(r.returncode, cmd)
+    objs = [obj for _, obj in jobs]
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
     if verbose:
         print(" ".join(cmd), flush=True)

@@ -133,13 +133,10 @@ static bool single_pass_forced() {
     return v == 1;
 }
 
-bool hpsi_multipass(int dtype, int n);
-// The Lanczos H*psi of this register runs as separate passes (so a step can fuse its
-// recurrence into pass L): a multi-pass size and the passes not switched off.
-bool hpsi_uses_passes(int dtype, int n) {
-    return (dtype == EMUSV_C64 || dtype == EMUSV_C128) && n >= pass_min_qubits(dtype) &&
-           !single_pass_forced() && hpsi_multipass(dtype, n);
-}
+bool lz_applies(int dtype, int n);
+// The Lanczos iteration of this register runs in the H-first order (hpsi_pass.cu): wider
+// than one pass-L tile and the passes not switched off.
+bool lanczos_h_first(int dtype, int n) { return !single_pass_forced() && lz_applies(dtype, n); }
 
 // Dispatch on dtype / real coefficients / mode.  Registers of at least one pass-L tile
 // use the two-pass kernels for H*psi (store and Lanczos modes); the single-pass kernel

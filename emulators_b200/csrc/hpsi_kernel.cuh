@@ -39,11 +39,20 @@ struct HpsiArgs {
     void *part_buf;    // two-pass H*psi: buffer for the partial sums of pass L
     int *err;          // device word receiving EMUSV_TIMEOUT if a bounded wait gives up
     const double *eshift;  // HP_LANCZOS, HP_STORE: if non-null, the diagonal is taken minus *eshift
-    // multi-pass Lanczos with the recurrence fused into pass L (launch_hpsi_stage)
-    const void *vj, *vp;    // stored v_j, v_{j-1}
-    const double *ocoef;    // device [3]: recurrence coefficients on the stored vectors
-    const double *oscale;   // device scale of v_j
-    double *part_o;         // partials of ||w||^2, <v_j, w>
+};
+
+// Arguments of the Lanczos iteration's pass L (k_pass_lz in hpsi_pass.cuh).
+struct LzArgs {
+    const void *u;         // stored v_j (v_j = su u_j)
+    const void *part;      // X_high u_j (unscaled); null with E0
+    const void *up;        // stored v_{j-1}, or null
+    void *out;             // w (stored form of v_{j+1})
+    const double *su;      // device scale of v_j
+    const double *ocoef;   // device [3]: a_re su_j, a_im su_j, b su_{j-1}
+    const double *eshift;  // device sigma, or null
+    double *partials;      // [gridDim.x * NRED]
+    const int *gate;
+    int *err;
 };
 
 struct SmemLayout {

@@ -112,11 +112,11 @@ static void fill_params(const HamParams &H, int TB, int RB, PassParams *P) {
     }
 }
 
-template <typename R, bool REALC, int EPI, bool NOISY, bool ORTH = false>
+template <typename R, bool REALC, int EPI, bool NOISY>
 static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
-    auto kern = k_pass_low<R, REALC, TB, RB, EPI, 0, NOISY, ORTH>;
+    auto kern = k_pass_low<R, REALC, TB, RB, EPI, 0, NOISY>;
     const size_t smem = pass_low_smem<C, TB>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -135,26 +135,28 @@ static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, in
 }
 
 // One strided pass over the group bits [hpos, hpos + TB - CMIN) with CMIN chunk bits;
-// group bits below TB were applied by pass L and are skipped.
+// group bits below hskip (the pass-L tile width) were applied by pass L and are skipped.
 template <typename R, bool REALC, int EPI, int CMIN>
 static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *part,
-                       cudaStream_t s, int *grid_out) {
+                       cudaStream_t s, int *grid_out, int hskip = PassShape<R>::TB) {
     typedef typename cvec<R>::T C;
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
+    constexpr bool HASPART = epi_has_part<EPI>();
     const int n = P.n, g = TB - CMIN;
     if (hpos < CMIN || hpos + g > n) return EMUSV_BAD_ARGUMENT;
     P.hg = g;
     P.hc = CMIN;
     P.hpos = hpos;
     P.pbh = 0;
-    P.hskip = TB;
+    P.hskip = hskip;
     P.hbox_rows = g > 8 ? 256 : (1 << g);
     PassHighMaps M;
+    memset(&M, 0, sizeof(M));
     if (!encode_pass_high(&M.u, A.u, n, (int)sizeof(C), P) ||
-        !encode_pass_high(&M.part, part, n, (int)sizeof(C), P))
+        (HASPART && !encode_pass_high(&M.part, part, n, (int)sizeof(C), P)))
         return EMUSV_CUDA_ERROR;
     auto kern = k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0>;
-    const size_t smem = pass_high_smem<C, TB>();
+    const size_t smem = pass_high_smem<C, TB, HASPART>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
@@ -177,11 +179,8 @@ static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *pa
 // pass L) are skipped, so every H pass keeps the compile-time chunk of CMIN bits.  The
 // partial sums live in HA.part_buf (which may be HA.out: every pass reads a tile before
 // writing it).
-// stages: bit 0 = pass L, bit 1 = the H passes, bit 2 = pass L with the Lanczos recurrence
-// fused in front (ORTH; the H passes of the same H*psi follow in a later call)
 template <typename R, bool REALC, int EPI_F, int CMIN, bool NOISY>
-static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out,
-                      int stages = 3) {
+static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB;
     const int n = H.n;
     PassParams P;
@@ -201,25 +200,11 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
     A.eshift = HA.eshift;  // null unless the caller shifts the diagonal
     int st;
     if (rem == 0) {
-        if (stages != 3) return EMUSV_BAD_ARGUMENT;
         A.out = HA.out;
         return launch_low<R, REALC, EPI_F, NOISY>(P, A, s, grid_out);
     }
     A.out = HA.part_buf;
-    if (stages & 4) {
-        if constexpr (!NOISY) {
-            A.vj = HA.vj;
-            A.vp = HA.vp;
-            A.ocoef = HA.ocoef;
-            A.oscale = HA.oscale;
-            A.part_o = HA.part_o;
-            return launch_low<R, REALC, EPI_PARTIAL, false, true>(P, A, s, grid_out);
-        }
-        return EMUSV_BAD_ARGUMENT;
-    }
-    if (stages & 1)
-        if ((st = launch_low<R, REALC, EPI_PARTIAL, NOISY>(P, A, s, nullptr))) return st;
-    if (!(stages & 2)) return EMUSV_OK;
+    if ((st = launch_low<R, REALC, EPI_PARTIAL, NOISY>(P, A, s, nullptr))) return st;
     if (rem > G) {
         if ((st = launch_high<R, REALC, EPI_PARTIAL, CMIN>(P, n - 2 * G, A, HA.part_buf, s, nullptr)))
             return st;
@@ -231,33 +216,10 @@ static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, in
 // 64-byte rows (PassShape CMIN) where two H passes cover the bits above pass L, else
 // 32-byte rows
 template <typename R, bool REALC, int EPI_F, bool NOISY = false>
-static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out,
-                      int stages = 3) {
+static int run_passes(const HamParams &H, const HpsiArgs &HA, cudaStream_t s, int *grid_out) {
     constexpr int TB = PassShape<R>::TB, CMIN = PassShape<R>::CMIN;
-    if (H.n - TB <= 2 * (TB - CMIN))
-        return run_passes<R, REALC, EPI_F, CMIN, NOISY>(H, HA, s, grid_out, stages);
-    return run_passes<R, REALC, EPI_F, CMIN - 1, NOISY>(H, HA, s, grid_out, stages);
-}
-
-// The stages of a multi-pass Lanczos H*psi launched separately (stages as run_passes):
-// 1 = pass L of v_0, 2 = the H passes (their partial sums from a previous pass L),
-// 4 = the recurrence of the previous iteration fused into this iteration's pass L.
-int launch_hpsi_stage(int dtype, int stages, const HamParams &H, const HpsiArgs &A, cudaStream_t s,
-                      int *grid_out) {
-    if (H.noisy) return EMUSV_BAD_ARGUMENT;
-    if (dtype == EMUSV_C64)
-        return H.real_coef ? run_passes<float, true, EPI_LANCZOS>(H, A, s, grid_out, stages)
-                           : run_passes<float, false, EPI_LANCZOS>(H, A, s, grid_out, stages);
-    if (dtype == EMUSV_C128)
-        return H.real_coef ? run_passes<double, true, EPI_LANCZOS>(H, A, s, grid_out, stages)
-                           : run_passes<double, false, EPI_LANCZOS>(H, A, s, grid_out, stages);
-    return EMUSV_BAD_ARGUMENT;
-}
-
-// Registers whose H*psi takes more than one pass (the fused recurrence needs pass L to
-// produce partial sums for later passes).
-bool hpsi_multipass(int dtype, int n) {
-    return n > (dtype == EMUSV_C64 ? PassShape<float>::TB : PassShape<double>::TB);
+    if (H.n - TB <= 2 * (TB - CMIN)) return run_passes<R, REALC, EPI_F, CMIN, NOISY>(H, HA, s, grid_out);
+    return run_passes<R, REALC, EPI_F, CMIN - 1, NOISY>(H, HA, s, grid_out);
 }
 
 // mode: HP_STORE or HP_LANCZOS (values of HpsiMode)
@@ -284,6 +246,120 @@ int launch_hpsi_passes(int dtype, int mode, const HamParams &H, const HpsiArgs &
                   : run_passes<double, false, EPI_STORE>(H, A, s, grid_out);
     }
     return EMUSV_BAD_ARGUMENT;
+}
+
+
+// ------------------------------------------------------ Lanczos iteration, H-first order
+// Pass L of the Lanczos iteration (k_pass_lz): 2^11-amplitude tiles; complex64 8
+// amplitudes per thread (256 threads, two CTAs per SM), complex128 4 per thread (512
+// threads, one CTA per SM).
+template <typename R> struct LzShape;
+template <> struct LzShape<float> {
+    static constexpr int TB = 11, RB = 3;
+};
+template <> struct LzShape<double> {
+    static constexpr int TB = 11, RB = 2;
+};
+
+// The Lanczos iteration of this register runs in the H-first order (pass H kernels, then
+// the recurrence pass L): registers wider than one pass-L tile.
+bool lz_applies(int dtype, int n) {
+    if (dtype == EMUSV_C64) return n > LzShape<float>::TB;
+    if (dtype == EMUSV_C128) return n > LzShape<double>::TB;
+    return false;
+}
+
+template <typename R, bool REALC, bool E0>
+static int launch_lz(const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
+    typedef typename cvec<R>::T C;
+    constexpr int TB = LzShape<R>::TB, RB = LzShape<R>::RB, NT = 1 << (TB - RB);
+    PassParams P;
+    fill_params(H, TB, RB, &P);
+    auto kern = k_pass_lz<R, REALC, TB, RB, E0>;
+    const size_t smem = pass_lz_smem<C, TB>();
+    EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int64_t ntiles = int64_t(1) << (H.n - TB);
+    int64_t grid = (int64_t)sm_count() * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    {
+        ProfScope ps_(PROF_HPSI, s);
+        kern<<<(unsigned)grid, NT, smem, s>>>(P, A);
+    }
+    EMUSV_CHECK_LAUNCH();
+    if (grid_out) *grid_out = (int)grid;
+    return EMUSV_OK;
+}
+
+// Start of a run: partials 4-5 of <u, (D - sigma + X_low) u> (A.u, A.eshift, A.partials,
+// A.gate, A.err).
+int lz_energy0(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
+    if (H.noisy || !lz_applies(dtype, H.n)) return EMUSV_BAD_ARGUMENT;
+    if (dtype == EMUSV_C64)
+        return H.real_coef ? launch_lz<float, true, true>(H, A, s, grid_out)
+                           : launch_lz<float, false, true>(H, A, s, grid_out);
+    return H.real_coef ? launch_lz<double, true, true>(H, A, s, grid_out)
+                       : launch_lz<double, false, true>(H, A, s, grid_out);
+}
+
+// The recurrence pass: w = H v_j - a v_j - b v_{j-1} (see k_pass_lz).
+int lz_low(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
+    if (H.noisy || !lz_applies(dtype, H.n)) return EMUSV_BAD_ARGUMENT;
+    if (dtype == EMUSV_C64)
+        return H.real_coef ? launch_lz<float, true, false>(H, A, s, grid_out)
+                           : launch_lz<float, false, false>(H, A, s, grid_out);
+    return H.real_coef ? launch_lz<double, true, false>(H, A, s, grid_out)
+                       : launch_lz<double, false, false>(H, A, s, grid_out);
+}
+
+// part = X_high u (unscaled flips of every bit above the pass-L tile) in one or two
+// strided passes; their <u, X u> partials go to partials[0 .. *nblocks_out) (rows of NRED).
+template <typename R, bool REALC, int CMIN>
+static int lz_high_t(const HamParams &H, const void *u, void *part, double *partials, const int *gate,
+                     int *err, cudaStream_t s, int *nblocks_out) {
+    constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, TBL = LzShape<R>::TB;
+    const int n = H.n, rem = n - TBL, G = TB - CMIN;
+    if (rem < 1 || rem > 2 * G) return EMUSV_BAD_ARGUMENT;
+    PassParams P;
+    fill_params(H, TB, RB, &P);
+    PassArgs A = {};
+    A.u = u;
+    A.su = 1.0;
+    A.out = part;
+    A.partials = partials;
+    A.gate = gate;
+    A.err = err;
+    int g1 = 0, g2 = 0, st;
+    if (rem > G) {
+        if ((st = launch_high<R, REALC, EPI_X_FIRST, CMIN>(P, n - 2 * G, A, nullptr, s, &g1, TBL))) return st;
+        A.partials = partials + (size_t)g1 * NRED;
+        if ((st = launch_high<R, REALC, EPI_X_ADD, CMIN>(P, n - G, A, part, s, &g2, TBL))) return st;
+    } else {
+        if ((st = launch_high<R, REALC, EPI_X_FIRST, CMIN>(P, n - G, A, nullptr, s, &g2, TBL))) return st;
+    }
+    *nblocks_out = g1 + g2;
+    return EMUSV_OK;
+}
+
+template <typename R, bool REALC>
+static int lz_high_rows(const HamParams &H, const void *u, void *part, double *partials, const int *gate,
+                        int *err, cudaStream_t s, int *nb) {
+    // 64-byte rows where two H passes cover the bits above pass L, else 32-byte rows
+    constexpr int TB = PassShape<R>::TB, CMIN = PassShape<R>::CMIN, TBL = LzShape<R>::TB;
+    if (H.n - TBL <= 2 * (TB - CMIN)) return lz_high_t<R, REALC, CMIN>(H, u, part, partials, gate, err, s, nb);
+    return lz_high_t<R, REALC, CMIN - 1>(H, u, part, partials, gate, err, s, nb);
+}
+
+int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,
+            int *err, cudaStream_t s, int *nblocks_out) {
+    if (H.noisy || !lz_applies(dtype, H.n)) return EMUSV_BAD_ARGUMENT;
+    if (dtype == EMUSV_C64)
+        return H.real_coef ? lz_high_rows<float, true>(H, u, part, partials, gate, err, s, nblocks_out)
+                           : lz_high_rows<float, false>(H, u, part, partials, gate, err, s, nblocks_out);
+    return H.real_coef ? lz_high_rows<double, true>(H, u, part, partials, gate, err, s, nblocks_out)
+                       : lz_high_rows<double, false>(H, u, part, partials, gate, err, s, nblocks_out);
 }
 
 }  // namespace emusv

@@ -40,7 +40,16 @@ enum PassEpi {
     EPI_PARTIAL = 0,  // store the partial sum (another pass follows)
     EPI_STORE = 1,    // store H v
     EPI_LANCZOS = 2,  // store H v; FP64 partials ||Hv||^2, <v,Hv>
+    // flips of the pass's group bits only, unscaled (the Lanczos iteration's pass H, which
+    // runs before its pass L): out = X u (first pass, no partial-sum input) or
+    // out = part + X u; FP64 partials of <u, X u> (0 re, 1 im)
+    EPI_X_FIRST = 3,
+    EPI_X_ADD = 4,
 };
+template <int EPI> __host__ __device__ constexpr bool epi_has_part() { return EPI != EPI_X_FIRST; }
+template <int EPI> __host__ __device__ constexpr bool epi_reduces() {
+    return EPI == EPI_LANCZOS || EPI == EPI_X_FIRST || EPI == EPI_X_ADD;
+}
 
 constexpr int PBMAX_ALL = 3;  // largest cluster (2^3 CTAs) either pass uses
 
@@ -72,12 +81,6 @@ struct PassArgs {
     const int *gate;        // kernel returns at once when *gate != 0
     int *err;               // receives EMUSV_TIMEOUT when a bounded wait gives up
     const double *eshift;   // pass L: if non-null, the diagonal is taken minus *eshift
-    // pass L with the Lanczos recurrence fused in front (ORTH): u holds H v_j and receives
-    // w = H v_j - a v_j - b v_{j-1} (in place, stored form), the pass works on w
-    const void *vj, *vp;    // stored v_j, v_{j-1} (vp may be null)
-    const double *ocoef;    // device [3]: a_re scale_j, a_im scale_j, b scale_{j-1}
-    const double *oscale;   // device scale_j (for <v_j, w>)
-    double *part_o;         // [gridDim.x * NRED]: ||w||^2, <v_j, w>
 };
 
 // ------------------------------------------------------------------ PTX helpers
@@ -144,6 +147,10 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
         ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
+}
+// Bulk prefetch of global memory into the L2 (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 // 5-D tiled tensor-map load (no multicast), completion on `bar`.
 __device__ __forceinline__ void tmap_load5(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
@@ -234,7 +241,7 @@ __device__ __forceinline__ void flip_reg(R cr, R ci, const C &w, Acc<R> &acc) {
 
 template <int EPI>
 __device__ __forceinline__ void write_partials(const PassArgs &A, double (&red)[NRED], double *scratch) {
-    if (EPI != EPI_LANCZOS) return;
+    if (!epi_reduces<EPI>()) return;
     block_sum<NRED>(red, scratch);
     if (threadIdx.x == 0) {
 #pragma unroll
@@ -258,14 +265,9 @@ __host__ __device__ constexpr size_t pass_low_smem() {
 }
 
 // NOISY: the diagonal has the imaginary part dc_im + dg_im * popcount(x) (noise term).
-// ORTH: each tile is first turned from H v_j into w = H v_j - a v_j - b v_{j-1} (the Lanczos
-// recurrence, written back in place and kept in shared memory for the pass), one tile
-// ahead of the flips so that the pass keeps one block barrier per tile; FP64 partials of
-// ||w||^2 and <v_j, w> go to A.part_o.  PB = 0, EPI_PARTIAL.
-template <typename R, bool REALC, int TB, int RB, int EPI, int PB, bool NOISY = false, bool ORTH = false>
+template <typename R, bool REALC, int TB, int RB, int EPI, int PB, bool NOISY = false>
 __global__ void __launch_bounds__(1 << (TB - RB), 2)
 k_pass_low(const PassParams P, PassArgs A) {
-    static_assert(!ORTH || (PB == 0 && EPI == EPI_PARTIAL && !NOISY), "ORTH: plain pass L only");
     const double eshift = A.eshift ? *A.eshift : 0.0;
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
@@ -306,55 +308,7 @@ k_pass_low(const PassParams P, PassArgs A) {
         }
     }
 
-    // ORTH: the recurrence's coefficients on the stored vectors, and the tile conversion
-    double ocr = 0.0, oci = 0.0, ocb = 0.0, osj = 0.0;
-    double ored[NRED];
-#pragma unroll
-    for (int k = 0; k < NRED; ++k) ored[k] = 0.0;
-    if (ORTH) {
-        ocr = A.ocoef[0];
-        oci = A.ocoef[1];
-        ocb = A.ocoef[2];
-        osj = *A.oscale;
-    }
-    auto convert = [&](int b, int64_t tbase) {
-        C *tl = tiles + ((int64_t)b << TB);
-        C *wout = const_cast<C *>(u);
-        const C *vj = reinterpret_cast<const C *>(A.vj);
-        const C *vp = reinterpret_cast<const C *>(A.vp);
-        C pj[NA], pp[NA];
-#pragma unroll
-        for (int a = 0; a < NA; ++a) {
-            const int64_t x = tbase + tid + a * NT;
-            pj[a] = vj[x];
-            pp[a] = vp ? vp[x] : cmake<C>(0.0, 0.0);
-        }
-#pragma unroll
-        for (int a = 0; a < NA; ++a) {
-            const int l = tid + a * NT;
-            const C h = tl[l];
-            const double jr = double(pj[a].x), ji = double(pj[a].y);
-            const double wr = double(h.x) - (ocr * jr - oci * ji) - ocb * double(pp[a].x);
-            const double wi = double(h.y) - (ocr * ji + oci * jr) - ocb * double(pp[a].y);
-            const C o = cmake<C>(wr, wi);
-            tl[l] = o;
-            wout[tbase + l] = o;
-            const double orr = double(o.x), oi = double(o.y);
-            const double vr = osj * jr, vi = osj * ji;
-            ored[0] += orr * orr + oi * oi;
-            ored[1] += vr * orr + vi * oi;  // <v_j, w>
-            ored[2] += vr * oi - vi * orr;
-        }
-    };
     bool ok = true;
-    if (ORTH && cid < nsuper) {  // the first tile, converted before the loop
-        if (!mbar_wait(&bars[0], 0)) {
-            ok = false;
-            report_timeout(A);
-        } else {
-            convert(0, ((((int64_t)cid) << PB) | rank) << TB);
-        }
-    }
 
     // per-thread constants: energy of the thread bits and thread x register crosses
     double ET = 0.0;
@@ -416,7 +370,7 @@ k_pass_low(const PassParams P, PassArgs A) {
                 sc[lane] = cx;  // crossT[0..SB) then crossR[0..RB)
             }
         }
-        if (!ORTH && ok && !mbar_wait(&bars[buf], phase)) {  // ORTH: waited when converted
+        if (ok && !mbar_wait(&bars[buf], phase)) {
             ok = false;
             report_timeout(A);
         }
@@ -527,19 +481,6 @@ k_pass_low(const PassParams P, PassArgs A) {
                 }
             }
         }
-        if (ORTH && ok) {  // convert the next tile (its buffer is not read before the barrier)
-            const int64_t s1 = s + nclusters;
-            if (s1 < nsuper) {
-                const int b1 = buf + 1 == SL ? 0 : buf + 1;
-                const uint32_t ph1 = buf + 1 == SL ? (phase ^ 1u) : phase;
-                if (!mbar_wait(&bars[b1], ph1)) {
-                    ok = false;
-                    report_timeout(A);
-                } else {
-                    convert(b1, s1 << TB);
-                }
-            }
-        }
         if (++buf == SL) {
             buf = 0;
             phase ^= 1u;
@@ -548,13 +489,6 @@ k_pass_low(const PassParams P, PassArgs A) {
     // no CTA may leave while a sibling can still read its shared memory
     if (PB) cluster_sync_all();
     write_partials<EPI>(A, red, red_scr);
-    if (ORTH) {
-        block_sum<NRED>(ored, red_scr);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < NRED; ++k) A.part_o[(int64_t)blockIdx.x * NRED + k] = ored[k];
-        }
-    }
 }
 
 // ------------------------------------------------------------------------- pass H
@@ -565,9 +499,9 @@ k_pass_low(const PassParams P, PassArgs A) {
 // by pass L when the group overlaps the pass-L tile) are skipped.
 // Tensor map (8-byte elements, dims innermost first): [2^c*K, 2^(hpos-c), 2^g, 2^pbh, rest]
 // with K = sizeof(C)/8.
-template <typename C, int TB>
+template <typename C, int TB, bool HASPART = true>
 __host__ __device__ constexpr size_t pass_high_smem() {
-    return 2 * SH * (sizeof(C) << TB) + 8 * SH + sizeof(double) * 8 * NRED;
+    return (HASPART ? 2 : 1) * SH * (sizeof(C) << TB) + 8 * SH + sizeof(double) * 8 * NRED;
 }
 
 struct PassHighMaps {
@@ -582,12 +516,14 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
     constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
+    constexpr bool HASPART = epi_has_part<EPI>();
+    constexpr int NBUF = HASPART ? 2 : 1;
     if (A.gate && *A.gate != 0) return;
     extern __shared__ __align__(128) unsigned char smem_pass[];
     C *tiles = reinterpret_cast<C *>(smem_pass);  // [SH][2^TB] values, then [SH][2^TB] partials
     C *parts = tiles + ((int64_t)SH << TB);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 2 * SH * TILE_BYTES);
-    double *red_scr = reinterpret_cast<double *>(smem_pass + 2 * SH * TILE_BYTES + 8 * SH);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + NBUF * SH * TILE_BYTES);
+    double *red_scr = reinterpret_cast<double *>(smem_pass + NBUF * SH * TILE_BYTES + 8 * SH);
     static_assert(CT >= 1 && CT <= TB - RB, "chunk bits must lie below the register bits");
     const int n = P.n, hpos = P.hpos;
     constexpr int c = CT, g = TB - CT;
@@ -612,12 +548,15 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     auto issue = [&](int64_t s, int buf) {
         const int slo = (int)(s & lowmask);
         const int shi = (int)(s >> lowbits);
-        mbar_expect_tx(&bars[buf], 2 * TILE_BYTES);
+        mbar_expect_tx(&bars[buf], NBUF * TILE_BYTES);
         for (int b = 0; b < nbox; ++b) {
             unsigned char *dv = reinterpret_cast<unsigned char *>(tiles + ((int64_t)buf << TB)) + b * box_bytes;
-            unsigned char *dp = reinterpret_cast<unsigned char *>(parts + ((int64_t)buf << TB)) + b * box_bytes;
             tmap_load5(dv, &M.u, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
-            tmap_load5(dp, &M.part, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
+            if (HASPART) {
+                unsigned char *dp =
+                    reinterpret_cast<unsigned char *>(parts + ((int64_t)buf << TB)) + b * box_bytes;
+                tmap_load5(dp, &M.part, 0, slo, b * rows, (int)rank, shi, &bars[buf]);
+            }
         }
     };
     if (tid == 0) {
@@ -718,8 +657,21 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
                     flip_reg<R, REALC>(ccr[r], cci[r],
                                        ld_cluster(raddr[r] + boff + (uint32_t)(a * NT * sizeof(C)),
                                                   (const C *)nullptr), acc);
-                const C pt = ptile[l];
-                if (EPI == EPI_PARTIAL) {  // another pass follows: unscaled running sum
+                const C pt = HASPART ? ptile[l] : cmake<C>(0.0, 0.0);
+                if (EPI == EPI_X_FIRST || EPI == EPI_X_ADD) {  // unscaled X u; <u, X u>
+                    if constexpr (std::is_same<R, float>::value) {
+                        const float2 t = upk2(acc.a);
+                        outp[x] = HASPART ? make_float2(pt.x + t.x, pt.y + t.y) : t;
+                        rf[0] = fmaf(v[a].x, t.x, fmaf(v[a].y, t.y, rf[0]));
+                        rf[1] = fmaf(v[a].x, t.y, fmaf(-v[a].y, t.x, rf[1]));
+                    } else {
+                        const double tr = acc.re(), ti = acc.im();
+                        outp[x] = HASPART ? cmake<C>(double(pt.x) + tr, double(pt.y) + ti) : cmake<C>(tr, ti);
+                        const double vr = double(v[a].x), vi = double(v[a].y);
+                        red[0] += vr * tr + vi * ti;
+                        red[1] += vr * ti - vi * tr;
+                    }
+                } else if (EPI == EPI_PARTIAL) {  // another pass follows: unscaled running sum
                     if constexpr (std::is_same<R, float>::value) {
                         const float2 t = upk2(acc.a);
                         outp[x] = make_float2(pt.x + t.x, pt.y + t.y);
@@ -753,6 +705,10 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
                     red[1] += su * double(rf[1]);
                     red[2] += su * double(rf[2]);
                 }
+                if (EPI == EPI_X_FIRST || EPI == EPI_X_ADD) {
+                    red[0] += double(rf[0]);
+                    red[1] += double(rf[1]);
+                }
             }
         }
         if (++buf == SH) {
@@ -762,6 +718,315 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
     }
     if (PBH) cluster_sync_all();
     write_partials<EPI>(A, red, red_scr);
+}
+
+
+// ------------------------------------------------------------- Lanczos pass L
+// The last pass of the Lanczos iteration (after the pass H kernels in EPI_X_FIRST /
+// EPI_X_ADD mode wrote part = X_high u_j, the flips of every bit above the tile, unscaled):
+// per tile of 2^TB consecutive amplitudes (bits 0..TB-1)
+//    H v_j = su_j ((D - sigma) u_j + X_low u_j + part)            (formed on chip only)
+//    w     = H v_j - (a_j su_j) u_j - (b_j su_{j-1}) u_{j-1}        (stored: u_{j+1})
+// with FP64 partials 0 ||w||^2, 1-2 <v_j, w>, 3 ||(H - sigma) v_j||^2 and 4 the part of the
+// NEXT iteration's <w, (H - sigma) w> that this tile can see, Re <w, (D - sigma + X_low) w>
+// (w is written into a shared-memory buffer whose flips are applied one tile later, after
+// the next tile's block barrier, so the pass keeps one barrier per tile).  The flips of
+// the higher bits of <w, H w> come from the next iteration's pass H, which reads w anyway.
+// E0: the start of a run: no recurrence, partials 4-5 = <u, (D - sigma + X_low) u>.
+// u_j arrives by cp.async.bulk into SL stages; part and u_{j-1} are read with streaming
+// loads one tile ahead into registers, after a bulk L2 prefetch two tiles ahead.  The
+// per-tile scalars of the diagonal (energy of the bits above the tile and their crosses
+// with the tile bits) are computed one tile ahead by all warps, one value per warp.
+// block_sum scratch: (threads / 32) * NRED doubles, up to 512 threads
+constexpr int LZ_MAX_THREADS = 512;
+template <typename C, int TB>
+__host__ __device__ constexpr size_t pass_lz_smem() {
+    return (SL + 2) * (sizeof(C) << TB) + 8 * SL +
+           sizeof(double) * (MAXQ * UPAD + MAXQ + SL * 64 + (LZ_MAX_THREADS / 32) * NRED);
+}
+
+template <typename C> __device__ __forceinline__ C ldcs_c(const C *p) { return __ldcs(p); }
+
+// (hr, hi) = acc + d v, in the accumulator's own precision (packed FP32x2 for complex64)
+template <typename R, typename C>
+__device__ __forceinline__ void acc_diag_parts(Acc<R> &acc, R d, const C &v, R &hr, R &hi) {
+    if constexpr (std::is_same<R, float>::value) {
+        acc.diag(d, v);
+        const float2 t = upk2(acc.a);
+        hr = t.x;
+        hi = t.y;
+    } else {
+        hr = fma(d, v.x, acc.r);
+        hi = fma(d, v.y, acc.i);
+    }
+}
+
+// Scalars of the tile at `base` (TB + 1 values into sc: crosses sum_{p >= TB, x_p = 1}
+// U[q][p] for q < TB, then the energy of the bits above the tile minus sigma), value i by
+// warp i mod NW, the high bits over the lanes.
+template <int TB>
+__device__ __forceinline__ void lz_tile_scalars(int64_t base, int n, const double *fld, const double *Ush,
+                                                double sigma, double *sc, int warp, int lane, int nw) {
+    const int p = TB + lane;
+    const bool on = p < n && ((base >> p) & 1);
+    for (int i = warp; i <= TB; i += nw) {
+        double v = 0.0;
+        if (on) {
+            if (i < TB) {
+                v = Ush[i * UPAD + p];
+            } else {
+                v = fld[p];
+                for (int p2 = p + 1; p2 < n; ++p2)
+                    if ((base >> p2) & 1) v += Ush[p * UPAD + p2];
+            }
+        }
+        v = warp_sum(v);
+        if (lane == 0) sc[i] = i == TB ? v - sigma : v;
+    }
+}
+
+template <typename R, bool REALC, int TB, int RB, bool E0>
+__global__ void __launch_bounds__(1 << (TB - RB), (sizeof(R) == 4) ? 2 : 1)
+k_pass_lz(const PassParams P, LzArgs A) {
+    typedef typename cvec<R>::T C;
+    constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB, NW = NT / 32;
+    constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
+    constexpr bool F32 = std::is_same<R, float>::value;
+    static_assert(NT <= LZ_MAX_THREADS, "block_sum scratch is sized for LZ_MAX_THREADS");
+    if (A.gate && *A.gate != 0) return;
+    extern __shared__ __align__(128) unsigned char smem_pass[];
+    C *tiles = reinterpret_cast<C *>(smem_pass);               // [SL][2^TB]: u_j
+    C *wsm = tiles + ((int64_t)SL << TB);                      // [2][2^TB]: w
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + (SL + 2) * TILE_BYTES);
+    double *Ush = reinterpret_cast<double *>(smem_pass + (SL + 2) * TILE_BYTES + 8 * SL);
+    double *fld = Ush + MAXQ * UPAD;
+    double *scal = fld + MAXQ;  // [SL][64]: crossT[SB] crossR[RB] eh
+    double *red_scr = scal + SL * 64;
+
+    const int n = P.n;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int64_t ntiles = int64_t(1) << (n - TB);
+    const int64_t grid = gridDim.x;
+    const C *__restrict__ u = reinterpret_cast<const C *>(A.u);
+    const C *__restrict__ part = reinterpret_cast<const C *>(A.part);
+    const C *__restrict__ up = reinterpret_cast<const C *>(A.up);
+    C *__restrict__ out = reinterpret_cast<C *>(A.out);
+
+    for (int k = tid; k < MAXQ * MAXQ; k += NT) Ush[(k / MAXQ) * UPAD + (k % MAXQ)] = P.U[k];
+    for (int k = tid; k < MAXQ; k += NT) fld[k] = P.field[k];
+    if (tid == 0) {
+        for (int b = 0; b < SL; ++b) mbar_init(&bars[b], 1);
+        fence_mbar_init();
+    }
+    const double sigma = A.eshift ? *A.eshift : 0.0;
+    __syncthreads();
+    if (tid == 0) {
+        for (int b = 0; b < SL - 1; ++b) {
+            const int64_t s0 = blockIdx.x + (int64_t)b * grid;
+            if (s0 >= ntiles) break;
+            mbar_expect_tx(&bars[b], TILE_BYTES);
+            bulk_load(tiles + ((int64_t)b << TB), u + (s0 << TB), TILE_BYTES, &bars[b]);
+            if (!E0 && b == 0) {  // the loop's L2 prefetch runs two tiles ahead: tile 1 here
+                const int64_t s2 = s0 + grid;
+                if (s2 < ntiles) {
+                    bulk_prefetch_l2(part + (s2 << TB), TILE_BYTES);
+                    if (up) bulk_prefetch_l2(up + (s2 << TB), TILE_BYTES);
+                }
+            }
+        }
+    }
+    // scalars of the first tile (visible after the loop's first barrier)
+    if ((int64_t)blockIdx.x < ntiles)
+        lz_tile_scalars<TB>((int64_t)blockIdx.x << TB, n, fld, Ush, sigma, scal, warp, lane, NW);
+    double su = 1.0, car = 0.0, cai = 0.0, cb = 0.0;
+    if (!E0) {
+        su = *A.su;
+        car = A.ocoef[0];
+        cai = A.ocoef[1];
+        cb = up ? A.ocoef[2] : 0.0;
+    }
+    const R suR = R(su), carR = R(car), caiR = R(cai), cbR = R(cb);
+
+    // per-thread constants: energy of the thread bits and thread x register crosses
+    double ET = 0.0;
+#pragma unroll
+    for (int q = 0; q < SB; ++q) {
+        if ((tid >> q) & 1) {
+            ET += P.field[q];
+#pragma unroll
+            for (int q2 = q + 1; q2 < SB; ++q2)
+                if ((tid >> q2) & 1) ET += P.U[q * MAXQ + q2];
+        }
+    }
+    double fR[RB];
+#pragma unroll
+    for (int k = 0; k < RB; ++k) {
+        double sacc = 0.0;
+#pragma unroll
+        for (int q = 0; q < SB; ++q)
+            if ((tid >> q) & 1) sacc += P.U[(SB + k) * MAXQ + q];
+        fR[k] = sacc;
+    }
+    double red[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) red[k] = 0.0;
+
+    // part and u_{j-1} of the next tile, in flight while the current one is computed
+    C pn[NA], qn[NA];
+    auto prefetch = [&](int64_t s) {
+        const int64_t b0 = (s << TB) + tid;
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+            pn[a] = ldcs_c(part + b0 + a * NT);
+            qn[a] = up ? ldcs_c(up + b0 + a * NT) : cmake<C>(0.0, 0.0);
+        }
+    };
+    // w of the previous tile (own amplitudes) and its shifted diagonal, for the energy
+    C wp[NA];
+    R dp[NA];
+    // Re <w, (D - sigma + X_low) w> of the tile held in wsm[wbuf]
+    auto tile_energy = [&](int wbuf) {
+        const C *wt = wsm + ((int64_t)wbuf << TB);
+        R e = R(0);
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+            const int l = tid + a * NT;
+            Acc<R> acc;
+#pragma unroll
+            for (int k = 0; k < SB; ++k)
+                flip_acc<R, REALC>(P, k, (tid >> k) & 1, wt[l ^ (1 << k)], acc);
+#pragma unroll
+            for (int k = 0; k < RB; ++k)
+                flip_acc<R, REALC>(P, SB + k, (a >> k) & 1, wp[a ^ (1 << k)], acc);
+            R fr, fi;
+            acc_diag_parts<R>(acc, dp[a], wp[a], fr, fi);
+            e += R(wp[a].x) * fr + R(wp[a].y) * fi;
+        }
+        red[4] += double(e);
+    };
+
+    bool ok = true, have_prev = false;
+    int buf = 0, wb = 0;
+    uint32_t phase = 0;
+    if (!E0 && (int64_t)blockIdx.x < ntiles) prefetch(blockIdx.x);
+    for (int64_t s = blockIdx.x; s < ntiles; s += grid) {
+        const int64_t base = s << TB;
+        C *tile = tiles + ((int64_t)buf << TB);
+        const double *sc = scal + buf * 64;
+        if (ok && !mbar_wait(&bars[buf], phase)) {
+            ok = false;
+            if (A.err) atomicExch(A.err, (int)EMUSV_TIMEOUT);
+        }
+        // the tile and its scalars are visible; everyone is done with the previous tile's
+        // u buffer and with the w buffer written two tiles ago
+        __syncthreads();
+        const int nbuf = buf == 0 ? SL - 1 : buf - 1;
+        if (tid == 0 && ok) {
+            const int64_t sn = s + (int64_t)(SL - 1) * grid;  // refill the freed buffer
+            if (sn < ntiles) {
+                mbar_expect_tx(&bars[nbuf], TILE_BYTES);
+                bulk_load(tiles + ((int64_t)nbuf << TB), u + (sn << TB), TILE_BYTES, &bars[nbuf]);
+            }
+            const int64_t s2 = s + 2 * grid;
+            if (!E0 && s2 < ntiles) {
+                bulk_prefetch_l2(part + (s2 << TB), TILE_BYTES);
+                if (up) bulk_prefetch_l2(up + (s2 << TB), TILE_BYTES);
+            }
+        }
+        {  // scalars of the next tile into the slot after this one
+            const int64_t s1 = s + grid;
+            const int b1 = buf + 1 == SL ? 0 : buf + 1;
+            if (s1 < ntiles) lz_tile_scalars<TB>(s1 << TB, n, fld, Ush, sigma, scal + b1 * 64, warp, lane, NW);
+        }
+        if (!E0 && have_prev && ok) tile_energy(wb ^ 1);
+        if (ok) {
+            double St = ET + sc[TB];
+#pragma unroll
+            for (int k = 0; k < SB; ++k)
+                if ((tid >> k) & 1) St += sc[k];
+            double hR[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) hR[k] = fR[k] + sc[SB + k];
+            const R StR = R(St);
+            R hRR[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) hRR[k] = R(hR[k]);
+            C pc[NA], qc[NA];
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                pc[a] = pn[a];
+                qc[a] = qn[a];
+            }
+            C v[NA];
+#pragma unroll
+            for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
+            R rq[4] = {R(0), R(0), R(0), R(0)};  // ||w||^2, <u_j, w> re/im, ||Hv||^2 (tile sums)
+            C *wt = wsm + ((int64_t)wb << TB);
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                const int l = tid + a * NT;
+                Acc<R> acc;
+#pragma unroll
+                for (int k = 0; k < SB; ++k)  // thread bits: partner in shared memory
+                    flip_acc<R, REALC>(P, k, (tid >> k) & 1, tile[l ^ (1 << k)], acc);
+#pragma unroll
+                for (int k = 0; k < RB; ++k)  // register bits
+                    flip_acc<R, REALC>(P, SB + k, (a >> k) & 1, v[a ^ (1 << k)], acc);
+                R d = StR + (F32 ? R(P.ERf[a]) : R(P.ER[a]));
+#pragma unroll
+                for (int k = 0; k < RB; ++k)
+                    if ((a >> k) & 1) d += hRR[k];
+                const R vr = v[a].x, vi = v[a].y;
+                R hur, hui;
+                acc_diag_parts<R>(acc, d, v[a], hur, hui);
+                if (E0) {  // <u, (D - sigma + X_low) u>
+                    rq[0] += vr * hur + vi * hui;
+                    rq[1] += vr * hui - vi * hur;
+                    continue;
+                }
+                const R hr = suR * (hur + R(pc[a].x)), hi = suR * (hui + R(pc[a].y));
+                const R wr = hr - (carR * vr - caiR * vi) - cbR * R(qc[a].x);
+                const R wi = hi - (carR * vi + caiR * vr) - cbR * R(qc[a].y);
+                const C o = cmake<C>(wr, wi);
+                out[base + l] = o;
+                wt[l] = o;
+                wp[a] = o;
+                dp[a] = d;
+                const R orr = o.x, oi = o.y;
+                rq[0] += orr * orr + oi * oi;
+                rq[1] += vr * orr + vi * oi;  // <u_j, w>
+                rq[2] += vr * oi - vi * orr;
+                rq[3] += hr * hr + hi * hi;
+            }
+            if (E0) {
+                red[4] += double(rq[0]);
+                red[5] += double(rq[1]);
+            } else {
+                red[0] += double(rq[0]);
+                red[1] += su * double(rq[1]);
+                red[2] += su * double(rq[2]);
+                red[3] += double(rq[3]);
+                const int64_t s1 = s + grid;
+                if (s1 < ntiles) prefetch(s1);
+            }
+        }
+        have_prev = true;
+        wb ^= 1;
+        if (++buf == SL) {
+            buf = 0;
+            phase ^= 1u;
+        }
+    }
+    if (!E0) {
+        __syncthreads();  // the last tile's w buffer is complete
+        if (have_prev && ok) tile_energy(wb ^ 1);
+    }
+    block_sum<NRED>(red, red_scr);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NRED; ++k) A.partials[(int64_t)blockIdx.x * NRED + k] = red[k];
+    }
 }
 
 }  // namespace emusv

@@ -1,14 +1,20 @@
 // Lanczos time step exp(-i dt H) psi on the GPU (C ABI emusv_krylov_step) and the
 // building blocks of the generic krylov_exp.
 //
-// Per Lanczos iteration j (reference emu_base/math/krylov_exp.py:49-96):
-//   1. k_hpsi<HP_LANCZOS>: w = H v_j stored into basis slot j+1, fused FP64 reductions
-//      ||Hv||^2, <v_j,Hv>, <v_{j-1},Hv>, <v_j,v_{j-1}>.
-//   2. k_orth: modified Gram-Schmidt against v_{j-1} then v_j (krylov_exp.py:55-58),
-//      coefficients derived from the fused reductions; ||w||^2 partials.
-//   3. k_small (one warp): ||w||, happy-breakdown test (krylov_exp.py:63-71), the
+// Per Lanczos iteration j (reference emu_base/math/krylov_exp.py:49-96), registers wider
+// than one pass-L tile (the H-first order, lanczos_run):
+//   1. pass H kernels (k_pass_high, EPI_X_FIRST / EPI_X_ADD): part = the flips of the bits
+//      above the pass-L tile applied to v_j, and their share of <v_j, H v_j>;
+//   2. k_lz_coef: a_j = <v_j, H v_j> - b_j <v_j, v_{j-1}> with b_j = ||w_{j-1}|| (the
+//      modified Gram-Schmidt values of krylov_exp.py:55-58 in exact arithmetic);
+//   3. pass L (k_pass_lz): H v_j formed tile by tile on chip, w = H v_j - a_j v_j -
+//      b_j v_{j-1} stored into basis slot j+1, FP64 partials of ||w||^2, <v_j, w>,
+//      ||H v_j||^2 and the pass-L share of the next <v, H v>;
+//   4. k_small_lz (one warp): ||w||, happy-breakdown test (krylov_exp.py:63-71), the
 //      exponential of the extended Krylov matrix and the Expokit error estimate
 //      (krylov_exp.py:77-86), all FP64 on the device.
+// Smaller registers: k_hpsi<HP_LANCZOS> (H v with its reductions), k_orth (the recurrence),
+// k_small.
 // Basis vectors are stored unnormalised with a device scale factor (v_k = scale_k u_k),
 // so no separate normalisation pass exists; the input vector is basis vector 0 in place.
 // Every kernel after the first reads a device status word and exits at once when the
@@ -24,9 +30,11 @@ namespace emusv {
 int hpsi_tile_bits(int n);
 int launch_hpsi(int dtype, int mode, const HamParams &P, HpsiArgs A, int max_grid,
                 cudaStream_t s, int *grid_out);
-int launch_hpsi_stage(int dtype, int stages, const HamParams &H, const HpsiArgs &A, cudaStream_t s,
-                      int *grid_out);
-bool hpsi_uses_passes(int dtype, int n);
+bool lanczos_h_first(int dtype, int n);
+int lz_energy0(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out);
+int lz_low(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out);
+int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,
+            int *err, cudaStream_t s, int *nblocks_out);
 int max_grid_blocks();
 
 struct Workspace {
@@ -174,25 +182,40 @@ k_orth(KState *ks, int j, const double *part_h, int nb_h, const void *vj_, const
         for (int k = 0; k < NRED; ++k) part_o[(i64)blockIdx.x * NRED + k] = acc[k];
 }
 
-// The recurrence coefficients of iteration j from the H*psi partials (as k_orth's
-// preamble), for the recurrence fused into the next iteration's pass L: on the stored
-// vectors, w = H v_j - ocoef[0..1] u_j - ocoef[2] u_{j-1}.
-__global__ void k_orth_coef(KState *ks, int j, const double *part_h, int nb_h) {
+// H-first iteration j: <v_j, (H - sigma) v_j> is the pass-L part el (computed by the pass
+// that produced v_j -- the previous iteration's pass L, or for j = 0 the start-of-run
+// energy pass, partials 4-5 of part_e0) plus the pass-H part (partials 0-1 of part_h, on
+// the stored vector: times scale_j^2); a, b and the recurrence coefficients on the stored
+// vectors follow.
+__global__ void k_lz_coef(KState *ks, int j, const double *part_h, int nb_h, const double *part_e0,
+                          int nb_e0) {
     if (ks->status != KS_RUNNING) return;
     __shared__ double red[(BLOCK / 32) * NRED];
-    double s[NRED];
+    double s[NRED], e0[NRED];
     sum_partials<NRED>(part_h, nb_h, NRED, s, red);
+    if (j == 0) sum_partials<NRED>(part_e0, nb_e0, NRED, e0, red);
     if (threadIdx.x == 0) {
+        const double sj = ks->scale[j], s2 = sj * sj;
+        double elr, eli;
+        if (j == 0) {
+            elr = e0[4] * s2;
+            eli = e0[5] * s2;
+            ks->el_re[0] = elr;
+            ks->el_im[0] = eli;
+        } else {
+            elr = ks->el_re[j];
+            eli = ks->el_im[j];
+        }
+        const double er = elr + s[0] * s2, ei = eli + s[1] * s2;
         const double b = j > 0 ? ks->r[j - 1] : 0.0;
         const double cr = j > 0 ? ks->vv_re[j] : 0.0, ci = j > 0 ? ks->vv_im[j] : 0.0;
-        const double ar = s[1] - b * cr, ai = s[2] - b * ci;
+        const double ar = er - b * cr, ai = ei - b * ci;
         ks->a_re[j] = ar;
         ks->a_im[j] = ai;
         ks->b_re[j] = b;
         ks->b_im[j] = 0.0;
-        const double sg = ks->shift;
-        ks->hn[j] = sqrt(fmax(0.0, s[0] + 2.0 * sg * s[1] + sg * sg));
-        const double sj = ks->scale[j], sp = j > 0 ? ks->scale[j - 1] : 0.0;
+        ks->e_re[j] = er;
+        const double sp = j > 0 ? ks->scale[j - 1] : 0.0;
         ks->ocoef[0] = ar * sj;
         ks->ocoef[1] = ai * sj;
         ks->ocoef[2] = b * sp;
@@ -224,6 +247,47 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
     vr = warp_sum(vr);
     vi = warp_sum(vi);
     krylov_decide(ks, j, v, vr, vi, dt, exp_tol, norm_tol, poll != 0, first_poll != 0, maxdim);
+}
+
+// Decide H-first iteration j from the pass-L partials (0 ||w||^2, 1-2 <v_j, w>,
+// 3 ||(H - sigma) v_j||^2, 4 the pass-L part of <w, (H - sigma) w>): ||H v_j||, then as
+// k_small, then the next iteration's el = <v_{j+1}, (D - sigma + X_low) v_{j+1}>.
+__global__ void __launch_bounds__(32)
+k_small_lz(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp_tol,
+           double norm_tol, int poll, int first_poll, int maxdim) {
+    if (ks->status != KS_RUNNING) return;
+    if (ks->kerr) {  // a streaming kernel gave up on a bounded wait
+        if (threadIdx.x == 0) {
+            ks->status = KS_TIMEOUT;
+            ks->iters = j + 1;
+        }
+        return;
+    }
+    const int lane = threadIdx.x;
+    double v = 0.0, vr = 0.0, vi = 0.0, hh = 0.0, el = 0.0;
+    for (int b = lane; b < nb_o; b += 32) {
+        v += part_o[(i64)b * NRED];
+        vr += part_o[(i64)b * NRED + 1];
+        vi += part_o[(i64)b * NRED + 2];
+        hh += part_o[(i64)b * NRED + 3];
+        el += part_o[(i64)b * NRED + 4];
+    }
+    v = warp_sum(v);
+    vr = warp_sum(vr);
+    vi = warp_sum(vi);
+    hh = warp_sum(hh);
+    el = warp_sum(el);
+    if (lane == 0) {
+        // ||H v||^2 = ||(H - sigma) v||^2 + 2 sigma Re<v,(H - sigma) v> + sigma^2
+        const double sg = ks->shift;
+        ks->hn[j] = sqrt(fmax(0.0, hh + 2.0 * sg * ks->e_re[j] + sg * sg));
+    }
+    __syncwarp();
+    krylov_decide(ks, j, v, vr, vi, dt, exp_tol, norm_tol, poll != 0, first_poll != 0, maxdim);
+    if (lane == 0) {
+        ks->el_re[j + 1] = v > 0.0 ? el / v : 0.0;  // v_{j+1} = w / ||w||
+        ks->el_im[j + 1] = 0.0;
+    }
 }
 
 // out = s0 * sum_k c_k scale_k stored_k ;  ||out||^2 partials.
@@ -491,71 +555,65 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
     EMUSV_CHECK_LAUNCH();
 
     int status = KS_RUNNING;
-    // Registers whose H*psi takes several passes run the recurrence of iteration j inside
-    // the pass L of iteration j+1 (one streaming pass fewer per iteration): pass L of v_0
-    // first, then per iteration the H passes, the coefficients, the fused pass L, k_small.
-    const bool fused = hpsi_uses_passes(dtype, nqubits);
-    if (fused) {
-        HpsiArgs A0 = {};
-        A0.u = stored(0);
-        A0.su_dev = &W.ks->scale[0];
-        A0.part_buf = part_vec;
-        A0.gate = &W.ks->status;
-        A0.err = &W.ks->kerr;
-        A0.eshift = &W.ks->shift;
-        A0.tile_bits = hpsi_tile_bits(nqubits);
-        int st = launch_hpsi_stage(dtype, 1, P, A0, s, nullptr);
+    // Registers wider than one pass-L tile run the H-first iteration: the pass H kernels
+    // write part = X_high v_j (the flips of the bits above the pass-L tile) and their share
+    // of <v_j, H v_j>; k_lz_coef forms a_j; the pass L kernel forms H v_j tile by tile and
+    // writes w = H v_j - a_j v_j - b_j v_{j-1} and the pass-L share of <w, H w> for the
+    // next a; k_small_lz decides.  Streamed vector units per iteration: pass L 4 (read v_j,
+    // part, v_{j-1}; write w), one H pass 2 (read v_j, write part) or two H passes 2 + 3.
+    const bool hfirst = lanczos_h_first(dtype, nqubits);
+    if (hfirst) {
+        LzArgs E = {};
+        E.u = stored(0);
+        E.eshift = &W.ks->shift;
+        E.partials = W.part_o;
+        E.gate = &W.ks->status;
+        E.err = &W.ks->kerr;
+        int ge0 = 0;
+        int st = lz_energy0(dtype, P, E, s, &ge0);
         if (st) return st;
-    }
-    for (int j = 0; fused && j < max_krylov_dim; ++j) {
-        if (j + 1 > capacity) {
-            int st = read_status(W.ks, s, &status);
-            if (st) return st;
-            if (status == KS_RUNNING) return EMUSV_WORKSPACE_TOO_SMALL;
-            break;
-        }
-        HpsiArgs A = {};
-        A.u = stored(j);
-        A.su_dev = &W.ks->scale[j];
-        A.out = const_cast<void *>(stored(j + 1));
-        A.partials = W.part_h;
-        A.tile_bits = hpsi_tile_bits(nqubits);
-        A.gate = &W.ks->status;
-        A.err = &W.ks->kerr;
-        A.part_buf = part_vec;
-        A.eshift = &W.ks->shift;
-        int gh = 0, go = 0;
-        int st = launch_hpsi_stage(dtype, 2, P, A, s, &gh);
-        if (st) return st;
-        {
-            ProfScope ps_(PROF_SMALL, s);
-            k_orth_coef<<<1, BLOCK, 0, s>>>(W.ks, j, W.part_h, gh);
-        }
-        EMUSV_CHECK_LAUNCH();
-        HpsiArgs B = A;
-        B.u = stored(j + 1);  // H v_j in, w out (in place)
-        B.su_dev = nullptr;
-        B.su = 1.0;
-        B.vj = stored(j);
-        B.vp = j > 0 ? stored(j - 1) : nullptr;
-        B.ocoef = W.ks->ocoef;
-        B.oscale = &W.ks->scale[j];
-        B.part_o = W.part_o;
-        if ((st = launch_hpsi_stage(dtype, 4, P, B, s, &go))) return st;
-        const int poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
-        {
-            ProfScope ps_(PROF_SMALL, s);
-            k_small<<<1, 32, 0, s>>>(W.ks, j, W.part_o, go, dt, exp_tolerance, norm_tolerance, 1,
-                                     j == 0, max_krylov_dim);
-        }
-        EMUSV_CHECK_LAUNCH();
-        if (poll) {
-            st = read_status(W.ks, s, &status);
-            if (st) return st;
-            if (status != KS_RUNNING) break;
+        for (int j = 0; j < max_krylov_dim; ++j) {
+            if (j + 1 > capacity) {
+                st = read_status(W.ks, s, &status);
+                if (st) return st;
+                if (status == KS_RUNNING) return EMUSV_WORKSPACE_TOO_SMALL;
+                break;
+            }
+            int gh = 0, go = 0;
+            if ((st = lz_high(dtype, P, stored(j), part_vec, W.part_h, &W.ks->status, &W.ks->kerr, s, &gh)))
+                return st;
+            {
+                ProfScope ps_(PROF_SMALL, s);
+                k_lz_coef<<<1, BLOCK, 0, s>>>(W.ks, j, W.part_h, gh, W.part_o, ge0);
+            }
+            EMUSV_CHECK_LAUNCH();
+            LzArgs B = {};
+            B.u = stored(j);
+            B.part = part_vec;
+            B.up = j > 0 ? stored(j - 1) : nullptr;
+            B.out = const_cast<void *>(stored(j + 1));
+            B.su = &W.ks->scale[j];
+            B.ocoef = W.ks->ocoef;
+            B.eshift = &W.ks->shift;
+            B.partials = W.part_o;
+            B.gate = &W.ks->status;
+            B.err = &W.ks->kerr;
+            if ((st = lz_low(dtype, P, B, s, &go))) return st;
+            const int poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
+            {
+                ProfScope ps_(PROF_SMALL, s);
+                k_small_lz<<<1, 32, 0, s>>>(W.ks, j, W.part_o, go, dt, exp_tolerance, norm_tolerance, 1,
+                                            j == 0, max_krylov_dim);
+            }
+            EMUSV_CHECK_LAUNCH();
+            if (poll) {
+                st = read_status(W.ks, s, &status);
+                if (st) return st;
+                if (status != KS_RUNNING) break;
+            }
         }
     }
-    for (int j = 0; !fused && j < max_krylov_dim; ++j) {
+    for (int j = 0; !hfirst && j < max_krylov_dim; ++j) {
         if (j + 1 > capacity) {
             int st = read_status(W.ks, s, &status);
             if (st) return st;

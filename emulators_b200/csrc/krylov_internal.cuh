@@ -26,6 +26,10 @@ struct KState {
     double scale[KMAX + 2];          // v_k = scale[k] * stored_k
     double c_re[KMAX + 2], c_im[KMAX + 2];  // result coefficients
     double ocoef[4];  // recurrence coefficients on the stored vectors (fused pass L)
+    // H-first iteration: <v_k, (H - sigma) v_k> (real part), and its part from the diagonal
+    // and the pass-L tile flips, which the pass producing v_k computes
+    double e_re[KMAX];
+    double el_re[KMAX + 2], el_im[KMAX + 2];
 };
 
 
