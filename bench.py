@@ -301,6 +301,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                                "over 2us, dt=5ns, tol=1e-10, complex64/FP64",
                    "nqubits": n, "dt_ns": 5.0, "tolerance": w.tolerance,
                    "krylov_iterations_mean": round(float(np.mean(timed_iters)), 2),
+                   "steps_window": [W, W + K - 1],
+                   "krylov_iterations_per_s": round(sum(timed_iters) / elapsed * world, 3),
                    "l2": "state and Krylov vectors (512 MiB each) exceed L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm",
@@ -324,10 +326,15 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "e2e": e2e,
     }
     if not args.no_plain and world == 1:
-        plain = plain_torch_c128(w, dev)
+        plain = plain_torch_c128(w, dev, steps=2, warm=W)
         plain["ours_c64_over_plain"] = round(value / world / plain["steps_per_s"], 2)
         result["secondary"]["plain_torch_c128_gpu"] = plain
         log(f"plain complex128 torch path: {plain}")
+    if not args.no_c128 and world == 1:
+        result["secondary"]["ladder_n26_c128"] = ladder_c128(dev, W)
+        log(f"ladder_n26 complex128: {result['secondary']['ladder_n26_c128']}")
+        result["secondary"]["lattice_n20_c128"] = lattice_c2(dev)
+        log(f"lattice_n20 complex128: {result['secondary']['lattice_n20_c128']}")
     if not args.no_batch and world == 1:
         result["secondary"]["batch_256_c64"] = batch_c4(dev)
         log(f"batch: {result['secondary']['batch_256_c64']}")
@@ -345,7 +352,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         result["secondary"]["precision"] = precision_check(w, dev)
         log(f"precision: {result['secondary']['precision']}")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
+        result["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds, start=W)
     if dist:
         dist.destroy_process_group()
     return result if rank == 0 else None
@@ -392,6 +399,122 @@ def run_e2e(w, W, K, dev, dist, world) -> dict:
             "d2h_bytes_per_step": int(d2h), "wall_s": round(wall, 3),
             "api": "SVBackendImpl(SVConfig(precision='c64'), SequenceData)._run()",
             "observations": n_obs}
+
+
+# ------------------------------------------------------------------ complex128 at N=26
+def ladder_c128(dev, W: int, K: int = 6) -> dict:
+    """The headline workload in complex128 vectors: W untimed steps, then K steps timed with
+    CUDA events (state resident in HBM), and the Lanczos iteration's roofline from the
+    library's per-kind device times over 3 further steps (6 D s algorithmic bytes, s = 16)."""
+    import torch
+
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian, _lib, krylov
+    from emulators_b200 import workloads as wl
+    from emulators_b200.krylov import fused_step
+
+    w = wl.ladder_n26()
+    n, D = w.nqubits, 1 << w.nqubits
+    L = _lib.load()
+    U = torch.as_tensor(w.U)
+    krylov.release_workspaces()
+    torch.cuda.empty_cache()
+    a = torch.zeros(D, dtype=torch.complex128, device=dev)
+    a[0] = 1.0
+    b = torch.empty_like(a)
+    iters = []
+
+    def step(k):
+        nonlocal a, b
+        H = RydbergHamiltonian(torch.as_tensor(w.omega[k]), torch.as_tensor(w.delta[k]),
+                               torch.as_tensor(w.phi[k]), U, dev)
+        _, info, st = fused_step(HamiltonianExpOperator(H, w.dt), a, w.tolerance, w.tolerance,
+                                 w.max_krylov_dim, out=b)
+        _lib.check(st, "krylov step")
+        iters.append(info.iterations)
+        a, b = b, a
+
+    for k in range(W):
+        step(k)
+    torch.cuda.synchronize()
+    iters.clear()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(W, W + K):
+        step(k)
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    timed = list(iters)
+    iters.clear()
+    L.emusv_profile_begin(1)
+    for k in range(W + K, W + K + 3):
+        step(k)
+    torch.cuda.synchronize()
+    pms = np.zeros(8)
+    pl = np.zeros(8, dtype=np.int64)
+    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
+    iter_s = (pms[0] + pms[7]) / max(sum(iters), 1) / 1e3
+    hbm, which = peaks()
+    ach = 6 * D * 16 / iter_s / 1e9
+    del a, b
+    krylov.release_workspaces()
+    torch.cuda.empty_cache()
+    return {"steps_per_s": round(K / el, 4), "ms_per_step": round(el / K * 1e3, 3),
+            "steps_window": [W, W + K - 1], "krylov_iterations": timed,
+            "krylov_iterations_per_s": round(sum(timed) / el, 3),
+            "roofline": {"achieved": round(ach, 1), "peak": hbm, "peak_source": which,
+                         "unit": "GB/s", "frac": round(ach / hbm, 4),
+                         "iteration_ms": round(iter_s * 1e3, 4),
+                         "note": "Lanczos iteration (pass H kernels + recurrence pass L), "
+                                 "6*D*16 algorithmic bytes"},
+            "note": "complex128 vectors, same kernels and step window as the complex64 headline"}
+
+
+# ------------------------------------------------------------------ config 2: N=20 lattice
+def lattice_c2(dev, plain_budget_s: float = 20.0) -> dict:
+    """The plain-method drop-in configuration: N=20 4x5 lattice at 6 um, sin^2 Omega (peak
+    2 pi), delta -15 -> 15 over 3 us, dt = 10 ns (300 steps), complex128, Krylov dim <= 30,
+    tolerance 1e-10, occupation and energy every 100 ns.  Ours: the whole run through
+    SVBackendImpl (state and results on the host at the end), CUDA events; the plain
+    complex128 torch path (reference algorithm in plain tensor ops) with the same
+    observables on the first steps of the same run, and ours on that same window."""
+    import torch
+
+    from emulators_b200 import krylov
+    from emulators_b200 import workloads as wl
+    from emulators_b200.runner import run_workload
+
+    w = wl.lattice_n20()
+    krylov.release_workspaces()
+    run_workload(w, nsteps=10)  # workspaces and kernels warm
+    torch.cuda.synchronize()
+
+    def timed(nsteps=None):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        r = run_workload(w, nsteps=nsteps)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, time.perf_counter() - t0, r
+
+    el, wall, r = timed()
+    # the plain path: as many steps of the same run as fit the budget (a multiple of the
+    # observation interval), from |g...g>
+    probe = plain_torch_c128(w, dev, steps=w.obs_every, warm=0, obs_every=w.obs_every)
+    per_step = 1.0 / probe["steps_per_s"]
+    kp = int(max(1, min(w.nsteps // w.obs_every, plain_budget_s / per_step / w.obs_every))) * w.obs_every
+    plain = plain_torch_c128(w, dev, steps=kp, warm=0, obs_every=w.obs_every)
+    el_w, _, _ = timed(kp)
+    krylov.release_workspaces()
+    return {"steps": w.nsteps, "steps_per_s": round(w.nsteps / el, 3),
+            "ms_per_step": round(el / w.nsteps * 1e3, 4), "wall_s": round(wall, 3),
+            "observations": int(len(r["energy"])),
+            "api": "SVBackendImpl(SVConfig(precision='c128'), SequenceData)._run(), "
+                   "occupation + energy every 10 steps",
+            "window_steps": kp, "ours_window_steps_per_s": round(kp / el_w, 3),
+            "plain_torch_c128_gpu": plain,
+            "ours_over_plain_same_window": round((kp / el_w) / plain["steps_per_s"], 2)}
 
 
 # ------------------------------------------------------------------ precision form check
@@ -441,7 +564,7 @@ def precision_check(w, dev) -> dict:
 
 
 # ------------------------------------------------------------------ plain complex128 GPU path
-def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1) -> dict:
+def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1, obs_every: int = 0) -> dict:
     """The plain complex128 GPU path: the reference's algorithm written with plain torch
     tensor ops (the reference modules themselves are not on the GPU machine) -- per-qubit
     strided-view flips, the diagonal rebuilt every step from view slices, the Lanczos loop
@@ -489,6 +612,7 @@ def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1) -> dict:
             T[j + 1, j] = n2
             if n2 < tol:
                 e = scipy.linalg.expm(T[:j + 1, :j + 1])[:, 0]
+                its.append(j + 1)
                 return nrm * sum(complex(e[i]) * V[i] for i in range(j + 1))
             V.append(wv / n2)
             T[j + 2, j + 1] = 1.0
@@ -496,13 +620,27 @@ def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1) -> dict:
             err1, err2 = abs(e[j + 1]), abs(e[j + 2] * nn)
             err = err1 if err1 < err2 else err1 * err2 / (err1 - err2)
             if err < tol:
+                its.append(j + 1)
                 return nrm * sum(complex(e[i]) * V[i] for i in range(j + 2))
         raise RecursionError("plain path did not converge")
 
+    def observe(k, psi):
+        # occupation per qubit and Re <psi|H psi> on the host, as the reference's
+        # callbacks return them (custom_callback_implementations.py:30-47,
+        # hamiltonian.py:164-172); the step's H (midpoint samples of step k)
+        coef = 0.5 * np.asarray(w.omega[k]) * np.exp(1j * np.asarray(w.phi[k]))
+        occ = torch.stack([psi.view(2 ** i, 2, -1)[:, 1].abs().pow(2).sum() for i in range(n)]).cpu()
+        en = torch.vdot(psi, hpsi(psi, diagonal(w.delta[k]), coef)).real.cpu()
+        return occ, en
+
+    its: list[int] = []
     psi = torch.zeros(D, dtype=torch.complex128, device=dev)
     psi[0] = 1.0
     for k in range(warm):
         psi = step(k, psi)
+        if obs_every and (k + 1) % obs_every == 0:
+            observe(k, psi)
+    its.clear()
     if dev.type != "cuda":  # host run (checks of this function only)
         for k in range(warm, warm + steps):
             psi = step(k, psi)
@@ -512,14 +650,20 @@ def plain_torch_c128(w, dev, steps: int = 2, warm: int = 1) -> dict:
     e0.record()
     for k in range(warm, warm + steps):
         psi = step(k, psi)
+        if obs_every and (k + 1) % obs_every == 0:
+            observe(k, psi)
     e1.record()
     torch.cuda.synchronize()
     el = e0.elapsed_time(e1) / 1e3
     del psi
     torch.cuda.empty_cache()
     return {"steps_per_s": round(steps / el, 4), "unit": UNIT,
-            "sample": f"steps {warm}..{warm + steps - 1} of ladder_n26 in complex128 after "
-                      f"{warm} warm-up step(s); CUDA events"}
+            "krylov_iterations": list(its),
+            "krylov_iterations_per_s": round(sum(its) / el, 4),
+            "sample": f"steps {warm}..{warm + steps - 1} of {w.name} in complex128 after "
+                      f"{warm} warm-up step(s) (the timed window of the ours arm starts at the "
+                      f"same step)" + (f", occupation and energy every {obs_every} steps"
+                                       if obs_every else "") + "; CUDA events"}
 
 
 # ------------------------------------------------------------------ plain complex128 GPU gradients
@@ -1010,9 +1154,10 @@ def lindblad_dm(dev, steps: int = 8) -> dict:
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
-def cpu_baseline(w, budget_s: float) -> dict:
+def cpu_baseline(w, budget_s: float, start: int = 0) -> dict:
     """The oracle (C/OpenMP restatement of the reference path, FP64/complex128) timed on
-    this host's cores on the first steps of the same workload; stops after budget_s."""
+    this host's cores on the same step window as the GPU arm: steps 0..start-1 run untimed
+    (the GPU arm's warm-up), then steps from `start` are timed until budget_s."""
     from oracle import oracle
 
     oracle.build()
@@ -1021,11 +1166,16 @@ def cpu_baseline(w, budget_s: float) -> dict:
     n = w.nqubits
     s = np.zeros(1 << n, dtype=np.complex128)
     s[0] = 1.0
+    for k in range(min(start, w.nsteps - 1)):
+        s, _, _ = oracle.evolve_step(w.dt, w.omega[k], w.delta[k], w.phi[k], w.U, s,
+                                     w.tolerance, w.max_krylov_dim)
+    k0 = min(start, w.nsteps - 1)
     t0 = time.perf_counter()
     done = 0
     iters = []
-    while done < w.nsteps:
-        s, _, info = oracle.evolve_step(w.dt, w.omega[done], w.delta[done], w.phi[done], w.U, s,
+    while k0 + done < w.nsteps:
+        k = k0 + done
+        s, _, info = oracle.evolve_step(w.dt, w.omega[k], w.delta[k], w.phi[k], w.U, s,
                                         w.tolerance, w.max_krylov_dim)
         iters.append(info.iteration_count)
         done += 1
@@ -1033,8 +1183,11 @@ def cpu_baseline(w, budget_s: float) -> dict:
             break
     el = time.perf_counter() - t0
     return {"value": round(done / el, 6), "unit": UNIT, "cores": oracle.num_threads(),
-            "kind": "port",
-            "sample": f"first {done} time step(s) of ladder_n26 in complex128 on the host "
+            "kind": "port", "steps_window": [k0, k0 + done - 1],
+            "krylov_iterations": iters,
+            "krylov_iterations_per_s": round(sum(iters) / el, 4),
+            "sample": f"time steps {k0}..{k0 + done - 1} of ladder_n26 (after the GPU arm's "
+                      f"{k0} warm-up steps, run untimed here) in complex128 on the host "
                       f"({el:.1f} s, Krylov iterations {iters})"}
 
 
@@ -1045,14 +1198,17 @@ def run_reference(args, rank: int) -> dict | None:
     from emulators_b200 import workloads as wl
 
     w = wl.ladder_n26()
-    cb = cpu_baseline(w, args.cpu_seconds)
+    cb = cpu_baseline(w, args.cpu_seconds, start=args.warmup)
     return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic",
             "config": {"workload": "ladder_n26 (same as the ours arm), reference algorithm "
                                    "restated on the host CPU (oracle port)",
-                       "steps_note": "each step is a bounded sample: time steps run until "
+                       "steps_window": cb["steps_window"],
+                       "krylov_iterations_per_s": cb["krylov_iterations_per_s"],
+                       "steps_note": "the warm-up steps run untimed, then time steps from the "
+                                     "same index as the ours arm's timed window run until "
                                      f"{args.cpu_seconds:.0f} s of CPU work"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -1074,6 +1230,8 @@ def main():
                     help="skip the batched evolution and batched gradient workloads")
     ap.add_argument("--no-noisy", action="store_true",
                     help="skip the Monte Carlo (noisy Hamiltonian, Arnoldi) workload")
+    ap.add_argument("--no-c128", action="store_true",
+                    help="skip the complex128 N=26 line and the N=20 lattice line")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the complex64-vs-complex128 run of the whole workload")
     args = ap.parse_args()

@@ -399,8 +399,10 @@ __device__ __forceinline__ void load_rows(const KState *ks, int m, double dt, do
 // applied to e_0 = (y, x1, x2) (krylov_exp.py:77-78); writes the coefficients
 // c[0..jj+1] = (y, x1) and returns the Expokit error estimate (krylov_exp.py:81-84).
 // One warp, Chebyshev form.
-static __device__ __noinline__ double krylov_eval(KState *ks, int jj, double dt) {
-    constexpr int NE = (KMAX + 2 + 31) / 32;
+// NE entries per lane: the smallest layout that holds the jj + 3 rows (the work of every
+// Chebyshev term scales with NE; each entry's arithmetic is the same in every layout).
+template <int NE>
+static __device__ __noinline__ double krylov_eval_ne(KState *ks, int jj, double dt) {
     const int lane = threadIdx.x & 31;
     const int m = jj + 1, M = m + 2;
     double2 d[NE], l[NE], u[NE], y[NE];
@@ -434,6 +436,14 @@ static __device__ __noinline__ double krylov_eval(KState *ks, int jj, double dt)
     }
     __syncwarp();
     return err1 < err2 ? err1 : (err1 * err2 / (err1 - err2));  // krylov_exp.py:84
+}
+static __device__ double krylov_eval(KState *ks, int jj, double dt) {
+    constexpr int NEMAX = (KMAX + 2 + 31) / 32;
+    const int M = jj + 3;
+    if (M <= 32) return krylov_eval_ne<1>(ks, jj, dt);
+    if (M <= 64) return krylov_eval_ne<2>(ks, jj, dt);
+    if (M <= 96) return krylov_eval_ne<3>(ks, jj, dt);
+    return krylov_eval_ne<NEMAX>(ks, jj, dt);
 }
 
 // Decide iteration j of a Lanczos run from the FP64 sums v = ||w_j||^2 and
