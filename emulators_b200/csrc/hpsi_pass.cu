@@ -136,7 +136,7 @@ static int launch_low(const PassParams &P, const PassArgs &A, cudaStream_t s, in
 
 // One strided pass over the group bits [hpos, hpos + TB - CMIN) with CMIN chunk bits;
 // group bits below hskip (the pass-L tile width) were applied by pass L and are skipped.
-template <typename R, bool REALC, int EPI, int CMIN>
+template <typename R, bool REALC, int EPI, int CMIN, bool CHUNKF = false>
 static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *part,
                        cudaStream_t s, int *grid_out, int hskip = PassShape<R>::TB) {
     typedef typename cvec<R>::T C;
@@ -155,7 +155,7 @@ static int launch_high(PassParams P, int hpos, const PassArgs &A, const void *pa
     if (!encode_pass_high(&M.u, A.u, n, (int)sizeof(C), P) ||
         (HASPART && !encode_pass_high(&M.part, part, n, (int)sizeof(C), P)))
         return EMUSV_CUDA_ERROR;
-    auto kern = k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0>;
+    auto kern = k_pass_high<R, REALC, TB, RB, EPI, CMIN, 0, CHUNKF>;
     const size_t smem = pass_high_smem<C, TB, HASPART>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -261,6 +261,12 @@ template <> struct LzShape<double> {
     static constexpr int TB = 11, RB = 2;
 };
 
+// The chunk bits of the pass H rows of this register (the bits the recurrence pass L
+// leaves out): 64-byte rows where two H passes cover the bits above pass L, else 32-byte.
+template <typename R> static int lz_chunk_bits(int n) {
+    constexpr int TB = PassShape<R>::TB, CMIN = PassShape<R>::CMIN, TBL = LzShape<R>::TB;
+    return n - TBL <= 2 * (TB - CMIN) ? CMIN : CMIN - 1;
+}
 // The Lanczos iteration of this register runs in the H-first order (pass H kernels, then
 // the recurrence pass L): registers wider than one pass-L tile.
 bool lz_applies(int dtype, int n) {
@@ -269,13 +275,13 @@ bool lz_applies(int dtype, int n) {
     return false;
 }
 
-template <typename R, bool REALC, bool E0>
-static int launch_lz(const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
+template <typename R, bool REALC, bool E0, int C0>
+static int launch_lz_c(const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = LzShape<R>::TB, RB = LzShape<R>::RB, NT = 1 << (TB - RB);
     PassParams P;
     fill_params(H, TB, RB, &P);
-    auto kern = k_pass_lz<R, REALC, TB, RB, E0>;
+    auto kern = k_pass_lz<R, REALC, TB, RB, E0, C0>;
     const size_t smem = pass_lz_smem<C, TB>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -291,6 +297,14 @@ static int launch_lz(const HamParams &H, const LzArgs &A, cudaStream_t s, int *g
     EMUSV_CHECK_LAUNCH();
     if (grid_out) *grid_out = (int)grid;
     return EMUSV_OK;
+}
+
+// The pass L leaves out the chunk bits of the register's pass H rows.
+template <typename R, bool REALC, bool E0>
+static int launch_lz(const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
+    constexpr int CMIN = PassShape<R>::CMIN;
+    if (lz_chunk_bits<R>(H.n) == CMIN) return launch_lz_c<R, REALC, E0, CMIN>(H, A, s, grid_out);
+    return launch_lz_c<R, REALC, E0, CMIN - 1>(H, A, s, grid_out);
 }
 
 // Start of a run: partials 4-5 of <u, (D - sigma + X_low) u> (A.u, A.eshift, A.partials,
@@ -314,11 +328,13 @@ int lz_low(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *
                        : launch_lz<double, false, false>(H, A, s, grid_out);
 }
 
-// part = X_high u (unscaled flips of every bit above the pass-L tile) in one or two
-// strided passes; their <u, X u> partials go to partials[0 .. *nblocks_out) (rows of NRED).
+// part = X_high u (unscaled flips of every bit above the pass-L tile, and of the CMIN
+// chunk bits of the pass H rows, applied by the last pass) in one or two strided passes;
+// their <u, X u> partials go to partials[0 .. *nblocks_out) (rows of NRED); *c0_out = CMIN
+// (the bits the recurrence pass L leaves out).
 template <typename R, bool REALC, int CMIN>
 static int lz_high_t(const HamParams &H, const void *u, void *part, double *partials, const int *gate,
-                     int *err, cudaStream_t s, int *nblocks_out) {
+                     int *err, cudaStream_t s, int *nblocks_out, int *c0_out) {
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, TBL = LzShape<R>::TB;
     const int n = H.n, rem = n - TBL, G = TB - CMIN;
     if (rem < 1 || rem > 2 * G) return EMUSV_BAD_ARGUMENT;
@@ -335,21 +351,23 @@ static int lz_high_t(const HamParams &H, const void *u, void *part, double *part
     if (rem > G) {
         if ((st = launch_high<R, REALC, EPI_X_FIRST, CMIN>(P, n - 2 * G, A, nullptr, s, &g1, TBL))) return st;
         A.partials = partials + (size_t)g1 * NRED;
-        if ((st = launch_high<R, REALC, EPI_X_ADD, CMIN>(P, n - G, A, part, s, &g2, TBL))) return st;
+        if ((st = launch_high<R, REALC, EPI_X_ADD, CMIN, true>(P, n - G, A, part, s, &g2, TBL))) return st;
     } else {
-        if ((st = launch_high<R, REALC, EPI_X_FIRST, CMIN>(P, n - G, A, nullptr, s, &g2, TBL))) return st;
+        if ((st = launch_high<R, REALC, EPI_X_FIRST, CMIN, true>(P, n - G, A, nullptr, s, &g2, TBL)))
+            return st;
     }
     *nblocks_out = g1 + g2;
+    *c0_out = CMIN;
     return EMUSV_OK;
 }
 
 template <typename R, bool REALC>
 static int lz_high_rows(const HamParams &H, const void *u, void *part, double *partials, const int *gate,
                         int *err, cudaStream_t s, int *nb) {
-    // 64-byte rows where two H passes cover the bits above pass L, else 32-byte rows
-    constexpr int TB = PassShape<R>::TB, CMIN = PassShape<R>::CMIN, TBL = LzShape<R>::TB;
-    if (H.n - TBL <= 2 * (TB - CMIN)) return lz_high_t<R, REALC, CMIN>(H, u, part, partials, gate, err, s, nb);
-    return lz_high_t<R, REALC, CMIN - 1>(H, u, part, partials, gate, err, s, nb);
+    constexpr int CMIN = PassShape<R>::CMIN;
+    int c0 = 0;
+    if (lz_chunk_bits<R>(H.n) == CMIN) return lz_high_t<R, REALC, CMIN>(H, u, part, partials, gate, err, s, nb, &c0);
+    return lz_high_t<R, REALC, CMIN - 1>(H, u, part, partials, gate, err, s, nb, &c0);
 }
 
 int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,

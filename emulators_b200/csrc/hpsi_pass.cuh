@@ -509,8 +509,11 @@ struct PassHighMaps {
     CUtensorMap part;  // partial sums of pass L
 };
 
-// CT: chunk bits c (compile time); PBH: cluster bits.
-template <typename R, bool REALC, int TB, int RB, int EPI, int CT, int PBH>
+// CT: chunk bits c (compile time); PBH: cluster bits.  CHUNKF (EPI_X_FIRST / EPI_X_ADD of
+// the Lanczos iteration): the pass also applies the flips of the chunk bits 0..c-1 (the
+// partners lie in the tile's rows) and counts them in <u, X u>; the recurrence pass L
+// then leaves those bits out.
+template <typename R, bool REALC, int TB, int RB, int EPI, int CT, int PBH, bool CHUNKF = false>
 __global__ void __launch_bounds__(1 << (TB - RB), 1)
 k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps M) {
     typedef typename cvec<R>::T C;
@@ -577,15 +580,16 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
         cci[r] = bit ? Coef<R>::uim(P, cpos + r) : Coef<R>::dim(P, cpos + r);
     }
     // tile bits whose flips this pass applies: group bits at or above P.hskip
-    uint32_t apply = 0;
+    uint32_t apply = CHUNKF ? (1u << c) - 1u : 0u;
     for (int k = c; k < TB; ++k)
         if (hpos + k - c >= P.hskip) apply |= 1u << k;
-    // coefficients of the shared-memory bits (direction fixed by the thread's own bits)
+    // coefficients of the shared-memory bits (direction fixed by the thread's own bits);
+    // tile bit k < c is bit k of x, tile bit k >= c is bit hpos + k - c
     R cr_s[SB], ci_s[SB];
 #pragma unroll
     for (int k = 0; k < SB; ++k) {
-        const int p = hpos + k - c;
-        const bool okk = k >= c;
+        const int p = k < c ? k : hpos + k - c;
+        const bool okk = k >= c || CHUNKF;
         const bool bit = (tid >> k) & 1;
         cr_s[k] = okk ? (bit ? Coef<R>::ure(P, p) : Coef<R>::dre(P, p)) : R(0);
         ci_s[k] = okk ? (bit ? Coef<R>::uim(P, p) : Coef<R>::dim(P, p)) : R(0);
@@ -641,7 +645,7 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
                 Acc<R> acc;
 #pragma unroll
                 for (int k = 0; k < SB; ++k) {
-                    if (k < c) continue;  // chunk bits were applied by pass L
+                    if (k < c && !CHUNKF) continue;  // chunk bits were applied by pass L
                     if (!((apply >> k) & 1)) continue;
                     flip_reg<R, REALC>(cr_s[k], ci_s[k], tile[l ^ (1 << k)], acc);
                 }
@@ -732,6 +736,8 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
 // (w is written into a shared-memory buffer whose flips are applied one tile later, after
 // the next tile's block barrier, so the pass keeps one barrier per tile).  The flips of
 // the higher bits of <w, H w> come from the next iteration's pass H, which reads w anyway.
+// X_low is the flips of tile bits C0..TB-1: the pass H kernels apply the flips of bits
+// 0..C0-1 (their rows' chunk bits) and count them in <v, H v>.
 // E0: the start of a run: no recurrence, partials 4-5 = <u, (D - sigma + X_low) u>.
 // u_j arrives by cp.async.bulk into SL stages; part and u_{j-1} are read with streaming
 // loads one tile ahead into registers, after a bulk L2 prefetch two tiles ahead.  The
@@ -785,7 +791,8 @@ __device__ __forceinline__ void lz_tile_scalars(int64_t base, int n, const doubl
     }
 }
 
-template <typename R, bool REALC, int TB, int RB, bool E0>
+// C0: bits 0..C0-1 are flipped (and counted in <v, H v>) by the pass H kernels.
+template <typename R, bool REALC, int TB, int RB, bool E0, int C0>
 __global__ void __launch_bounds__(1 << (TB - RB), (sizeof(R) == 4) ? 2 : 1)
 k_pass_lz(const PassParams P, LzArgs A) {
     typedef typename cvec<R>::T C;
@@ -886,6 +893,10 @@ k_pass_lz(const PassParams P, LzArgs A) {
     C wp[NA];
     R dp[NA];
     // Re <w, (D - sigma + X_low) w> of the tile held in wsm[wbuf]
+    // (lane bits and register bits: the flip sums; warp bits: the pair form
+    // <w, X_p w> = 2 Re sum_{x: bit p = 0} conj(w[x]) dn_p w[x ^ 2^p] of a Hermitian flip,
+    // read by the warps whose bit p is 0; bits below c0 are the pass H kernels')
+    constexpr int LB = SB < 5 ? SB : 5;  // lane bits
     auto tile_energy = [&](int wbuf) {
         const C *wt = wsm + ((int64_t)wbuf << TB);
         R e = R(0);
@@ -894,7 +905,7 @@ k_pass_lz(const PassParams P, LzArgs A) {
             const int l = tid + a * NT;
             Acc<R> acc;
 #pragma unroll
-            for (int k = 0; k < SB; ++k)
+            for (int k = C0; k < LB; ++k)
                 flip_acc<R, REALC>(P, k, (tid >> k) & 1, wt[l ^ (1 << k)], acc);
 #pragma unroll
             for (int k = 0; k < RB; ++k)
@@ -903,6 +914,21 @@ k_pass_lz(const PassParams P, LzArgs A) {
             acc_diag_parts<R>(acc, dp[a], wp[a], fr, fi);
             e += R(wp[a].x) * fr + R(wp[a].y) * fi;
         }
+        R pr = R(0);
+#pragma unroll
+        for (int k = (C0 > 5 ? C0 : 5); k < SB; ++k) {
+            if ((tid >> k) & 1) continue;  // uniform in the warp
+            const R cr = Coef<R>::dre(P, k), ci = REALC ? R(0) : Coef<R>::dim(P, k);
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                const C q = wt[(tid ^ (1 << k)) + a * NT];
+                const R wr = wp[a].x, wi = wp[a].y;
+                // Re(conj(w) (cr + i ci) q) = cr (wr qr + wi qi) - ci (wr qi - wi qr)
+                pr += cr * (wr * R(q.x) + wi * R(q.y));
+                if (!REALC) pr -= ci * (wr * R(q.y) - wi * R(q.x));
+            }
+        }
+        e += R(2) * pr;
         red[4] += double(e);
     };
 
@@ -968,7 +994,7 @@ k_pass_lz(const PassParams P, LzArgs A) {
                 const int l = tid + a * NT;
                 Acc<R> acc;
 #pragma unroll
-                for (int k = 0; k < SB; ++k)  // thread bits: partner in shared memory
+                for (int k = C0; k < SB; ++k)  // thread bits: partner in shared memory
                     flip_acc<R, REALC>(P, k, (tid >> k) & 1, tile[l ^ (1 << k)], acc);
 #pragma unroll
                 for (int k = 0; k < RB; ++k)  // register bits
