@@ -78,6 +78,7 @@ SIGNATURES: dict[str, tuple] = {
                                          _SZ, _P]),
     "emusv_batch_adjoint_launch": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "emusv_batch_adjoint_iterations": (_I, [_I, _P, _P, _P]),
+    "emusv_batch_set_barrier_test": (_I, [_P, ctypes.c_longlong, _I]),
     "emusv_batch_max_blocks_per_sm": (_I, [_I, _I]),
     "emusv_batch_results": (_I, [_I, _I, _P, _P, _P, _P]),
     "emusv_vec_dot": (_I, [_I64, _I, _P, _P, _P, _P, _SZ, _P]),
@@ -94,6 +95,14 @@ _lib = None
 
 class WorkspaceTooSmall(Exception):
     """Raised internally when the Krylov basis outgrew its workspace (then retried)."""
+
+
+class NonFiniteError(FloatingPointError, RecursionError):
+    """A NaN or infinity met in a reduction (EMUSV_NONFINITE).  The reference's Lanczos loop
+    (emu_base/math/krylov_exp.py:49-131) never converges on a non-finite state and raises
+    RecursionError once it reaches max_krylov_dim; the device detects the value at once, so
+    this error is both a FloatingPointError and, for callers written against the
+    reference, a RecursionError."""
 
 
 def load(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -127,7 +136,7 @@ def check(code: int, what: str) -> None:
     if code == BAD_ARGUMENT:
         raise ValueError(msg)
     if code == NONFINITE:
-        raise FloatingPointError(msg)
+        raise NonFiniteError(msg)
     if code == WORKSPACE_TOO_SMALL:
         raise WorkspaceTooSmall(msg)
     if code == TIMEOUT:

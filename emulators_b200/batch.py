@@ -114,6 +114,16 @@ class BatchEvolution:
         self.shape = (tile_bits, capacity)
         self.graph = None
 
+    def set_barrier_test(self, wait_cycles: int = 0, skip_first_arrival: bool = False) -> None:
+        """Failure-path test switch of the prepared workspace (off by default; reset by
+        :meth:`prepare`): grid-barrier waits give up after ``wait_cycles`` SM clock cycles
+        (0: the default, about 1 s) and, with ``skip_first_arrival``, one CTA never arrives
+        at a launch's first barrier, so the launch ends with ``TimeoutError`` in
+        :meth:`results` and the device stays usable."""
+        st = _lib.load().emusv_batch_set_barrier_test(self.ws.data_ptr(), int(wait_cycles),
+                                                      1 if skip_first_arrival else 0)
+        _lib.check(st, "batch barrier test switch")
+
     def launch(self, blocks_per_sm: int) -> None:
         st = _lib.load().emusv_batch_launch(self.code, self.shape[0], blocks_per_sm,
                                             self.ws.data_ptr(), _lib.stream_of(self.states))

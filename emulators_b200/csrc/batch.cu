@@ -100,6 +100,11 @@ struct BArgs {
     void *hist;           // optional: states after every hist_every-th step
     int hist_every;
     long long hist_stride;  // amplitudes per history slot
+    // grid barrier: clock cycles a wait lasts at most (BAR_LIMIT unless a test shortens
+    // it) and the failure-path test switch (emusv_batch_set_barrier_test): the last CTA
+    // does not arrive at a launch's first barrier, so every other CTA's wait runs out
+    long long bar_limit;
+    int test_skip_arrival;
 };
 
 // Adjoint step (k_batch_adj): jobs 2i (state psi_i) and 2i+1 (gradient g_i) of instance i.
@@ -118,15 +123,18 @@ constexpr int NCP = 6 * BMAXQ;  // per bit: T_re, T_im, U_re, U_im, S_re, S_im
 
 // ---------------------------------------------------------------- grid barrier
 // Arrival counter + generation; the last arriver also clears the tile counter of the
-// phase after next.  Returns false (and every CTA then returns) on a timeout.
-__device__ bool grid_sync(BCtl *ctl, unsigned &ph) {
+// phase after next.  Returns false (and every CTA then returns) on a timeout: a wait
+// gives up after A.bar_limit clock cycles or as soon as another CTA recorded an error.
+__device__ bool grid_sync(const BArgs &A, unsigned &ph) {
+    BCtl *ctl = A.ctl;
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned *genp = &ctl->bar_gen;
         const unsigned g = *genp;
         __threadfence();
-        const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
-        if (arrived == gridDim.x - 1) {
+        const bool skip = A.test_skip_arrival && ph == 0 && blockIdx.x == gridDim.x - 1;
+        const unsigned arrived = skip ? 0u : atomicAdd(&ctl->bar_count, 1u);
+        if (!skip && arrived == gridDim.x - 1) {
             ctl->bar_count = 0;
             ctl->tile_ctr[(ph + 1) & 1] = 0;
             __threadfence();
@@ -137,7 +145,7 @@ __device__ bool grid_sync(BCtl *ctl, unsigned &ph) {
             while (*genp == g) {
                 if (++polls == 64) {
                     polls = 0;
-                    if (clock64() - t0 > BAR_LIMIT || *(volatile int *)&ctl->err) {
+                    if (clock64() - t0 > A.bar_limit || *(volatile int *)&ctl->err) {
                         atomicExch(&ctl->err, EMUSV_TIMEOUT);
                         break;
                     }
@@ -515,7 +523,7 @@ __device__ bool krylov_rounds(const BArgs &A, int gstep, int rstep, unsigned &ph
                 tile_hpsi<R, T>(A, I, i, t, gstep, j, sj);
             }
         }
-        if (!grid_sync(A.ctl, ph)) return false;
+        if (!grid_sync(A, ph)) return false;
         // does any job still iterate?
         if (warp == 0) {
             int any = 0;
@@ -560,7 +568,7 @@ __device__ bool krylov_rounds(const BArgs &A, int gstep, int rstep, unsigned &ph
                 tile_orth<R, T>(A, I, i, t, j, car, cai, cb, sj);
             }
         }
-        if (!grid_sync(A.ctl, ph)) return false;
+        if (!grid_sync(A, ph)) return false;
         ++round;
     }
 }
@@ -672,11 +680,11 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch(const BArgs A) {
     unsigned ph = 0;
     int round = 0;  // phase-B rounds so far (the same in every CTA)
     norm_phase<R, T>(A, ph);
-    if (!grid_sync(A.ctl, ph)) return;
+    if (!grid_sync(A, ph)) return;
     for (int step = 0; step < A.run_steps; ++step) {
         if (!krylov_rounds<R, T>(A, A.first_step + step, step, ph, round, s_flag)) return;
         combine_phase<R, T>(A, step, ph);
-        if (!grid_sync(A.ctl, ph)) return;
+        if (!grid_sync(A, ph)) return;
     }
     if (threadIdx.x < 32) {  // final statuses
         for (int i = blockIdx.x * 32 + lane; i < A.ninst; i += gridDim.x * 32) {
@@ -763,7 +771,7 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_rounds(const BA
     unsigned ph = 0;
     int round = 0;
     norm_phase<R, T>(A, ph);
-    if (!grid_sync(A.ctl, ph)) return;
+    if (!grid_sync(A, ph)) return;
     krylov_rounds<R, T>(A, D.step, 0, ph, round, s_flag);
 }
 
@@ -830,7 +838,7 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_post(const BArg
             }
         }
     }
-    if (!grid_sync(A.ctl, ph)) return;
+    if (!grid_sync(A, ph)) return;
 
     // ---------------- contractions over state tiles; the last tile of an instance turns
     // its sums into the step's gradients (torch.py:324-353)
@@ -1233,6 +1241,8 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
     A.hist = nullptr;
     A.hist_every = 1;
     A.hist_stride = L.inst_amps;
+    A.bar_limit = BAR_LIMIT;
+    A.test_skip_arrival = 0;
     if (adjoint) {
         BAdj &D = P.D;
         D.ninst = ninst;
@@ -1454,6 +1464,20 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
     EMUSV_CHECK_LAUNCH();
     EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl), s));
     return cooperative_launch(k3, blocks_per_sm, args, s, nullptr, PROF_ADJOINT);
+}
+
+// Failure-path test switch of a prepared workspace (forward or adjoint): later launches
+// wait at most wait_cycles clock cycles at a grid barrier (<= 0: the default, about 1 s)
+// and, when skip_first_arrival != 0, the last CTA does not arrive at each launch's first
+// barrier, so the others' bounded waits run out and the launch reports EMUSV_TIMEOUT.
+int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival) {
+    if (!workspace) return EMUSV_BAD_ARGUMENT;
+    std::lock_guard<std::mutex> g(g_args_mu);
+    auto it = g_args.find(workspace);
+    if (it == g_args.end()) return EMUSV_BAD_ARGUMENT;
+    it->second.A.bar_limit = wait_cycles > 0 ? wait_cycles : BAR_LIMIT;
+    it->second.A.test_skip_arrival = skip_first_arrival ? 1 : 0;
+    return EMUSV_OK;
 }
 
 // Krylov iteration counts of the last adjoint launch: [ninst][2] (state, gradient basis).

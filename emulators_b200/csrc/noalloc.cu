@@ -2,23 +2,25 @@
 // file-scope static device array owned by this library.
 //
 // Who needs it: code that must not allocate device memory at the point of the call --
-// for example a caller recording its work into a CUDA graph or running under an
-// external memory manager that forbids cudaMalloc/cudaFree, or a host runtime (a C or
-// Fortran simulator, an FFI binding) that has no device allocator of its own to hand
-// over a scratch buffer.  emusv_expect needs a caller-provided scratch buffer; this entry
-// point needs none.
+// for example a caller running under an external memory manager that forbids
+// cudaMalloc/cudaFree, or a host runtime (a C or Fortran simulator, an FFI binding) that
+// has no device allocator of its own to hand over a scratch buffer.  emusv_expect needs a
+// caller-provided scratch buffer; this entry point needs none.
 //
 // Limits and sharing:
 //  * the scratch holds FP64 partial sums of at most NOALLOC_BLOCKS thread blocks plus the
 //    final sums (about 66 KB per GPU); it lives on every GPU that loads the library until
 //    the process exits;
 //  * registers of up to EMUSV_MAX_QUBITS qubits are accepted (the launch never uses more
-//    blocks than the scratch holds); larger requests are rejected with
-//    EMUSV_BAD_ARGUMENT;
+//    blocks than the scratch holds: larger registers are walked grid-stride); larger
+//    requests are rejected with EMUSV_BAD_ARGUMENT;
 //  * every call shares the one array: calls whose work overlaps on the GPU (different
 //    streams without ordering) race on it and must be serialised by the caller;
 //  * nothing in the array has to start at zero: every block overwrites its own partial
-//    sums before they are added up.
+//    sums before they are added up;
+//  * the array's device address is resolved by the first call on each device and kept for
+//    the process; a cudaDeviceReset of that device invalidates it, so a process that
+//    resets a device must not call this entry point on it afterwards.
 #include <mutex>
 
 #include "hpsi_kernel.cuh"
@@ -41,8 +43,8 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 double *g_scratch_ptr[MAX_DEVICES] = {};
 
-// Device address of the static scratch on the current device.  The first call on a device
-// resolves it with cudaGetSymbolAddress (which must not run inside a stream capture).
+// Device address of the static scratch on the current device: the first call on a device
+// resolves it with cudaGetSymbolAddress (with that device current) and keeps it.
 int scratch_address(double **out) {
     int dev = 0;
     EMUSV_CHECK(cudaGetDevice(&dev));
@@ -93,9 +95,11 @@ extern "C" int emusv_expect_noalloc(int nqubits, int dtype, const double *omegas
     A.partials = scratch;
     A.tile_bits = hpsi_tile_bits(nqubits);
     int grid = 0;
+    // max_grid = NOALLOC_BLOCKS: the energy reduction (single-pass kernel) never launches
+    // more blocks than that, walking larger registers grid-stride, so the partial sums
+    // fit the static array
     st = launch_hpsi(dtype, HP_ENERGY, P, A, NOALLOC_BLOCKS, s, &grid);
     if (st) return st;
-    if (grid < 1 || grid > NOALLOC_BLOCKS) return EMUSV_BAD_ARGUMENT;
     {
         ProfScope ps_(PROF_SMALL, s);
         k_noalloc_finish<<<1, BLOCK, 0, s>>>(scratch, grid, result_dev);

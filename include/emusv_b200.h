@@ -89,12 +89,13 @@ int emusv_expect(int nqubits, int dtype, const double *omegas, const double *del
 /* The same energy moments as emusv_expect with no scratch argument and no allocation:
  * the partial sums go to a static device array inside the library (about 66 KB per GPU,
  * kept until the process exits).  For callers that cannot allocate device memory at the
- * call site (graph-recording code, external memory managers, host runtimes without a
- * device allocator).  Registers up to EMUSV_MAX_QUBITS; larger ones give
+ * call site (code under an external memory manager that forbids cudaMalloc/cudaFree, host
+ * runtimes without a device allocator).  Registers up to EMUSV_MAX_QUBITS; larger ones give
  * EMUSV_BAD_ARGUMENT.  The first call on a device resolves the array's address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the
- * array, so calls that overlap on the GPU race.  No counterpart in the reference: it has
- * no C interface. */
+ * (cudaGetSymbolAddress, with that device current) and should come before any stream
+ * capture; the address is kept for the process, so the entry point must not be used on a
+ * device after a cudaDeviceReset of it.  All calls share the array, so calls that overlap
+ * on the GPU race.  No counterpart in the reference: it has no C interface. */
 int emusv_expect_noalloc(int nqubits, int dtype, const double *omegas, const double *deltas,
                          const double *phis, const double *interaction, const void *psi,
                          double *result_dev, void *stream);
@@ -329,6 +330,14 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
 /* Krylov iteration counts of the last adjoint launch, [ninst][2] (state basis, gradient
  * basis), to a host array.  Synchronises the stream. */
 int emusv_batch_adjoint_iterations(int ninst, void *workspace, int *iterations_out, void *stream);
+/* Failure-path test switch of a prepared batch workspace (forward or adjoint; no
+ * counterpart in the reference, whose loop has no device-side waits): later launches wait
+ * at most wait_cycles SM clock cycles at a grid barrier (<= 0 restores the default, about
+ * 1 s), and with skip_first_arrival != 0 the last CTA does not arrive at each launch's
+ * first barrier, so every other CTA's bounded wait runs out, all CTAs return and
+ * emusv_batch_results reports EMUSV_TIMEOUT; the device stays usable.  Off by default;
+ * for tests.  Host-side only (takes effect at the next launch). */
+int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival);
 
 /* ---- building blocks of the generic krylov_exp(op, v, ...) (krylov_exp.py:23-106) ----
  * For an arbitrary operator applied by the caller, these give the FP64-accumulated

@@ -5,7 +5,9 @@ memory managers, host runtimes without a device allocator).
 
 It is compared through the C ABI with emusv_expect (which takes a caller scratch
 buffer) on the same state, twice in a row, so that reusing the shared static array is
-covered too.  This file is collected last on purpose."""
+covered too, and with the oracle's energy and ||H psi||^2 of the same state.  The larger
+registers (n = 22, 26) launch as many blocks as the static array holds and walk the state
+grid-stride.  This file is collected last on purpose."""
 
 import numpy as np
 import pytest
@@ -14,8 +16,9 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n,dtype,rtol", [(12, torch.complex128, 1e-12), (18, torch.complex64, 1e-6)])
-def test_expect_noalloc_matches_expect(n, dtype, rtol):
+@pytest.mark.parametrize("n,dtype,rtol", [(12, torch.complex128, 1e-12), (18, torch.complex64, 1e-6),
+                                          (22, torch.complex64, 1e-6), (26, torch.complex64, 1e-6)])
+def test_expect_noalloc_matches_expect(oracle, n, dtype, rtol):
     from emulators_b200 import _lib
     from emulators_b200 import workloads as wl
 
@@ -42,6 +45,14 @@ def test_expect_noalloc_matches_expect(n, dtype, rtol):
         r, g = ref.cpu().numpy(), got.cpu().numpy()
         scale = max(abs(r[0]), np.sqrt(abs(r[2])))
         np.testing.assert_allclose(g, r, rtol=rtol, atol=rtol * scale, err_msg=f"call {call}")
+        if call == 0:  # the oracle's moments of the same (stored) state, in FP64
+            host = psi.cpu().to(torch.complex128).numpy()
+            hpsi = oracle.Hamiltonian(om, de, ph, U).apply(host)
+            e = np.vdot(host, hpsi)
+            want = np.array([e.real, e.imag, np.vdot(hpsi, hpsi).real])
+            tol = max(rtol, 2e-6 if dtype == torch.complex64 else rtol)
+            np.testing.assert_allclose(g, want, rtol=tol, atol=tol * scale, err_msg="oracle")
+            del host, hpsi
 
 
 def test_expect_noalloc_rejects_bad_sizes():
