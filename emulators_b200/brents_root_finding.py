@@ -5,8 +5,8 @@ The Monte Carlo stepper brackets the time of a quantum jump (where ||psi(t)||^2 
 jump threshold) and asks for one abscissa at a time, evolving the state between requests.
 The steps are Brent's published method: inverse quadratic interpolation, the secant step
 when two ordinates nearly coincide, and bisection whenever the interpolated step leaves the
-bracket or does not shrink it fast enough; the same tests and bookkeeping as the reference,
-so that the same ordinates give the same abscissae.
+bracket or does not shrink it fast enough.  The tests and their floating-point order are
+the reference's, so that the same ordinates give the same abscissae.
 """
 
 from __future__ import annotations
@@ -15,58 +15,65 @@ from typing import Callable, Optional
 
 
 class BrentsRootFinder:
-    """brents_root_finding.py:4-94."""
+    """brents_root_finding.py:4-94.  The bracket is kept as the best abscissa so far
+    (smallest |ordinate|) and the opposite end of the bracket (ordinate of the other sign);
+    the two previous best abscissae steer the choice between an interpolated step and
+    bisection."""
 
     def __init__(self, *, start: float, end: float, f_start: float, f_end: float,
                  epsilon: float = 1e-6):
         self.epsilon = epsilon
-        assert start <= end
-        self.a, self.b = start, end
-        self.fa, self.fb = f_start, f_end
-        assert self.fa * self.fb < 0, "Function root needs to be between a and b"
-        if abs(self.fa) < abs(self.fb):  # b is the better guess
-            self.a, self.b, self.fa, self.fb = self.b, self.a, self.fb, self.fa
-        self.c, self.fc = self.a, self.fa
-        self.d = self.c
-        self.bisection = True
-        self.current_guess = self.b
+        assert start <= end, "the bracket needs start <= end"
+        self._far, self._best = start, end
+        self._f_far, self._f_best = f_start, f_end
+        assert self._f_far * self._f_best < 0, "f(start) and f(end) must have opposite signs"
+        self._keep_best_smallest()
+        self._prev, self._f_prev = self._far, self._f_far
+        self._prev2 = self._prev
+        self._bisected = True
+        self.current_guess = self._best
         self.next_abscissa: Optional[float] = None
 
+    def _keep_best_smallest(self) -> None:
+        if abs(self._f_far) < abs(self._f_best):
+            self._far, self._best = self._best, self._far
+            self._f_far, self._f_best = self._f_best, self._f_far
+
     def get_next_abscissa(self) -> float:
-        a, b, c, fa, fb, fc = self.a, self.b, self.c, self.fa, self.fb, self.fc
-        if abs(fc - fa) < self.epsilon or abs(fc - fb) < self.epsilon:
-            dx = fb * (b - a) / (fa - fb)  # secant
-        else:  # inverse quadratic interpolation through (a, fa), (b, fb), (c, fc)
-            s, r, t = fb / fa, fb / fc, fa / fc
+        x0, x1, xp = self._far, self._best, self._prev
+        f0, f1, fp = self._f_far, self._f_best, self._f_prev
+        if abs(fp - f0) < self.epsilon or abs(fp - f1) < self.epsilon:
+            step = f1 * (x1 - x0) / (f0 - f1)  # secant through the bracket ends
+        else:  # inverse quadratic interpolation through the three points
+            s, r, t = f1 / f0, f1 / fp, f0 / fp
             q = (t - 1) * (s - 1) * (r - 1)
-            p = s * (t * (r - t) * (c - b) + (r - 1) * (b - a))
-            dx = p / q
-        tol = abs(2 * self.epsilon * b)
-        adx, dbc, dcd, dab = abs(dx), abs(b - c), abs(c - self.d), a - b
-        reject = (adx >= abs(3 * dab / 4) or dx * dab < 0
-                  or (adx >= (dbc if self.bisection else dcd) / 2)
-                  or ((dbc if self.bisection else dcd) < tol))
-        if reject:
-            dx = dab / 2
-        self.bisection = reject
-        self.next_abscissa = b + dx
-        self.d = c
-        self.c, self.fc = b, fb
+            p = s * (t * (r - t) * (xp - x1) + (r - 1) * (x1 - x0))
+            step = p / q
+        tol = abs(2 * self.epsilon * x1)
+        span = x0 - x1
+        recent = abs(x1 - xp) if self._bisected else abs(xp - self._prev2)
+        leaves_bracket = abs(step) >= abs(3 * span / 4) or step * span < 0
+        too_slow = abs(step) >= recent / 2 or recent < tol
+        self._bisected = leaves_bracket or too_slow
+        if self._bisected:
+            step = span / 2
+        self.next_abscissa = x1 + step
+        self._prev2 = xp
+        self._prev, self._f_prev = x1, f1
         return self.next_abscissa
 
     def provide_ordinate(self, abscissa: float, ordinate: float) -> None:
         assert self.next_abscissa is not None and abscissa == self.next_abscissa, \
-            "Something went wrong"
-        if self.fa * ordinate < 0:
-            self.b, self.fb = abscissa, ordinate
+            "provide_ordinate expects the ordinate of the last get_next_abscissa"
+        if self._f_far * ordinate < 0:
+            self._best, self._f_best = abscissa, ordinate
         else:
-            self.a, self.fa = abscissa, ordinate
-        if abs(self.fa) < abs(self.fb):
-            self.a, self.b, self.fa, self.fb = self.b, self.a, self.fb, self.fa
-        self.current_guess = self.b
+            self._far, self._f_far = abscissa, ordinate
+        self._keep_best_smallest()
+        self.current_guess = self._best
 
     def is_converged(self, tolerance: float) -> bool:
-        return abs(self.b - self.a) < tolerance
+        return abs(self._best - self._far) < tolerance
 
 
 def find_root_brents(f: Callable[[float], float], *, start: float, end: float,

@@ -71,7 +71,7 @@ def _ops8(ops) -> np.ndarray:
            for L in ops]
     for L in ops:
         if tuple(torch.as_tensor(L).shape) != (2, 2):
-            raise ValueError("Only single-qubit lindblad operators are supported")
+            raise ValueError("the Lindbladian takes single-qubit (2 x 2) jump operators")
     return np.ascontiguousarray(np.concatenate(out) if out else np.zeros(8))
 
 

@@ -28,7 +28,8 @@ def get_lindblad_operators(*, noise_type: str, noise_model, interact_type: str =
     if noise_type == "dephasing":
         if noise_model.hyperfine_dephasing_rate != 0.0:
             raise NotImplementedError(
-                "hyperfine_dephasing_rate is supported only in the digital basis")
+                "hyperfine dephasing acts on the digital basis, which this emulator does not "
+                "simulate (only the ground-Rydberg basis)")
         c = math.sqrt(noise_model.dephasing_rate / 2)
         return [torch.diag(torch.tensor([c, -c], dtype=dtype))]
     if noise_type == "depolarizing":  # sqrt(rate/4) X, Y, Z
@@ -40,7 +41,7 @@ def get_lindblad_operators(*, noise_type: str, noise_model, interact_type: str =
     if noise_type == "eff_noise":
         ops = [torch.tensor(op, dtype=dtype) for op in noise_model.eff_noise_opers]
         if not all(op.shape == (dim, dim) for op in ops):
-            raise ValueError(f"Only {dim} by {dim} effective noise operator matrices are supported")
+            raise ValueError(f"effective noise operators must be {dim} x {dim} matrices")
         out = [math.sqrt(rate) * op for rate, op in zip(noise_model.eff_noise_rates, ops)]
         if interact_type == "ising":  # pulser's ising basis order to emu-sv's
             for t in out:
@@ -48,13 +49,13 @@ def get_lindblad_operators(*, noise_type: str, noise_model, interact_type: str =
         return out
     if noise_type == "leakage":
         return []
-    raise ValueError(f"Unknown noise type: {noise_type}")
+    raise ValueError(f"no Lindblad operators for the noise type {noise_type!r}")
 
 
 def compute_noise_from_lindbladians(lindbladians: list[torch.Tensor], dim: int = 2) -> torch.Tensor:
     """-0.5i sum_j L_j^dag L_j (jump_lindblad_operators.py:79-93)."""
     assert all(L.shape == (dim, dim) for L in lindbladians), \
-        "Only single-qubit lindblad operators are supported"
+        f"the noise term takes single-qubit ({dim} x {dim}) Lindblad operators"
     acc = torch.zeros(dim, dim, dtype=dtype)
     for L in lindbladians:
         L = torch.as_tensor(L).to(dtype)

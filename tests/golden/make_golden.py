@@ -1,8 +1,8 @@
 """Generate the golden fixtures under tests/golden/ by running the REFERENCE emu-sv code.
 
 This script is the only place that executes the reference implementation.  It runs in
-the build container where the reference checkout is readable (pass its path with
-``--reference``; default ``/root/reference``) and writes small ``.npz`` fixtures that the
+the build container where the reference checkout is readable (its path is the required
+``--reference`` argument) and writes small ``.npz`` fixtures that the
 test suite reads on any machine.  Nothing else in the repository imports it.
 
 The reference's package ``__init__`` files pull in ``pulser``, which is not installed,
@@ -406,6 +406,7 @@ def gen_observables(R):
     Ham = R["ham"].RydbergHamiltonian
     out, k = {}, 0
     g = torch.Generator().manual_seed(99)
+    torch.manual_seed(98)  # randn_interaction_matrix draws from the global generator
     for n in [1, 2, 3, 5, 8, 11]:
         s = torch.randn(2**n, dtype=torch.complex128, generator=g)
         s = s / s.norm()
@@ -792,7 +793,8 @@ GENERATORS["target_times"] = gen_target_times
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="checkout of the reference repository (read only)")
     ap.add_argument("--only", nargs="*", default=None)
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     a = ap.parse_args()
