@@ -287,6 +287,43 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                         "streamed_frac": round(units * D * es_ / t1 / 1e9 / hbm, 4)}
         del v, o
 
+    # ---- energy moments (emusv_expect: <psi|H|psi>, ||H psi||^2) of the N=26 state
+    emom = {}
+    for name, dt_ in (("c64", torch.complex64),):
+        v = torch.randn(D, dtype=dt_, device=dev)
+        v /= torch.linalg.vector_norm(v)
+        H = ham(0)
+        res = torch.empty(3, dtype=torch.float64, device=dev)
+        code_ = _lib.dtype_code(dt_)
+        sc = torch.empty(L.emusv_scratch_bytes(n, code_), dtype=torch.uint8, device=dev)
+        strm = torch.cuda.current_stream().cuda_stream
+
+        def mom():
+            _lib.check(L.emusv_expect(n, code_, *H._params(), v.data_ptr(), res.data_ptr(),
+                                      sc.data_ptr(), sc.numel(), strm), "expect")
+
+        for _ in range(2):
+            mom()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        s0.record()
+        for _ in range(reps):
+            mom()
+        s1.record()
+        torch.cuda.synchronize()
+        t1 = s0.elapsed_time(s1) / 1e3 / reps
+        es_ = 8 if name == "c64" else 16
+        # pass H x2 (read psi 2x, read/write the scratch vector 3x) + the moments pass
+        # (read psi and the scratch vector): 7 vector units
+        emom[name] = {"ms": round(t1 * 1e3, 4), "streamed_units": 7,
+                      "streamed_GB/s": round(7 * D * es_ / t1 / 1e9, 1),
+                      "streamed_frac": round(7 * D * es_ / t1 / 1e9 / hbm, 4),
+                      "read_psi_GB/s": round(D * es_ / t1 / 1e9, 1),
+                      "note": "<psi|H|psi> and ||H psi||^2 (energy, variance, second "
+                              "moment) of a random N=26 state; CUDA events, 10 calls"}
+        del v, sc
+
     # ---- end-to-end through the public backend API, host buffers
     e2e = None
     if not args.no_e2e:
@@ -322,7 +359,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                      "kernel_time_shares": shares},
         "gpu_launches": int(launches.sum()),
         "clocks": clk.summary(),
-        "secondary": {"hpsi_standalone": hstand},
+        "secondary": {"hpsi_standalone": hstand, "energy_moments": emom},
         "e2e": e2e,
     }
     if not args.no_plain and world == 1:

@@ -134,6 +134,8 @@ static bool single_pass_forced() {
 }
 
 bool lz_applies(int dtype, int n);
+int lz_moments(int dtype, const HamParams &H, const void *psi, void *part, double *partials,
+               double *part_h, int *err, cudaStream_t s, int *grid_out);
 // The Lanczos iteration of this register runs in the H-first order (hpsi_pass.cu): wider
 // than one pass-L tile and the passes not switched off.
 bool lanczos_h_first(int dtype, int n) { return !single_pass_forced() && lz_applies(dtype, n); }
@@ -329,11 +331,22 @@ const char *emusv_status_string(int status) {
     }
 }
 
-size_t emusv_scratch_bytes(int nqubits, int dtype) {
-    (void)dtype;
-    if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS) return 0;
+// Scratch of the observables: FP64 partial sums, and for the moments of H on registers
+// wider than one pass-L tile (emusv_expect through the streaming passes) one vector of
+// the register's size for the flips of the high bits.
+static size_t scratch_head_bytes() {
     const size_t per = (size_t)MAXQ * MAXQ > NRED ? (size_t)MAXQ * MAXQ : NRED;
-    return sizeof(double) * ((size_t)max_grid_blocks() * per + 64);
+    return ((sizeof(double) * ((size_t)max_grid_blocks() * per + 64)) + 255) / 256 * 256;
+}
+static bool expect_by_passes(int dtype, int n) {
+    return (dtype == EMUSV_C64 || dtype == EMUSV_C128) && lanczos_h_first(dtype, n);
+}
+
+size_t emusv_scratch_bytes(int nqubits, int dtype) {
+    if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS) return 0;
+    size_t b = scratch_head_bytes();
+    if (expect_by_passes(dtype, nqubits)) b += (size_t(1) << nqubits) * (dtype == EMUSV_C128 ? 16 : 8);
+    return b;
 }
 
 int emusv_hamiltonian_diag(int nqubits, const double *deltas, const double *interaction,
@@ -394,14 +407,23 @@ int emusv_expect(int nqubits, int dtype, const double *omegas, const double *del
     cudaStream_t s = as_stream(stream);
     double *partials = reinterpret_cast<double *>(scratch);
     double *sums = partials + (size_t)max_grid_blocks() * NRED;
-    HpsiArgs A = {};
-    A.u = psi;
-    A.su = 1.0;
-    A.partials = partials;
-    A.tile_bits = hpsi_tile_bits(nqubits);
-    int grid = 0;
-    int st = launch_hpsi(dtype, HP_ENERGY, P, A, max_grid_blocks(), s, &grid);
-    if (st) return st;
+    int grid = 0, st;
+    if (expect_by_passes(dtype, nqubits) && !P.noisy) {
+        // streaming passes: X_high psi into the scratch vector, then H psi per tile
+        if (reinterpret_cast<uintptr_t>(psi) & 15) return EMUSV_BAD_ARGUMENT;
+        unsigned char *vec = reinterpret_cast<unsigned char *>(scratch) + scratch_head_bytes();
+        double *part_h = sums + 64;  // the pass H kernels' partials (not used here)
+        st = lz_moments(dtype, P, psi, vec, partials, part_h, device_error_word(), s, &grid);
+        if (st) return st;
+    } else {
+        HpsiArgs A = {};
+        A.u = psi;
+        A.su = 1.0;
+        A.partials = partials;
+        A.tile_bits = hpsi_tile_bits(nqubits);
+        st = launch_hpsi(dtype, HP_ENERGY, P, A, max_grid_blocks(), s, &grid);
+        if (st) return st;
+    }
     {
         ProfScope ps_(PROF_SMALL, s);
         k_sum_partials<<<1, BLOCK, 0, s>>>(partials, grid, sums);

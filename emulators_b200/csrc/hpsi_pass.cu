@@ -275,13 +275,13 @@ bool lz_applies(int dtype, int n) {
     return false;
 }
 
-template <typename R, bool REALC, bool E0, int C0>
+template <typename R, bool REALC, int MODE, int C0>
 static int launch_lz_c(const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
     typedef typename cvec<R>::T C;
     constexpr int TB = LzShape<R>::TB, RB = LzShape<R>::RB, NT = 1 << (TB - RB);
     PassParams P;
     fill_params(H, TB, RB, &P);
-    auto kern = k_pass_lz<R, REALC, TB, RB, E0, C0>;
+    auto kern = k_pass_lz<R, REALC, TB, RB, MODE, C0>;
     const size_t smem = pass_lz_smem<C, TB>();
     EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -300,32 +300,31 @@ static int launch_lz_c(const HamParams &H, const LzArgs &A, cudaStream_t s, int 
 }
 
 // The pass L leaves out the chunk bits of the register's pass H rows.
-template <typename R, bool REALC, bool E0>
+template <typename R, bool REALC, int MODE>
 static int launch_lz(const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
     constexpr int CMIN = PassShape<R>::CMIN;
-    if (lz_chunk_bits<R>(H.n) == CMIN) return launch_lz_c<R, REALC, E0, CMIN>(H, A, s, grid_out);
-    return launch_lz_c<R, REALC, E0, CMIN - 1>(H, A, s, grid_out);
+    if (lz_chunk_bits<R>(H.n) == CMIN) return launch_lz_c<R, REALC, MODE, CMIN>(H, A, s, grid_out);
+    return launch_lz_c<R, REALC, MODE, CMIN - 1>(H, A, s, grid_out);
+}
+template <int MODE>
+static int launch_lz_mode(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
+    if (H.noisy || !lz_applies(dtype, H.n)) return EMUSV_BAD_ARGUMENT;
+    if (dtype == EMUSV_C64)
+        return H.real_coef ? launch_lz<float, true, MODE>(H, A, s, grid_out)
+                           : launch_lz<float, false, MODE>(H, A, s, grid_out);
+    return H.real_coef ? launch_lz<double, true, MODE>(H, A, s, grid_out)
+                       : launch_lz<double, false, MODE>(H, A, s, grid_out);
 }
 
 // Start of a run: partials 4-5 of <u, (D - sigma + X_low) u> (A.u, A.eshift, A.partials,
 // A.gate, A.err).
 int lz_energy0(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
-    if (H.noisy || !lz_applies(dtype, H.n)) return EMUSV_BAD_ARGUMENT;
-    if (dtype == EMUSV_C64)
-        return H.real_coef ? launch_lz<float, true, true>(H, A, s, grid_out)
-                           : launch_lz<float, false, true>(H, A, s, grid_out);
-    return H.real_coef ? launch_lz<double, true, true>(H, A, s, grid_out)
-                       : launch_lz<double, false, true>(H, A, s, grid_out);
+    return launch_lz_mode<LZ_E0>(dtype, H, A, s, grid_out);
 }
 
 // The recurrence pass: w = H v_j - a v_j - b v_{j-1} (see k_pass_lz).
 int lz_low(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out) {
-    if (H.noisy || !lz_applies(dtype, H.n)) return EMUSV_BAD_ARGUMENT;
-    if (dtype == EMUSV_C64)
-        return H.real_coef ? launch_lz<float, true, false>(H, A, s, grid_out)
-                           : launch_lz<float, false, false>(H, A, s, grid_out);
-    return H.real_coef ? launch_lz<double, true, false>(H, A, s, grid_out)
-                       : launch_lz<double, false, false>(H, A, s, grid_out);
+    return launch_lz_mode<LZ_ITER>(dtype, H, A, s, grid_out);
 }
 
 // part = X_high u (unscaled flips of every bit above the pass-L tile, and of the CMIN
@@ -368,6 +367,26 @@ static int lz_high_rows(const HamParams &H, const void *u, void *part, double *p
     int c0 = 0;
     if (lz_chunk_bits<R>(H.n) == CMIN) return lz_high_t<R, REALC, CMIN>(H, u, part, partials, gate, err, s, nb, &c0);
     return lz_high_t<R, REALC, CMIN - 1>(H, u, part, partials, gate, err, s, nb, &c0);
+}
+
+int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,
+            int *err, cudaStream_t s, int *nblocks_out);
+
+// Moments of H on psi through the passes (registers wider than one pass-L tile): the pass
+// H kernels write part = X_high psi into `part` (a vector of the register's size), then the
+// moments pass forms H psi tile by tile: partials 0 ||H psi||^2, 1-2 <psi, H psi> into
+// `partials` (*grid_out rows); the pass H kernels' own partials go to `part_h`.
+int lz_moments(int dtype, const HamParams &H, const void *psi, void *part, double *partials,
+               double *part_h, int *err, cudaStream_t s, int *grid_out) {
+    int nh = 0;
+    int st = lz_high(dtype, H, psi, part, part_h, nullptr, err, s, &nh);
+    if (st) return st;
+    LzArgs A = {};
+    A.u = psi;
+    A.part = part;
+    A.partials = partials;
+    A.err = err;
+    return launch_lz_mode<LZ_M2>(dtype, H, A, s, grid_out);
 }
 
 int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,

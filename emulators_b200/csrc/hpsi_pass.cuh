@@ -791,10 +791,16 @@ __device__ __forceinline__ void lz_tile_scalars(int64_t base, int n, const doubl
     }
 }
 
+// Modes of k_pass_lz: the recurrence pass of a Lanczos iteration; the start-of-run energy
+// pass; and the moments of H (emusv_expect): H u = (D + X_low) u + part formed per tile
+// (no store), partials 0 ||H u||^2, 1-2 <u, H u>.
+enum LzMode { LZ_ITER = 0, LZ_E0 = 1, LZ_M2 = 2 };
+
 // C0: bits 0..C0-1 are flipped (and counted in <v, H v>) by the pass H kernels.
-template <typename R, bool REALC, int TB, int RB, bool E0, int C0>
+template <typename R, bool REALC, int TB, int RB, int MODE, int C0>
 __global__ void __launch_bounds__(1 << (TB - RB), (sizeof(R) == 4) ? 2 : 1)
 k_pass_lz(const PassParams P, LzArgs A) {
+    constexpr bool E0 = MODE == LZ_E0, M2 = MODE == LZ_M2;
     typedef typename cvec<R>::T C;
     constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB, NW = NT / 32;
     constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
@@ -847,7 +853,7 @@ k_pass_lz(const PassParams P, LzArgs A) {
     if ((int64_t)blockIdx.x < ntiles)
         lz_tile_scalars<TB>((int64_t)blockIdx.x << TB, n, fld, Ush, sigma, scal, warp, lane, NW);
     double su = 1.0, car = 0.0, cai = 0.0, cb = 0.0;
-    if (!E0) {
+    if (MODE == LZ_ITER) {
         su = *A.su;
         car = A.ocoef[0];
         cai = A.ocoef[1];
@@ -965,7 +971,7 @@ k_pass_lz(const PassParams P, LzArgs A) {
             const int b1 = buf + 1 == SL ? 0 : buf + 1;
             if (s1 < ntiles) lz_tile_scalars<TB>(s1 << TB, n, fld, Ush, sigma, scal + b1 * 64, warp, lane, NW);
         }
-        if (!E0 && have_prev && ok) tile_energy(wb ^ 1);
+        if (MODE == LZ_ITER && have_prev && ok) tile_energy(wb ^ 1);
         if (ok) {
             double St = ET + sc[TB];
 #pragma unroll
@@ -1011,6 +1017,13 @@ k_pass_lz(const PassParams P, LzArgs A) {
                     rq[1] += vr * hui - vi * hur;
                     continue;
                 }
+                if (M2) {  // H u = (D + X_low) u + part: ||H u||^2, <u, H u>
+                    const R hr = hur + R(pc[a].x), hi = hui + R(pc[a].y);
+                    rq[0] += hr * hr + hi * hi;
+                    rq[1] += vr * hr + vi * hi;
+                    rq[2] += vr * hi - vi * hr;
+                    continue;
+                }
                 const R hr = suR * (hur + R(pc[a].x)), hi = suR * (hui + R(pc[a].y));
                 const R wr = hr - (carR * vr - caiR * vi) - cbR * R(qc[a].x);
                 const R wi = hi - (carR * vi + caiR * vr) - cbR * R(qc[a].y);
@@ -1028,6 +1041,12 @@ k_pass_lz(const PassParams P, LzArgs A) {
             if (E0) {
                 red[4] += double(rq[0]);
                 red[5] += double(rq[1]);
+            } else if (M2) {
+                red[0] += double(rq[0]);
+                red[1] += double(rq[1]);
+                red[2] += double(rq[2]);
+                const int64_t s1 = s + grid;
+                if (s1 < ntiles) prefetch(s1);
             } else {
                 red[0] += double(rq[0]);
                 red[1] += su * double(rq[1]);
@@ -1044,7 +1063,7 @@ k_pass_lz(const PassParams P, LzArgs A) {
             phase ^= 1u;
         }
     }
-    if (!E0) {
+    if (MODE == LZ_ITER) {
         __syncthreads();  // the last tile's w buffer is complete
         if (have_prev && ok) tile_energy(wb ^ 1);
     }

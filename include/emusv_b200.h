@@ -75,11 +75,16 @@ int emusv_hpsi(int nqubits, int dtype, const double *omegas, const double *delta
                const double *phis, const double *interaction, const void *psi, void *out,
                void *stream);
 
-/* Bytes of device scratch the reduction entry points below need (FP64 partial sums). */
+/* Bytes of device scratch the reduction entry points below need: FP64 partial sums, and
+ * for emusv_expect on registers wider than one streaming tile (complex64 and complex128
+ * from 12 qubits) one vector of the register's size, which holds the flips of the high
+ * bits between the streaming passes.  The scratch must be 256-byte aligned. */
 size_t emusv_scratch_bytes(int nqubits, int dtype);
 
 /* result_dev[0..1] = <psi|H|psi> (re, im), result_dev[2] = <H psi|H psi>; device
- * float64 [3], no vector store, no synchronisation.  Replaces RydbergHamiltonian.expect
+ * float64 [3], no synchronisation.  Registers wider than one streaming tile run the
+ * pass H kernels (the flips of the high bits into the scratch vector) and one pass that
+ * forms H psi tile by tile without storing it; smaller ones one fused pass.  Replaces RydbergHamiltonian.expect
  * (hamiltonian.py:164-172) and the vdot(h, h) of energy_second_moment_sv_impl /
  * energy_variance_sv_impl (emu_sv/custom_callback_implementations.py:131-185). */
 int emusv_expect(int nqubits, int dtype, const double *omegas, const double *deltas,

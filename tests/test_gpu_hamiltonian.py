@@ -87,6 +87,36 @@ def test_observables_match_reference_fixtures():
                    - float(c["second_moment"])) < 1e-10
 
 
+@pytest.mark.parametrize("n,dtype,phase", [(12, torch.complex128, True), (16, torch.complex64, True),
+                                           (22, torch.complex128, False), (24, torch.complex64, True),
+                                           (26, torch.complex64, False)])
+def test_energy_moments_vs_oracle(oracle, n, dtype, phase):
+    """Energy, variance and second moment (hamiltonian.py:164-172,
+    custom_callback_implementations.py:131-185) through the streaming passes (one and two
+    pass H kernels, real and complex drives) against the oracle's H psi of the same state."""
+    from emulators_b200 import RydbergHamiltonian, StateVector
+    from emulators_b200 import workloads as wl
+    from emulators_b200.observables import energy_second_moment_sv_impl, energy_variance_sv_impl
+
+    rng = np.random.default_rng(300 + n)
+    om, de = rng.uniform(0, 2 * np.pi, n), rng.uniform(-20, 20, n)
+    ph = rng.normal(size=n) if phase else np.zeros(n)
+    U = wl.interaction_matrix(wl.ladder(n // 2, 5.5))
+    t = torch.randn(1 << n, dtype=dtype, device=DEV)
+    t /= torch.linalg.vector_norm(t)
+    H = RydbergHamiltonian(*(torch.as_tensor(a) for a in (om, de, ph, U)), DEV)
+    st = StateVector(t)
+    got = [H.expect(st).item(), energy_variance_sv_impl(state=st, hamiltonian=H).item(),
+           energy_second_moment_sv_impl(state=st, hamiltonian=H).item()]
+    host = t.cpu().to(torch.complex128).numpy()
+    hpsi = oracle.Hamiltonian(om, de, ph, U).apply(host)
+    e, m2 = np.vdot(host, hpsi).real, np.vdot(hpsi, hpsi).real
+    want = [e, m2 - e * e, m2]
+    rtol = 1e-12 if dtype == torch.complex128 else 2e-6
+    for g, w in zip(got, want):
+        assert abs(g - w) <= rtol * m2 ** 0.5 * max(1.0, m2 ** 0.5), (n, got, want)
+
+
 @pytest.mark.parametrize("n,dtype", [(12, torch.complex128), (19, torch.complex64), (22, torch.complex128)])
 def test_occupation_correlation_vs_oracle(oracle, n, dtype):
     rng = np.random.default_rng(100 + n)
