@@ -84,6 +84,8 @@ SIGNATURES: dict[str, tuple] = {
     "emusv_vec_dot": (_I, [_I64, _I, _P, _P, _P, _P, _SZ, _P]),
     "emusv_vec_axpy": (_I, [_I64, _I, _P, _P, _P, _P]),
     "emusv_vec_combine": (_I, [_I64, _I, _I, _P, _P, _P, _P]),
+    "emusv_dense_expm_scratch_bytes": (_SZ, [_I]),
+    "emusv_dense_expm_col": (_I, [_I, _P, _P, _P, _SZ, _P]),
     "emusv_tridiag_scratch_bytes": (_SZ, []),
     "emusv_tridiag_expm_col": (_I, [_I, _P, _P, _P, _P, _P, _SZ, _P]),
     "emusv_profile_begin": (None, [_I]),

@@ -505,6 +505,28 @@ __device__ double arn_eval(KState *ks, const ArnState *as, int jj, double dt, do
     return err1 < err2 ? err1 : (err1 * err2 / (err1 - err2));
 }
 
+// y = exp(A) e_0 for a caller's dense complex M x M matrix (row-major, complex128, in
+// global memory): one block, the Arnoldi decision's Taylor routine; *status = 0, or
+// EMUSV_NONFINITE when the matrix norm is not finite or too large for the substeps.
+__global__ void __launch_bounds__(DECIDE_THREADS)
+k_dense_expm_col(int M, const double2 *a_rowmajor, double2 *x, int *status) {
+    extern __shared__ __align__(16) unsigned char arn_smem[];
+    double2 *A = reinterpret_cast<double2 *>(arn_smem);
+    double2 *y = A + M * M;
+    double2 *t = y + M;
+    double2 *tn = t + M;
+    double *red = reinterpret_cast<double *>(tn + M);  // [DECIDE_THREADS]
+    for (int i = threadIdx.x; i < M * M; i += DECIDE_THREADS) {
+        const int r = i / M, c = i % M;
+        A[c * M + r] = a_rowmajor[i];
+    }
+    __syncthreads();
+    const bool ok = arn_expm_col0(A, M, y, t, tn, red);
+    for (int k = threadIdx.x; k < M; k += DECIDE_THREADS)
+        x[k] = ok ? y[k] : make_double2(nan(""), nan(""));
+    if (threadIdx.x == 0) *status = ok ? EMUSV_OK : EMUSV_NONFINITE;
+}
+
 __global__ void __launch_bounds__(DECIDE_THREADS)
 k_arn_decide(KState *ks, ArnState *as, int j, const double *part, int nb, double dt, double exp_tol,
              double norm_tol, int poll, int first_poll, int maxdim) {
@@ -630,6 +652,38 @@ static int launch_lagged(int pass, const KState *ks, const ArnState *as, int j, 
 using namespace emusv;
 
 extern "C" {
+
+static size_t dense_expm_smem(int m) {
+    return sizeof(double2) * ((size_t)m * m + 3 * (size_t)m) + sizeof(double) * DECIDE_THREADS;
+}
+
+size_t emusv_dense_expm_scratch_bytes(int m) {
+    if (m < 1 || m > ARN_M) return 0;
+    return align_up(sizeof(double2) * (size_t)m * m, 256) + align_up(sizeof(double2) * m, 256) + 256;
+}
+
+int emusv_dense_expm_col(int m, const double *a, double *x_dev, void *scratch, size_t scratch_bytes,
+                         void *stream) {
+    if (m < 1 || m > ARN_M || !a || !x_dev || !scratch || scratch_bytes < emusv_dense_expm_scratch_bytes(m))
+        return EMUSV_BAD_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    unsigned char *p = reinterpret_cast<unsigned char *>(scratch);
+    double2 *A = reinterpret_cast<double2 *>(p);
+    int *status = reinterpret_cast<int *>(p + align_up(sizeof(double2) * (size_t)m * m, 256) +
+                                          align_up(sizeof(double2) * m, 256));
+    EMUSV_CHECK(cudaMemcpyAsync(A, a, sizeof(double2) * (size_t)m * m, cudaMemcpyHostToDevice, s));
+    const size_t smem = dense_expm_smem(m);
+    EMUSV_CHECK(cudaFuncSetAttribute(k_dense_expm_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    {
+        ProfScope ps_(PROF_SMALL, s);
+        k_dense_expm_col<<<1, DECIDE_THREADS, smem, s>>>(m, A, reinterpret_cast<double2 *>(x_dev), status);
+    }
+    EMUSV_CHECK_LAUNCH();
+    int h = 0;
+    EMUSV_CHECK(cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    EMUSV_CHECK(cudaStreamSynchronize(s));  // the host matrix may be reused once this returns
+    return h;
+}
 
 size_t emusv_arnoldi_workspace_bytes(int nqubits, int dtype, int basis_capacity) {
     if (nqubits < 1 || nqubits > EMUSV_MAX_QUBITS || basis_capacity < 0 ||

@@ -7,9 +7,10 @@ Two routes behind the reference signature:
   the whole Lanczos step runs in ``emusv_krylov_step`` -- fused H*psi with FP64 reductions,
   Gram-Schmidt, and the exponential of the extended Krylov matrix with the Expokit error
   estimate computed on the GPU.
-* any other callable (Hermitian case): the reference's Lanczos loop driven from Python,
-  with the vector arithmetic in this package's kernels (FP64-accumulated dots, axpy,
-  multi-vector combination) and the small exponential on the GPU.
+* any other callable: the reference's Lanczos (Hermitian) or Arnoldi loop driven from
+  Python, with the vector arithmetic in this package's kernels (FP64-accumulated dots,
+  axpy, multi-vector combination) and the small exponential (tridiagonal, or dense for
+  Arnoldi) on the GPU.
 * ``is_hermitian=False`` with a :class:`HamiltonianExpOperator` (the Monte Carlo stepper's
   noisy Hamiltonian): the whole Arnoldi step runs in ``emusv_arnoldi_step``.
 """
@@ -244,6 +245,23 @@ def _combine(coef: torch.Tensor, V: list[torch.Tensor]) -> torch.Tensor:
     return out
 
 
+def dense_expm_col(T: np.ndarray, device) -> torch.Tensor:
+    """exp(T) e_0 for a small dense complex matrix on the GPU (device complex128 [m])."""
+    m = T.shape[0]
+    L = _lib.load()
+    a = np.ascontiguousarray(T, dtype=np.complex128)
+    x = torch.empty(m, dtype=torch.complex128, device=device)
+    nb = L.emusv_dense_expm_scratch_bytes(m)
+    if nb == 0:
+        raise ValueError(f"dense exponential of a {m} x {m} matrix: at most "
+                         f"{_MAX_ARNOLDI_DIM + 2} rows")
+    sc = _lib.scratch(device, nb)
+    _lib.check(L.emusv_dense_expm_col(m, a.ctypes.data, x.data_ptr(), sc.data_ptr(), sc.numel(),
+                                      torch.cuda.current_stream(device).cuda_stream),
+               "dense exponential")
+    return x
+
+
 def _tri_parts(T: np.ndarray, m: int):
     d = np.array([T[k, k] for k in range(m)], dtype=np.complex128)
     up = np.array([T[k - 1, k] if k > 0 else 0 for k in range(m)], dtype=np.complex128)
@@ -251,8 +269,12 @@ def _tri_parts(T: np.ndarray, m: int):
     return d, up, lo
 
 
-def _generic_lanczos(op, v: torch.Tensor, exp_tolerance, norm_tolerance, max_krylov_dim):
-    """krylov_exp.py:23-106 for Hermitian op, vector arithmetic on the GPU."""
+def _generic_krylov(op, v: torch.Tensor, is_hermitian: bool, exp_tolerance, norm_tolerance,
+                    max_krylov_dim):
+    """krylov_exp.py:23-106 for any callable ``op`` (a vector or tensor of any shape):
+    Lanczos (Gram-Schmidt against the last two vectors) for a Hermitian op, Arnoldi (against
+    every vector, T upper Hessenberg) otherwise; the vector arithmetic and the small
+    exponentials (tridiagonal, or dense for Arnoldi) on the GPU."""
     v = _lib.require_cuda_vector(v, "vector")
     shape = v.shape
     v = v.reshape(-1)
@@ -265,6 +287,11 @@ def _generic_lanczos(op, v: torch.Tensor, exp_tolerance, norm_tolerance, max_kry
         r = res.cpu()
         return complex(r[0].item(), r[1].item())
 
+    def expm(m: int) -> torch.Tensor:  # exp(T[:m, :m]) e_0
+        if is_hermitian:
+            return tridiag_expm_col(*_tri_parts(T, m), v.device)
+        return dense_expm_col(T[:m, :m], v.device)
+
     initial_norm = np.sqrt(dot(v, v).real)  # 43
     v = v / initial_norm  # 44
     V = [v]
@@ -273,20 +300,21 @@ def _generic_lanczos(op, v: torch.Tensor, exp_tolerance, norm_tolerance, max_kry
     for j in range(max_krylov_dim):
         w = _lib.require_cuda_vector(op(V[-1].reshape(shape)), "op(v)").reshape(-1).clone()  # 50
         n = np.sqrt(dot(w, w).real)  # 52
-        for k in range(max(0, j - 1), j + 1):  # 54-58
+        k_start = max(0, j - 1) if is_hermitian else 0  # 54
+        for k in range(k_start, j + 1):  # 55-58
             ov = dot(V[k], w)
             T[k, j] = ov
             _axpy(-ov, V[k], w)
         n2 = np.sqrt(dot(w, w).real)  # 60
         T[j + 1, j] = n2
         if n2 < norm_tolerance:  # 63-71
-            e = tridiag_expm_col(*_tri_parts(T, j + 1), v.device)
+            e = expm(j + 1)
             r = initial_norm * _combine(e, V)
             return KrylovExpResult(r.reshape(shape), True, True, j + 1)
         w /= n2
         V.append(w)
         T[j + 2, j + 1] = 1  # 77
-        expd = tridiag_expm_col(*_tri_parts(T, j + 3), v.device)  # 78
+        expd = expm(j + 3)  # 78
         e_host = expd.cpu().numpy()
         err1 = abs(e_host[j + 1])
         err2 = abs(e_host[j + 2] * n)
@@ -304,8 +332,9 @@ def krylov_exp_impl(op, v: torch.Tensor, is_hermitian: bool, exp_tolerance: floa
     """Same contract as krylov_exp.py:23-106 (the input ``v`` becomes invalid)."""
     if not is_hermitian:
         if not isinstance(op, HamiltonianExpOperator):
-            raise NotImplementedError("emulators_b200: the non-Hermitian (Arnoldi) Krylov "
-                                      "exponential takes a HamiltonianExpOperator")
+            if max_krylov_dim > _MAX_ARNOLDI_DIM:
+                raise ValueError(f"max_krylov_dim must be in 1..{_MAX_ARNOLDI_DIM} for Arnoldi")
+            return _generic_krylov(op, v, False, exp_tolerance, norm_tolerance, max_krylov_dim)
         out, info, st = fused_arnoldi_step(op, v, exp_tolerance, norm_tolerance, max_krylov_dim)
         return KrylovExpResult(out, st == _lib.OK, bool(info.happy_breakdown), info.iterations)
     if isinstance(op, HamiltonianExpOperator):
@@ -313,7 +342,7 @@ def krylov_exp_impl(op, v: torch.Tensor, is_hermitian: bool, exp_tolerance: floa
             raise ValueError("a Hamiltonian with the noise term is not Hermitian")
         out, info, st = fused_step(op, v, exp_tolerance, norm_tolerance, max_krylov_dim)
         return KrylovExpResult(out, st == _lib.OK, bool(info.happy_breakdown), info.iterations)
-    return _generic_lanczos(op, v, exp_tolerance, norm_tolerance, max_krylov_dim)
+    return _generic_krylov(op, v, True, exp_tolerance, norm_tolerance, max_krylov_dim)
 
 
 def krylov_exp(op, v: torch.Tensor, exp_tolerance: float, norm_tolerance: float,

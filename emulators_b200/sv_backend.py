@@ -157,16 +157,41 @@ class BitStrings(Observable):
         return state.sample(self.num_shots)
 
 
+class Statistics(Observable):
+    """Per-step statistics (sv_backend_impl.py:32-71): the wall time of the step just taken
+    and the peak device memory so far (MB, the largest over the GPUs), logged at INFO and
+    stored under the tag ``statistics`` at every step of the time loop."""
+
+    tag = "statistics"
+
+    def __init__(self, timestep_count: int):
+        super().__init__(None)
+        self.durations: list[float] = []
+        self.timestep_count = timestep_count
+
+    def apply(self, *, config, state, hamiltonian):
+        duration = self.durations[-1]
+        if state.data.is_cuda:
+            mem = max(torch.cuda.max_memory_allocated(d) * 1e-6 for d in range(torch.cuda.device_count()))
+        else:  # pragma: no cover - the package keeps its states on the GPU
+            import resource
+
+            mem = resource.getrusage(resource.RUSAGE_SELF).ru_maxrss * 1e-3
+        logger.info(f"step = {len(self.durations)}/{self.timestep_count}, RSS = {mem:.3f} MB, "
+                    f"\u0394t = {duration:.3f} s")
+        return {"RSS": mem, "duration": duration}
+
+
 class Results:
     """Per-observable time series: ``results.get(tag)`` -> list of values,
-    ``results.times(tag)`` -> their normalised times."""
+    ``results.times(tag)`` -> their normalised times; ``results.statistics`` the
+    per-step statistics (tag ``statistics``)."""
 
     def __init__(self, atom_order: Sequence[str], total_duration: int):
         self.atom_order = tuple(atom_order)
         self.total_duration = total_duration
         self._data: dict[str, list] = {}
         self._times: dict[str, list] = {}
-        self.statistics: list[dict] = []
 
     def _store(self, tag: str, t: float, value) -> None:
         self._data.setdefault(tag, []).append(value)
@@ -243,6 +268,10 @@ class SequenceData:
     qubit_ids: tuple = ()
     lindblad_ops: list = dataclasses.field(default_factory=list)
     has_stochastic_noise: bool = False
+    # state-preparation errors: the atoms of this run that were badly prepared (drawn per
+    # run by the sequence sampler) and the error probability
+    bad_atoms: tuple = ()
+    state_prep_error: float = 0.0
 
     def U(self, t: float) -> torch.Tensor:
         if callable(self.interaction_matrix):
@@ -310,18 +339,55 @@ class SVBackendImpl:
         else:
             self.state = StateVector.make(self.nqubits, dtype=config.vector_dtype)
         self.results = Results(data.qubit_ids, int(self.target_times[-1]))
+        self.statistics = Statistics(self.nsteps)
         self._current_H: RydbergHamiltonian | None = None
+        self.init_dark_qubits()
+        if config.initial_state is not None and data.state_prep_error > 0.0:
+            raise NotImplementedError(
+                "an initial state cannot be combined with a state-preparation error")
         self.time = time.time()
+
+    def init_dark_qubits(self) -> None:
+        """sv_backend_impl.py:162-184: with a state-preparation error, the badly prepared
+        atoms of the run are dark -- their Omega, delta and phi are zero at every step and
+        their rows and columns of the interaction matrix are zero (the caller's samples are
+        left untouched)."""
+        self.dark_qubits = None
+        if self._data.state_prep_error > 0.0:
+            mask = torch.as_tensor(tuple(bool(b) for b in self._data.bad_atoms), dtype=torch.bool)
+            if mask.numel() != self.nqubits:
+                raise ValueError(f"bad_atoms has {mask.numel()} entries for {self.nqubits} atoms")
+            self.dark_qubits = mask
+            self.omega, self.delta, self.phi = (a.clone() for a in (self.omega, self.delta, self.phi))
+            for a in (self.omega, self.delta, self.phi):
+                a[:, mask] = 0.0
+
+    def _U(self, t: float) -> torch.Tensor:
+        U = self._data.U(t)
+        if self.dark_qubits is not None:
+            U = torch.as_tensor(U).clone()
+            U[self.dark_qubits, :] = 0.0
+            U[:, self.dark_qubits] = 0.0
+        return U
 
     def step(self, step_idx: int) -> None:
         dt = self.target_times[step_idx + 1] - self.target_times[step_idx]
         self._current_H = None
+        torch.cuda.nvtx.range_push(f"step {step_idx + 1}")
         self.state.data, self._current_H = self.stepper.apply(
             dt * _TIME_CONVERSION_COEFF, self.omega[step_idx], self.delta[step_idx],
-            self.phi[step_idx], self._data.U(self.target_times[step_idx]), self.state.data,
+            self.phi[step_idx], self._U(self.target_times[step_idx]), self.state.data,
             self._config.krylov_tolerance, self._data.lindblad_ops)
         self._apply_observables(step_idx + 1)
-        self.results.statistics.append({"step": step_idx + 1, "duration": time.time() - self.time})
+        torch.cuda.nvtx.range_pop()
+        self._save_statistics(step_idx + 1)
+
+    def _save_statistics(self, step_idx: int) -> None:
+        """sv_backend_impl.py:244-255: after every step (not only at observation times)."""
+        t = self.target_times[step_idx] / self.target_times[-1]
+        self.statistics.durations.append(time.time() - self.time)
+        self.results._store(self.statistics.name, t, self.statistics.apply(
+            config=self._config, state=self.state, hamiltonian=self._current_H))
         self.time = time.time()
 
     def _apply_observables(self, step_idx: int) -> None:
@@ -338,7 +404,7 @@ class SVBackendImpl:
             state = self.state
         if self._current_H is None:  # t = 0 (sv_backend_impl.py:224-234)
             self._current_H = self.stepper.get_hamiltonian(
-                self.omega[0], self.delta[0], self.phi[0], self._data.lindblad_ops, self._data.U(
+                self.omega[0], self.delta[0], self.phi[0], self._data.lindblad_ops, self._U(
                     0.5 * (self.target_times[step_idx] + self.target_times[step_idx + 1])),
                 state.data.device)
         for o in due:

@@ -363,6 +363,14 @@ int emusv_vec_combine(int64_t len, int dtype, int k, const double *coef_dev, con
  * by host complex arrays diag[m], upper[m] (upper[k] = A[k-1][k]) and lower[m]
  * (lower[k] = A[k+1][k]); FP64 Taylor series with scaling, on the device.  Replaces the
  * torch.linalg.matrix_exp of krylov_exp.py:66,78.  Synchronises the stream. */
+/* x_dev (device complex128 [m]) = exp(A) e_0 for a dense complex m x m matrix A (host,
+ * row-major, complex128 interleaved: a[2*(r*m + c)] real, +1 imaginary), m <= 102: the
+ * matrix_exp(T)[:, 0] of the non-Hermitian (Arnoldi) krylov_exp_impl (krylov_exp.py:65,
+ * 78), whose T is upper Hessenberg plus the extension entry.  EMUSV_NONFINITE when the
+ * norm of A is not finite.  Synchronises the stream (the host matrix may be reused). */
+size_t emusv_dense_expm_scratch_bytes(int m);
+int emusv_dense_expm_col(int m, const double *a, double *x_dev, void *scratch, size_t scratch_bytes,
+                         void *stream);
 size_t emusv_tridiag_scratch_bytes(void);
 int emusv_tridiag_expm_col(int m, const double *diag, const double *upper, const double *lower,
                            double *x_dev, void *scratch, size_t scratch_bytes, void *stream);

@@ -41,6 +41,10 @@ Fixtures (inputs and reference outputs, all complex128/float64):
                        density-matrix observables (emu_sv/lindblad_operator.py).
 * pchip.npz            PCHIP1D (emu_base/math/pchip_torch.py): the reference's test data,
                        random knots with extrapolated queries, drive-like 1 ns signals.
+* krylov_nonhermitian.npz  the Arnoldi krylov_exp_impl for arbitrary callables (the
+                       reference's test_krylov_with_matrix case and two more).
+* dark_qubits.npz      state-preparation errors: the reference's init_dark_qubits on a
+                       9-atom chain and 12 stepper steps on the masked data.
 * noisy.npz            the Monte Carlo path: H*psi with the noise term, Arnoldi
                        krylov_exp (is_hermitian=False), expect_batch / apply, Brent's
                        abscissae, and EvolveMonteCarlo steps (N=8, 40 steps, two seeds of
@@ -791,6 +795,103 @@ def gen_target_times(R):
 GENERATORS["target_times"] = gen_target_times
 
 
+def load_backend_impl(R, ref: str):
+    """emu_sv/sv_backend_impl.py with stand-ins for what it imports besides the hot-path
+    modules already loaded (emu_base's adapter helpers, the config and state classes)."""
+    import emu_base  # the package shell of load_reference
+
+    for name in ("SequenceData", "get_max_rss_cpu", "get_max_rss_gpu"):
+        setattr(emu_base, name, getattr(R["adapter"], name, _Placeholder))
+    emu_base.is_evaluation_time = R["adapter"].is_evaluation_time
+    for name in ("emu_sv.dense_state", "emu_sv.sv_config"):
+        sys.modules[name] = _FakeModule(name)
+    spec = importlib.util.spec_from_file_location("emu_sv.solver", os.path.join(ref, "emu_sv/solver.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["emu_sv.solver"] = mod
+    spec.loader.exec_module(mod)
+    te = sys.modules["emu_sv.time_evolution"]
+    for name in ("EvolveStateVector", "EvolveDensityMatrix", "EvolveMonteCarlo"):
+        setattr(te, name, getattr(R["impl"], name))
+    spec = importlib.util.spec_from_file_location("emu_sv.sv_backend_impl",
+                                                  os.path.join(ref, "emu_sv/sv_backend_impl.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["emu_sv.sv_backend_impl"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def gen_dark_qubits(R):
+    """State-preparation errors: the reference's SVBackendImpl.init_dark_qubits
+    (sv_backend_impl.py:162-184) on a 9-atom chain with atoms 0, 4 and 7 badly prepared
+    (Omega, delta, phi of those atoms zeroed, their interaction rows and columns zeroed),
+    then 12 steps of the reference stepper chain on the masked data."""
+    impl = load_backend_impl(R, R["ref_path"])
+    n, steps = 9, 12
+    rng = np.random.default_rng(21)
+    pos = wl.chain(n, 6.0)
+    U0 = torch.as_tensor(wl.interaction_matrix(pos))
+    om = torch.as_tensor(rng.uniform(1.0, 6.0, (steps, n)))
+    de = torch.as_tensor(rng.uniform(-10.0, 10.0, (steps, n)))
+    ph = torch.as_tensor(rng.normal(size=(steps, n)))
+    bad = (True, False, False, False, True, False, False, True, False)
+    ns = types.SimpleNamespace(
+        _data=types.SimpleNamespace(state_prep_error=0.1, bad_atoms=bad),
+        interaction_matrix=lambda t: U0.unsqueeze(0), omega=om.clone(), delta=de.clone(),
+        phi=ph.clone())
+    impl.SVBackendImpl.init_dark_qubits(ns)
+    U = ns.interaction_matrix(0.0)[0]
+    DSE = R["torch"].DifferentiableStateVectorEvolution
+    s = torch.zeros(2**n, dtype=torch.complex128)
+    s[0] = 1.0
+    dt = 0.01
+    for k in range(steps):
+        s, _ = DSE.apply(dt, ns.omega[k], ns.delta[k], ns.phi[k], U, s, 1e-10, 100)
+    return {"omega": np_(om), "delta": np_(de), "phi": np_(ph), "U": np_(U0),
+            "bad_atoms": np.array(bad), "dt": np.array(dt),
+            "omega_masked": np_(ns.omega), "delta_masked": np_(ns.delta),
+            "phi_masked": np_(ns.phi), "U_masked": np_(U), "final": np_(s)}
+
+
+GENERATORS["dark_qubits"] = gen_dark_qubits
+
+
+def gen_krylov_nonhermitian(R):
+    """The Arnoldi branch of krylov_exp_impl (is_hermitian=False) for arbitrary callables:
+    the reference's own test_krylov_with_matrix case (test/emu_base/math/test_krylov_exp.py:
+    194-218: seed 1211, a random 256 x 256 operator of unit norm applied to a random 256 x
+    256 tensor, tolerances 1e-6), a random non-Hermitian operator on a vector at 1e-10, and
+    a rank-2 operator (happy breakdown)."""
+    K = R["krylov"]
+    c = torch.complex128
+    out = {}
+
+    def run(pre, A, x, tol):
+        r = K.krylov_exp_impl(lambda y: A @ y, x.clone(), is_hermitian=False, exp_tolerance=tol,
+                              norm_tolerance=tol, max_krylov_dim=100)
+        out[pre + "op"], out[pre + "in"], out[pre + "result"] = np_(A), np_(x), np_(r.result)
+        out[pre + "iters"] = np.array(r.iteration_count)
+        out[pre + "happy"] = np.array(r.happy_breakdown)
+        out[pre + "converged"] = np.array(r.converged)
+        out[pre + "tol"] = np.array(tol)
+
+    torch.random.manual_seed(1211)
+    A = torch.rand(256, 256, dtype=c)
+    A = A / A.norm()
+    X = torch.rand(256, 256, dtype=c)
+    run("m_", A, X, 1e-6)
+    g = torch.Generator().manual_seed(17)
+    B = (torch.rand(128, 128, dtype=c, generator=g) - (0.5 + 0.5j)) * 0.4
+    v = torch.rand(128, dtype=c, generator=g) - (0.5 + 0.5j)
+    run("v_", B, v, 1e-10)
+    u = torch.rand(64, 2, dtype=c, generator=g)
+    w = torch.rand(2, 64, dtype=c, generator=g)
+    run("r_", u @ w, torch.rand(64, dtype=c, generator=g), 1e-10)
+    return out
+
+
+GENERATORS["krylov_nonhermitian"] = gen_krylov_nonhermitian
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True,
@@ -800,6 +901,7 @@ def main():
     a = ap.parse_args()
     torch.set_num_threads(a.threads)
     R = load_reference(a.reference)
+    R["ref_path"] = a.reference
     for name, fn in GENERATORS.items():
         if a.only and name not in a.only:
             continue

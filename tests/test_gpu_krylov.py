@@ -170,3 +170,28 @@ def test_iteration_hint_matches_testing_every_iteration():
     for r in runs[1:]:
         assert r[1] == runs[0][1]
         np.testing.assert_array_equal(r[0], runs[0][0])
+
+
+def test_generic_arnoldi_matches_reference():
+    """krylov_exp_impl(is_hermitian=False) for arbitrary callables (reference
+    krylov_exp.py:23-106; its test/emu_base/math/test_krylov_exp.py:194-218 case on a
+    256 x 256 tensor, a vector case, and a rank-2 operator's happy breakdown): iteration
+    counts, flags and results of the reference."""
+    from emulators_b200 import krylov_exp, krylov_exp_impl
+
+    g = golden("krylov_nonhermitian")
+    for p in ("m_", "v_", "r_"):
+        A = torch.as_tensor(g[p + "op"]).to(DEV)
+        x = torch.as_tensor(g[p + "in"]).to(DEV)
+        tol = float(g[p + "tol"])
+        r = krylov_exp_impl(lambda y: A @ y, x.clone(), False, tol, tol, 100)
+        assert r.iteration_count == int(g[p + "iters"]), p
+        assert r.happy_breakdown == bool(g[p + "happy"]) and r.converged == bool(g[p + "converged"])
+        ref = g[p + "result"]
+        assert r.result.shape == x.shape
+        np.testing.assert_allclose(r.result.cpu().numpy(), ref, atol=1e-12 * np.abs(ref).max(), rtol=0)
+    # the reference test's own check: close to the dense exponential
+    A = torch.as_tensor(g["m_op"]).to(DEV)
+    X = torch.as_tensor(g["m_in"]).to(DEV)
+    out = krylov_exp(lambda y: A @ y, X.clone(), 1e-6, 1e-6, is_hermitian=False, max_krylov_dim=100)
+    assert torch.allclose(out, torch.linalg.matrix_exp(A) @ X)

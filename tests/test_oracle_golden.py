@@ -109,3 +109,38 @@ def test_oracle_happy_breakdown_and_identity(oracle):
     r = oracle.krylov_exp_impl(lambda x: eye @ x, v, True, 1e-6, 1e-12, 80)
     assert r.happy_breakdown and r.iteration_count == 1
     np.testing.assert_allclose(r.result, np.e * v, atol=1e-9)
+
+
+def test_oracle_arnoldi_for_callables(oracle):
+    """The oracle's krylov_exp_impl(is_hermitian=False) on the reference's fixtures of the
+    Arnoldi branch for arbitrary operators (krylov_nonhermitian.npz, including the
+    reference's own test_krylov_with_matrix case on a 256 x 256 tensor)."""
+    g = golden("krylov_nonhermitian")
+    for p in ("m_", "v_", "r_"):
+        A, x = g[p + "op"], g[p + "in"]
+        shape = x.shape
+        r = oracle.krylov_exp_impl(lambda y: (A @ y.reshape(shape)).reshape(-1), x.reshape(-1).copy(),
+                                   False, float(g[p + "tol"]), float(g[p + "tol"]), 100)
+        assert r.iteration_count == int(g[p + "iters"])
+        assert r.happy_breakdown == bool(g[p + "happy"]) and r.converged == bool(g[p + "converged"])
+        ref = g[p + "result"].reshape(-1)
+        np.testing.assert_allclose(r.result, ref, atol=1e-12 * np.abs(ref).max())
+
+
+def test_oracle_dark_qubits(oracle):
+    """State-preparation errors (sv_backend_impl.py:162-184): the masks the reference applies
+    and its 12-step chain on the masked data (dark_qubits.npz)."""
+    g = golden("dark_qubits")
+    bad = g["bad_atoms"].astype(bool)
+    om, de, ph, U = (g[k].copy() for k in ("omega", "delta", "phi", "U"))
+    for a in (om, de, ph):
+        a[:, bad] = 0.0
+    U[bad, :] = 0.0
+    U[:, bad] = 0.0
+    for k, a in (("omega", om), ("delta", de), ("phi", ph), ("U", U)):
+        np.testing.assert_array_equal(a, g[k + "_masked"])
+    s = np.zeros(1 << U.shape[0], dtype=np.complex128)
+    s[0] = 1.0
+    for k in range(om.shape[0]):
+        s, _, _ = oracle.evolve_step(float(g["dt"]), om[k], de[k], ph[k], U, s, 1e-10)
+    np.testing.assert_allclose(s, g["final"], atol=1e-11)
