@@ -19,7 +19,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import re
 import os
 import statistics
 import subprocess
@@ -45,17 +44,12 @@ def peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def ncu_traffic() -> int | None:
-    """DRAM bytes (read + write) of one Lanczos iteration at N=26 from the committed ncu
-    summary (profiles/lanczos_iteration_fused_pass_low_n25_c64.md: captures at N=25
-    scaled by 2)."""
-    p = os.path.join(REPO, "profiles", "lanczos_iteration_fused_pass_low_n25_c64.md")
-    try:
-        with open(p) as f:
-            m = re.search(r"traffic_bytes_per_lanczos_iteration_at_n26:\s*(\d+)", f.read())
-        return int(m.group(1)) if m else None
-    except OSError:
-        return None
+# DRAM bytes (read + write) of one Lanczos iteration at N=26, complex64: ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum of the iteration's three kernels at N=25
+# (python -m emulators_b200.profile_case --n 25 --steps 1 --hpsi 0 --max-krylov-dim 20,
+# launches 4-6 of k_pass_(lz|high): 1610.8 MB read, 669.5 MB written), doubled.  A constant
+# of the kernels it was measured on; the CUDA-event split reports the streamed units live.
+ITERATION_TRAFFIC_N26_C64 = 2 * (1610.8 + 669.5) * 1e6
 
 
 def log(msg: str) -> None:
@@ -349,10 +343,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                                "bytes (H*psi 2 D s + recurrence 4 D s) / iteration time",
                      "achieved": round(achieved, 1), "peak": hbm, "peak_source": which,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                     "traffic": ncu_traffic() if n == 26 and es == 8 else None,
-                     "traffic_source": "ncu --set full of the fused pass L and the pass H kernels "
-                                       "at N=25, x2 (profiles/lanczos_iteration_fused_pass_low_"
-                                       "n25_c64.md)",
+                     "traffic": int(ITERATION_TRAFFIC_N26_C64) if n == 26 and es == 8 else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                       "iteration's three kernels at N=25, x2 (profiles/"
+                                       "lanczos_iteration_h_first_n24_n25_c64.md)",
                      "algorithmic_bytes_per_launch": alg_iter,
                      "avg_launch_ms": round(iter_s * 1e3, 4),
                      "per_kernel": per_pass,
@@ -877,8 +871,18 @@ def batch_c4(dev, per_instance_sample: int = 8) -> dict:
     amp = lambda ws: sum((1 << w.nqubits) * w.nsteps for w in ws)  # noqa: E731
     per_rate = nst / el1
     per_rate_weighted = total / (el1 * amp(regs) / amp(per))
+    # algorithmic bytes of the batch: (7 m + 1) D s per register-step (m Lanczos iterations
+    # of H*psi 2 D s + recurrence 4 D s, the combination (m + 1) D s), s = 8
+    dims = np.array([1 << w.nqubits for w in regs], dtype=np.float64)
+    alg = float(((7.0 * iters + 1.0) * (iters > 0)).sum(axis=1) @ dims) * 8.0
+    hbm, which = peaks()
     return {"instances": len(regs), "instance_steps": total,
             "ms": round(el * 1e3, 2), "instance_steps_per_s": round(total / el, 1),
+            "roofline": {"algorithmic_bytes": int(alg), "achieved": round(alg / el / 1e9, 1),
+                         "peak": hbm, "peak_source": which, "unit": "GB/s",
+                         "frac": round(alg / el / 1e9 / hbm, 4),
+                         "note": "(7 m + 1) D s per register-step from the recorded "
+                                 "iteration counts"},
             "launch": {"tile_bits": t.tile_bits, "blocks_per_sm": t.blocks_per_sm,
                        "krylov_capacity": t.capacity, "autotune_ms": t.ms,
                        "graph": "one cooperative persistent kernel replayed from a CUDA graph"},

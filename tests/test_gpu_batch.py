@@ -64,6 +64,23 @@ def test_batch_c128_matches_oracle(oracle, tile_bits):
         assert list(iters[i, :len(its)]) == its, (i, list(iters[i]), its)
 
 
+def test_batch_c128_large_registers_match_oracle(oracle):
+    """The top of the batched size range (config 4 draws 12-18 qubits; the engine takes up
+    to 20): complex128 registers of 14, 16, 18 and 20 qubits with complex phases against
+    the oracle's chain, states and every step's Krylov iteration count."""
+    from emulators_b200.batch import BatchEvolution
+
+    regs = _random_batch([14, 20, 16, 18], [4, 3, 4, 3], seed=29, phase=True)
+    b = BatchEvolution(regs, precision="c128", max_krylov_dim=100)
+    status, iters = b.run(tune=False, tile_bits=9, blocks_per_sm=1, capacity=40)
+    assert (status == 0).all()
+    for i, r in enumerate(regs):
+        ref, its = _oracle_chain(oracle, r)
+        got = b.state(i).cpu().numpy()
+        assert np.abs(got - ref).max() < 1e-10, (i, np.abs(got - ref).max())
+        assert list(iters[i, :len(its)]) == its, (i, list(iters[i]), its)
+
+
 def test_batch_c64_matches_single_register_path():
     """complex64 batch vs the single-register fused step (same precision form)."""
     from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian
