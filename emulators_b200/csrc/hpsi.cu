@@ -135,7 +135,7 @@ static bool single_pass_forced() {
 
 bool lz_applies(int dtype, int n);
 int lz_moments(int dtype, const HamParams &H, const void *psi, void *part, double *partials,
-               double *part_h, int *err, cudaStream_t s, int *grid_out);
+               double *part_h, unsigned *cnt, int *err, cudaStream_t s, int *grid_out);
 // The Lanczos iteration of this register runs in the H-first order (hpsi_pass.cu): wider
 // than one pass-L tile and the passes not switched off.
 bool lanczos_h_first(int dtype, int n) { return !single_pass_forced() && lz_applies(dtype, n); }
@@ -413,7 +413,8 @@ int emusv_expect(int nqubits, int dtype, const double *omegas, const double *del
         if (reinterpret_cast<uintptr_t>(psi) & 15) return EMUSV_BAD_ARGUMENT;
         unsigned char *vec = reinterpret_cast<unsigned char *>(scratch) + scratch_head_bytes();
         double *part_h = sums + 64;  // the pass H kernels' partials (not used here)
-        st = lz_moments(dtype, P, psi, vec, partials, part_h, device_error_word(), s, &grid);
+        unsigned *cnt = reinterpret_cast<unsigned *>(part_h + (size_t)max_grid_blocks() * NRED);
+        st = lz_moments(dtype, P, psi, vec, partials, part_h, cnt, device_error_word(), s, &grid);
         if (st) return st;
     } else {
         HpsiArgs A = {};

@@ -1,5 +1,6 @@
 // Host side of the two-pass H*psi: layout choice, parameter tables, cluster launches.
 #include <cudaTypedefs.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <mutex>
@@ -267,6 +268,20 @@ template <typename R> static int lz_chunk_bits(int n) {
     constexpr int TB = PassShape<R>::TB, CMIN = PassShape<R>::CMIN, TBL = LzShape<R>::TB;
     return n - TBL <= 2 * (TB - CMIN) ? CMIN : CMIN - 1;
 }
+// The two pass H groups of the Lanczos iteration run as two launches unless
+// EMUSV_FUSED_PASS_H=1 selects the fused persistent kernel (k_pass_hh).  Measured on B200 at
+// N=26 complex64: the fused kernel moves about 2 vector units of DRAM traffic instead of 5
+// but takes 0.90 ms against 0.49 ms for the two launches -- its tiles wait on thread 0's
+// gpu-scope fences (each drains that thread's own stores) and on the work counter.
+static bool hh_forced_off() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("EMUSV_FUSED_PASS_H");
+        v = (e && e[0] == '1') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 // The Lanczos iteration of this register runs in the H-first order (pass H kernels, then
 // the recurrence pass L): registers wider than one pass-L tile.
 bool lz_applies(int dtype, int n) {
@@ -327,13 +342,65 @@ int lz_low(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *
     return launch_lz_mode<LZ_ITER>(dtype, H, A, s, grid_out);
 }
 
+// Both groups of a two-group pass H in one persistent launch (k_pass_hh): group 1 on the
+// g bits from hskip (the pass-L tile width), applying [hskip, n - g); group 2 on the top g
+// bits.  cnt: HH_CNT_WORDS zero-initialised words of device memory.
+template <typename R, bool REALC, int CMIN>
+static int launch_hh(PassParams P, const PassArgs &A, unsigned *cnt, int hskip, cudaStream_t s,
+                     int *grid_out) {
+    typedef typename cvec<R>::T C;
+    constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, NT = 1 << (TB - RB);
+    const int n = P.n, g = TB - CMIN, hs = hskip, hpos2 = n - g, nsb = hs - CMIN, tb = n - hs - g;
+    if (!cnt || nsb < 1 || nsb > HH_MAX_NS_BITS || tb < 1 || hpos2 > hs + g) return EMUSV_BAD_ARGUMENT;
+    static_assert(HH_CNT_WORDS <= 1040, "KState::hh_cnt holds the fused pass H counters");
+    auto kern = k_pass_hh<R, REALC, TB, RB, CMIN>;
+    const size_t smem = pass_hh_smem<C, TB>();
+    EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int64_t grid = (int64_t)sm_count() * per_sm;
+    P.hg = g;
+    P.hc = CMIN;
+    P.pbh = 0;
+    P.hskip = hskip;
+    P.hbox_rows = g > 8 ? 256 : (1 << g);
+    PassHHMaps M;
+    memset(&M, 0, sizeof(M));
+    P.hpos = hs;
+    if (!encode_pass_high(&M.u1, A.u, n, (int)sizeof(C), P)) return EMUSV_CUDA_ERROR;
+    P.hpos = hpos2;
+    if (!encode_pass_high(&M.u2, A.u, n, (int)sizeof(C), P) ||
+        !encode_pass_high(&M.p2, A.out, n, (int)sizeof(C), P))
+        return EMUSV_CUDA_ERROR;
+    HHArgs H = {};
+    H.u = A.u;
+    H.part = A.out;
+    H.partials = A.partials;
+    H.gate = A.gate;
+    H.err = A.err;
+    H.cnt = cnt;
+    H.hs = hs;
+    H.hpos2 = hpos2;
+    H.ns_bits = nsb;
+    H.tps_bits = tb;
+    EMUSV_CHECK(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * ((size_t(1) << nsb) + 1), s));
+    {
+        ProfScope ps_(PROF_HPSI_HIGH, s);
+        kern<<<(unsigned)grid, NT, smem, s>>>(P, H, M);
+    }
+    EMUSV_CHECK_LAUNCH();
+    if (grid_out) *grid_out = (int)grid;
+    return EMUSV_OK;
+}
+
 // part = X_high u (unscaled flips of every bit above the pass-L tile, and of the CMIN
 // chunk bits of the pass H rows, applied by the last pass) in one or two strided passes;
 // their <u, X u> partials go to partials[0 .. *nblocks_out) (rows of NRED); *c0_out = CMIN
 // (the bits the recurrence pass L leaves out).
 template <typename R, bool REALC, int CMIN>
 static int lz_high_t(const HamParams &H, const void *u, void *part, double *partials, const int *gate,
-                     int *err, cudaStream_t s, int *nblocks_out, int *c0_out) {
+                     int *err, unsigned *cnt, cudaStream_t s, int *nblocks_out, int *c0_out) {
     constexpr int TB = PassShape<R>::TB, RB = PassShape<R>::RB, TBL = LzShape<R>::TB;
     const int n = H.n, rem = n - TBL, G = TB - CMIN;
     if (rem < 1 || rem > 2 * G) return EMUSV_BAD_ARGUMENT;
@@ -347,6 +414,12 @@ static int lz_high_t(const HamParams &H, const void *u, void *part, double *part
     A.gate = gate;
     A.err = err;
     int g1 = 0, g2 = 0, st;
+    *c0_out = CMIN;
+    if (rem > G && !hh_forced_off() &&
+        launch_hh<R, REALC, CMIN>(P, A, cnt, TBL, s, &g2) == EMUSV_OK) {  // one fused launch
+        *nblocks_out = g2;
+        return EMUSV_OK;
+    }
     if (rem > G) {
         if ((st = launch_high<R, REALC, EPI_X_FIRST, CMIN>(P, n - 2 * G, A, nullptr, s, &g1, TBL))) return st;
         A.partials = partials + (size_t)g1 * NRED;
@@ -356,30 +429,29 @@ static int lz_high_t(const HamParams &H, const void *u, void *part, double *part
             return st;
     }
     *nblocks_out = g1 + g2;
-    *c0_out = CMIN;
     return EMUSV_OK;
 }
 
 template <typename R, bool REALC>
 static int lz_high_rows(const HamParams &H, const void *u, void *part, double *partials, const int *gate,
-                        int *err, cudaStream_t s, int *nb) {
+                        int *err, unsigned *cnt, cudaStream_t s, int *nb) {
     constexpr int CMIN = PassShape<R>::CMIN;
     int c0 = 0;
-    if (lz_chunk_bits<R>(H.n) == CMIN) return lz_high_t<R, REALC, CMIN>(H, u, part, partials, gate, err, s, nb, &c0);
-    return lz_high_t<R, REALC, CMIN - 1>(H, u, part, partials, gate, err, s, nb, &c0);
+    if (lz_chunk_bits<R>(H.n) == CMIN) return lz_high_t<R, REALC, CMIN>(H, u, part, partials, gate, err, cnt, s, nb, &c0);
+    return lz_high_t<R, REALC, CMIN - 1>(H, u, part, partials, gate, err, cnt, s, nb, &c0);
 }
 
 int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,
-            int *err, cudaStream_t s, int *nblocks_out);
+            int *err, unsigned *cnt, cudaStream_t s, int *nblocks_out);
 
 // Moments of H on psi through the passes (registers wider than one pass-L tile): the pass
 // H kernels write part = X_high psi into `part` (a vector of the register's size), then the
 // moments pass forms H psi tile by tile: partials 0 ||H psi||^2, 1-2 <psi, H psi> into
 // `partials` (*grid_out rows); the pass H kernels' own partials go to `part_h`.
 int lz_moments(int dtype, const HamParams &H, const void *psi, void *part, double *partials,
-               double *part_h, int *err, cudaStream_t s, int *grid_out) {
+               double *part_h, unsigned *cnt, int *err, cudaStream_t s, int *grid_out) {
     int nh = 0;
-    int st = lz_high(dtype, H, psi, part, part_h, nullptr, err, s, &nh);
+    int st = lz_high(dtype, H, psi, part, part_h, nullptr, err, cnt, s, &nh);
     if (st) return st;
     LzArgs A = {};
     A.u = psi;
@@ -390,13 +462,13 @@ int lz_moments(int dtype, const HamParams &H, const void *psi, void *part, doubl
 }
 
 int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,
-            int *err, cudaStream_t s, int *nblocks_out) {
+            int *err, unsigned *cnt, cudaStream_t s, int *nblocks_out) {
     if (H.noisy || !lz_applies(dtype, H.n)) return EMUSV_BAD_ARGUMENT;
     if (dtype == EMUSV_C64)
-        return H.real_coef ? lz_high_rows<float, true>(H, u, part, partials, gate, err, s, nblocks_out)
-                           : lz_high_rows<float, false>(H, u, part, partials, gate, err, s, nblocks_out);
-    return H.real_coef ? lz_high_rows<double, true>(H, u, part, partials, gate, err, s, nblocks_out)
-                       : lz_high_rows<double, false>(H, u, part, partials, gate, err, s, nblocks_out);
+        return H.real_coef ? lz_high_rows<float, true>(H, u, part, partials, gate, err, cnt, s, nblocks_out)
+                           : lz_high_rows<float, false>(H, u, part, partials, gate, err, cnt, s, nblocks_out);
+    return H.real_coef ? lz_high_rows<double, true>(H, u, part, partials, gate, err, cnt, s, nblocks_out)
+                       : lz_high_rows<double, false>(H, u, part, partials, gate, err, cnt, s, nblocks_out);
 }
 
 }  // namespace emusv

@@ -725,6 +725,299 @@ k_pass_high(const PassParams P, PassArgs A, const __grid_constant__ PassHighMaps
 }
 
 
+// ------------------------------------------------ fused two-group pass H (persistent)
+// The two strided passes over the bits above the pass-L tile of a large register, in ONE
+// persistent launch, so that the second group reads its inputs from the L2:
+//  * group 1: tiles of the chunk bits [0, c) x the g bits [hs, hs + g) (hs = the pass-L
+//    tile width), applying the flips of the bits [hs, hpos2): part = X_1 u;
+//  * group 2: tiles of the chunk bits x the top g bits [hpos2, n) (hpos2 = n - g), applying
+//    those flips and the chunk bits': part = part + X_2 u.
+// A "super-tile" is a value of the bits [c, hs): it is both a union of 2^(n-hs-g) group-1
+// tiles (tile index: the bits [hs + g, n)) and of as many group-2 tiles (bits [hs, hpos2)),
+// so a group-2 tile needs exactly the group-1 tiles of its super-tile (2^(c + n - hs)
+// amplitudes: 2 MB of complex64 at N = 26).  Items run in one order: the
+// group-1 stream first by LAG items, then the two streams alternate, then the rest of the
+// group-2 stream; CTAs take the next item from a global counter when they prefetch it.
+// Ordering: the CTA adds a group-1 tile to its super-tile's counter after the next tile's
+// block barrier, thread 0 fencing first (cumulative over the block's stores that the
+// barrier ordered before it).  A group-2 tile's intermediate sums are loaded by tensor map
+// after an acquire of that counter and a proxy fence: at prefetch time if the counter is
+// already complete, else when the tile is computed (a bounded wait, about 2 s of clock,
+// then EMUSV_TIMEOUT in *A.err).  Waits happen only when computing, only on tiles taken
+// earlier, so they end.
+constexpr int HH_MAX_NS_BITS = 10;  // super-tiles of the fused pass H: at most 2^10
+constexpr int HH_LAG = 512;         // group-1 items ahead of the first group-2 item
+constexpr int HH_CNT_WORDS = (1 << HH_MAX_NS_BITS) + 1;
+struct HHArgs {
+    const void *u;        // stored v (unscaled)
+    void *part;           // the sums (written by group 1, completed by group 2)
+    double *partials;     // [gridDim.x * NRED]: <u, X u> of the applied bits (0 re, 1 im)
+    const int *gate;
+    int *err;
+    unsigned *cnt;        // [2^ns_bits + 1]: group-1 tiles done per super-tile, then the
+                          // item counter; zero at launch (HH_CNT_WORDS words at most)
+    int hs, hpos2, ns_bits, tps_bits;
+};
+struct PassHHMaps {
+    CUtensorMap u1;  // input, group-1 layout (hpos = hs)
+    CUtensorMap u2;  // input, group-2 layout (hpos = hpos2)
+    CUtensorMap p2;  // intermediate sums, group-2 layout
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+template <typename C, int TB>
+__host__ __device__ constexpr size_t pass_hh_smem() {
+    return 2 * SH * (sizeof(C) << TB) + 16 * SH + 16 * SH + sizeof(double) * 8 * NRED;
+}
+
+template <typename R, bool REALC, int TB, int RB, int CT>
+__global__ void __launch_bounds__(1 << (TB - RB), 1)
+k_pass_hh(const PassParams P, HHArgs A, const __grid_constant__ PassHHMaps M) {
+    typedef typename cvec<R>::T C;
+    constexpr int SB = TB - RB, NT = 1 << SB, NA = 1 << RB;
+    constexpr uint32_t TILE_BYTES = sizeof(C) << TB;
+    constexpr int c = CT, g = TB - CT;
+    static_assert(CT >= 1 && CT <= TB - RB, "chunk bits must lie below the register bits");
+    if (A.gate && *A.gate != 0) return;
+    extern __shared__ __align__(128) unsigned char smem_pass[];
+    C *tiles = reinterpret_cast<C *>(smem_pass);  // [SH][2^TB] u
+    C *parts = tiles + ((int64_t)SH << TB);       // [SH][2^TB] intermediate sums (group 2)
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_pass + 2 * SH * TILE_BYTES);  // [SH] u
+    uint64_t *pbars = bars + SH;                                                       // [SH] sums
+    int64_t *ring = reinterpret_cast<int64_t *>(pbars + SH);  // [SH] item in each buffer
+    int *defer = reinterpret_cast<int *>(ring + SH);           // [SH] sums not loaded yet
+    double *red_scr = reinterpret_cast<double *>(smem_pass + 2 * SH * TILE_BYTES + 32 * SH);
+    const int tid = threadIdx.x;
+    const int nsb = A.ns_bits, tb = A.tps_bits;
+    const int64_t TPS = int64_t(1) << tb, NT1 = int64_t(1) << (nsb + tb);
+    const int64_t nitems = 2 * NT1;
+    const int64_t LAG = NT1 < HH_LAG ? NT1 : HH_LAG;
+    const int rows = P.hbox_rows, nbox = (1 << g) / rows;
+    const uint32_t box_bytes = TILE_BYTES / nbox;
+    const int64_t cmask = (int64_t(1) << c) - 1;
+    unsigned *next_item = A.cnt + (int64_t(1) << nsb);
+
+    // item q -> (group 1 or 2, super-tile s, tile t within it)
+    auto decode = [&](int64_t q, int &grp, int64_t &s, int64_t &t) {
+        int64_t i;
+        if (q < LAG) {
+            grp = 1;
+            i = q;
+        } else {
+            const int64_t r = q - LAG;
+            if (r < 2 * (NT1 - LAG)) {
+                grp = (r & 1) ? 1 : 2;
+                i = (r & 1) ? LAG + (r >> 1) : (r >> 1);
+            } else {
+                grp = 2;
+                i = (NT1 - LAG) + (r - 2 * (NT1 - LAG));
+            }
+        }
+        s = i >> tb;
+        t = i & (TPS - 1);
+    };
+    auto load_sums = [&](int64_t s, int64_t t, int buf) {
+        fence_proxy_async_global();
+        mbar_expect_tx(&pbars[buf], TILE_BYTES);
+        const int slo = (int)(s | (t << nsb));
+        for (int b = 0; b < nbox; ++b) {
+            unsigned char *dp = reinterpret_cast<unsigned char *>(parts + ((int64_t)buf << TB)) + b * box_bytes;
+            tmap_load5(dp, &M.p2, 0, slo, b * rows, 0, 0, &pbars[buf]);
+        }
+    };
+    // take item q into buffer buf and start its loads (thread 0, never blocks); the item
+    // numbers come from the global counter one tile ahead of their use
+    auto take = [&](int buf, int64_t q) {
+        ring[buf] = q;
+        defer[buf] = 0;
+        if (q >= nitems) return;
+        int grp;
+        int64_t s, t;
+        decode(q, grp, s, t);
+        mbar_expect_tx(&bars[buf], TILE_BYTES);
+        for (int b = 0; b < nbox; ++b) {
+            unsigned char *dv = reinterpret_cast<unsigned char *>(tiles + ((int64_t)buf << TB)) + b * box_bytes;
+            if (grp == 1) tmap_load5(dv, &M.u1, 0, (int)s, b * rows, 0, (int)t, &bars[buf]);
+            else tmap_load5(dv, &M.u2, 0, (int)(s | (t << nsb)), b * rows, 0, 0, &bars[buf]);
+        }
+        if (grp == 2) {
+            if (ld_acquire_u32(A.cnt + s) >= (unsigned)TPS) load_sums(s, t, buf);
+            else defer[buf] = 1;
+        }
+    };
+
+    if (tid == 0) {
+        for (int b = 0; b < SH; ++b) {
+            mbar_init(&bars[b], 1);
+            mbar_init(&pbars[b], 1);
+        }
+        fence_mbar_init();
+        for (int b = 0; b < SH - 1; ++b) take(b, (int64_t)atomicAdd(next_item, 1u));
+    }
+    // thread 0: the item number for the next take, requested a tile ahead
+    unsigned next_q = tid == 0 ? atomicAdd(next_item, 1u) : 0u;
+    __syncthreads();
+    bool ok = true;
+    C *__restrict__ outp = reinterpret_cast<C *>(A.part);
+    double red[2] = {0.0, 0.0};
+    int64_t pend = -1;  // super-tile of the last group-1 tile, counted after the next barrier
+    int buf = 0;
+    uint32_t vph = 0, pph = 0;  // mbarrier phase bits per buffer
+    for (;;) {
+        const int64_t q = ring[buf];
+        if (q >= nitems) break;
+        int grp;
+        int64_t s, t;
+        decode(q, grp, s, t);
+        const int hpos = grp == 1 ? A.hs : A.hpos2;
+        const C *tile = tiles + ((int64_t)buf << TB);
+        const C *ptile = parts + ((int64_t)buf << TB);
+        if (ok && !mbar_wait(&bars[buf], (vph >> buf) & 1u)) {
+            ok = false;
+            if (A.err) atomicExch(A.err, (int)EMUSV_TIMEOUT);
+        }
+        vph ^= 1u << buf;
+        // the tile is here; everyone is done with the previous buffer and has issued the
+        // previous tile's stores
+        __syncthreads();
+        if (tid == 0) {
+            if (pend >= 0) {
+                __threadfence();
+                atomicAdd(A.cnt + pend, 1u);
+            }
+            pend = -1;
+            const int64_t qt = (int64_t)next_q;
+            if (ok && qt < nitems) next_q = atomicAdd(next_item, 1u);
+            if (ok) take(buf == 0 ? SH - 1 : buf - 1, qt);
+            else ring[buf == 0 ? SH - 1 : buf - 1] = nitems;
+            if (grp == 2 && defer[buf]) {  // group 1 of this super-tile was not done at take
+                bool got = ok;
+                const long long t0 = clock64();
+                while (got && ld_acquire_u32(A.cnt + s) < (unsigned)TPS) {
+                    __nanosleep(64);
+                    if (clock64() - t0 > 4000000000LL || (A.err && *(volatile int *)A.err)) {
+                        got = false;
+                        if (A.err) atomicExch(A.err, (int)EMUSV_TIMEOUT);
+                    }
+                }
+                if (got) {
+                    load_sums(s, t, buf);
+                } else {
+                    ok = false;
+                    mbar_expect_tx(&pbars[buf], 0);  // release the waiters: nothing will arrive
+                }
+            }
+        }
+        if (grp == 2) {
+            if (!mbar_wait(&pbars[buf], (pph >> buf) & 1u)) {
+                ok = false;
+                if (A.err) atomicExch(A.err, (int)EMUSV_TIMEOUT);
+            }
+            pph ^= 1u << buf;
+        }
+        if (A.err && *(volatile int *)A.err) ok = false;
+        if (ok) {
+            // this group's geometry: tile bit k < c is bit k of x, k >= c bit hpos + k - c;
+            // applied: group 1 the bits [hs, hpos2), group 2 all its bits and the chunk bits
+            uint32_t apply = grp == 2 ? (1u << c) - 1u : 0u;
+            for (int k = c; k < TB; ++k)
+                if (grp == 2 || hpos + k - c < A.hpos2) apply |= 1u << k;
+            R cr_s[SB], ci_s[SB];
+#pragma unroll
+            for (int k = 0; k < SB; ++k) {
+                const int p = k < c ? k : hpos + k - c;
+                const bool bit = (tid >> k) & 1;
+                const bool on = (apply >> k) & 1;
+                cr_s[k] = on ? (bit ? Coef<R>::ure(P, p) : Coef<R>::dre(P, p)) : R(0);
+                ci_s[k] = on ? (bit ? Coef<R>::uim(P, p) : Coef<R>::dim(P, p)) : R(0);
+            }
+            R ur_r[RB], ui_r[RB], dr_r[RB], di_r[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                const int p = hpos + SB + k - c;
+                const bool on = (apply >> (SB + k)) & 1;
+                ur_r[k] = on ? Coef<R>::ure(P, p) : R(0);
+                ui_r[k] = on ? Coef<R>::uim(P, p) : R(0);
+                dr_r[k] = on ? Coef<R>::dre(P, p) : R(0);
+                di_r[k] = on ? Coef<R>::dim(P, p) : R(0);
+            }
+            const int64_t base = grp == 1 ? ((s << c) | (t << (hpos + g))) : ((s | (t << nsb)) << c);
+            const int64_t xt = (tid & cmask) + ((int64_t)(tid >> c) << hpos);
+            const int ash = hpos + SB - c;
+            float rf[2] = {0.f, 0.f};
+            C v[NA];
+#pragma unroll
+            for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                const int l = tid + a * NT;
+                const int64_t x = base + xt + ((int64_t)a << ash);
+                Acc<R> acc;
+#pragma unroll
+                for (int k = 0; k < SB; ++k) {
+                    if (!((apply >> k) & 1)) continue;
+                    flip_reg<R, REALC>(cr_s[k], ci_s[k], tile[l ^ (1 << k)], acc);
+                }
+#pragma unroll
+                for (int k = 0; k < RB; ++k) {
+                    if (!((apply >> (SB + k)) & 1)) continue;
+                    const bool bit = (a >> k) & 1;
+                    flip_reg<R, REALC>(bit ? ur_r[k] : dr_r[k], bit ? ui_r[k] : di_r[k], v[a ^ (1 << k)], acc);
+                }
+                if constexpr (std::is_same<R, float>::value) {
+                    const float2 tt = upk2(acc.a);
+                    if (grp == 2) {
+                        const C pt = ptile[l];
+                        outp[x] = make_float2(pt.x + tt.x, pt.y + tt.y);
+                    } else {
+                        outp[x] = tt;
+                    }
+                    rf[0] = fmaf(v[a].x, tt.x, fmaf(v[a].y, tt.y, rf[0]));
+                    rf[1] = fmaf(v[a].x, tt.y, fmaf(-v[a].y, tt.x, rf[1]));
+                } else {
+                    const double tr = acc.re(), ti = acc.im();
+                    if (grp == 2) {
+                        const C pt = ptile[l];
+                        outp[x] = cmake<C>(double(pt.x) + tr, double(pt.y) + ti);
+                    } else {
+                        outp[x] = cmake<C>(tr, ti);
+                    }
+                    const double vr = double(v[a].x), vi = double(v[a].y);
+                    red[0] += vr * tr + vi * ti;
+                    red[1] += vr * ti - vi * tr;
+                }
+            }
+            if constexpr (std::is_same<R, float>::value) {
+                red[0] += double(rf[0]);
+                red[1] += double(rf[1]);
+            }
+            if (grp == 1) pend = s;  // counted after the next block barrier
+        }
+        if (++buf == SH) buf = 0;
+    }
+    __syncthreads();
+    if (tid == 0 && pend >= 0) {
+        __threadfence();
+        atomicAdd(A.cnt + pend, 1u);
+    }
+    double rr[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) rr[k] = k < 2 ? red[k] : 0.0;
+    block_sum<NRED>(rr, red_scr);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NRED; ++k) A.partials[(int64_t)blockIdx.x * NRED + k] = rr[k];
+    }
+}
+
 // ------------------------------------------------------------- Lanczos pass L
 // The last pass of the Lanczos iteration (after the pass H kernels in EPI_X_FIRST /
 // EPI_X_ADD mode wrote part = X_high u_j, the flips of every bit above the tile, unscaled):

@@ -34,7 +34,7 @@ bool lanczos_h_first(int dtype, int n);
 int lz_energy0(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out);
 int lz_low(int dtype, const HamParams &H, const LzArgs &A, cudaStream_t s, int *grid_out);
 int lz_high(int dtype, const HamParams &H, const void *u, void *part, double *partials, const int *gate,
-            int *err, cudaStream_t s, int *nblocks_out);
+            int *err, unsigned *cnt, cudaStream_t s, int *nblocks_out);
 int max_grid_blocks();
 
 struct Workspace {
@@ -580,7 +580,8 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
                 break;
             }
             int gh = 0, go = 0;
-            if ((st = lz_high(dtype, P, stored(j), part_vec, W.part_h, &W.ks->status, &W.ks->kerr, s, &gh)))
+            if ((st = lz_high(dtype, P, stored(j), part_vec, W.part_h, &W.ks->status, &W.ks->kerr,
+                              W.ks->hh_cnt, s, &gh)))
                 return st;
             {
                 ProfScope ps_(PROF_SMALL, s);

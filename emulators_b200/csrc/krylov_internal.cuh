@@ -30,6 +30,7 @@ struct KState {
     // and the pass-L tile flips, which the pass producing v_k computes
     double e_re[KMAX];
     double el_re[KMAX + 2], el_im[KMAX + 2];
+    unsigned hh_cnt[1040];  // fused pass H: group-1 tiles per super-tile, the item counter
 };
 
 

@@ -195,3 +195,45 @@ def test_generic_arnoldi_matches_reference():
     X = torch.as_tensor(g["m_in"]).to(DEV)
     out = krylov_exp(lambda y: A @ y, X.clone(), 1e-6, 1e-6, is_hermitian=False, max_krylov_dim=100)
     assert torch.allclose(out, torch.linalg.matrix_exp(A) @ X)
+
+
+@pytest.mark.parametrize("n,dtype", [(23, torch.complex128), (24, torch.complex64)])
+def test_krylov_step_large_vs_oracle(oracle, n, dtype):
+    """One time step of a register whose pass H takes two bit groups in one fused launch
+    (8 super-tiles), from a random state with complex phases, against the oracle's
+    Lanczos step: result and iteration count."""
+    from emulators_b200 import HamiltonianExpOperator, RydbergHamiltonian
+    from emulators_b200 import workloads as wl
+    from emulators_b200.krylov import fused_step
+
+    rng = np.random.default_rng(40 + n)
+    om, de, ph = rng.uniform(0, 2 * np.pi, n), rng.uniform(-20, 20, n), rng.normal(size=n)
+    U = wl.interaction_matrix(wl.chain(n, 6.0))
+    psi = torch.randn(1 << n, dtype=dtype, device=DEV)
+    psi /= torch.linalg.vector_norm(psi)
+    host = psi.cpu().to(torch.complex128).numpy()
+    H = RydbergHamiltonian(*(torch.as_tensor(a) for a in (om, de, ph, U)), DEV)
+    out, info, st = fused_step(HamiltonianExpOperator(H, 0.005), psi.clone(), 1e-10, 1e-10, 100)
+    assert st == 0
+    ref, _, rinfo = oracle.evolve_step(0.005, om, de, ph, U, host, 1e-10)
+    tol = 1e-10 if dtype == torch.complex128 else 5e-6
+    assert np.abs(out.cpu().to(torch.complex128).numpy() - ref).max() < tol
+    if dtype == torch.complex128:
+        assert info.iterations == rinfo.iteration_count
+
+
+def test_fused_pass_h_kernel_vs_oracle(tmp_path):
+    """The fused two-group pass H (EMUSV_FUSED_PASS_H=1, read once per process): the
+    large-register steps of test_krylov_step_large_vs_oracle in a child process with the
+    switch on."""
+    import os
+    import subprocess
+    import sys
+
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, EMUSV_FUSED_PASS_H="1")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p", "no:cacheprovider",
+                        os.path.join(repo, "tests", "test_gpu_krylov.py"), "-k", "large_vs_oracle"],
+                       env=env, cwd=repo, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "2 passed" in r.stdout
