@@ -10,7 +10,9 @@
 //   3. pass L (k_pass_lz): H v_j formed tile by tile on chip, w = H v_j - a_j v_j -
 //      b_j v_{j-1} stored into basis slot j+1, FP64 partials of ||w||^2, <v_j, w>,
 //      ||H v_j||^2 and the pass-L share of the next <v, H v>;
-//   4. k_small_lz (one warp): ||w||, happy-breakdown test (krylov_exp.py:63-71), the
+//   4. k_lz_norms (one warp): ||w||, ||H v_j||, the next scale and the happy-breakdown
+//      test (krylov_exp.py:63-71) -- all the next iteration needs;
+//   5. k_lz_decide (one warp, on a second stream, overlapping iteration j+1): the
 //      exponential of the extended Krylov matrix and the Expokit error estimate
 //      (krylov_exp.py:77-86), all FP64 on the device.
 // Smaller registers: k_hpsi<HP_LANCZOS> (H v with its reductions), k_orth (the recurrence),
@@ -21,6 +23,8 @@
 // iteration has already finished, so the host only synchronises where it tests
 // convergence.
 #include <string.h>
+
+#include <mutex>
 
 #include "krylov_device.cuh"
 #include "profile.cuh"
@@ -249,20 +253,13 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
     krylov_decide(ks, j, v, vr, vi, dt, exp_tol, norm_tol, poll != 0, first_poll != 0, maxdim);
 }
 
-// Decide H-first iteration j from the pass-L partials (0 ||w||^2, 1-2 <v_j, w>,
-// 3 ||(H - sigma) v_j||^2, 4 the pass-L part of <w, (H - sigma) w>): ||H v_j||, then as
-// k_small, then the next iteration's el = <v_{j+1}, (D - sigma + X_low) v_{j+1}>.
+// H-first iteration j, first part (on the step's stream): from the pass-L partials
+// (0 ||w||^2, 1-2 <v_j, w>, 3 ||(H - sigma) v_j||^2, 4 the pass-L part of <w, (H - sigma) w>)
+// ||H v_j||, ||w||, <v_{j+1}, v_j>, scale_{j+1} and the next el -- everything iteration
+// j+1 needs -- and the outcome flag; no status change.
 __global__ void __launch_bounds__(32)
-k_small_lz(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp_tol,
-           double norm_tol, int poll, int first_poll, int maxdim) {
+k_lz_norms(KState *ks, int j, const double *part_o, int nb_o, double dt, double norm_tol) {
     if (ks->status != KS_RUNNING) return;
-    if (ks->kerr) {  // a streaming kernel gave up on a bounded wait
-        if (threadIdx.x == 0) {
-            ks->status = KS_TIMEOUT;
-            ks->iters = j + 1;
-        }
-        return;
-    }
     const int lane = threadIdx.x;
     double v = 0.0, vr = 0.0, vi = 0.0, hh = 0.0, el = 0.0;
     for (int b = lane; b < nb_o; b += 32) {
@@ -283,11 +280,50 @@ k_small_lz(KState *ks, int j, const double *part_o, int nb_o, double dt, double 
         ks->hn[j] = sqrt(fmax(0.0, hh + 2.0 * sg * ks->e_re[j] + sg * sg));
     }
     __syncwarp();
-    krylov_decide(ks, j, v, vr, vi, dt, exp_tol, norm_tol, poll != 0, first_poll != 0, maxdim);
+    const int flag = krylov_norms(ks, j, v, vr, vi, dt, norm_tol);
     if (lane == 0) {
+        ks->lz_flag[j] = flag;
         ks->el_re[j + 1] = v > 0.0 ? el / v : 0.0;  // v_{j+1} = w / ||w||
         ks->el_im[j + 1] = 0.0;
     }
+}
+
+// Second part (on the decision stream, in iteration order, overlapping the next
+// iteration's passes): every status change of iteration j (krylov_conclude), and a timeout
+// a streaming kernel recorded.
+__global__ void __launch_bounds__(32)
+k_lz_decide(KState *ks, int j, double dt, double exp_tol, int poll, int first_poll, int maxdim) {
+    if (ks->status != KS_RUNNING) return;
+    if (ks->kerr) {  // a streaming kernel gave up on a bounded wait
+        if (threadIdx.x == 0) {
+            ks->status = KS_TIMEOUT;
+            ks->iters = j + 1;
+        }
+        return;
+    }
+    krylov_conclude(ks, j, ks->lz_flag[j], dt, exp_tol, poll != 0, first_poll != 0, maxdim);
+}
+
+// The decision stream of the H-first iteration, one per device (created on first use).
+// Used for vectors of at most 32 MB, where the decision (about 20 us) is a large share of
+// an iteration (N=20 complex128: 1.99 -> 1.79 ms per 23-iteration step).  On larger
+// registers every SM's register file is full of a streaming kernel's CTAs, so the
+// decision warp only delays one of them and lengthens that kernel by about as much as it
+// saves (N=26 complex64: 0.891 -> 0.914 ms per iteration): there it stays on the step's
+// stream.
+static bool decision_overlaps(int dtype, int n) {
+    const double bytes = (double)(1ll << n) * (dtype == EMUSV_C128 ? 16.0 : 8.0);
+    return bytes <= 32.0 * 1024 * 1024;
+}
+static cudaStream_t decision_stream() {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> g(mu);
+    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
+        streams[dev] = nullptr;
+    return streams[dev];
 }
 
 // out = s0 * sum_k c_k scale_k stored_k ;  ||out||^2 partials.
@@ -559,10 +595,38 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
     // write part = X_high v_j (the flips of the bits above the pass-L tile) and their share
     // of <v_j, H v_j>; k_lz_coef forms a_j; the pass L kernel forms H v_j tile by tile and
     // writes w = H v_j - a_j v_j - b_j v_{j-1} and the pass-L share of <w, H w> for the
-    // next a; k_small_lz decides.  Streamed vector units per iteration: pass L 4 (read v_j,
+    // next a; k_lz_norms and k_lz_decide conclude the iteration.  Streamed vector units per iteration: pass L 4 (read v_j,
     // part, v_{j-1}; write w), one H pass 2 (read v_j, write part) or two H passes 2 + 3.
     const bool hfirst = lanczos_h_first(dtype, nqubits);
     if (hfirst) {
+        // with `overlap`, the decision of iteration j (k_lz_decide) runs on a second stream
+        // while the main stream goes on with iteration j+1, which needs only k_lz_norms'
+        // outputs (k_lz_decide reads a, r, b up to index j and hn[j]; iteration j+1 writes
+        // index j+1 and above); kernels launched after the device decided return at once,
+        // and the host reads the status only after the decision stream's event
+        const bool overlap = decision_overlaps(dtype, nqubits);
+        cudaStream_t sd = overlap ? decision_stream() : s;
+        cudaEvent_t ev_n = nullptr, ev_d = nullptr;
+        if ((overlap && !sd) || cudaEventCreateWithFlags(&ev_n, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_d, cudaEventDisableTiming) != cudaSuccess) {
+            if (ev_n) cudaEventDestroy(ev_n);
+            return EMUSV_CUDA_ERROR;
+        }
+        struct Events {
+            cudaEvent_t a, b;
+            ~Events() {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } evs{ev_n, ev_d};
+        // status after every decision taken so far (main stream joins the decision stream)
+        auto status_now = [&](int *out) -> int {
+            if (overlap) {
+                EMUSV_CHECK(cudaEventRecord(ev_d, sd));
+                EMUSV_CHECK(cudaStreamWaitEvent(s, ev_d, 0));
+            }
+            return read_status(W.ks, s, out);
+        };
         LzArgs E = {};
         E.u = stored(0);
         E.eshift = &W.ks->shift;
@@ -572,9 +636,11 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
         int ge0 = 0;
         int st = lz_energy0(dtype, P, E, s, &ge0);
         if (st) return st;
+        bool joined = false;
         for (int j = 0; j < max_krylov_dim; ++j) {
             if (j + 1 > capacity) {
-                st = read_status(W.ks, s, &status);
+                st = status_now(&status);
+                joined = true;
                 if (st) return st;
                 if (status == KS_RUNNING) return EMUSV_WORKSPACE_TOO_SMALL;
                 break;
@@ -600,18 +666,33 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
             B.gate = &W.ks->status;
             B.err = &W.ks->kerr;
             if ((st = lz_low(dtype, P, B, s, &go))) return st;
-            const int poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
             {
                 ProfScope ps_(PROF_SMALL, s);
-                k_small_lz<<<1, 32, 0, s>>>(W.ks, j, W.part_o, go, dt, exp_tolerance, norm_tolerance, 1,
-                                            j == 0, max_krylov_dim);
+                k_lz_norms<<<1, 32, 0, s>>>(W.ks, j, W.part_o, go, dt, norm_tolerance);
             }
             EMUSV_CHECK_LAUNCH();
+            if (overlap) {
+                EMUSV_CHECK(cudaEventRecord(ev_n, s));
+                EMUSV_CHECK(cudaStreamWaitEvent(sd, ev_n, 0));
+            }
+            {
+                ProfScope ps_(PROF_SMALL, sd);
+                k_lz_decide<<<1, 32, 0, sd>>>(W.ks, j, dt, exp_tolerance, 1, j == 0, max_krylov_dim);
+            }
+            EMUSV_CHECK_LAUNCH();
+            const int poll = (j + 1 >= krylov_dim_hint) || (j + 1 >= max_krylov_dim);
             if (poll) {
-                st = read_status(W.ks, s, &status);
+                st = status_now(&status);
+                joined = true;
                 if (st) return st;
                 if (status != KS_RUNNING) break;
+            } else {
+                joined = false;
             }
+        }
+        if (overlap && !joined) {  // the step's later work (the combination) follows every decision
+            EMUSV_CHECK(cudaEventRecord(ev_d, sd));
+            EMUSV_CHECK(cudaStreamWaitEvent(s, ev_d, 0));
         }
     }
     for (int j = 0; !hfirst && j < max_krylov_dim; ++j) {

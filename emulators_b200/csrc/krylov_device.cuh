@@ -447,29 +447,26 @@ static __device__ double krylov_eval(KState *ks, int jj, double dt) {
 }
 
 // Decide iteration j of a Lanczos run from the FP64 sums v = ||w_j||^2 and
-// (vr, vi) = <v_j, w_j>: ||w_j||, happy breakdown (every iteration), and, when `poll`, the
-// extended exponential and the error estimate.  Iterations that were not polled are not
-// tested, so when the first poll (`first_poll`) already converges the warp tests the
-// earlier iterations in order and stops at the first that converges -- where the
-// reference, which tests every iteration, stops.  Callers start polling a few iterations
-// before the expected count, so that scan is rare.  One warp; ks->status must be
-// KS_RUNNING.
-static __device__ void krylov_decide(KState *ks, int j, double v, double vr, double vi, double dt,
-                              double exp_tol, double norm_tol, bool poll, bool first_poll,
-                              int maxdim) {
+// (vr, vi) = <v_j, w_j>, in two parts.
+// krylov_norms: ||w_j||, <v_{j+1}, v_j> and scale_{j+1} (what iteration j+1 needs), and
+// the outcome flag: KD_NONFINITE (a non-finite value), KD_HAPPY (the happy breakdown of
+// krylov_exp.py:63-71, tested every iteration) or 0.  Writes no status.
+// krylov_conclude: every status change of iteration j -- NONFINITE, HAPPY (with the
+// exponential of T[:j+1,:j+1]) or, when `poll`, the extended exponential, the error
+// estimate and CONVERGED / MAXDIM.  Iterations that were not polled are not tested, so
+// when the first poll (`first_poll`) already converges the warp tests the earlier
+// iterations in order and stops at the first that converges -- where the reference, which
+// tests every iteration, stops.  One warp each; ks->status must be KS_RUNNING.
+enum { KD_OK = 0, KD_NONFINITE = 1, KD_HAPPY = 2 };
+
+static __device__ int krylov_norms(KState *ks, int j, double v, double vr, double vi, double dt,
+                                   double norm_tol) {
     const int lane = threadIdx.x & 31;
     const double r = sqrt(v);
-    const double adt = fabs(dt);
-    const double n2 = adt * r;  // ||w|| of the operator -i dt H (krylov_exp.py:60)
+    const double n2 = fabs(dt) * r;  // ||w|| of the operator -i dt H (krylov_exp.py:60)
     if (!isfinite(r) || !isfinite(ks->hn[j]) || !isfinite(ks->a_re[j]) || !isfinite(ks->a_im[j]) ||
-        !isfinite(ks->b_re[j]) || !isfinite(ks->b_im[j])) {
-        if (lane == 0) {
-            ks->status = KS_NONFINITE;
-            ks->iters = j + 1;
-        }
-        __syncwarp();
-        return;
-    }
+        !isfinite(ks->b_re[j]) || !isfinite(ks->b_im[j]))
+        return KD_NONFINITE;
     if (lane == 0) {
         ks->r[j] = r;
         ks->vv_re[j + 1] = vr / r;  // <v_{j+1}, v_j> = conj(<v_j, w>) / ||w||
@@ -477,8 +474,22 @@ static __device__ void krylov_decide(KState *ks, int j, double v, double vr, dou
         ks->scale[j + 1] = 1.0 / r;
     }
     __syncwarp();
+    return n2 < norm_tol ? KD_HAPPY : KD_OK;
+}
+
+static __device__ void krylov_conclude(KState *ks, int j, int flag, double dt, double exp_tol, bool poll,
+                                       bool first_poll, int maxdim) {
+    const int lane = threadIdx.x & 31;
+    if (flag == KD_NONFINITE) {
+        if (lane == 0) {
+            ks->status = KS_NONFINITE;
+            ks->iters = j + 1;
+        }
+        __syncwarp();
+        return;
+    }
     const int m = j + 1;
-    if (n2 < norm_tol) {  // krylov_exp.py:63-71: exp(T[:j+1,:j+1]) e_0 over j+1 vectors
+    if (flag == KD_HAPPY) {  // krylov_exp.py:63-71: exp(T[:j+1,:j+1]) e_0 over j+1 vectors
         constexpr int NE = (KMAX + 2 + 31) / 32;
         double2 d[NE], l[NE], u[NE], y[NE];
         double td[NE], tr[NE];
@@ -528,6 +539,15 @@ static __device__ void krylov_decide(KState *ks, int j, double v, double vr, dou
             ks->status = KS_MAXDIM;
     }
     __syncwarp();
+}
+
+// Both parts in one warp (the single-kernel decision of the batched engine and of the
+// small registers' iteration).
+static __device__ void krylov_decide(KState *ks, int j, double v, double vr, double vi, double dt,
+                              double exp_tol, double norm_tol, bool poll, bool first_poll,
+                              int maxdim) {
+    const int flag = krylov_norms(ks, j, v, vr, vi, dt, norm_tol);
+    krylov_conclude(ks, j, flag, dt, exp_tol, poll, first_poll, maxdim);
 }
 
 }  // namespace emusv

@@ -31,6 +31,7 @@ struct KState {
     double e_re[KMAX];
     double el_re[KMAX + 2], el_im[KMAX + 2];
     unsigned hh_cnt[1040];  // fused pass H: group-1 tiles per super-tile, the item counter
+    int lz_flag[KMAX];      // H-first iteration: outcome flag of iteration k (krylov_norms)
 };
 
 
