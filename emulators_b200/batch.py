@@ -116,9 +116,9 @@ class BatchEvolution:
 
     def set_barrier_test(self, wait_cycles: int = 0, skip_first_arrival: bool = False) -> None:
         """Failure-path test switch of the prepared workspace (off by default; reset by
-        :meth:`prepare`): grid-barrier waits give up after ``wait_cycles`` SM clock cycles
-        (0: the default, about 1 s) and, with ``skip_first_arrival``, one CTA never arrives
-        at a launch's first barrier, so the launch ends with ``TimeoutError`` in
+        :meth:`prepare`): device waits give up after ``wait_cycles`` SM clock cycles
+        (0: the default, about 1 s) and, with ``skip_first_arrival``, the completion of job
+        0's first phase never arrives, so the launch ends with ``TimeoutError`` in
         :meth:`results` and the device stays usable."""
         st = _lib.load().emusv_batch_set_barrier_test(self.ws.data_ptr(), int(wait_cycles),
                                                       1 if skip_first_arrival else 0)
@@ -151,6 +151,7 @@ class BatchEvolution:
                                              status.ctypes.data, iters.ctypes.data,
                                              _lib.stream_of(self.states))
         self.iterations = iters
+        self.last_code = st
         if raise_on_error and st != _lib.OK:
             _lib.check(st, f"batch ({int((status != 0).sum())} instance(s) failed)")
         return status, iters
@@ -176,6 +177,10 @@ class BatchEvolution:
             else:
                 self.launch(blocks_per_sm)
             status, iters = self.results(raise_on_error=False)
+            if self.last_code != _lib.OK and not status.any():
+                # a launch-wide failure (a wait that ran out, a CUDA error): no per-instance
+                # status was written
+                _lib.check(self.last_code, "batch launch")
             if (status == _lib.WORKSPACE_TOO_SMALL).any() and capacity < self.max_krylov_dim:
                 capacity = min(self.max_krylov_dim, 2 * capacity)
                 continue
@@ -227,6 +232,8 @@ def autotune(b: BatchEvolution, probe_steps: int = 3, reps: int = 2) -> TuneResu
                 torch.cuda.synchronize()
                 ms.append(e0.elapsed_time(e1))
             status, iters = probe.results(raise_on_error=False)
+            if probe.last_code != _lib.OK and not status.any():
+                _lib.check(probe.last_code, "batch autotune probe")  # a launch-wide failure
             max_iters = max(max_iters, int(iters.max()))
             t = min(ms[1:])
             timings[f"T{T}_b{bps}"] = round(t, 3)

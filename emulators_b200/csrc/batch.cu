@@ -15,16 +15,22 @@
 //    inside the thread, bits >= T by coalesced loads of the partner tile; the diagonal is
 //    rebuilt from an FP64 per-instance table of the low-bit pair energies plus per-tile
 //    fields of the high bits.
-//  * per Lanczos iteration j, two grid-wide phases: A_j (H v_j for every running
-//    instance, FP64 partials of ||Hv||^2 and <v_j,Hv>) and B_j (three-term recurrence and
-//    partials of ||w||^2, <v_j,w>).  The per-instance decision for iteration j (norm,
-//    happy breakdown, extended tridiagonal exponential, error estimate: krylov_decide)
-//    runs in warp 0 of one CTA per instance during phase A_{j+1}, overlapping the next
-//    H v, whose result is discarded if the instance converged.  After the iterations of
-//    a step, a combination phase writes psi' = s0 sum_k c_k v_k in place and its norm.
-//  * grid barriers are an arrival counter plus a generation word; every wait is bounded
-//    (about a second of SM clock): on a timeout the kernel records EMUSV_TIMEOUT and
-//    every CTA returns.  The launch is cooperative, so all CTAs are co-resident.
+//  * per Lanczos iteration j, two tile phases per job: A_j (H v_j, FP64 partials of
+//    ||Hv||^2 and <v_j,Hv>) and B_j (three-term recurrence, partials of ||w||^2, <v_j,w>).
+//    The rounds of a step are dataflow, not lock-step: the work items (round, phase,
+//    tile) are taken in order from one counter, and a tile waits (bounded) only for its
+//    own job's previous phase -- B_j for A_j of the job, A_j for B_{j-1} -- through
+//    per-job completion marks.  The warp that completes B_j of a job takes the job's
+//    decision for iteration j (norm, happy breakdown, extended tridiagonal exponential,
+//    error estimate: krylov_decide) while the other warps go on with A_{j+1}, whose
+//    result is discarded if the job ended.  No grid barrier inside a step's rounds.
+//    After the rounds, a combination phase writes psi' = s0 sum_k c_k v_k in place and
+//    its norm; the warp that completes a job's combination starts the job's next step.
+//  * one grid barrier per step (an arrival counter plus a generation word).  Every wait
+//    is bounded (about a second of SM clock): on a timeout the kernel records
+//    EMUSV_TIMEOUT and every CTA returns at its next barrier.  The launch is cooperative,
+//    so all CTAs are co-resident, and a tile waits only for work taken before it, so the
+//    waits always end.
 //  * convergence is tested from a per-instance hint (the previous step's count - 3); a
 //    first test that already converges tests the skipped iterations in order
 //    (krylov_decide), so each instance stops where the reference would.
@@ -69,10 +75,12 @@ struct BCoef {
 };
 
 struct BCtl {
-    unsigned bar_count, bar_gen;
+    unsigned bar_count, bar_gen;  // grid barrier of the adjoint post-processing kernel
     unsigned tile_ctr[2];
     int err;
-    int pad[3];
+    unsigned idle;                // jobs with no phase left in this launch
+    unsigned long long item;      // next work item of the phase engine
+    unsigned long long steps_done;  // steps completed, summed over the jobs
 };
 
 struct BArgs {
@@ -88,7 +96,9 @@ struct BArgs {
     double *partA, *partB, *partN;  // [total_tiles][4] per-tile FP64 partial sums
     double *sumA, *sumB, *sumN;     // [ninst][4] their per-instance totals
     unsigned *cnt;                  // [3][ninst] tiles done per phase kind (A, B, N)
-    int *ranB;                      // [ninst] 1 + last round whose phase B ran the instance
+    unsigned long long *jst;        // [ninst] job state: (phases completed << 32) | the code
+                                    // of its next phase (see run_jobs)
+    unsigned long long *take;       // [ninst] (current phase << 32) | its tiles taken
     void *v0[2];          // buffers holding every job's vector 0 (forward: the packed states,
                           // evolved in place; adjoint: states and incoming gradients)
     unsigned char *slots;  // slots 1..capacity
@@ -96,15 +106,17 @@ struct BArgs {
     BCtl *ctl;
     // set per launch
     int first_step;       // absolute index of the launch's first step
-    int run_steps;        // steps this launch takes
+    int run_steps;        // steps this launch takes (at most 65535)
+    int combine;          // 1: each step ends with the combination (forward); 0: the
+                          // launch builds one step's Krylov bases (adjoint)
     void *hist;           // optional: states after every hist_every-th step
     int hist_every;
     long long hist_stride;  // amplitudes per history slot
-    // grid barrier: clock cycles a wait lasts at most (BAR_LIMIT unless a test shortens
-    // it) and the failure-path test switch (emusv_batch_set_barrier_test): the last CTA
-    // does not arrive at a launch's first barrier, so every other CTA's wait runs out
+    // clock cycles a wait lasts at most (BAR_LIMIT unless a test shortens it) and the
+    // failure-path test switch (emusv_batch_set_barrier_test): the completion of job 0's
+    // first phase is not published, so every wait for job 0's next phase runs out
     long long bar_limit;
-    int test_skip_arrival;
+    int test_hold;
 };
 
 // Adjoint step (k_batch_adj): jobs 2i (state psi_i) and 2i+1 (gradient g_i) of instance i.
@@ -123,18 +135,19 @@ constexpr int NCP = 6 * BMAXQ;  // per bit: T_re, T_im, U_re, U_im, S_re, S_im
 
 // ---------------------------------------------------------------- grid barrier
 // Arrival counter + generation; the last arriver also clears the tile counter of the
-// phase after next.  Returns false (and every CTA then returns) on a timeout: a wait
-// gives up after A.bar_limit clock cycles or as soon as another CTA recorded an error.
+// next phase.  Returns false (and every CTA then returns)
+// once an error is recorded: a wait gives up after A.bar_limit clock cycles or as soon as
+// another CTA recorded an error.
 __device__ bool grid_sync(const BArgs &A, unsigned &ph) {
+    __shared__ int s_ok;  // the CTA's verdict, read by every thread (all return together)
     BCtl *ctl = A.ctl;
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned *genp = &ctl->bar_gen;
         const unsigned g = *genp;
         __threadfence();
-        const bool skip = A.test_skip_arrival && ph == 0 && blockIdx.x == gridDim.x - 1;
-        const unsigned arrived = skip ? 0u : atomicAdd(&ctl->bar_count, 1u);
-        if (!skip && arrived == gridDim.x - 1) {
+        const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
+        if (arrived == gridDim.x - 1) {
             ctl->bar_count = 0;
             ctl->tile_ctr[(ph + 1) & 1] = 0;
             __threadfence();
@@ -154,10 +167,11 @@ __device__ bool grid_sync(const BArgs &A, unsigned &ph) {
             }
         }
         __threadfence();
+        s_ok = *(volatile int *)&ctl->err == 0;
     }
     __syncthreads();
     ++ph;
-    return *(volatile int *)&ctl->err == 0;
+    return s_ok != 0;
 }
 
 // ---------------------------------------------------------------- helpers
@@ -191,8 +205,8 @@ __device__ __forceinline__ double3 inst_sum(const double *part, int tile0, int n
 
 // After a warp wrote its tile's partials: count the tile; the warp that completes the
 // instance adds the instance's partials (inst_sum: the same order whichever warp it is)
-// into sum[4 i..] and clears the counter for the next phase of this kind.
-__device__ __forceinline__ void tile_done(unsigned *cnt, const double *part, double *sum, int i,
+// into sum[4 i..], clears the counter for the next phase of this kind and returns true.
+__device__ __forceinline__ bool tile_done(unsigned *cnt, const double *part, double *sum, int i,
                                           int tile0, int ntiles) {
     const int lane = threadIdx.x & 31;
     unsigned old = 0;
@@ -201,7 +215,8 @@ __device__ __forceinline__ void tile_done(unsigned *cnt, const double *part, dou
         old = atomicAdd(&cnt[i], 1u);
     }
     old = __shfl_sync(0xffffffffu, old, 0);
-    if (old == (unsigned)ntiles - 1) {
+    const bool last = old == (unsigned)ntiles - 1;
+    if (last) {
         __threadfence();
         const double3 s = inst_sum(part, tile0, ntiles);
         if (lane == 0) {
@@ -213,6 +228,7 @@ __device__ __forceinline__ void tile_done(unsigned *cnt, const double *part, dou
         }
     }
     __syncwarp();
+    return last;
 }
 
 __device__ __forceinline__ double3 ld_sum(const double *sum, int i) {
@@ -252,7 +268,7 @@ __device__ __forceinline__ void cfma(R cr, R ci, C w, R &ar, R &ai) {
 
 // ---------------------------------------------------------------- phase A: H v_j on a tile
 template <typename R, int T>
-__device__ void tile_hpsi(const BArgs &A, const BInst &I, int i, int t, int step, int j,
+__device__ bool tile_hpsi(const BArgs &A, const BInst &I, int i, int t, int step, int j,
                           double sj) {
     typedef typename cvec<R>::T C;
     constexpr int AMP = 1 << (T - 5);
@@ -359,12 +375,12 @@ __device__ void tile_hpsi(const BArgs &A, const BInst &I, int i, int t, int step
         pa[1] = s_r;
         pa[2] = s_i;
     }
-    tile_done(A.cnt, A.partA, A.sumA, i, I.tile0, I.ntiles);
+    return tile_done(A.cnt, A.partA, A.sumA, i, I.tile0, I.ntiles);
 }
 
 // ---------------------------------------------------------------- phase B: recurrence
 template <typename R, int T>
-__device__ void tile_orth(const BArgs &A, const BInst &I, int i, int t, int j, double car,
+__device__ bool tile_orth(const BArgs &A, const BInst &I, int i, int t, int j, double car,
                           double cai, double cb, double sj) {
     typedef typename cvec<R>::T C;
     constexpr int AMP = 1 << (T - 5);
@@ -409,11 +425,11 @@ __device__ void tile_orth(const BArgs &A, const BInst &I, int i, int t, int j, d
         pb[1] = acc1;
         pb[2] = acc2;
     }
-    tile_done(A.cnt + A.ninst, A.partB, A.sumB, i, I.tile0, I.ntiles);
+    return tile_done(A.cnt + A.ninst, A.partB, A.sumB, i, I.tile0, I.ntiles);
 }
 
 template <typename R, int T>
-__device__ void tile_norm(const BArgs &A, const BInst &I, int i, int t) {
+__device__ bool tile_norm(const BArgs &A, const BInst &I, int i, int t) {
     typedef typename cvec<R>::T C;
     constexpr int AMP = 1 << (T - 5);
     const int lane = threadIdx.x & 31;
@@ -424,7 +440,7 @@ __device__ void tile_norm(const BArgs &A, const BInst &I, int i, int t) {
     for (int a = 0; a < AMP; ++a) add_sq(nrm, ldcg(u + base + lane + 32 * a));
     nrm = warp_sum(nrm);
     if (lane == 0) A.partN[4 * (size_t)t] = nrm;
-    tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
+    return tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
 }
 
 __device__ __forceinline__ int ld_status(const KState *ks) {
@@ -432,145 +448,146 @@ __device__ __forceinline__ int ld_status(const KState *ks) {
 }
 __device__ __forceinline__ int ld_vol(const int *p) { return *(volatile const int *)p; }
 
-// ---------------------------------------------------------------- phases
-// Phase bookkeeping keeps every job's tiles either all processed or all skipped in a
-// phase (so the per-job tile counters complete): phase A_j runs a job if its step starts
-// (j = 0) or if phase B of the previous round ran it (ranB), never from a status that the
-// decisions of the same phase may be changing.
+// ---------------------------------------------------------------- the phase engine
+// Every job runs its own sequence of phases: the norm of its vector 0, then per step
+// A_0, B_0, A_1, B_1, ..., B_e (e: the decision that ends the step) and the combination
+// C; then the next step's A_0, and so on, until the job is idle.  A job's state word holds
+// the number of phases it completed and the code of its next phase; the warp that
+// completes a phase (the last of its tiles) takes the phase's decision and publishes the
+// next code.
+enum { PK_NORM = 0, PK_A = 1, PK_B = 2, PK_C = 3, PK_IDLE = 4 };
+constexpr int BCHUNK = 4;     // tiles a warp takes per visit
+constexpr int BSTEP_LEAD = 2;  // steps a job may run ahead of the live jobs' average
 
-// Norms of every job's vector 0 (into sumN).
-template <typename R, int T>
-__device__ void norm_phase(const BArgs &A, unsigned ph) {
-    for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
-        const int i = inst_of_tile(A, t);
-        tile_norm<R, T>(A, A.inst[i], i, t);
+__device__ __forceinline__ unsigned pcode(int kind, int rstep, int j) {
+    return (unsigned)kind << 24 | ((unsigned)rstep & 0xffffu) << 8 | (unsigned)j;
+}
+__device__ __forceinline__ int pkind(unsigned c) { return (int)(c >> 24); }
+__device__ __forceinline__ int prstep(unsigned c) { return (int)((c >> 8) & 0xffffu); }
+__device__ __forceinline__ int pj(unsigned c) { return (int)(c & 0xffu); }
+
+__device__ __forceinline__ unsigned long long ld_acq64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_rel64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_vol_u(const unsigned *p) { return *(volatile const unsigned *)p; }
+
+// Warp-collective bounded wait until job i completed `phi` phases or is idle; the state
+// word in w.  False once the wait ran out (it records EMUSV_TIMEOUT) or another warp
+// recorded an error.
+__device__ bool wait_phase(const BArgs &A, int i, unsigned phi, unsigned long long &w) {
+    unsigned long long v = 0;
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        v = ld_acq64(&A.jst[i]);
+        if ((unsigned)(v >> 32) < phi && pkind((unsigned)v) != PK_IDLE) {
+            const long long t0 = clock64();
+            for (int polls = 1;; ++polls) {
+                __nanosleep(64);
+                v = ld_acq64(&A.jst[i]);
+                if ((unsigned)(v >> 32) >= phi || pkind((unsigned)v) == PK_IDLE) break;
+                if ((polls & 15) == 0 && (clock64() - t0 > A.bar_limit || ld_vol(&A.ctl->err))) {
+                    atomicCAS(&A.ctl->err, 0, EMUSV_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
     }
+    __syncwarp();
+    w = __shfl_sync(0xffffffffu, v, 0);
+    return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
-// All Lanczos iterations of one step of every job (krylov_exp.py:49-106 per job).
-// gstep: absolute step (coefficients, whether the job still has this step); rstep: the
-// launch-relative step (iteration record).  Returns false if a barrier gave up.
-template <typename R, int T>
-__device__ bool krylov_rounds(const BArgs &A, int gstep, int rstep, unsigned &ph, int &round,
-                              int &s_flag) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int j = 0;; ++j) {
-        // ---------------- phase A_j: decisions for j-1 (init at j = 0), tiles H v_j
-        if (warp == 0) {
-            for (int i = blockIdx.x; i < A.ninst; i += gridDim.x) {
-                const BInst I = A.inst[i];
-                KState *ks = A.ks + i;
-                if (j == 0) {
-                    if (lane == 0) {
-                        const double s0 = sqrt(__ldcg(A.sumN + 4 * (size_t)i));
-                        int st = KS_RUNNING;
-                        const int f = ld_vol(&A.fail[i]);
-                        if (f) st = f;
-                        else if (gstep >= I.nsteps) st = BS_IDLE;
-                        else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
-                        ks->s0 = s0;
-                        ks->shift = 0.0;
-                        ks->scale[0] = 1.0 / s0;
-                        ks->iters = 0;
-                        ks->nvec = 0;
-                        ks->kerr = 0;
-                        ks->err = 0.0;
-                        A.polled[i] = 0;
-                        ks->status = st;
-                        if (st == KS_NONFINITE) A.fail[i] = st;
-                    }
-                    __syncwarp();
-                    continue;
-                }
-                if (ld_status(ks) != KS_RUNNING) continue;
-                const int jj = j - 1;
-                const double3 sb = ld_sum(A.sumB, i);
-                const int hint = A.hint[i];
-                const bool poll = (jj + 1 >= hint) || (jj + 1 >= A.maxdim);
-                const bool first = poll && !A.polled[i];
-                __syncwarp();
-                if (lane == 0 && poll) A.polled[i] = 1;
-                krylov_decide(ks, jj, sb.x, sb.y, sb.z, I.dt, A.exp_tol, A.norm_tol, poll, first,
-                              A.maxdim);
-                if (lane == 0) {
-                    int st = ks->status;
-                    if (st == KS_RUNNING && jj + 2 > A.capacity) {
-                        st = BS_CAPACITY;
-                        ks->status = st;
-                    }
-                    if (st == KS_NONFINITE || st == BS_CAPACITY) A.fail[i] = st;
-                    if (st != KS_RUNNING) {
-                        A.iters_out[(size_t)i * A.max_steps + rstep] = ks->iters;
-                        A.hint[i] = ks->iters > 3 ? ks->iters - 3 : 0;  // poll a little early
-                    }
-                }
-                __syncwarp();
-            }
-        }
-        if (j < A.maxdim && j + 1 <= A.capacity) {
-            for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
-                const int i = inst_of_tile(A, t);
-                const BInst I = A.inst[i];
-                double sj;
-                if (j == 0) {
-                    if (gstep >= I.nsteps || ld_vol(&A.fail[i])) continue;
-                    sj = 1.0 / sqrt(__ldcg(A.sumN + 4 * (size_t)i));
-                } else {
-                    if (ld_vol(&A.ranB[i]) != round) continue;  // B ran it last round
-                    sj = 1.0 / sqrt(__ldcg(A.sumB + 4 * (size_t)i));
-                }
-                if (!isfinite(sj) || sj <= 0.0) continue;  // the same for all its tiles
-                tile_hpsi<R, T>(A, I, i, t, gstep, j, sj);
-            }
-        }
-        if (!grid_sync(A, ph)) return false;
-        // does any job still iterate?
-        if (warp == 0) {
-            int any = 0;
-            for (int i = lane; i < A.ninst; i += 32) any |= ld_status(A.ks + i) == KS_RUNNING;
-            any = __any_sync(0xffffffffu, any);
-            if (lane == 0) s_flag = any;
-        }
-        __syncthreads();
-        if (!s_flag) return true;
-        // ---------------- phase B_j: w = H v_j - a v_j - b v_{j-1}
-        {
-            int ci = -1;
-            double car = 0, cai = 0, cb = 0, sj = 0;
-            for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
-                const int i = inst_of_tile(A, t);
-                KState *ks = A.ks + i;
-                if (ld_status(ks) != KS_RUNNING) continue;
-                const BInst I = A.inst[i];
-                if (i != ci) {
-                    const double3 sa = ld_sum(A.sumA, i);
-                    const double b = j > 0 ? __ldcg(&ks->r[j - 1]) : 0.0;
-                    const double vr = j > 0 ? __ldcg(&ks->vv_re[j]) : 0.0;
-                    const double vi = j > 0 ? __ldcg(&ks->vv_im[j]) : 0.0;
-                    const double ar = sa.y - b * vr, ai = sa.z - b * vi;
-                    sj = __ldcg(&ks->scale[j]);
-                    const double sp = j > 0 ? __ldcg(&ks->scale[j - 1]) : 0.0;
-                    car = ar * sj;
-                    cai = ai * sj;
-                    cb = b * sp;
-                    ci = i;
-                    // the warp of the job's first tile records T_H's column j (a warp meets a
-                    // given job's first tile before any other of its tiles)
-                    if (t == I.tile0 && lane == 0) {
-                        ks->a_re[j] = ar;
-                        ks->a_im[j] = ai;
-                        ks->b_re[j] = b;
-                        ks->b_im[j] = 0.0;
-                        ks->hn[j] = sqrt(sa.x);
-                        A.ranB[i] = round + 1;  // 0 (cleared at launch) = never
-                    }
-                }
-                tile_orth<R, T>(A, I, i, t, j, car, cai, cb, sj);
-            }
-        }
-        if (!grid_sync(A, ph)) return false;
-        ++round;
+// Phase phi of job i is complete: publish phase phi + 1 with code c, then open its tiles
+// (lane 0 of the completing warp; its tiles' writes and the phase's sums precede both
+// releases, and a warp whose take lands on the new phase finds its code published).
+__device__ void publish(const BArgs &A, int i, unsigned phi, unsigned c) {
+    if ((threadIdx.x & 31) == 0 && !(A.test_hold && i == 0 && phi == 0)) {
+        __threadfence();
+        st_rel64(&A.jst[i], (unsigned long long)(phi + 1) << 32 | c);
+        st_rel64(&A.take[i], (unsigned long long)(phi + 1) << 32);  // the new phase's tiles
     }
+    __syncwarp();
+}
+
+// The job has no phase left in this launch: its final status, then the idle count.
+__device__ void job_idle(const BArgs &A, int i, unsigned phi) {
+    if ((threadIdx.x & 31) == 0) {
+        const int st = ld_status(A.ks + i);
+        const int f = ld_vol(&A.fail[i]);
+        A.status_out[i] = f ? f : (st == BS_IDLE ? KS_CONVERGED : st);
+    }
+    publish(A, i, phi, pcode(PK_IDLE, 0, 0));
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence();
+        atomicAdd(&A.ctl->idle, 1u);
+    }
+    __syncwarp();
+}
+
+// Start of step gstep for job i, from the norm of its vector 0 in sumN: the step's
+// Krylov state; true if the job iterates (false: idle, failed or a non-finite norm).
+__device__ bool job_init(const BArgs &A, int i, int gstep) {
+    int st = KS_RUNNING;
+    if ((threadIdx.x & 31) == 0) {
+        KState *ks = A.ks + i;
+        const double s0 = sqrt(__ldcg(A.sumN + 4 * (size_t)i));
+        const int f = ld_vol(&A.fail[i]);
+        if (f) st = f;
+        else if (gstep >= A.inst[i].nsteps) st = BS_IDLE;
+        else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
+        ks->s0 = s0;
+        ks->shift = 0.0;
+        ks->scale[0] = 1.0 / s0;
+        ks->iters = 0;
+        ks->nvec = 0;
+        ks->kerr = 0;
+        ks->err = 0.0;
+        A.polled[i] = 0;
+        ks->status = st;
+        if (st == KS_NONFINITE) A.fail[i] = st;
+    }
+    __syncwarp();
+    return __shfl_sync(0xffffffffu, st, 0) == KS_RUNNING;
+}
+
+// Decision for iteration j of job i (krylov_exp.py:60-96), by the warp that completed
+// phase B_j (not inlined: its registers would otherwise crowd the tile loops, which then
+// spill): convergence is tested from the job's hint (the previous step's count - 3); a
+// first test that already converges tests the skipped iterations in order
+// (krylov_decide), so each job stops where the reference would.  True if the job's step
+// goes on.
+__device__ __noinline__ bool job_decide(const BArgs &A, int i, int j, int rstep) {
+    const int lane = threadIdx.x & 31;
+    KState *ks = A.ks + i;
+    const double3 sb = ld_sum(A.sumB, i);
+    const int hint = ld_vol(&A.hint[i]);
+    const bool poll = (j + 1 >= hint) || (j + 1 >= A.maxdim);
+    const bool first = poll && !ld_vol(&A.polled[i]);
+    __syncwarp();
+    if (lane == 0 && poll) A.polled[i] = 1;
+    krylov_decide(ks, j, sb.x, sb.y, sb.z, A.inst[i].dt, A.exp_tol, A.norm_tol, poll, first,
+                  A.maxdim);
+    int st = KS_RUNNING;
+    if (lane == 0) {
+        st = ks->status;
+        if (st == KS_RUNNING && j + 2 > A.capacity) {
+            st = BS_CAPACITY;
+            ks->status = st;
+        }
+        if (st == KS_NONFINITE || st == BS_CAPACITY) A.fail[i] = st;
+        if (st != KS_RUNNING) {
+            A.iters_out[(size_t)i * A.max_steps + rstep] = ks->iters;
+            A.hint[i] = ks->iters > 3 ? ks->iters - 3 : 0;  // poll a little early
+        }
+    }
+    __syncwarp();
+    return __shfl_sync(0xffffffffu, st, 0) == KS_RUNNING;
 }
 
 // Lane k % 32 holds coefficient block k / 32 (k < 128): f * c_k with f = s0 scale_k, or
@@ -634,65 +651,204 @@ __device__ double tile_lincomb(const BArgs &A, const BInst &I, int t, int nvec, 
     return warp_sum(nrm);
 }
 
-// psi' = s0 sum_k c_k v_k for every job that took the step (norm partials for the next
-// step), optionally also into the history buffer.
+// Combination tile of step rstep: psi' = s0 sum_k c_k v_k in place for a job whose step
+// ended with a result (optionally also into the history buffer), else (failed) the norm
+// of the kept state; the tile's norm partial.  True for the warp that completes the job.
 template <typename R, int T>
-__device__ void combine_phase(const BArgs &A, int rstep, unsigned ph) {
+__device__ bool tile_combine(const BArgs &A, const BInst &I, int i, int t, int rstep) {
     typedef typename cvec<R>::T C;
     const int lane = threadIdx.x & 31;
-    int ci = -1, nvec = 0;
+    const KState *ks = A.ks + i;
+    const int st = ld_status(ks);
+    if (st != KS_CONVERGED && st != KS_HAPPY && st != KS_MAXDIM) return tile_norm<R, T>(A, I, i, t);
+    const int nvec = __ldcg(&ks->nvec);
     double cr[4], cim[4];
-    const bool hist = A.hist && ((rstep + 1) % A.hist_every) == 0;
-    for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
-        const int i = inst_of_tile(A, t);
-        const KState *ks = A.ks + i;
-        const int st = ld_status(ks);
-        const BInst I = A.inst[i];
-        if (st != KS_CONVERGED && st != KS_HAPPY && st != KS_MAXDIM) {
-            tile_norm<R, T>(A, I, i, t);  // idle or failed: keep the state, refresh its norm
-            continue;
+    load_coefs(ks, nvec, false, cr, cim);
+    C *out = vec_ptr<C>(A, 0, I);
+    const double nrm = tile_lincomb<R, T>(A, I, t, nvec, cr, cim, out);
+    if (A.hist && ((rstep + 1) % A.hist_every) == 0) {  // the new tile into the history slot
+        constexpr int AMP = 1 << (T - 5);
+        const long long base = (long long)(t - I.tile0) << T;
+        C *h = reinterpret_cast<C *>(A.hist) +
+               (size_t)((rstep + 1) / A.hist_every - 1) * (size_t)A.hist_stride + I.off0;
+        __syncwarp();
+        for (int a = 0; a < AMP; ++a) h[base + lane + 32 * a] = out[base + lane + 32 * a];
+    }
+    if (lane == 0) A.partN[4 * (size_t)t] = nrm;
+    return tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
+}
+
+// The phase engine (krylov_exp.py:23-131 per job and step, every job of the batch in one
+// persistent launch).  Warps never wait for a particular phase: a cursor over the tiles
+// of all jobs picks the jobs to visit (so a job is visited in proportion to its size),
+// and the warp takes up to BCHUNK tiles of each visited job's current phase from the
+// job's take counter, (phase << 32) | tiles taken.  A job whose current phase has no tile
+// left (its last tiles are still running, or it is idle) is passed over; an idle job's
+// tiles are jumped over (atomicMax on the cursor).  The warp that completes a phase (the
+// last of its tiles) takes the phase's decision, publishes the next phase's code, then
+// resets the take counter.  The launch ends when every job is idle.
+enum { V_WORK = 0, V_BUSY = 1, V_IDLE = 2, V_STOP = 3 };
+
+// One visit of job i (cursor sweep `sweep`): take up to BCHUNK tiles of its current
+// phase and run them.  cphi / c cache the phase's scalars (A: sj; B: car, cai, cb, sjb)
+// for the warp's current job.
+template <typename R, int T>
+__device__ int visit_job(const BArgs &A, int i, const BInst &I, unsigned long long sweep,
+                         unsigned &cphi, double (&c)[4]) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long w = 0, tk = 0;
+    int gated = 0;
+    if (lane == 0) {
+        w = ld_acq64(&A.jst[i]);
+        const unsigned c = (unsigned)w;
+        if (pkind(c) == PK_A && pj(c) == 0 && prstep(c) >= BSTEP_LEAD) {
+            // the step gate: a job starts step r only while the jobs still running have
+            // completed (r - BSTEP_LEAD) steps on average, so no job runs far ahead and
+            // the jobs with the most iterations are not left to finish alone (the job
+            // furthest behind is never gated)
+            const unsigned long long done = *(volatile unsigned long long *)&A.ctl->steps_done;
+            const unsigned live = (unsigned)A.ninst - ld_vol_u(&A.ctl->idle);
+            gated = done < (unsigned long long)(prstep(c) - BSTEP_LEAD) * live;
         }
-        if (i != ci) {
-            nvec = __ldcg(&ks->nvec);
-            load_coefs(ks, nvec, false, cr, cim);
-            ci = i;
+        if (!gated && pkind(c) != PK_IDLE) tk = atomicAdd(&A.take[i], (unsigned long long)BCHUNK);
+    }
+    if (__shfl_sync(0xffffffffu, gated, 0)) return V_BUSY;
+    w = __shfl_sync(0xffffffffu, w, 0);
+    tk = __shfl_sync(0xffffffffu, tk, 0);
+    unsigned code = (unsigned)w, phi = (unsigned)(w >> 32);
+    if (pkind(code) == PK_IDLE) {
+        if (lane == 0)
+            atomicMax(&A.ctl->item, sweep * (unsigned long long)A.total_tiles +
+                                        (unsigned long long)(I.tile0 + I.ntiles));
+        return V_IDLE;
+    }
+    const unsigned phit = (unsigned)(tk >> 32), n0 = (unsigned)tk;
+    if (phit != phi || n0 >= (unsigned)I.ntiles) {
+        if (!(phit > phi && n0 < (unsigned)I.ntiles)) return V_BUSY;  // nothing free now
+        // the take counter was already reset for a later phase: these tiles are that
+        // phase's, whose code was published just before the reset
+        if (!wait_phase(A, i, phit, w)) return V_STOP;
+        code = (unsigned)w;
+        phi = phit;
+        if (pkind(code) == PK_IDLE) return V_IDLE;  // the job went idle: no tiles
+        if ((unsigned)(w >> 32) != phit) {  // cannot happen
+            if (lane == 0) atomicCAS(&A.ctl->err, 0, EMUSV_BAD_ARGUMENT);
+            return V_STOP;
         }
-        C *out = vec_ptr<C>(A, 0, I);
-        const double nrm = tile_lincomb<R, T>(A, I, t, nvec, cr, cim, out);
-        if (hist) {  // copy the new tile into the history slot
-            constexpr int AMP = 1 << (T - 5);
-            const long long base = (long long)(t - I.tile0) << T;
-            C *h = reinterpret_cast<C *>(A.hist) +
-                   (size_t)((rstep + 1) / A.hist_every - 1) * (size_t)A.hist_stride + I.off0;
+    }
+    const int kind = pkind(code), j = pj(code), rstep = prstep(code);
+    KState *ks = A.ks + i;
+    if (phi != cphi) {  // the phase's scalars
+        cphi = phi;
+        if (kind == PK_A) {
+            const double sn = __ldcg((j == 0 ? A.sumN : A.sumB) + 4 * (size_t)i);
+            c[0] = 1.0 / sqrt(sn);
+            // ||w_{j-1}|| zero or not finite: the decision of j - 1 ended the step unless
+            // a tolerance of zero let it go on; the tiles run on zeros
+            if (!isfinite(c[0]) || c[0] <= 0.0) c[0] = 0.0;
+        } else if (kind == PK_B) {
+            const double3 sa = ld_sum(A.sumA, i);
+            const double b = j > 0 ? __ldcg(&ks->r[j - 1]) : 0.0;
+            const double vr = j > 0 ? __ldcg(&ks->vv_re[j]) : 0.0;
+            const double vi = j > 0 ? __ldcg(&ks->vv_im[j]) : 0.0;
+            const double ar = sa.y - b * vr, ai = sa.z - b * vi;
+            c[3] = __ldcg(&ks->scale[j]);
+            const double sp = j > 0 ? __ldcg(&ks->scale[j - 1]) : 0.0;
+            c[0] = ar * c[3];
+            c[1] = ai * c[3];
+            c[2] = b * sp;
+            // the warp that took the job's first tile records T_H's column j (read by the
+            // decision, which follows every tile of the phase)
+            if (n0 == 0 && lane == 0) {
+                ks->a_re[j] = ar;
+                ks->a_im[j] = ai;
+                ks->b_re[j] = b;
+                ks->b_im[j] = 0.0;
+                ks->hn[j] = sqrt(sa.x);
+            }
             __syncwarp();
-            for (int a = 0; a < AMP; ++a) h[base + lane + 32 * a] = out[base + lane + 32 * a];
         }
-        if (lane == 0) A.partN[4 * (size_t)t] = nrm;
-        tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
+    }
+    const int n1 = min((int)n0 + BCHUNK, I.ntiles);
+    for (int t = I.tile0 + (int)n0; t < I.tile0 + n1; ++t) {
+        if (kind == PK_NORM) {
+            if (tile_norm<R, T>(A, I, i, t)) {
+                if (job_init(A, i, A.first_step + rstep)) publish(A, i, phi, pcode(PK_A, rstep, 0));
+                else job_idle(A, i, phi);
+            }
+        } else if (kind == PK_A) {  // H v_j
+            if (tile_hpsi<R, T>(A, I, i, t, A.first_step + rstep, j, c[0]))
+                publish(A, i, phi, pcode(PK_B, rstep, j));
+        } else if (kind == PK_B) {  // w = H v_j - a v_j - b v_{j-1}, then the decision
+            if (tile_orth<R, T>(A, I, i, t, j, c[0], c[1], c[2], c[3])) {
+                if (job_decide(A, i, j, rstep)) publish(A, i, phi, pcode(PK_A, rstep, j + 1));
+                else if (A.combine) publish(A, i, phi, pcode(PK_C, rstep, 0));
+                else job_idle(A, i, phi);
+            }
+        } else {  // PK_C: the combination, then the next step
+            if (tile_combine<R, T>(A, I, i, t, rstep)) {
+                if (lane == 0) atomicAdd(&A.ctl->steps_done, 1ull);
+                if (rstep + 1 < A.run_steps && job_init(A, i, A.first_step + rstep + 1))
+                    publish(A, i, phi, pcode(PK_A, rstep + 1, 0));
+                else job_idle(A, i, phi);
+            }
+        }
+    }
+    return V_WORK;
+}
+
+template <typename R, int T>
+__device__ void run_jobs(const BArgs &A) {
+    const int lane = threadIdx.x & 31;
+    BCtl *ctl = A.ctl;
+    const unsigned long long total = (unsigned long long)A.total_tiles;
+    int ci = -1;                  // the warp's current job, its BInst and phase scalars
+    BInst I = {};
+    unsigned cphi = 0xffffffffu;
+    double c[4] = {0.0, 0.0, 0.0, 0.0};
+    unsigned long long qn = 0;    // the next visit, taken while this one runs
+    if (lane == 0) qn = atomicAdd(&ctl->item, (unsigned long long)BCHUNK);
+    // a warp that finds no tile to run for A.bar_limit clock cycles gives up (a phase
+    // completion that never comes): EMUSV_TIMEOUT, and every warp returns
+    long long idle_since = -1;
+    for (;;) {
+        const unsigned long long q0 = __shfl_sync(0xffffffffu, qn, 0);
+        if (lane == 0) qn = atomicAdd(&ctl->item, (unsigned long long)BCHUNK);
+        const unsigned long long sweep = q0 / total;
+        const int t0 = (int)(q0 - sweep * total);
+        // every job whose tiles meet [t0, t0 + BCHUNK) (a job smaller than a visit is
+        // never passed over)
+        for (int tj = t0;; tj = I.tile0 + I.ntiles) {
+            if (ci < 0 || tj < I.tile0 || tj >= I.tile0 + I.ntiles) {
+                const int ni = inst_of_tile(A, tj);
+                if (ni != ci) cphi = 0xffffffffu;
+                ci = ni;
+                I = A.inst[ci];
+            }
+            const int v = visit_job<R, T>(A, ci, I, sweep, cphi, c);
+            if (v == V_STOP) return;
+            if (v == V_WORK) {
+                idle_since = -1;
+            } else {
+                if (v == V_IDLE && ld_vol_u(&ctl->idle) >= (unsigned)A.ninst) return;
+                const long long now = clock64();
+                if (idle_since < 0) idle_since = now;
+                if (now - idle_since > A.bar_limit) {
+                    if (lane == 0) atomicCAS(&ctl->err, 0, EMUSV_TIMEOUT);
+                    return;
+                }
+                if (ld_vol(&ctl->err)) return;
+                if (v == V_BUSY) __nanosleep(128);
+            }
+            if (I.tile0 + I.ntiles >= t0 + BCHUNK || ci + 1 >= A.ninst) break;
+        }
     }
 }
 
 // ---------------------------------------------------------------- forward kernel
 template <typename R, int T, int MINB>
 __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch(const BArgs A) {
-    __shared__ int s_flag;
-    const int lane = threadIdx.x & 31;
-    unsigned ph = 0;
-    int round = 0;  // phase-B rounds so far (the same in every CTA)
-    norm_phase<R, T>(A, ph);
-    if (!grid_sync(A, ph)) return;
-    for (int step = 0; step < A.run_steps; ++step) {
-        if (!krylov_rounds<R, T>(A, A.first_step + step, step, ph, round, s_flag)) return;
-        combine_phase<R, T>(A, step, ph);
-        if (!grid_sync(A, ph)) return;
-    }
-    if (threadIdx.x < 32) {  // final statuses
-        for (int i = blockIdx.x * 32 + lane; i < A.ninst; i += gridDim.x * 32) {
-            const int st = ld_status(A.ks + i);
-            const int f = A.fail[i];
-            A.status_out[i] = f ? f : (st == BS_IDLE ? KS_CONVERGED : st);
-        }
-    }
+    run_jobs<R, T>(A);
 }
 
 // ---------------------------------------------------------------- adjoint kernel
@@ -765,14 +921,11 @@ __global__ void __launch_bounds__(BWARPS * 32) k_batch_dS(const BArgs A, const B
     }
 }
 
+// The adjoint's Krylov bases of one step: the phase engine without the combination (the
+// launch sets first_step = the step, run_steps = 1, combine = 0).
 template <typename R, int T, int MINB>
 __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_rounds(const BArgs A, const BAdj D) {
-    __shared__ int s_flag;
-    unsigned ph = 0;
-    int round = 0;
-    norm_phase<R, T>(A, ph);
-    if (!grid_sync(A, ph)) return;
-    krylov_rounds<R, T>(A, D.step, 0, ph, round, s_flag);
+    run_jobs<R, T>(A);
 }
 
 template <typename R, int T, int MINB>
@@ -1011,6 +1164,13 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_post(const BArg
 // ---------------------------------------------------------------- host side
 static size_t al256(size_t v) { return (v + 255) / 256 * 256; }
 
+// Integer region after the control block, per job: the state word and the take counter
+// (two ints each), fail, status, the tile counters (3) -- cleared by every launch -- then
+// hint and polled
+// (carried from one adjoint launch to the next), then the adjoint's counters (per instance).
+constexpr int BINTS_LAUNCH = 9;  // per-job ints every launch clears
+constexpr int BINTS_JOB = 11;    // per-job ints in all
+
 // Workspace layout.  Forward: one job per instance.  Adjoint: jobs 2i (state) and 2i+1
 // (gradient) per instance, plus the adjoint's own arrays.
 struct BLayout {
@@ -1043,12 +1203,13 @@ static bool layout(int ninst, const int *nq, const int *nsteps, int es, int T, i
     size_t off = 0;
     auto take = [&](size_t b) { const size_t o = off; off += al256(b); return o; };
     L->args = take(sizeof(BArgs));
-    // control block and integer flags, contiguous so that a launch clears them in one go:
-    // hint, polled, fail, status, ranB, cnt[3] per job, then the adjoint's counters
+    // control block and integer region (BINTS_JOB per job, then the adjoint's counters),
+    // contiguous so that a launch clears them in one go; the state words are 8-byte
+    // aligned (the control block is 32 bytes)
     L->ctl = off;
     off += sizeof(BCtl);
     L->ints = off;
-    off += sizeof(int) * (8 * (size_t)nj + ninst);
+    off += sizeof(int) * (BINTS_JOB * (size_t)nj + ninst);
     off = al256(off);
     L->inst = take(sizeof(BInst) * nj);
     L->coef = take(sizeof(BCoef) * (coefs > 0 ? coefs : 1));
@@ -1217,12 +1378,13 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
     A.Elow = reinterpret_cast<double *>(ws + L.elow);
     A.ks = reinterpret_cast<KState *>(ws + L.ks);
     int *ints = reinterpret_cast<int *>(ws + L.ints);
-    A.hint = ints;
-    A.polled = ints + nj;
-    A.fail = ints + 2 * nj;
-    A.status_out = ints + 3 * nj;
-    A.ranB = ints + 4 * nj;
-    A.cnt = reinterpret_cast<unsigned *>(ints + 5 * nj);
+    A.jst = reinterpret_cast<unsigned long long *>(ints);
+    A.take = reinterpret_cast<unsigned long long *>(ints + 2 * nj);
+    A.fail = ints + 4 * nj;
+    A.status_out = ints + 5 * nj;
+    A.cnt = reinterpret_cast<unsigned *>(ints + 6 * nj);
+    A.hint = ints + BINTS_LAUNCH * nj;
+    A.polled = ints + (BINTS_LAUNCH + 1) * nj;
     double *sums = reinterpret_cast<double *>(ws + L.sums);
     A.sumA = sums;
     A.sumB = sums + 4 * nj;
@@ -1241,8 +1403,9 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
     A.hist = nullptr;
     A.hist_every = 1;
     A.hist_stride = L.inst_amps;
+    A.combine = adjoint ? 0 : 1;
     A.bar_limit = BAR_LIMIT;
-    A.test_skip_arrival = 0;
+    A.test_hold = 0;
     if (adjoint) {
         BAdj &D = P.D;
         D.ninst = ninst;
@@ -1251,14 +1414,14 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
         D.E = ws + L.E;
         D.inst_amps = L.inst_amps;
         D.partC = reinterpret_cast<double *>(ws + L.partC);
-        D.cntC = reinterpret_cast<unsigned *>(ints + 8 * nj);
+        D.cntC = reinterpret_cast<unsigned *>(ints + BINTS_JOB * nj);
     }
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.args, &A, sizeof(A), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.inst, inst.data(), sizeof(BInst) * nj, cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.coef, coef.data(), sizeof(BCoef) * coef.size(), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.ubits, ub.data(), sizeof(double) * ub.size(), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.elow, elow.data(), sizeof(double) * elow.size(), cudaMemcpyHostToDevice, s));
-    EMUSV_CHECK(cudaMemsetAsync(ws + L.ctl, 0, sizeof(BCtl) + sizeof(int) * (8 * (size_t)nj + ninst), s));
+    EMUSV_CHECK(cudaMemsetAsync(ws + L.ctl, 0, sizeof(BCtl) + sizeof(int) * (BINTS_JOB * (size_t)nj + ninst), s));
     EMUSV_CHECK(cudaStreamSynchronize(s));  // the host tables go out of scope
     {
         std::lock_guard<std::mutex> g(g_args_mu);
@@ -1337,7 +1500,7 @@ int emusv_batch_launch_steps(int dtype, int tile_bits, int blocks_per_sm, int fi
     Prepared P;
     if (!kern || !workspace || blocks_per_sm < 1 || lookup(workspace, false, &P)) return EMUSV_BAD_ARGUMENT;
     BArgs A = P.A;
-    if (first_step < 0 || steps < 0 || first_step + steps > P.L.max_steps || history_every < 1 ||
+    if (first_step < 0 || steps < 1 || steps > 65535 || first_step + steps > P.L.max_steps || history_every < 1 ||
         (states && (reinterpret_cast<uintptr_t>(states) & 15)))
         return EMUSV_BAD_ARGUMENT;
     if (A.T != tile_bits) return EMUSV_BAD_ARGUMENT;
@@ -1348,8 +1511,9 @@ int emusv_batch_launch_steps(int dtype, int tile_bits, int blocks_per_sm, int fi
     A.hist_every = history_every;
     cudaStream_t s = as_stream(stream);
     unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
-    // control block, flags, hints and tile counters start at zero
-    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * 8 * (size_t)A.ninst, s));
+    // control block, job states, flags, hints and tile counters start at zero (every
+    // job's first phase: the norm of its vector 0)
+    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * BINTS_JOB * (size_t)A.ninst, s));
     void *args[] = {(void *)&A};
     return cooperative_launch(kern, blocks_per_sm, args, s, nullptr);
 }
@@ -1443,16 +1607,18 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
     A.v0[0] = const_cast<void *>(states);
     A.v0[1] = const_cast<void *>(grad_in);
     D.step = step;
+    A.first_step = step;  // the engine's one "step": the bases of this adjoint step
+    A.run_steps = 1;
     D.grads = grads_dev;
     D.gout = grad_out;
     D.astatus = status_dev;
     cudaStream_t s = as_stream(stream);
     unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
-    // clear the control block and everything after the hints and polled flags (the
-    // hints carry from one step to the next)
+    // clear the control block, job states, flags and counters (the hints and polled flags
+    // carry from one step to the next)
     const int nj = A.ninst;
-    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl), s));
-    EMUSV_CHECK(cudaMemsetAsync(A.fail, 0, sizeof(int) * (6 * (size_t)nj + D.ninst), s));
+    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * BINTS_LAUNCH * (size_t)nj, s));
+    EMUSV_CHECK(cudaMemsetAsync(D.cntC, 0, sizeof(unsigned) * D.ninst, s));
     void *args[] = {(void *)&A, (void *)&D};
     int st = cooperative_launch(k1, blocks_per_sm, args, s, nullptr);
     if (st) return st;
@@ -1467,16 +1633,17 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
 }
 
 // Failure-path test switch of a prepared workspace (forward or adjoint): later launches
-// wait at most wait_cycles clock cycles at a grid barrier (<= 0: the default, about 1 s)
-// and, when skip_first_arrival != 0, the last CTA does not arrive at each launch's first
-// barrier, so the others' bounded waits run out and the launch reports EMUSV_TIMEOUT.
+// wait at most wait_cycles clock cycles for a job's previous phase or at a grid barrier
+// (<= 0: the default, about 1 s) and, when skip_first_arrival != 0, the completion of job
+// 0's first phase is never published (its tiles' work "does not arrive"), so the waits for
+// job 0's next phase run out and the launch reports EMUSV_TIMEOUT.
 int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival) {
     if (!workspace) return EMUSV_BAD_ARGUMENT;
     std::lock_guard<std::mutex> g(g_args_mu);
     auto it = g_args.find(workspace);
     if (it == g_args.end()) return EMUSV_BAD_ARGUMENT;
     it->second.A.bar_limit = wait_cycles > 0 ? wait_cycles : BAR_LIMIT;
-    it->second.A.test_skip_arrival = skip_first_arrival ? 1 : 0;
+    it->second.A.test_hold = skip_first_arrival ? 1 : 0;
     return EMUSV_OK;
 }
 

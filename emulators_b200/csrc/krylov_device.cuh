@@ -457,6 +457,35 @@ static __device__ double krylov_eval(KState *ks, int jj, double dt) {
 // when the first poll (`first_poll`) already converges the warp tests the earlier
 // iterations in order and stops at the first that converges -- where the reference, which
 // tests every iteration, stops.  One warp each; ks->status must be KS_RUNNING.
+// Happy breakdown after m vectors: c = exp(T[:m,:m]) e_0 (krylov_exp.py:63-71), in the
+// smallest register layout that holds the m rows (a separate, non-inlined function per
+// layout, so the large layouts do not raise the register demand of the kernels that call
+// the decision).
+template <int NE>
+static __device__ __noinline__ void krylov_happy_ne(KState *ks, int m, double dt) {
+    const int lane = threadIdx.x & 31;
+    double2 d[NE], l[NE], u[NE], y[NE];
+    double td[NE], tr[NE];
+    load_rows<NE>(ks, m, dt, d, l, u, td, tr);
+    cheb_expm<NE>(d, l, u, -1, make_double2(0.0, 0.0), 0, dt, td, tr, m, y);
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        const int k = lane * NE + e;
+        if (k < m) {
+            ks->c_re[k] = y[e].x;
+            ks->c_im[k] = y[e].y;
+        }
+    }
+    __syncwarp();
+}
+static __device__ void krylov_happy(KState *ks, int m, double dt) {
+    constexpr int NEMAX = (KMAX + 2 + 31) / 32;
+    if (m <= 32) krylov_happy_ne<1>(ks, m, dt);
+    else if (m <= 64) krylov_happy_ne<2>(ks, m, dt);
+    else if (m <= 96) krylov_happy_ne<3>(ks, m, dt);
+    else krylov_happy_ne<NEMAX>(ks, m, dt);
+}
+
 enum { KD_OK = 0, KD_NONFINITE = 1, KD_HAPPY = 2 };
 
 static __device__ int krylov_norms(KState *ks, int j, double v, double vr, double vi, double dt,
@@ -490,19 +519,7 @@ static __device__ void krylov_conclude(KState *ks, int j, int flag, double dt, d
     }
     const int m = j + 1;
     if (flag == KD_HAPPY) {  // krylov_exp.py:63-71: exp(T[:j+1,:j+1]) e_0 over j+1 vectors
-        constexpr int NE = (KMAX + 2 + 31) / 32;
-        double2 d[NE], l[NE], u[NE], y[NE];
-        double td[NE], tr[NE];
-        load_rows<NE>(ks, m, dt, d, l, u, td, tr);
-        cheb_expm<NE>(d, l, u, -1, make_double2(0.0, 0.0), 0, dt, td, tr, m, y);
-#pragma unroll
-        for (int e = 0; e < NE; ++e) {
-            const int k = lane * NE + e;
-            if (k < m) {
-                ks->c_re[k] = y[e].x;
-                ks->c_im[k] = y[e].y;
-            }
-        }
+        krylov_happy(ks, m, dt);
         if (lane == 0) {
             ks->nvec = m;
             ks->iters = j + 1;

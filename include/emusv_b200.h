@@ -337,11 +337,11 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
 int emusv_batch_adjoint_iterations(int ninst, void *workspace, int *iterations_out, void *stream);
 /* Failure-path test switch of a prepared batch workspace (forward or adjoint; no
  * counterpart in the reference, whose loop has no device-side waits): later launches wait
- * at most wait_cycles SM clock cycles at a grid barrier (<= 0 restores the default, about
- * 1 s), and with skip_first_arrival != 0 the last CTA does not arrive at each launch's
- * first barrier, so every other CTA's bounded wait runs out, all CTAs return and
- * emusv_batch_results reports EMUSV_TIMEOUT; the device stays usable.  Off by default;
- * for tests.  Host-side only (takes effect at the next launch). */
+ * at most wait_cycles SM clock cycles for a job's previous phase or at a grid barrier
+ * (<= 0 restores the default, about 1 s), and with skip_first_arrival != 0 the completion
+ * of job 0's first phase is never published, so every wait for job 0's next phase runs
+ * out, all warps return and emusv_batch_results reports EMUSV_TIMEOUT; the device stays
+ * usable.  Off by default; for tests.  Host-side only (takes effect at the next launch). */
 int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival);
 
 /* ---- building blocks of the generic krylov_exp(op, v, ...) (krylov_exp.py:23-106) ----
