@@ -73,6 +73,7 @@ SIGNATURES: dict[str, tuple] = {
                                  _SZ, _P]),
     "emusv_batch_launch": (_I, [_I, _I, _I, _P, _P]),
     "emusv_batch_launch_steps": (_I, [_I, _I, _I, _I, _I, _P, _P, _I, _P, _P]),
+    "emusv_batch_set_engine": (_I, [_P, _I]),
     "emusv_batch_adjoint_workspace_bytes": (_SZ, [_I, _P, _P, _I, _I, _I]),
     "emusv_batch_adjoint_prepare": (_I, [_I, _P, _P, _P, _I, _P, _P, _P, _P, _D, _I, _I, _I, _P,
                                          _SZ, _P]),

@@ -35,6 +35,7 @@ class TuneResult:
     blocks_per_sm: int
     capacity: int
     ms: dict
+    engine: int = 0  # 0 lock-step rounds, 1 per-register phases (emusv_batch_set_engine)
 
 
 _tuned: dict = {}
@@ -116,13 +117,20 @@ class BatchEvolution:
 
     def set_barrier_test(self, wait_cycles: int = 0, skip_first_arrival: bool = False) -> None:
         """Failure-path test switch of the prepared workspace (off by default; reset by
-        :meth:`prepare`): device waits give up after ``wait_cycles`` SM clock cycles
-        (0: the default, about 1 s) and, with ``skip_first_arrival``, the completion of job
-        0's first phase never arrives, so the launch ends with ``TimeoutError`` in
+        :meth:`prepare`): grid-barrier waits give up after ``wait_cycles`` SM clock cycles
+        (0: the default, about 1 s) and, with ``skip_first_arrival``, one CTA never arrives
+        at a launch's first barrier, so the launch ends with ``TimeoutError`` in
         :meth:`results` and the device stays usable."""
         st = _lib.load().emusv_batch_set_barrier_test(self.ws.data_ptr(), int(wait_cycles),
                                                       1 if skip_first_arrival else 0)
         _lib.check(st, "batch barrier test switch")
+
+    def set_engine(self, engine: int) -> None:
+        """Scheduling of the prepared workspace's launches (reset by :meth:`prepare`): 0
+        lock-step rounds of the whole batch, 1 every register's own sequence of phases.
+        Same results; the autotuner times both."""
+        _lib.check(_lib.load().emusv_batch_set_engine(self.ws.data_ptr(), int(engine)),
+                   "batch engine")
 
     def launch(self, blocks_per_sm: int) -> None:
         st = _lib.load().emusv_batch_launch(self.code, self.shape[0], blocks_per_sm,
@@ -158,19 +166,23 @@ class BatchEvolution:
 
     # ---------------------------------------------------------------- one call
     def run(self, tune: bool = True, graph: bool = False, tile_bits: int | None = None,
-            blocks_per_sm: int | None = None, capacity: int | None = None):
+            blocks_per_sm: int | None = None, capacity: int | None = None,
+            engine: int | None = None):
         """Evolve every instance through all its steps from the initial states; returns
         (statuses, iterations [ninst, max_steps])."""
         if tune and tile_bits is None:
             t = autotune(self)
             tile_bits, blocks_per_sm = t.tile_bits, t.blocks_per_sm
             capacity = capacity or t.capacity
+            engine = t.engine if engine is None else engine
         tile_bits = tile_bits or default_tile_bits(self)
         blocks_per_sm = blocks_per_sm or 1
         capacity = capacity or self.max_krylov_dim
         while True:
             self.reset()
             self.prepare(tile_bits, capacity)
+            if engine:
+                self.set_engine(engine)
             if graph:
                 self.capture(blocks_per_sm)
                 self.replay()
@@ -196,8 +208,9 @@ def default_tile_bits(b: BatchEvolution) -> int:
 
 
 def autotune(b: BatchEvolution, probe_steps: int = 3, reps: int = 2) -> TuneResult:
-    """Time every launch shape on the first ``probe_steps`` steps of the batch (on a copy
-    of its states) and keep the fastest; the Krylov capacity is the probe's largest
+    """Time every launch shape (tile bits x CTAs per SM x scheduling engine) on the first
+    ``probe_steps`` steps of the batch (on a copy of its states) and keep the fastest; the
+    Krylov capacity is the probe's largest
     iteration count plus a margin.  Cached per batch signature."""
     key = b.signature()
     if key in _tuned:
@@ -220,7 +233,8 @@ def autotune(b: BatchEvolution, probe_steps: int = 3, reps: int = 2) -> TuneResu
             continue
         probe.prepare(T, b.max_krylov_dim)
         cap = L.emusv_batch_max_blocks_per_sm(b.code, T)
-        for bps in range(1, max(cap, 1) + 1):
+        for engine, bps in [(e, k) for e in (0, 1) for k in range(1, max(cap, 1) + 1)]:
+            probe.set_engine(engine)
             ms = []
             for _ in range(reps + 1):
                 probe.reset()
@@ -236,11 +250,11 @@ def autotune(b: BatchEvolution, probe_steps: int = 3, reps: int = 2) -> TuneResu
                 _lib.check(probe.last_code, "batch autotune probe")  # a launch-wide failure
             max_iters = max(max_iters, int(iters.max()))
             t = min(ms[1:])
-            timings[f"T{T}_b{bps}"] = round(t, 3)
+            timings[f"T{T}_b{bps}" + ("_phases" if engine else "")] = round(t, 3)
             if best is None or t < best[0]:
-                best = (t, T, bps)
+                best = (t, T, bps, engine)
     capacity = min(b.max_krylov_dim, max(16, int(np.ceil(1.5 * max_iters)) + 4))
-    res = TuneResult(best[1], best[2], capacity, timings)
+    res = TuneResult(best[1], best[2], capacity, timings, best[3])
     _tuned[key] = res
     return res
 

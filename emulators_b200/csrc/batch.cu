@@ -15,22 +15,16 @@
 //    inside the thread, bits >= T by coalesced loads of the partner tile; the diagonal is
 //    rebuilt from an FP64 per-instance table of the low-bit pair energies plus per-tile
 //    fields of the high bits.
-//  * per Lanczos iteration j, two tile phases per job: A_j (H v_j, FP64 partials of
-//    ||Hv||^2 and <v_j,Hv>) and B_j (three-term recurrence, partials of ||w||^2, <v_j,w>).
-//    The rounds of a step are dataflow, not lock-step: the work items (round, phase,
-//    tile) are taken in order from one counter, and a tile waits (bounded) only for its
-//    own job's previous phase -- B_j for A_j of the job, A_j for B_{j-1} -- through
-//    per-job completion marks.  The warp that completes B_j of a job takes the job's
-//    decision for iteration j (norm, happy breakdown, extended tridiagonal exponential,
-//    error estimate: krylov_decide) while the other warps go on with A_{j+1}, whose
-//    result is discarded if the job ended.  No grid barrier inside a step's rounds.
-//    After the rounds, a combination phase writes psi' = s0 sum_k c_k v_k in place and
-//    its norm; the warp that completes a job's combination starts the job's next step.
-//  * one grid barrier per step (an arrival counter plus a generation word).  Every wait
-//    is bounded (about a second of SM clock): on a timeout the kernel records
-//    EMUSV_TIMEOUT and every CTA returns at its next barrier.  The launch is cooperative,
-//    so all CTAs are co-resident, and a tile waits only for work taken before it, so the
-//    waits always end.
+//  * per Lanczos iteration j, two grid-wide phases: A_j (H v_j for every running
+//    instance, FP64 partials of ||Hv||^2 and <v_j,Hv>) and B_j (three-term recurrence and
+//    partials of ||w||^2, <v_j,w>).  The per-instance decision for iteration j (norm,
+//    happy breakdown, extended tridiagonal exponential, error estimate: krylov_decide)
+//    runs in warp 0 of one CTA per instance during phase A_{j+1}, overlapping the next
+//    H v, whose result is discarded if the instance converged.  After the iterations of
+//    a step, a combination phase writes psi' = s0 sum_k c_k v_k in place and its norm.
+//  * grid barriers are an arrival counter plus a generation word; every wait is bounded
+//    (about a second of SM clock): on a timeout the kernel records EMUSV_TIMEOUT and
+//    every CTA returns.  The launch is cooperative, so all CTAs are co-resident.
 //  * convergence is tested from a per-instance hint (the previous step's count - 3); a
 //    first test that already converges tests the skipped iterations in order
 //    (krylov_decide), so each instance stops where the reference would.
@@ -75,12 +69,11 @@ struct BCoef {
 };
 
 struct BCtl {
-    unsigned bar_count, bar_gen;  // grid barrier of the adjoint post-processing kernel
+    unsigned bar_count, bar_gen;
     unsigned tile_ctr[2];
     int err;
-    unsigned idle;                // jobs with no phase left in this launch
-    unsigned long long item;      // next work item of the phase engine
-    unsigned long long steps_done;  // steps completed, summed over the jobs
+    unsigned idle;                // phase engine: jobs with no phase left in this launch
+    unsigned long long item;      // phase engine: the visit cursor
 };
 
 struct BArgs {
@@ -96,9 +89,10 @@ struct BArgs {
     double *partA, *partB, *partN;  // [total_tiles][4] per-tile FP64 partial sums
     double *sumA, *sumB, *sumN;     // [ninst][4] their per-instance totals
     unsigned *cnt;                  // [3][ninst] tiles done per phase kind (A, B, N)
-    unsigned long long *jst;        // [ninst] job state: (phases completed << 32) | the code
-                                    // of its next phase (see run_jobs)
-    unsigned long long *take;       // [ninst] (current phase << 32) | its tiles taken
+    int *ranB;                      // [ninst] 1 + last round whose phase B ran the instance
+    unsigned long long *jst;        // [ninst] phase engine: (phases completed << 32) | the
+                                    // code of the job's next phase (see run_jobs)
+    unsigned long long *take;       // [ninst] phase engine: (current phase << 32) | tiles taken
     void *v0[2];          // buffers holding every job's vector 0 (forward: the packed states,
                           // evolved in place; adjoint: states and incoming gradients)
     unsigned char *slots;  // slots 1..capacity
@@ -106,17 +100,17 @@ struct BArgs {
     BCtl *ctl;
     // set per launch
     int first_step;       // absolute index of the launch's first step
-    int run_steps;        // steps this launch takes (at most 65535)
-    int combine;          // 1: each step ends with the combination (forward); 0: the
-                          // launch builds one step's Krylov bases (adjoint)
+    int run_steps;        // steps this launch takes
+    int combine;          // phase engine: 1 ends each step with the combination, 0 (the
+                          // adjoint's bases) leaves the step's Krylov basis
     void *hist;           // optional: states after every hist_every-th step
     int hist_every;
     long long hist_stride;  // amplitudes per history slot
-    // clock cycles a wait lasts at most (BAR_LIMIT unless a test shortens it) and the
-    // failure-path test switch (emusv_batch_set_barrier_test): the completion of job 0's
-    // first phase is not published, so every wait for job 0's next phase runs out
+    // grid barrier: clock cycles a wait lasts at most (BAR_LIMIT unless a test shortens
+    // it) and the failure-path test switch (emusv_batch_set_barrier_test): the last CTA
+    // does not arrive at a launch's first barrier, so every other CTA's wait runs out
     long long bar_limit;
-    int test_hold;
+    int test_skip_arrival;
 };
 
 // Adjoint step (k_batch_adj): jobs 2i (state psi_i) and 2i+1 (gradient g_i) of instance i.
@@ -135,9 +129,8 @@ constexpr int NCP = 6 * BMAXQ;  // per bit: T_re, T_im, U_re, U_im, S_re, S_im
 
 // ---------------------------------------------------------------- grid barrier
 // Arrival counter + generation; the last arriver also clears the tile counter of the
-// next phase.  Returns false (and every CTA then returns)
-// once an error is recorded: a wait gives up after A.bar_limit clock cycles or as soon as
-// another CTA recorded an error.
+// phase after next.  Returns false (and every CTA then returns) on a timeout: a wait
+// gives up after A.bar_limit clock cycles or as soon as another CTA recorded an error.
 __device__ bool grid_sync(const BArgs &A, unsigned &ph) {
     __shared__ int s_ok;  // the CTA's verdict, read by every thread (all return together)
     BCtl *ctl = A.ctl;
@@ -146,8 +139,9 @@ __device__ bool grid_sync(const BArgs &A, unsigned &ph) {
         volatile unsigned *genp = &ctl->bar_gen;
         const unsigned g = *genp;
         __threadfence();
-        const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
-        if (arrived == gridDim.x - 1) {
+        const bool skip = A.test_skip_arrival && ph == 0 && blockIdx.x == gridDim.x - 1;
+        const unsigned arrived = skip ? 0u : atomicAdd(&ctl->bar_count, 1u);
+        if (!skip && arrived == gridDim.x - 1) {
             ctl->bar_count = 0;
             ctl->tile_ctr[(ph + 1) & 1] = 0;
             __threadfence();
@@ -266,6 +260,27 @@ __device__ __forceinline__ void cfma(R cr, R ci, C w, R &ar, R &ai) {
     ai = fma(cr, (R)w.y, fma(ci, (R)w.x, ai));
 }
 
+// ---------------------------------------------------------------- partner-tile stages
+// Each warp of the H v phase owns PSTAGES shared-memory stages of one tile (2^T amplitudes)
+// in the kernel's dynamic shared memory.
+constexpr int PSTAGES = 3;
+template <typename C, int T>
+__host__ __device__ constexpr size_t hpsi_stage_bytes() {
+    return (size_t)BWARPS * PSTAGES * (sizeof(C) << T);
+}
+template <typename C, int T>
+__device__ __forceinline__ C *hpsi_stages() {
+    extern __shared__ __align__(16) unsigned char bsm[];
+    return reinterpret_cast<C *>(bsm + (size_t)(threadIdx.x >> 5) * PSTAGES * (sizeof(C) << T));
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // ---------------------------------------------------------------- phase A: H v_j on a tile
 template <typename R, int T>
 __device__ bool tile_hpsi(const BArgs &A, const BInst &I, int i, int t, int step, int j,
@@ -350,13 +365,38 @@ __device__ bool tile_hpsi(const BArgs &A, const BInst &I, int i, int t, int step
             cfma(bit ? ucr : dcr, bit ? uci : dci, v[a ^ (1 << k)], ar[a], ai[a]);
         }
     }
-    for (int p = T; p < n; ++p) {  // bits above the tile: the partner tile, from L2
+    // bits above the tile: the partner tiles, staged through the warp's shared-memory
+    // stages by cp.async (PSTAGES partner tiles in flight and no registers held by the
+    // copies), then read back in the lanes' amplitude layout
+    C *stage0 = hpsi_stages<C, T>();
+    auto issue = [&](int p, int st) {
+        const char *src = reinterpret_cast<const char *>(u + (base ^ (1LL << p)));
+        char *dst = reinterpret_cast<char *>(stage0 + ((size_t)st << T));
+        constexpr int CP = (int)(sizeof(C) << T) / (16 * 32);  // 16-byte copies per lane
+#pragma unroll
+        for (int m = 0; m < CP; ++m) cp_async16(dst + 16 * (lane + 32 * m), src + 16 * (lane + 32 * m));
+        cp_async_commit();
+    };
+    const int np = n - T;
+    for (int q = 0; q < PSTAGES - 1; ++q) {
+        if (q < np) issue(T + q, q);
+        else cp_async_commit();  // empty groups keep the group count uniform
+    }
+    for (int q = 0; q < np; ++q) {
+        const int qn = q + PSTAGES - 1;  // into the stage read in iteration q - 1
+        if (qn < np) issue(T + qn, qn % PSTAGES);
+        else cp_async_commit();
+        cp_async_wait<PSTAGES - 1>();  // this lane's copies of partner tile q landed
+        __syncwarp();                  // and every lane's
+        const int p = T + q;
         R cr, ci;
         coef(p, (int)((base >> p) & 1), cr, ci);
-        const C *w = u + (base ^ (1LL << p)) + lane;
+        const C *w = stage0 + ((size_t)(q % PSTAGES) << T) + lane;
 #pragma unroll
-        for (int a = 0; a < AMP; ++a) cfma(cr, ci, ldcg(w + 32 * a), ar[a], ai[a]);
+        for (int a = 0; a < AMP; ++a) cfma(cr, ci, w[32 * a], ar[a], ai[a]);
+        __syncwarp();  // the stage is read before it is refilled
     }
+    cp_async_wait<0>();
     // H v = sj * H stored_j; partials ||Hv||^2 and <v_j, Hv> = sj^2 <stored, H stored>
     R h2 = 0, dr = 0, di = 0;
 #pragma unroll
@@ -448,127 +488,19 @@ __device__ __forceinline__ int ld_status(const KState *ks) {
 }
 __device__ __forceinline__ int ld_vol(const int *p) { return *(volatile const int *)p; }
 
-// ---------------------------------------------------------------- the phase engine
-// Every job runs its own sequence of phases: the norm of its vector 0, then per step
-// A_0, B_0, A_1, B_1, ..., B_e (e: the decision that ends the step) and the combination
-// C; then the next step's A_0, and so on, until the job is idle.  A job's state word holds
-// the number of phases it completed and the code of its next phase; the warp that
-// completes a phase (the last of its tiles) takes the phase's decision and publishes the
-// next code.
-enum { PK_NORM = 0, PK_A = 1, PK_B = 2, PK_C = 3, PK_IDLE = 4 };
-constexpr int BCHUNK = 4;     // tiles a warp takes per visit
-constexpr int BSTEP_LEAD = 2;  // steps a job may run ahead of the live jobs' average
-
-__device__ __forceinline__ unsigned pcode(int kind, int rstep, int j) {
-    return (unsigned)kind << 24 | ((unsigned)rstep & 0xffffu) << 8 | (unsigned)j;
-}
-__device__ __forceinline__ int pkind(unsigned c) { return (int)(c >> 24); }
-__device__ __forceinline__ int prstep(unsigned c) { return (int)((c >> 8) & 0xffffu); }
-__device__ __forceinline__ int pj(unsigned c) { return (int)(c & 0xffu); }
-
-__device__ __forceinline__ unsigned long long ld_acq64(const unsigned long long *p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_rel64(unsigned long long *p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_vol_u(const unsigned *p) { return *(volatile const unsigned *)p; }
-
-// Warp-collective bounded wait until job i completed `phi` phases or is idle; the state
-// word in w.  False once the wait ran out (it records EMUSV_TIMEOUT) or another warp
-// recorded an error.
-__device__ bool wait_phase(const BArgs &A, int i, unsigned phi, unsigned long long &w) {
-    unsigned long long v = 0;
-    int ok = 1;
-    if ((threadIdx.x & 31) == 0) {
-        v = ld_acq64(&A.jst[i]);
-        if ((unsigned)(v >> 32) < phi && pkind((unsigned)v) != PK_IDLE) {
-            const long long t0 = clock64();
-            for (int polls = 1;; ++polls) {
-                __nanosleep(64);
-                v = ld_acq64(&A.jst[i]);
-                if ((unsigned)(v >> 32) >= phi || pkind((unsigned)v) == PK_IDLE) break;
-                if ((polls & 15) == 0 && (clock64() - t0 > A.bar_limit || ld_vol(&A.ctl->err))) {
-                    atomicCAS(&A.ctl->err, 0, EMUSV_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-    }
-    __syncwarp();
-    w = __shfl_sync(0xffffffffu, v, 0);
-    return __shfl_sync(0xffffffffu, ok, 0) != 0;
-}
-
-// Phase phi of job i is complete: publish phase phi + 1 with code c, then open its tiles
-// (lane 0 of the completing warp; its tiles' writes and the phase's sums precede both
-// releases, and a warp whose take lands on the new phase finds its code published).
-__device__ void publish(const BArgs &A, int i, unsigned phi, unsigned c) {
-    if ((threadIdx.x & 31) == 0 && !(A.test_hold && i == 0 && phi == 0)) {
-        __threadfence();
-        st_rel64(&A.jst[i], (unsigned long long)(phi + 1) << 32 | c);
-        st_rel64(&A.take[i], (unsigned long long)(phi + 1) << 32);  // the new phase's tiles
-    }
-    __syncwarp();
-}
-
-// The job has no phase left in this launch: its final status, then the idle count.
-__device__ void job_idle(const BArgs &A, int i, unsigned phi) {
-    if ((threadIdx.x & 31) == 0) {
-        const int st = ld_status(A.ks + i);
-        const int f = ld_vol(&A.fail[i]);
-        A.status_out[i] = f ? f : (st == BS_IDLE ? KS_CONVERGED : st);
-    }
-    publish(A, i, phi, pcode(PK_IDLE, 0, 0));
-    if ((threadIdx.x & 31) == 0) {
-        __threadfence();
-        atomicAdd(&A.ctl->idle, 1u);
-    }
-    __syncwarp();
-}
-
-// Start of step gstep for job i, from the norm of its vector 0 in sumN: the step's
-// Krylov state; true if the job iterates (false: idle, failed or a non-finite norm).
-__device__ bool job_init(const BArgs &A, int i, int gstep) {
-    int st = KS_RUNNING;
-    if ((threadIdx.x & 31) == 0) {
-        KState *ks = A.ks + i;
-        const double s0 = sqrt(__ldcg(A.sumN + 4 * (size_t)i));
-        const int f = ld_vol(&A.fail[i]);
-        if (f) st = f;
-        else if (gstep >= A.inst[i].nsteps) st = BS_IDLE;
-        else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
-        ks->s0 = s0;
-        ks->shift = 0.0;
-        ks->scale[0] = 1.0 / s0;
-        ks->iters = 0;
-        ks->nvec = 0;
-        ks->kerr = 0;
-        ks->err = 0.0;
-        A.polled[i] = 0;
-        ks->status = st;
-        if (st == KS_NONFINITE) A.fail[i] = st;
-    }
-    __syncwarp();
-    return __shfl_sync(0xffffffffu, st, 0) == KS_RUNNING;
-}
-
-// Decision for iteration j of job i (krylov_exp.py:60-96), by the warp that completed
-// phase B_j (not inlined: its registers would otherwise crowd the tile loops, which then
-// spill): convergence is tested from the job's hint (the previous step's count - 3); a
-// first test that already converges tests the skipped iterations in order
-// (krylov_decide), so each job stops where the reference would.  True if the job's step
-// goes on.
+// ---------------------------------------------------------------- phases
+// Decision for iteration j of job i (krylov_exp.py:60-96) by warp 0 of the job's CTA
+// (not inlined: its registers would otherwise crowd the tile loops, which then spill):
+// convergence is tested from the job's hint (the previous step's count - 3); a first test
+// that already converges tests the skipped iterations in order (krylov_decide), so each
+// job stops where the reference would.
 __device__ __noinline__ bool job_decide(const BArgs &A, int i, int j, int rstep) {
     const int lane = threadIdx.x & 31;
     KState *ks = A.ks + i;
     const double3 sb = ld_sum(A.sumB, i);
-    const int hint = ld_vol(&A.hint[i]);
+    const int hint = A.hint[i];
     const bool poll = (j + 1 >= hint) || (j + 1 >= A.maxdim);
-    const bool first = poll && !ld_vol(&A.polled[i]);
+    const bool first = poll && !A.polled[i];
     __syncwarp();
     if (lane == 0 && poll) A.polled[i] = 1;
     krylov_decide(ks, j, sb.x, sb.y, sb.z, A.inst[i].dt, A.exp_tol, A.norm_tol, poll, first,
@@ -588,6 +520,125 @@ __device__ __noinline__ bool job_decide(const BArgs &A, int i, int j, int rstep)
     }
     __syncwarp();
     return __shfl_sync(0xffffffffu, st, 0) == KS_RUNNING;
+}
+
+// Phase bookkeeping keeps every job's tiles either all processed or all skipped in a
+// phase (so the per-job tile counters complete): phase A_j runs a job if its step starts
+// (j = 0) or if phase B of the previous round ran it (ranB), never from a status that the
+// decisions of the same phase may be changing.
+
+// Norms of every job's vector 0 (into sumN).
+template <typename R, int T>
+__device__ void norm_phase(const BArgs &A, unsigned ph) {
+    for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+        const int i = inst_of_tile(A, t);
+        tile_norm<R, T>(A, A.inst[i], i, t);
+    }
+}
+
+// All Lanczos iterations of one step of every job (krylov_exp.py:49-106 per job).
+// gstep: absolute step (coefficients, whether the job still has this step); rstep: the
+// launch-relative step (iteration record).  Returns false if a barrier gave up.
+template <typename R, int T>
+__device__ bool krylov_rounds(const BArgs &A, int gstep, int rstep, unsigned &ph, int &round,
+                              int &s_flag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = 0;; ++j) {
+        // ---------------- phase A_j: decisions for j-1 (init at j = 0), tiles H v_j
+        if (warp == 0) {
+            for (int i = blockIdx.x; i < A.ninst; i += gridDim.x) {
+                const BInst I = A.inst[i];
+                KState *ks = A.ks + i;
+                if (j == 0) {
+                    if (lane == 0) {
+                        const double s0 = sqrt(__ldcg(A.sumN + 4 * (size_t)i));
+                        int st = KS_RUNNING;
+                        const int f = ld_vol(&A.fail[i]);
+                        if (f) st = f;
+                        else if (gstep >= I.nsteps) st = BS_IDLE;
+                        else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
+                        ks->s0 = s0;
+                        ks->shift = 0.0;
+                        ks->scale[0] = 1.0 / s0;
+                        ks->iters = 0;
+                        ks->nvec = 0;
+                        ks->kerr = 0;
+                        ks->err = 0.0;
+                        A.polled[i] = 0;
+                        ks->status = st;
+                        if (st == KS_NONFINITE) A.fail[i] = st;
+                    }
+                    __syncwarp();
+                    continue;
+                }
+                if (ld_status(ks) != KS_RUNNING) continue;
+                job_decide(A, i, j - 1, rstep);
+            }
+        }
+        if (j < A.maxdim && j + 1 <= A.capacity) {
+            for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+                const int i = inst_of_tile(A, t);
+                const BInst I = A.inst[i];
+                double sj;
+                if (j == 0) {
+                    if (gstep >= I.nsteps || ld_vol(&A.fail[i])) continue;
+                    sj = 1.0 / sqrt(__ldcg(A.sumN + 4 * (size_t)i));
+                } else {
+                    if (ld_vol(&A.ranB[i]) != round) continue;  // B ran it last round
+                    sj = 1.0 / sqrt(__ldcg(A.sumB + 4 * (size_t)i));
+                }
+                if (!isfinite(sj) || sj <= 0.0) continue;  // the same for all its tiles
+                tile_hpsi<R, T>(A, I, i, t, gstep, j, sj);
+            }
+        }
+        if (!grid_sync(A, ph)) return false;
+        // does any job still iterate?
+        if (warp == 0) {
+            int any = 0;
+            for (int i = lane; i < A.ninst; i += 32) any |= ld_status(A.ks + i) == KS_RUNNING;
+            any = __any_sync(0xffffffffu, any);
+            if (lane == 0) s_flag = any;
+        }
+        __syncthreads();
+        if (!s_flag) return true;
+        // ---------------- phase B_j: w = H v_j - a v_j - b v_{j-1}
+        {
+            int ci = -1;
+            double car = 0, cai = 0, cb = 0, sj = 0;
+            for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+                const int i = inst_of_tile(A, t);
+                KState *ks = A.ks + i;
+                if (ld_status(ks) != KS_RUNNING) continue;
+                const BInst I = A.inst[i];
+                if (i != ci) {
+                    const double3 sa = ld_sum(A.sumA, i);
+                    const double b = j > 0 ? __ldcg(&ks->r[j - 1]) : 0.0;
+                    const double vr = j > 0 ? __ldcg(&ks->vv_re[j]) : 0.0;
+                    const double vi = j > 0 ? __ldcg(&ks->vv_im[j]) : 0.0;
+                    const double ar = sa.y - b * vr, ai = sa.z - b * vi;
+                    sj = __ldcg(&ks->scale[j]);
+                    const double sp = j > 0 ? __ldcg(&ks->scale[j - 1]) : 0.0;
+                    car = ar * sj;
+                    cai = ai * sj;
+                    cb = b * sp;
+                    ci = i;
+                    // the warp of the job's first tile records T_H's column j (a warp meets a
+                    // given job's first tile before any other of its tiles)
+                    if (t == I.tile0 && lane == 0) {
+                        ks->a_re[j] = ar;
+                        ks->a_im[j] = ai;
+                        ks->b_re[j] = b;
+                        ks->b_im[j] = 0.0;
+                        ks->hn[j] = sqrt(sa.x);
+                        A.ranB[i] = round + 1;  // 0 (cleared at launch) = never
+                    }
+                }
+                tile_orth<R, T>(A, I, i, t, j, car, cai, cb, sj);
+            }
+        }
+        if (!grid_sync(A, ph)) return false;
+        ++round;
+    }
 }
 
 // Lane k % 32 holds coefficient block k / 32 (k < 128): f * c_k with f = s0 scale_k, or
@@ -651,6 +702,174 @@ __device__ double tile_lincomb(const BArgs &A, const BInst &I, int t, int nvec, 
     return warp_sum(nrm);
 }
 
+// psi' = s0 sum_k c_k v_k for every job that took the step (norm partials for the next
+// step), optionally also into the history buffer.
+template <typename R, int T>
+__device__ void combine_phase(const BArgs &A, int rstep, unsigned ph) {
+    typedef typename cvec<R>::T C;
+    const int lane = threadIdx.x & 31;
+    int ci = -1, nvec = 0;
+    double cr[4], cim[4];
+    const bool hist = A.hist && ((rstep + 1) % A.hist_every) == 0;
+    for (int t = next_tile(A.ctl, ph); t < A.total_tiles; t = next_tile(A.ctl, ph)) {
+        const int i = inst_of_tile(A, t);
+        const KState *ks = A.ks + i;
+        const int st = ld_status(ks);
+        const BInst I = A.inst[i];
+        if (st != KS_CONVERGED && st != KS_HAPPY && st != KS_MAXDIM) {
+            tile_norm<R, T>(A, I, i, t);  // idle or failed: keep the state, refresh its norm
+            continue;
+        }
+        if (i != ci) {
+            nvec = __ldcg(&ks->nvec);
+            load_coefs(ks, nvec, false, cr, cim);
+            ci = i;
+        }
+        C *out = vec_ptr<C>(A, 0, I);
+        const double nrm = tile_lincomb<R, T>(A, I, t, nvec, cr, cim, out);
+        if (hist) {  // copy the new tile into the history slot
+            constexpr int AMP = 1 << (T - 5);
+            const long long base = (long long)(t - I.tile0) << T;
+            C *h = reinterpret_cast<C *>(A.hist) +
+                   (size_t)((rstep + 1) / A.hist_every - 1) * (size_t)A.hist_stride + I.off0;
+            __syncwarp();
+            for (int a = 0; a < AMP; ++a) h[base + lane + 32 * a] = out[base + lane + 32 * a];
+        }
+        if (lane == 0) A.partN[4 * (size_t)t] = nrm;
+        tile_done(A.cnt + 2 * A.ninst, A.partN, A.sumN, i, I.tile0, I.ntiles);
+    }
+}
+
+// ---------------------------------------------------------------- forward kernel
+template <typename R, int T, int MINB>
+__global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch(const BArgs A) {
+    __shared__ int s_flag;
+    const int lane = threadIdx.x & 31;
+    unsigned ph = 0;
+    int round = 0;  // phase-B rounds so far (the same in every CTA)
+    norm_phase<R, T>(A, ph);
+    if (!grid_sync(A, ph)) return;
+    for (int step = 0; step < A.run_steps; ++step) {
+        if (!krylov_rounds<R, T>(A, A.first_step + step, step, ph, round, s_flag)) return;
+        combine_phase<R, T>(A, step, ph);
+        if (!grid_sync(A, ph)) return;
+    }
+    if (threadIdx.x < 32) {  // final statuses
+        for (int i = blockIdx.x * 32 + lane; i < A.ninst; i += gridDim.x * 32) {
+            const int st = ld_status(A.ks + i);
+            const int f = A.fail[i];
+            A.status_out[i] = f ? f : (st == BS_IDLE ? KS_CONVERGED : st);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- the phase engine
+// Every job runs its own sequence of phases: the norm of its vector 0, then per step
+// A_0, B_0, A_1, B_1, ..., B_e (e: the decision that ends the step) and the combination
+// C; then the next step's A_0, and so on, until the job is idle.  A job's state word holds
+// the number of phases it completed and the code of its next phase; the warp that
+// completes a phase (the last of its tiles) takes the phase's decision and publishes the
+// next code.
+enum { PK_NORM = 0, PK_A = 1, PK_B = 2, PK_C = 3, PK_IDLE = 4 };
+constexpr int BCHUNK = 4;  // tiles a warp takes per visit
+
+__device__ __forceinline__ unsigned pcode(int kind, int rstep, int j) {
+    return (unsigned)kind << 24 | ((unsigned)rstep & 0xffffu) << 8 | (unsigned)j;
+}
+__device__ __forceinline__ int pkind(unsigned c) { return (int)(c >> 24); }
+__device__ __forceinline__ int prstep(unsigned c) { return (int)((c >> 8) & 0xffffu); }
+__device__ __forceinline__ int pj(unsigned c) { return (int)(c & 0xffu); }
+
+__device__ __forceinline__ unsigned long long ld_acq64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_rel64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_vol_u(const unsigned *p) { return *(volatile const unsigned *)p; }
+
+// Warp-collective bounded wait until job i completed `phi` phases or is idle; the state
+// word in w.  False once the wait ran out (it records EMUSV_TIMEOUT) or another warp
+// recorded an error.
+__device__ bool wait_phase(const BArgs &A, int i, unsigned phi, unsigned long long &w) {
+    unsigned long long v = 0;
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        v = ld_acq64(&A.jst[i]);
+        if ((unsigned)(v >> 32) < phi && pkind((unsigned)v) != PK_IDLE) {
+            const long long t0 = clock64();
+            for (int polls = 1;; ++polls) {
+                __nanosleep(64);
+                v = ld_acq64(&A.jst[i]);
+                if ((unsigned)(v >> 32) >= phi || pkind((unsigned)v) == PK_IDLE) break;
+                if ((polls & 15) == 0 && (clock64() - t0 > A.bar_limit || ld_vol(&A.ctl->err))) {
+                    atomicCAS(&A.ctl->err, 0, EMUSV_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    w = __shfl_sync(0xffffffffu, v, 0);
+    return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+// Phase phi of job i is complete: publish phase phi + 1 with code c, then open its tiles
+// (lane 0 of the completing warp; its tiles' writes and the phase's sums precede both
+// releases, and a warp whose take lands on the new phase finds its code published).
+__device__ void publish(const BArgs &A, int i, unsigned phi, unsigned c) {
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence();
+        st_rel64(&A.jst[i], (unsigned long long)(phi + 1) << 32 | c);
+        st_rel64(&A.take[i], (unsigned long long)(phi + 1) << 32);  // the new phase's tiles
+    }
+    __syncwarp();
+}
+
+// The job has no phase left in this launch: its final status, then the idle count.
+__device__ void job_idle(const BArgs &A, int i, unsigned phi) {
+    if ((threadIdx.x & 31) == 0) {
+        const int st = ld_status(A.ks + i);
+        const int f = ld_vol(&A.fail[i]);
+        A.status_out[i] = f ? f : (st == BS_IDLE ? KS_CONVERGED : st);
+    }
+    publish(A, i, phi, pcode(PK_IDLE, 0, 0));
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence();
+        atomicAdd(&A.ctl->idle, 1u);
+    }
+    __syncwarp();
+}
+
+// Start of step gstep for job i, from the norm of its vector 0 in sumN: the step's
+// Krylov state; true if the job iterates (false: idle, failed or a non-finite norm).
+__device__ bool job_init(const BArgs &A, int i, int gstep) {
+    int st = KS_RUNNING;
+    if ((threadIdx.x & 31) == 0) {
+        KState *ks = A.ks + i;
+        const double s0 = sqrt(__ldcg(A.sumN + 4 * (size_t)i));
+        const int f = ld_vol(&A.fail[i]);
+        if (f) st = f;
+        else if (gstep >= A.inst[i].nsteps) st = BS_IDLE;
+        else if (!(isfinite(s0) && s0 > 0.0)) st = KS_NONFINITE;
+        ks->s0 = s0;
+        ks->shift = 0.0;
+        ks->scale[0] = 1.0 / s0;
+        ks->iters = 0;
+        ks->nvec = 0;
+        ks->kerr = 0;
+        ks->err = 0.0;
+        A.polled[i] = 0;
+        ks->status = st;
+        if (st == KS_NONFINITE) A.fail[i] = st;
+    }
+    __syncwarp();
+    return __shfl_sync(0xffffffffu, st, 0) == KS_RUNNING;
+}
+
 // Combination tile of step rstep: psi' = s0 sum_k c_k v_k in place for a job whose step
 // ended with a result (optionally also into the history buffer), else (failed) the norm
 // of the kept state; the tile's norm partial.  True for the warp that completes the job.
@@ -697,22 +916,11 @@ __device__ int visit_job(const BArgs &A, int i, const BInst &I, unsigned long lo
                          unsigned &cphi, double (&c)[4]) {
     const int lane = threadIdx.x & 31;
     unsigned long long w = 0, tk = 0;
-    int gated = 0;
-    if (lane == 0) {
+    if (lane == 0) {  // the state and the take in one round trip (a take of an idle job is
+                      // never used)
+        tk = atomicAdd(&A.take[i], (unsigned long long)BCHUNK);
         w = ld_acq64(&A.jst[i]);
-        const unsigned c = (unsigned)w;
-        if (pkind(c) == PK_A && pj(c) == 0 && prstep(c) >= BSTEP_LEAD) {
-            // the step gate: a job starts step r only while the jobs still running have
-            // completed (r - BSTEP_LEAD) steps on average, so no job runs far ahead and
-            // the jobs with the most iterations are not left to finish alone (the job
-            // furthest behind is never gated)
-            const unsigned long long done = *(volatile unsigned long long *)&A.ctl->steps_done;
-            const unsigned live = (unsigned)A.ninst - ld_vol_u(&A.ctl->idle);
-            gated = done < (unsigned long long)(prstep(c) - BSTEP_LEAD) * live;
-        }
-        if (!gated && pkind(c) != PK_IDLE) tk = atomicAdd(&A.take[i], (unsigned long long)BCHUNK);
     }
-    if (__shfl_sync(0xffffffffu, gated, 0)) return V_BUSY;
     w = __shfl_sync(0xffffffffu, w, 0);
     tk = __shfl_sync(0xffffffffu, tk, 0);
     unsigned code = (unsigned)w, phi = (unsigned)(w >> 32);
@@ -787,7 +995,6 @@ __device__ int visit_job(const BArgs &A, int i, const BInst &I, unsigned long lo
             }
         } else {  // PK_C: the combination, then the next step
             if (tile_combine<R, T>(A, I, i, t, rstep)) {
-                if (lane == 0) atomicAdd(&A.ctl->steps_done, 1ull);
                 if (rstep + 1 < A.run_steps && job_init(A, i, A.first_step + rstep + 1))
                     publish(A, i, phi, pcode(PK_A, rstep + 1, 0));
                 else job_idle(A, i, phi);
@@ -845,9 +1052,11 @@ __device__ void run_jobs(const BArgs &A) {
     }
 }
 
-// ---------------------------------------------------------------- forward kernel
+// The forward steps by the phase engine (each job at its own pace, emusv_batch_set_engine
+// 1): the choice for batches whose registers need similar iteration counts, where the
+// lock-step rounds above spend little on waiting but the phases' finer-grained overlap wins.
 template <typename R, int T, int MINB>
-__global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch(const BArgs A) {
+__global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_phase(const BArgs A) {
     run_jobs<R, T>(A);
 }
 
@@ -921,8 +1130,10 @@ __global__ void __launch_bounds__(BWARPS * 32) k_batch_dS(const BArgs A, const B
     }
 }
 
-// The adjoint's Krylov bases of one step: the phase engine without the combination (the
-// launch sets first_step = the step, run_steps = 1, combine = 0).
+// The adjoint's Krylov bases of one step (the state's and the incoming gradient's per
+// instance): the phase engine without the combination (the launch sets first_step = the
+// step, run_steps = 1, combine = 0).  Each job runs norm, A_0, B_0, ... to its ending
+// decision at its own pace, with no round in which a finished job is passed over.
 template <typename R, int T, int MINB>
 __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_rounds(const BArgs A, const BAdj D) {
     run_jobs<R, T>(A);
@@ -1164,13 +1375,6 @@ __global__ void __launch_bounds__(BWARPS * 32, MINB) k_batch_adj_post(const BArg
 // ---------------------------------------------------------------- host side
 static size_t al256(size_t v) { return (v + 255) / 256 * 256; }
 
-// Integer region after the control block, per job: the state word and the take counter
-// (two ints each), fail, status, the tile counters (3) -- cleared by every launch -- then
-// hint and polled
-// (carried from one adjoint launch to the next), then the adjoint's counters (per instance).
-constexpr int BINTS_LAUNCH = 9;  // per-job ints every launch clears
-constexpr int BINTS_JOB = 11;    // per-job ints in all
-
 // Workspace layout.  Forward: one job per instance.  Adjoint: jobs 2i (state) and 2i+1
 // (gradient) per instance, plus the adjoint's own arrays.
 struct BLayout {
@@ -1203,13 +1407,14 @@ static bool layout(int ninst, const int *nq, const int *nsteps, int es, int T, i
     size_t off = 0;
     auto take = [&](size_t b) { const size_t o = off; off += al256(b); return o; };
     L->args = take(sizeof(BArgs));
-    // control block and integer region (BINTS_JOB per job, then the adjoint's counters),
-    // contiguous so that a launch clears them in one go; the state words are 8-byte
-    // aligned (the control block is 32 bytes)
+    // control block and integer flags, contiguous so that a launch clears them in one go:
+    // per job the phase engine's state and take words (two ints each, 8-byte aligned after
+    // the 32-byte control block), hint, polled, fail, status, ranB, cnt[3], then the
+    // adjoint's counters
     L->ctl = off;
     off += sizeof(BCtl);
     L->ints = off;
-    off += sizeof(int) * (BINTS_JOB * (size_t)nj + ninst);
+    off += sizeof(int) * (12 * (size_t)nj + ninst);
     off = al256(off);
     L->inst = take(sizeof(BInst) * nj);
     L->coef = take(sizeof(BCoef) * (coefs > 0 ? coefs : 1));
@@ -1240,11 +1445,13 @@ struct Shape {
     static constexpr int MINB = (sizeof(R) == 4 ? T >= 10 : T >= 9) ? 1 : 2;
 };
 
-// kind 0: forward; 1: adjoint rounds; 2: adjoint post-processing
+// kind 0: forward (lock-step rounds); 1: adjoint rounds; 2: adjoint post-processing;
+// 3: forward (phase engine)
 static void *pick_kernel(int dtype, int T, int kind) {
 #define EMUSV_K(R, TT)                                                                   \
     (kind == 1   ? reinterpret_cast<void *>(k_batch_adj_rounds<R, TT, Shape<R, TT>::MINB>) \
      : kind == 2 ? reinterpret_cast<void *>(k_batch_adj_post<R, TT, Shape<R, TT>::MINB>)   \
+     : kind == 3 ? reinterpret_cast<void *>(k_batch_phase<R, TT, Shape<R, TT>::MINB>)      \
                  : reinterpret_cast<void *>(k_batch<R, TT, Shape<R, TT>::MINB>))
     if (dtype == EMUSV_C64) {
         if (T == 8) return EMUSV_K(float, 8);
@@ -1258,6 +1465,20 @@ static void *pick_kernel(int dtype, int T, int kind) {
     return nullptr;
 }
 
+// Dynamic shared memory of a kernel kind: the H v phase's partner-tile stages (kinds 0
+// and 1; the post-processing kernel has none).  Set as the kernel's limit before its
+// occupancy is queried or it is launched.
+static size_t kernel_smem(int dtype, int T, int kind) {
+    if (kind == 2) return 0;
+    const size_t es = dtype == EMUSV_C128 ? 16 : 8;
+    return (size_t)BWARPS * PSTAGES * (es << T);
+}
+static int configure_smem(void *kern, size_t smem) {
+    if (!smem) return EMUSV_OK;
+    EMUSV_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return EMUSV_OK;
+}
+
 // Host copies of the argument blocks prepared per workspace (launches pass them by value,
 // so the kernel reads them from the parameter bank).
 struct Prepared {
@@ -1265,6 +1486,7 @@ struct Prepared {
     BAdj D;
     BLayout L;
     bool adjoint;
+    int engine;  // forward launches: 0 lock-step rounds, 1 phase engine
 };
 static std::mutex g_args_mu;
 static std::unordered_map<const void *, Prepared> g_args;
@@ -1281,6 +1503,12 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
         return EMUSV_BAD_ARGUMENT;
     for (int i = 0; i < ninst; ++i)
         if (!isfinite(dt[i])) return EMUSV_BAD_ARGUMENT;
+    // the shared-memory limits of the kernels the launches may use (host calls, so that a
+    // launch recorded into a CUDA graph issues none)
+    for (int kind : {0, 1, 3}) {
+        const int st = configure_smem(pick_kernel(dtype, T, kind), kernel_smem(dtype, T, kind));
+        if (st) return st;
+    }
     const int es = dtype == EMUSV_C128 ? 16 : 8;
     BLayout L;
     if (!layout(ninst, nqubits, nsteps, es, T, capacity, adjoint, &L)) return EMUSV_BAD_ARGUMENT;
@@ -1380,11 +1608,12 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
     int *ints = reinterpret_cast<int *>(ws + L.ints);
     A.jst = reinterpret_cast<unsigned long long *>(ints);
     A.take = reinterpret_cast<unsigned long long *>(ints + 2 * nj);
-    A.fail = ints + 4 * nj;
-    A.status_out = ints + 5 * nj;
-    A.cnt = reinterpret_cast<unsigned *>(ints + 6 * nj);
-    A.hint = ints + BINTS_LAUNCH * nj;
-    A.polled = ints + (BINTS_LAUNCH + 1) * nj;
+    A.hint = ints + 4 * nj;
+    A.polled = ints + 5 * nj;
+    A.fail = ints + 6 * nj;
+    A.status_out = ints + 7 * nj;
+    A.ranB = ints + 8 * nj;
+    A.cnt = reinterpret_cast<unsigned *>(ints + 9 * nj);
     double *sums = reinterpret_cast<double *>(ws + L.sums);
     A.sumA = sums;
     A.sumB = sums + 4 * nj;
@@ -1403,9 +1632,9 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
     A.hist = nullptr;
     A.hist_every = 1;
     A.hist_stride = L.inst_amps;
-    A.combine = adjoint ? 0 : 1;
     A.bar_limit = BAR_LIMIT;
-    A.test_hold = 0;
+    A.test_skip_arrival = 0;
+    A.combine = adjoint ? 0 : 1;
     if (adjoint) {
         BAdj &D = P.D;
         D.ninst = ninst;
@@ -1414,14 +1643,14 @@ static int prepare_common(int ninst, const int *nqubits, const int *nsteps, cons
         D.E = ws + L.E;
         D.inst_amps = L.inst_amps;
         D.partC = reinterpret_cast<double *>(ws + L.partC);
-        D.cntC = reinterpret_cast<unsigned *>(ints + BINTS_JOB * nj);
+        D.cntC = reinterpret_cast<unsigned *>(ints + 12 * nj);
     }
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.args, &A, sizeof(A), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.inst, inst.data(), sizeof(BInst) * nj, cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.coef, coef.data(), sizeof(BCoef) * coef.size(), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.ubits, ub.data(), sizeof(double) * ub.size(), cudaMemcpyHostToDevice, s));
     EMUSV_CHECK(cudaMemcpyAsync(ws + L.elow, elow.data(), sizeof(double) * elow.size(), cudaMemcpyHostToDevice, s));
-    EMUSV_CHECK(cudaMemsetAsync(ws + L.ctl, 0, sizeof(BCtl) + sizeof(int) * (BINTS_JOB * (size_t)nj + ninst), s));
+    EMUSV_CHECK(cudaMemsetAsync(ws + L.ctl, 0, sizeof(BCtl) + sizeof(int) * (12 * (size_t)nj + ninst), s));
     EMUSV_CHECK(cudaStreamSynchronize(s));  // the host tables go out of scope
     {
         std::lock_guard<std::mutex> g(g_args_mu);
@@ -1439,9 +1668,9 @@ static int lookup(const void *workspace, bool adjoint, Prepared *out) {
 }
 
 static int cooperative_launch(void *kern, int blocks_per_sm, void **args, cudaStream_t s,
-                              int *grid_out, int prof_kind = PROF_BATCH) {
+                              int *grid_out, int prof_kind = PROF_BATCH, size_t smem = 0) {
     int per_sm = 0;
-    EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BWARPS * 32, 0));
+    EMUSV_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BWARPS * 32, smem));
     if (per_sm < 1) return EMUSV_CUDA_ERROR;
     const int bps = blocks_per_sm < per_sm ? blocks_per_sm : per_sm;
     const int grid = bps * sm_count();
@@ -1450,7 +1679,7 @@ static int cooperative_launch(void *kern, int blocks_per_sm, void **args, cudaSt
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(BWARPS * 32);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -1496,11 +1725,14 @@ int emusv_batch_prepare(int ninst, const int *nqubits, const int *nsteps, const 
 int emusv_batch_launch_steps(int dtype, int tile_bits, int blocks_per_sm, int first_step,
                              int steps, void *states, void *history, int history_every,
                              void *workspace, void *stream) {
-    void *kern = pick_kernel(dtype, tile_bits, 0);
     Prepared P;
-    if (!kern || !workspace || blocks_per_sm < 1 || lookup(workspace, false, &P)) return EMUSV_BAD_ARGUMENT;
+    if (!workspace || blocks_per_sm < 1 || lookup(workspace, false, &P)) return EMUSV_BAD_ARGUMENT;
+    const int kind = P.engine ? 3 : 0;
+    void *kern = pick_kernel(dtype, tile_bits, kind);
+    if (!kern) return EMUSV_BAD_ARGUMENT;
     BArgs A = P.A;
-    if (first_step < 0 || steps < 1 || steps > 65535 || first_step + steps > P.L.max_steps || history_every < 1 ||
+    if (first_step < 0 || steps < 0 || (P.engine && (steps < 1 || steps > 65535)) ||
+        first_step + steps > P.L.max_steps || history_every < 1 ||
         (states && (reinterpret_cast<uintptr_t>(states) & 15)))
         return EMUSV_BAD_ARGUMENT;
     if (A.T != tile_bits) return EMUSV_BAD_ARGUMENT;
@@ -1511,11 +1743,22 @@ int emusv_batch_launch_steps(int dtype, int tile_bits, int blocks_per_sm, int fi
     A.hist_every = history_every;
     cudaStream_t s = as_stream(stream);
     unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
-    // control block, job states, flags, hints and tile counters start at zero (every
-    // job's first phase: the norm of its vector 0)
-    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * BINTS_JOB * (size_t)A.ninst, s));
+    // control block, flags, hints and tile counters start at zero
+    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * 12 * (size_t)A.ninst, s));
     void *args[] = {(void *)&A};
-    return cooperative_launch(kern, blocks_per_sm, args, s, nullptr);
+    return cooperative_launch(kern, blocks_per_sm, args, s, nullptr, PROF_BATCH,
+                              kernel_smem(dtype, tile_bits, kind));
+}
+
+// Scheduling of a prepared forward workspace's launches: 0 (default) lock-step rounds,
+// 1 the phase engine.  Host-side only (takes effect at the next launch).
+int emusv_batch_set_engine(void *workspace, int engine) {
+    if (!workspace || engine < 0 || engine > 1) return EMUSV_BAD_ARGUMENT;
+    std::lock_guard<std::mutex> g(g_args_mu);
+    auto it = g_args.find(workspace);
+    if (it == g_args.end() || it->second.adjoint) return EMUSV_BAD_ARGUMENT;
+    it->second.engine = engine;
+    return EMUSV_OK;
 }
 
 // Clears the control block and launches the persistent kernel over every step on the
@@ -1531,8 +1774,10 @@ int emusv_batch_launch(int dtype, int tile_bits, int blocks_per_sm, void *worksp
 int emusv_batch_max_blocks_per_sm(int dtype, int tile_bits) {
     void *kern = pick_kernel(dtype, tile_bits, 0);
     if (!kern) return 0;
+    const size_t smem = kernel_smem(dtype, tile_bits, 0);
+    if (configure_smem(kern, smem)) return 0;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BWARPS * 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BWARPS * 32, smem) != cudaSuccess)
         return 0;
     return per_sm;
 }
@@ -1607,20 +1852,21 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
     A.v0[0] = const_cast<void *>(states);
     A.v0[1] = const_cast<void *>(grad_in);
     D.step = step;
-    A.first_step = step;  // the engine's one "step": the bases of this adjoint step
+    A.first_step = step;  // the phase engine's one "step": the bases of this adjoint step
     A.run_steps = 1;
     D.grads = grads_dev;
     D.gout = grad_out;
     D.astatus = status_dev;
     cudaStream_t s = as_stream(stream);
     unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
-    // clear the control block, job states, flags and counters (the hints and polled flags
-    // carry from one step to the next)
+    // clear the control block and everything after the hints and polled flags (the
+    // hints carry from one step to the next)
     const int nj = A.ninst;
-    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * BINTS_LAUNCH * (size_t)nj, s));
-    EMUSV_CHECK(cudaMemsetAsync(D.cntC, 0, sizeof(unsigned) * D.ninst, s));
+    EMUSV_CHECK(cudaMemsetAsync(ws + P.L.ctl, 0, sizeof(BCtl) + sizeof(int) * 4 * (size_t)nj, s));
+    EMUSV_CHECK(cudaMemsetAsync(A.fail, 0, sizeof(int) * (6 * (size_t)nj + D.ninst), s));
     void *args[] = {(void *)&A, (void *)&D};
-    int st = cooperative_launch(k1, blocks_per_sm, args, s, nullptr);
+    int st = cooperative_launch(k1, blocks_per_sm, args, s, nullptr, PROF_BATCH,
+                                kernel_smem(dtype, tile_bits, 1));
     if (st) return st;
     {
         ProfScope ps_(PROF_ADJOINT, s);
@@ -1633,17 +1879,16 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
 }
 
 // Failure-path test switch of a prepared workspace (forward or adjoint): later launches
-// wait at most wait_cycles clock cycles for a job's previous phase or at a grid barrier
-// (<= 0: the default, about 1 s) and, when skip_first_arrival != 0, the completion of job
-// 0's first phase is never published (its tiles' work "does not arrive"), so the waits for
-// job 0's next phase run out and the launch reports EMUSV_TIMEOUT.
+// wait at most wait_cycles clock cycles at a grid barrier (<= 0: the default, about 1 s)
+// and, when skip_first_arrival != 0, the last CTA does not arrive at each launch's first
+// barrier, so the others' bounded waits run out and the launch reports EMUSV_TIMEOUT.
 int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival) {
     if (!workspace) return EMUSV_BAD_ARGUMENT;
     std::lock_guard<std::mutex> g(g_args_mu);
     auto it = g_args.find(workspace);
     if (it == g_args.end()) return EMUSV_BAD_ARGUMENT;
     it->second.A.bar_limit = wait_cycles > 0 ? wait_cycles : BAR_LIMIT;
-    it->second.A.test_hold = skip_first_arrival ? 1 : 0;
+    it->second.A.test_skip_arrival = skip_first_arrival ? 1 : 0;
     return EMUSV_OK;
 }
 

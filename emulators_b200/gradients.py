@@ -39,7 +39,7 @@ class PulseGradientBatch:
                  precision: str = "c128", checkpoint_every: int = 16, tolerance: float = 1e-10,
                  max_krylov_dim: int = 100, capacity: int | None = None,
                  tile_bits: int | None = None,
-                 blocks_per_sm: int = 1, device="cuda"):
+                 blocks_per_sm: int = 1, device="cuda", engine: int = 1):
         self.U = np.ascontiguousarray(U, dtype=np.float64)
         self.n = self.U.shape[0]
         self.dt = float(dt)
@@ -57,6 +57,10 @@ class PulseGradientBatch:
         self.capacity = int(min(capacity or max_krylov_dim, max_krylov_dim))
         self.T = tile_bits or (9 if self.n >= 9 else 8)
         self.bps = int(blocks_per_sm)
+        # forward scheduling (emusv_batch_set_engine): the parameter sets are registers of
+        # one size with similar iteration counts, where each register's own phase sequence
+        # beats lock-step rounds
+        self.engine = int(engine)
         self.device = torch.device(device)
         if self.n > BMAXQ or self.n < self.T:
             raise ValueError(f"register of {self.n} qubits outside the batched range")
@@ -96,6 +100,7 @@ class PulseGradientBatch:
         _lib.check(L.emusv_batch_prepare(*args, self.states.data_ptr(), self.tol, self.tol,
                                          self.maxdim, self.T, self.capacity, self.ws_f.data_ptr(),
                                          nf, stream), "batch prepare")
+        _lib.check(L.emusv_batch_set_engine(self.ws_f.data_ptr(), self.engine), "batch engine")
         _lib.check(L.emusv_batch_adjoint_prepare(*args, self.tol, self.maxdim, self.T, self.capacity,
                                                  self.ws_a.data_ptr(), na, stream),
                    "batch adjoint prepare")

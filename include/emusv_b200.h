@@ -335,13 +335,20 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
 /* Krylov iteration counts of the last adjoint launch, [ninst][2] (state basis, gradient
  * basis), to a host array.  Synchronises the stream. */
 int emusv_batch_adjoint_iterations(int ninst, void *workspace, int *iterations_out, void *stream);
+/* Scheduling of a prepared forward batch workspace (no counterpart in the reference):
+ * engine 0 (the default) runs every register's Lanczos iterations in lock-step rounds of
+ * the whole batch, engine 1 lets each register run its own sequence of phases (norm,
+ * H v, recurrence, ..., combination) with no grid barrier.  Results are the same; the
+ * faster one depends on the batch (BatchEvolution's autotuner times both).  Host-side
+ * only (takes effect at the next launch); EMUSV_BAD_ARGUMENT for an adjoint workspace. */
+int emusv_batch_set_engine(void *workspace, int engine);
 /* Failure-path test switch of a prepared batch workspace (forward or adjoint; no
  * counterpart in the reference, whose loop has no device-side waits): later launches wait
- * at most wait_cycles SM clock cycles for a job's previous phase or at a grid barrier
- * (<= 0 restores the default, about 1 s), and with skip_first_arrival != 0 the completion
- * of job 0's first phase is never published, so every wait for job 0's next phase runs
- * out, all warps return and emusv_batch_results reports EMUSV_TIMEOUT; the device stays
- * usable.  Off by default; for tests.  Host-side only (takes effect at the next launch). */
+ * at most wait_cycles SM clock cycles at a grid barrier (<= 0 restores the default, about
+ * 1 s), and with skip_first_arrival != 0 the last CTA does not arrive at each launch's
+ * first barrier, so every other CTA's bounded wait runs out, all CTAs return and
+ * emusv_batch_results reports EMUSV_TIMEOUT; the device stays usable.  Off by default;
+ * for tests.  Host-side only (takes effect at the next launch). */
 int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival);
 
 /* ---- building blocks of the generic krylov_exp(op, v, ...) (krylov_exp.py:23-106) ----

@@ -47,15 +47,18 @@ def _oracle_chain(oracle, r):
     return s, its
 
 
+@pytest.mark.parametrize("engine", [0, 1])
 @pytest.mark.parametrize("tile_bits", [8, 9])
-def test_batch_c128_matches_oracle(oracle, tile_bits):
-    """Uneven registers and step counts, complex phases: every instance's final state
-    and every step's Krylov iteration count equal the oracle's chain."""
+def test_batch_c128_matches_oracle(oracle, tile_bits, engine):
+    """Uneven registers and step counts, complex phases, both scheduling engines (lock-step
+    rounds, per-register phases): every instance's final state and every step's Krylov
+    iteration count equal the oracle's chain."""
     from emulators_b200.batch import BatchEvolution
 
     regs = _random_batch([9, 13, 10, 12, 11, 9], [7, 12, 10, 5, 11, 12], seed=3, phase=True)
     b = BatchEvolution(regs, precision="c128", max_krylov_dim=100)
-    status, iters = b.run(tune=False, tile_bits=tile_bits, blocks_per_sm=1, capacity=40)
+    status, iters = b.run(tune=False, tile_bits=tile_bits, blocks_per_sm=1, capacity=40,
+                          engine=engine)
     assert (status == 0).all()
     for i, r in enumerate(regs):
         ref, its = _oracle_chain(oracle, r)

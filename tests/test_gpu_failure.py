@@ -1,10 +1,9 @@
 """Failure paths on the GPU, in forms that fault no GPU.
 
-* A bounded device wait made to run out: the batched engine's wait for a job's previous
-  phase, with a short wait limit and one phase completion that never arrives
-  (emusv_batch_set_barrier_test).  Every waiting warp gives up, the launch reports
-  EMUSV_TIMEOUT (TimeoutError), and the same workspace then runs the batch and matches the
-  oracle.
+* A bounded device wait made to run out: the batched engine's grid barrier with a short
+  wait limit and one CTA that never arrives (emusv_batch_set_barrier_test).  Every other
+  CTA gives up, the launch reports EMUSV_TIMEOUT (TimeoutError), and the same workspace then
+  runs the batch and matches the oracle.
 * A non-finite state, copied in from a host buffer holding a NaN: the Lanczos step, the
   Arnoldi step and the adjoint step report EMUSV_NONFINITE, raised as NonFiniteError -- a
   FloatingPointError and, like the reference's Lanczos loop, which never converges on such a
@@ -62,7 +61,7 @@ def test_batch_barrier_timeout_then_recovers(oracle):
     b = BatchEvolution(regs, precision="c128", max_krylov_dim=100)
     b.reset()
     b.prepare(8, 40)
-    # a wait of 2e6 SM cycles (about 1 ms) for a phase completion that never arrives
+    # a wait of 2e6 SM cycles (about 1 ms) with one CTA that never arrives
     b.set_barrier_test(wait_cycles=2_000_000, skip_first_arrival=True)
     b.launch(1)
     with pytest.raises(TimeoutError):
