@@ -501,7 +501,7 @@ def ladder_c128(dev, W: int, K: int = 6) -> dict:
             "note": "complex128 vectors, same kernels and step window as the complex64 headline"}
 
 
-# ------------------------------------------------------------------ config 2: N=20 lattice
+# ------------------------------------------------------------------ the N=20 4x5 lattice
 def lattice_c2(dev, plain_budget_s: float = 20.0) -> dict:
     """The plain-method drop-in configuration: N=20 4x5 lattice at 6 um, sin^2 Omega (peak
     2 pi), delta -15 -> 15 over 3 us, dt = 10 ns (300 steps), complex128, Krylov dim <= 30,
@@ -946,8 +946,26 @@ def grads_c5(dev) -> dict:
     ps = 2 * gw.steps_per_segment
     plain = plain_torch_grads_c128(gw, dev, p=0, steps=ps)
     plain_gps = 1.0 / (plain["s"] * b.nsteps / ps)
+    # algorithmic bytes, an estimate from the recorded forward iteration counts m per
+    # set-step (vectors of D s = 2^16 x 16 bytes): a Lanczos basis of m iterations streams
+    # (7 m + 1) D s; each step's basis is built by the forward, again by the checkpoint
+    # recomputation (all steps but the last of a segment), and twice by the adjoint (the
+    # state's basis, of the forward's size, and the incoming gradient's, taken as the same
+    # size); the adjoint's post-processing reads both bases and writes and reads the E
+    # vectors, (m + 3 m) D s
+    m = np.asarray(b.forward_iterations, dtype=np.float64)
+    Ds = float(1 << n) * 16.0
+    last = (np.arange(b.nsteps) % b.ck) == b.ck - 1
+    lz = (7.0 * m + 1.0) * Ds
+    alg = float(lz.sum() + lz[:, ~last].sum() + 2.0 * lz.sum() + (4.0 * m * Ds).sum())
+    peak, src = peaks()
+    roof = {"algorithmic_bytes": alg, "achieved": round(alg / el / 1e9, 1), "peak": peak,
+            "peak_source": src, "unit": "GB/s", "frac": round(alg / el / 1e9 / peak, 4),
+            "note": "estimate: forward, recomputation and the two adjoint bases at (7 m + 1) "
+                    "D s each from the forward's iteration counts, plus 4 m D s of "
+                    "post-processing per set-step"}
     return {"sets": b.nsets, "steps": b.nsteps, "s": round(el, 3),
-            "grads_per_s": round(b.nsets / el, 3), "max_krylov_dim": kd,
+            "grads_per_s": round(b.nsets / el, 3), "max_krylov_dim": kd, "roofline": roof,
             "plain_torch_c128_gpu": {
                 "sample": f"set 0, steps 0..{ps - 1} forward and backward (loss after step "
                           f"{ps - 1}), the reference's per-step backward in plain torch ops, "

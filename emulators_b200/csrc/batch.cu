@@ -12,9 +12,10 @@
 //    global counter (dynamic balance; neighbouring tiles run together, so partner tiles of
 //    the bits above T are read from L2).
 //  * a warp owns a tile: lane bits (tile bits 0-4) flip by shuffles, register bits (5..T-1)
-//    inside the thread, bits >= T by coalesced loads of the partner tile; the diagonal is
-//    rebuilt from an FP64 per-instance table of the low-bit pair energies plus per-tile
-//    fields of the high bits.
+//    inside the thread, bits >= T from the partner tiles, staged through the warp's
+//    shared-memory stages by cp.async (three in flight); the diagonal is rebuilt from an
+//    FP64 per-instance table of the low-bit pair energies plus per-tile fields of the high
+//    bits.
 //  * per Lanczos iteration j, two grid-wide phases: A_j (H v_j for every running
 //    instance, FP64 partials of ||Hv||^2 and <v_j,Hv>) and B_j (three-term recurrence and
 //    partials of ||w||^2, <v_j,w>).  The per-instance decision for iteration j (norm,
@@ -28,6 +29,15 @@
 //  * convergence is tested from a per-instance hint (the previous step's count - 3); a
 //    first test that already converges tests the skipped iterations in order
 //    (krylov_decide), so each instance stops where the reference would.
+//  * a second scheduler, the phase engine (run_jobs, below), lets every register run its
+//    own sequence of phases -- norm, A_0, B_0, ..., B_e, combination -- with no grid
+//    barrier: warps visit registers in proportion to their size and take tiles of the
+//    visited register's current phase from its take counter.  It builds the adjoint's
+//    two bases per step (k_batch_adj_rounds) and is a forward choice
+//    (emusv_batch_set_engine; BatchEvolution's autotuner times both).  The lock-step
+//    rounds win on batches of uneven registers (256 registers of 12-18 qubits, 150
+//    steps: 0.79 s against 0.92 s), the phases on uniform ones (64 registers of 16 qubits,
+//    the gradient batch's forward).
 #include <math.h>
 #include <string.h>
 

@@ -68,8 +68,8 @@ def test_batch_c128_matches_oracle(oracle, tile_bits, engine):
 
 
 def test_batch_c128_large_registers_match_oracle(oracle):
-    """The top of the batched size range (config 4 draws 12-18 qubits; the engine takes up
-    to 20): complex128 registers of 14, 16, 18 and 20 qubits with complex phases against
+    """The top of the batched size range (the 256-register batch draws 12-18 qubits; the
+    engine takes up to 20): complex128 registers of 14, 16, 18 and 20 qubits with complex phases against
     the oracle's chain, states and every step's Krylov iteration count."""
     from emulators_b200.batch import BatchEvolution
 
