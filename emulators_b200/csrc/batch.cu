@@ -142,7 +142,7 @@ constexpr int NCP = 6 * BMAXQ;  // per bit: T_re, T_im, U_re, U_im, S_re, S_im
 // phase after next.  Returns false (and every CTA then returns) on a timeout: a wait
 // gives up after A.bar_limit clock cycles or as soon as another CTA recorded an error.
 __device__ bool grid_sync(const BArgs &A, unsigned &ph) {
-    __shared__ int s_ok;  // the CTA's verdict, read by every thread (all return together)
+    __shared__ int s_ok;  // the CTA's outcome, read by every thread (all return together)
     BCtl *ctl = A.ctl;
     __syncthreads();
     if (threadIdx.x == 0) {
