@@ -594,8 +594,8 @@ def precision_check(w, dev) -> dict:
             "c128_steps_per_s_untimed_loop": round(rates[torch.complex128], 3),
             "note": "errors of the complex64 run against this package's complex128 run of "
                     "the same kernels (not against the FP64 oracle, which cannot run 400 "
-                    "steps at N=26; the complex128 path matches the oracle's steps to "
-                    "1e-10 and better in the GPU tests up to N=22)"}
+                    "steps at N=26; the complex128 steps match the oracle's to 1e-10 in "
+                    "the GPU tests, up to N=23)"}
 
 
 # ------------------------------------------------------------------ plain complex128 GPU path
