@@ -257,23 +257,17 @@ k_small(KState *ks, int j, const double *part_o, int nb_o, double dt, double exp
 // (0 ||w||^2, 1-2 <v_j, w>, 3 ||(H - sigma) v_j||^2, 4 the pass-L part of <w, (H - sigma) w>)
 // ||H v_j||, ||w||, <v_{j+1}, v_j>, scale_{j+1} and the next el -- everything iteration
 // j+1 needs -- and the outcome flag; no status change.
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(BLOCK)
 k_lz_norms(KState *ks, int j, const double *part_o, int nb_o, double dt, double norm_tol) {
     if (ks->status != KS_RUNNING) return;
+    // the whole block sums the partial rows (one row or two per thread, all loads in
+    // flight at once), then warp 0 decides
+    __shared__ double red[(BLOCK / 32) * NRED];
+    double sums[NRED];
+    sum_partials<NRED>(part_o, nb_o, NRED, sums, red);
+    if (threadIdx.x >= 32) return;
     const int lane = threadIdx.x;
-    double v = 0.0, vr = 0.0, vi = 0.0, hh = 0.0, el = 0.0;
-    for (int b = lane; b < nb_o; b += 32) {
-        v += part_o[(i64)b * NRED];
-        vr += part_o[(i64)b * NRED + 1];
-        vi += part_o[(i64)b * NRED + 2];
-        hh += part_o[(i64)b * NRED + 3];
-        el += part_o[(i64)b * NRED + 4];
-    }
-    v = warp_sum(v);
-    vr = warp_sum(vr);
-    vi = warp_sum(vi);
-    hh = warp_sum(hh);
-    el = warp_sum(el);
+    const double v = sums[0], vr = sums[1], vi = sums[2], hh = sums[3], el = sums[4];
     if (lane == 0) {
         // ||H v||^2 = ||(H - sigma) v||^2 + 2 sigma Re<v,(H - sigma) v> + sigma^2
         const double sg = ks->shift;
@@ -668,7 +662,7 @@ int lanczos_run(const HamParams &P, int dtype, double dt, const void *v0, KState
             if ((st = lz_low(dtype, P, B, s, &go))) return st;
             {
                 ProfScope ps_(PROF_SMALL, s);
-                k_lz_norms<<<1, 32, 0, s>>>(W.ks, j, W.part_o, go, dt, norm_tolerance);
+                k_lz_norms<<<1, BLOCK, 0, s>>>(W.ks, j, W.part_o, go, dt, norm_tolerance);
             }
             EMUSV_CHECK_LAUNCH();
             if (overlap) {
