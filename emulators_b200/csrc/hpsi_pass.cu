@@ -271,8 +271,11 @@ template <typename R> static int lz_chunk_bits(int n) {
 // The two pass H groups of the Lanczos iteration run as two launches unless
 // EMUSV_FUSED_PASS_H=1 selects the fused persistent kernel (k_pass_hh).  Measured on B200 at
 // N=26 complex64: the fused kernel moves about 2 vector units of DRAM traffic instead of 5
-// but takes 0.90 ms against 0.49 ms for the two launches -- its tiles wait on thread 0's
-// gpu-scope fences (each drains that thread's own stores) and on the work counter.
+// and leaves the sums in the L2 for the recurrence pass L (0.383 against 0.409 ms), but
+// takes 0.556 ms against 0.509 ms for the two launches (its tile work compiled per group;
+// 0.90 ms when the group was a run-time branch of the amplitude loop): it executes the same
+// instructions at a lower issue rate, waiting at each tile's block barrier for the
+// completion counting and the next take.  Iteration 0.955 against 0.935 ms.
 static bool hh_forced_off() {
     static int v = -1;
     if (v < 0) {

@@ -888,12 +888,14 @@ k_pass_hh(const PassParams P, HHArgs A, const __grid_constant__ PassHHMaps M) {
         // the tile is here; everyone is done with the previous buffer and has issued the
         // previous tile's stores
         __syncthreads();
+        // warp 1 counts the previous group-1 tile (its fence waits for the block's stores)
+        // while thread 0 takes the next item, so the two serial chains overlap
+        if (tid == 32 && pend >= 0) {
+            __threadfence();
+            atomicAdd(A.cnt + pend, 1u);
+        }
+        pend = -1;
         if (tid == 0) {
-            if (pend >= 0) {
-                __threadfence();
-                atomicAdd(A.cnt + pend, 1u);
-            }
-            pend = -1;
             const int64_t qt = (int64_t)next_q;
             if (ok && qt < nitems) next_q = atomicAdd(next_item, 1u);
             if (ok) take(buf == 0 ? SH - 1 : buf - 1, qt);
@@ -924,12 +926,15 @@ k_pass_hh(const PassParams P, HHArgs A, const __grid_constant__ PassHHMaps M) {
             pph ^= 1u << buf;
         }
         if (A.err && *(volatile int *)A.err) ok = false;
-        if (ok) {
+        // the tile's work, compiled once per group (GRP 1 or 2) so that the group tests
+        // leave the amplitude loop
+        auto work = [&](auto grp_c) {
+            constexpr int GRP = decltype(grp_c)::value;
             // this group's geometry: tile bit k < c is bit k of x, k >= c bit hpos + k - c;
             // applied: group 1 the bits [hs, hpos2), group 2 all its bits and the chunk bits
-            uint32_t apply = grp == 2 ? (1u << c) - 1u : 0u;
+            uint32_t apply = GRP == 2 ? (1u << c) - 1u : 0u;
             for (int k = c; k < TB; ++k)
-                if (grp == 2 || hpos + k - c < A.hpos2) apply |= 1u << k;
+                if (GRP == 2 || hpos + k - c < A.hpos2) apply |= 1u << k;
             R cr_s[SB], ci_s[SB];
 #pragma unroll
             for (int k = 0; k < SB; ++k) {
@@ -949,10 +954,11 @@ k_pass_hh(const PassParams P, HHArgs A, const __grid_constant__ PassHHMaps M) {
                 dr_r[k] = on ? Coef<R>::dre(P, p) : R(0);
                 di_r[k] = on ? Coef<R>::dim(P, p) : R(0);
             }
-            const int64_t base = grp == 1 ? ((s << c) | (t << (hpos + g))) : ((s | (t << nsb)) << c);
+            const int64_t base = GRP == 1 ? ((s << c) | (t << (hpos + g))) : ((s | (t << nsb)) << c);
             const int64_t xt = (tid & cmask) + ((int64_t)(tid >> c) << hpos);
             const int ash = hpos + SB - c;
-            float rf[2] = {0.f, 0.f};
+            float rf[2] = {0.f, 0.f};  // complex64: per-tile FP32 sums
+            (void)rf;
             C v[NA];
 #pragma unroll
             for (int a = 0; a < NA; ++a) v[a] = tile[tid + a * NT];
@@ -974,7 +980,7 @@ k_pass_hh(const PassParams P, HHArgs A, const __grid_constant__ PassHHMaps M) {
                 }
                 if constexpr (std::is_same<R, float>::value) {
                     const float2 tt = upk2(acc.a);
-                    if (grp == 2) {
+                    if constexpr (GRP == 2) {
                         const C pt = ptile[l];
                         outp[x] = make_float2(pt.x + tt.x, pt.y + tt.y);
                     } else {
@@ -984,7 +990,7 @@ k_pass_hh(const PassParams P, HHArgs A, const __grid_constant__ PassHHMaps M) {
                     rf[1] = fmaf(v[a].x, tt.y, fmaf(-v[a].y, tt.x, rf[1]));
                 } else {
                     const double tr = acc.re(), ti = acc.im();
-                    if (grp == 2) {
+                    if constexpr (GRP == 2) {
                         const C pt = ptile[l];
                         outp[x] = cmake<C>(double(pt.x) + tr, double(pt.y) + ti);
                     } else {
@@ -999,6 +1005,10 @@ k_pass_hh(const PassParams P, HHArgs A, const __grid_constant__ PassHHMaps M) {
                 red[0] += double(rf[0]);
                 red[1] += double(rf[1]);
             }
+        };
+        if (ok) {
+            if (grp == 1) work(std::integral_constant<int, 1>{});
+            else work(std::integral_constant<int, 2>{});
             if (grp == 1) pend = s;  // counted after the next block barrier
         }
         if (++buf == SH) buf = 0;
