@@ -829,9 +829,11 @@ __device__ bool wait_phase(const BArgs &A, int i, unsigned phi, unsigned long lo
 
 // Phase phi of job i is complete: publish phase phi + 1 with code c, then open its tiles
 // (lane 0 of the completing warp; its tiles' writes and the phase's sums precede both
-// releases, and a warp whose take lands on the new phase finds its code published).
+// releases, and a warp whose take lands on the new phase finds its code published).  The
+// failure-path test switch withholds job 0's first publication: no warp then finds work
+// for job 0 again, and every warp's starvation limit runs out.
 __device__ void publish(const BArgs &A, int i, unsigned phi, unsigned c) {
-    if ((threadIdx.x & 31) == 0) {
+    if ((threadIdx.x & 31) == 0 && !(A.test_skip_arrival && i == 0 && phi == 0)) {
         __threadfence();
         st_rel64(&A.jst[i], (unsigned long long)(phi + 1) << 32 | c);
         st_rel64(&A.take[i], (unsigned long long)(phi + 1) << 32);  // the new phase's tiles
@@ -1889,9 +1891,11 @@ int emusv_batch_adjoint_launch(int dtype, int tile_bits, int blocks_per_sm, int 
 }
 
 // Failure-path test switch of a prepared workspace (forward or adjoint): later launches
-// wait at most wait_cycles clock cycles at a grid barrier (<= 0: the default, about 1 s)
-// and, when skip_first_arrival != 0, the last CTA does not arrive at each launch's first
-// barrier, so the others' bounded waits run out and the launch reports EMUSV_TIMEOUT.
+// wait at most wait_cycles clock cycles at a grid barrier or for work (<= 0: the default,
+// about 1 s) and, when skip_first_arrival != 0, the last CTA does not arrive at each
+// launch's first barrier (lock-step rounds) or register 0's first phase is never
+// published (phase engine), so the bounded waits run out and the launch reports
+// EMUSV_TIMEOUT.
 int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival) {
     if (!workspace) return EMUSV_BAD_ARGUMENT;
     std::lock_guard<std::mutex> g(g_args_mu);

@@ -346,7 +346,8 @@ int emusv_batch_set_engine(void *workspace, int engine);
  * counterpart in the reference, whose loop has no device-side waits): later launches wait
  * at most wait_cycles SM clock cycles at a grid barrier (<= 0 restores the default, about
  * 1 s), and with skip_first_arrival != 0 the last CTA does not arrive at each launch's
- * first barrier, so every other CTA's bounded wait runs out, all CTAs return and
+ * first barrier (lock-step rounds; with the phase engine, register 0's first phase is never
+ * published), so every other CTA's bounded wait runs out, all CTAs return and
  * emusv_batch_results reports EMUSV_TIMEOUT; the device stays usable.  Off by default;
  * for tests.  Host-side only (takes effect at the next launch). */
 int emusv_batch_set_barrier_test(void *workspace, long long wait_cycles, int skip_first_arrival);

@@ -1,9 +1,11 @@
 """Failure paths on the GPU, in forms that fault no GPU.
 
-* A bounded device wait made to run out: the batched engine's grid barrier with a short
-  wait limit and one CTA that never arrives (emusv_batch_set_barrier_test).  Every other
-  CTA gives up, the launch reports EMUSV_TIMEOUT (TimeoutError), and the same workspace then
-  runs the batch and matches the oracle.
+* A bounded device wait made to run out, under both batch schedulers: the lock-step
+  engine's grid barrier with a short wait limit and one CTA that never arrives, and the
+  phase engine with one register's first phase never published
+  (emusv_batch_set_barrier_test).  Every waiting warp gives up, the launch reports
+  EMUSV_TIMEOUT (TimeoutError), and the same workspace then runs the batch and matches the
+  oracle.
 * A non-finite state, copied in from a host buffer holding a NaN: the Lanczos step, the
   Arnoldi step and the adjoint step report EMUSV_NONFINITE, raised as NonFiniteError -- a
   FloatingPointError and, like the reference's Lanczos loop, which never converges on such a
@@ -54,14 +56,19 @@ def _oracle_chain(oracle, r):
     return s
 
 
-def test_batch_barrier_timeout_then_recovers(oracle):
+@pytest.mark.parametrize("engine", [0, 1])
+def test_batch_barrier_timeout_then_recovers(oracle, engine):
+    """Both schedulers: lock-step rounds (a CTA that never arrives at the first grid
+    barrier) and the phase engine (register 0's first phase never published, so the warps
+    find no work and their starvation limit runs out)."""
     from emulators_b200.batch import BatchEvolution
 
     regs = _batch([9, 10, 11, 12], 3, seed=11)
     b = BatchEvolution(regs, precision="c128", max_krylov_dim=100)
     b.reset()
     b.prepare(8, 40)
-    # a wait of 2e6 SM cycles (about 1 ms) with one CTA that never arrives
+    b.set_engine(engine)
+    # a wait of 2e6 SM cycles (about 1 ms) for an arrival that never comes
     b.set_barrier_test(wait_cycles=2_000_000, skip_first_arrival=True)
     b.launch(1)
     with pytest.raises(TimeoutError):
@@ -70,6 +77,7 @@ def test_batch_barrier_timeout_then_recovers(oracle):
     b.set_barrier_test(0, False)
     b.reset()
     b.prepare(8, 40)
+    b.set_engine(engine)
     b.launch(1)
     status, _ = b.results()
     assert (status == 0).all()
