@@ -190,9 +190,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
             a, b = b, a
         e1.record(stream)
         torch.cuda.synchronize()
-    ms_by = (np.zeros(8)).astype(np.float64)
-    launches = np.zeros(8, dtype=np.int64)
-    L.emusv_profile_end(ms_by.ctypes.data, launches.ctypes.data, 8)
+    ms_by = (np.zeros(9)).astype(np.float64)
+    launches = np.zeros(9, dtype=np.int64)
+    L.emusv_profile_end(ms_by.ctypes.data, launches.ctypes.data, 9)
     elapsed, value = replica_rate(e0.elapsed_time(e1) / 1e3, K, world, dist, dev)
     if dist:
         dist.barrier()
@@ -207,14 +207,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         step(k, a, b)
         a, b = b, a
     torch.cuda.synchronize()
-    pms = np.zeros(8)
-    pl = np.zeros(8, dtype=np.int64)
-    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
+    pms = np.zeros(9)
+    pl = np.zeros(9, dtype=np.int64)
+    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 9)
     # One Lanczos iteration (H-first order) = one or two strided pass H kernels (kind 7: the
     # flips of the bits above the pass-L tile; 2 vector units for the first, 3 for a second
     # that adds to the first's sums) + the recurrence pass L (kind 0: read v_j, the pass H
-    # sums and v_{j-1}, write w; 4 units), plus per step one read-only energy pass over v_0
-    # (kind 0, 1 unit).  Algorithmic bytes per iteration: H*psi 2 D s + recurrence 4 D s.
+    # sums and v_{j-1}, write w; 4 units); per step one read-only energy pass over v_0
+    # (kind 8, 1 unit).  Algorithmic bytes per iteration: H*psi 2 D s + recurrence 4 D s.
     m_total = max(int(sum(iters)), 1)
     nsteps_p = max(len(iters), 1)
     iter_s = (pms[0] + pms[7]) / m_total / 1e3
@@ -224,18 +224,23 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     alg_iter = 6 * D * es
     achieved = alg_iter / iter_s / 1e9
     total_ms = pms.sum()
-    kinds = ["hpsi_pass_low", "orth", "small", "combine", "obs", "adjoint", "batch", "hpsi_pass_high"]
-    shares = {kinds[i]: round(pms[i] / total_ms, 4) for i in range(8) if pl[i]}
+    kinds = ["hpsi_pass_low", "orth", "small", "combine", "obs", "adjoint", "batch", "hpsi_pass_high",
+             "hpsi_energy_pass"]
+    shares = {kinds[i]: round(pms[i] / total_ms, 4) for i in range(9) if pl[i]}
     h_per_iter = pl[7] / m_total
     h_units = 2.0 if h_per_iter < 1.5 else 5.0  # one H pass: 2 units; two: 2 + 3
-    low_units_mean = (4 * m_total + nsteps_p) / max(pl[0], 1)
-    iter_units = h_units + 4 + nsteps_p / m_total
+    iter_units = h_units + 4
+    e0_s = pms[8] / max(pl[8], 1) / 1e3 if pl[8] else 0.0
     per_pass = {
-        "pass_low": {"ms": round(passl_s * 1e3, 4), "units_mean": round(low_units_mean, 3),
+        "pass_low": {"ms": round(passl_s * 1e3, 4), "units_mean": 4.0,
                      "note": "recurrence pass L: read v_j, the pass H sums, v_{j-1}; write w "
-                             "(4 D s); the mean includes the step's energy pass over v_0 (1 D s)",
-                     "GB/s": round(low_units_mean * D * es / passl_s / 1e9, 1),
-                     "frac": round(low_units_mean * D * es / passl_s / 1e9 / hbm, 4)},
+                             "(4 D s)",
+                     "GB/s": round(4 * D * es / passl_s / 1e9, 1),
+                     "frac": round(4 * D * es / passl_s / 1e9 / hbm, 4)},
+        "energy_pass": {"ms": round(e0_s * 1e3, 4), "units": 1.0, "launches": int(pl[8]),
+                        "note": "once per step: <v_0, (D - sigma + X_low) v_0> (read v_0, 1 D s)",
+                        "GB/s": round(D * es / e0_s / 1e9, 1) if e0_s else None,
+                        "frac": round(D * es / e0_s / 1e9 / hbm, 4) if e0_s else None},
         "pass_high": {"ms": round(passh_s * 1e3, 4),
                       "units_mean": round(h_units / max(h_per_iter, 1e-9), 3),
                       "launches_per_iteration": round(h_per_iter, 2),
@@ -481,9 +486,9 @@ def ladder_c128(dev, W: int, K: int = 6) -> dict:
     for k in range(W + K, W + K + 3):
         step(k)
     torch.cuda.synchronize()
-    pms = np.zeros(8)
-    pl = np.zeros(8, dtype=np.int64)
-    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 8)
+    pms = np.zeros(9)
+    pl = np.zeros(9, dtype=np.int64)
+    L.emusv_profile_end(pms.ctypes.data, pl.ctypes.data, 9)
     iter_s = (pms[0] + pms[7]) / max(sum(iters), 1) / 1e3
     hbm, which = peaks()
     ach = 6 * D * 16 / iter_s / 1e9

@@ -309,7 +309,7 @@ static int launch_lz_c(const HamParams &H, const LzArgs &A, cudaStream_t s, int 
     int64_t grid = (int64_t)sm_count() * per_sm;
     if (grid > ntiles) grid = ntiles;
     {
-        ProfScope ps_(PROF_HPSI, s);
+        ProfScope ps_(MODE == LZ_ITER ? PROF_HPSI : PROF_HPSI_AUX, s);
         kern<<<(unsigned)grid, NT, smem, s>>>(P, A);
     }
     EMUSV_CHECK_LAUNCH();

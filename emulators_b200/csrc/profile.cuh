@@ -14,7 +14,8 @@ enum ProfKind {
     PROF_ADJOINT = 5,  // adjoint contractions
     PROF_BATCH = 6,    // batched persistent evolution
     PROF_HPSI_HIGH = 7,  // pass H of the two-pass H*psi
-    PROF_KINDS = 8
+    PROF_HPSI_AUX = 8,   // the Lanczos pass L's other modes: start-of-step energy, moments
+    PROF_KINDS = 9
 };
 
 void prof_begin_launch(int kind, cudaStream_t s, void **token);
